@@ -1,0 +1,411 @@
+"""Benchmark of the per-timestep hot path on the PMB brittle-fracture
+notched-plate impact (plate 0.2 x 0.1 x 0.009 m, dx = 0.2/800 ->
+800 x 400 x 36 = 11.52 M particles, delta = 3.01 dx, two 0.05 m notches,
+16.5 m/s impact strip held by a zero-force BC).
+
+One bench step = one velocity-Verlet time step of the whole plate: bond
+break test + PMB force over every directed bond, force BC, both half-step
+updates. Metric: bond-updates/s = (directed neighbour entries, broken ones
+included, since the kernel visits them) x steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun, one rank per GPU): every rank advances its own plate
+(independent specimens, no data-path collective; weak scaling); value is
+all ranks' bond updates over the slowest rank's device time.
+--impl reference: the CPU oracle (the reference's algorithm restated in
+C++/OpenMP; the reference itself needs Kokkos + Cabana + MPI and cannot be
+built here) on all host threads, rank 0 only, each step a bounded slab of
+the same plate.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from cabanapd_b200 import problems as P  # noqa: E402
+
+PLATE_CELLS = (800, 400, 36)
+CPU_SLAB_X = 50  # bounded CPU sample: the first 50 x-columns of the plate
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_bond():
+    """DRAM bytes per directed bond of the force kernel from the committed ncu
+    summary (profiles/pmb_force_plate.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "pmb_force_plate.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("dram_bytes_per_bond:"):
+                return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg, device):
+    if pg is None:
+        return
+    if device == "cpu":
+        pg.barrier()
+        return
+    import torch
+    pg.barrier(device_ids=[device])
+    torch.cuda.synchronize(device)
+
+
+def aggregate(pg, device, ms_local, bonds_local, steps):
+    """Whole-job throughput: every rank's bond updates over the slowest
+    rank's device time (max over ranks)."""
+    ms = reduce_max(pg, ms_local, device)
+    total = reduce_sum(pg, float(bonds_local), device)
+    return total * steps / (ms / 1e3), ms, total
+
+
+def visible_index(local):
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    ids = [c for c in cvd.split(",") if c.strip()]
+    if ids and ids[min(local, len(ids) - 1)].strip().isdigit():
+        return int(ids[min(local, len(ids) - 1)])
+    return local
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample_problem():
+    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=1)
+    nx, ny, nz = PLATE_CELLS
+    ix = np.arange(prob["x"].shape[0]) % nx
+    keep = ix < CPU_SLAB_X
+    remap = -np.ones(keep.size, dtype=np.int64)
+    remap[keep] = np.arange(int(keep.sum()))
+    sub = dict(prob)
+    for k in ("x", "vol", "rho", "nofail", "v0"):
+        sub[k] = np.ascontiguousarray(prob[k][keep])
+    sub["bcs"] = [(kind, c, remap[idx[keep[idx]]], vals) for kind, c, idx, vals in prob["bcs"]]
+    return sub
+
+
+def time_cpu_sample(target_seconds=15.0, max_steps=200):
+    """Oracle on all host threads over the bounded slab; returns a dict."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    threads = os.cpu_count() or 1
+    pyoracle.set_num_threads(threads)
+    sub = cpu_sample_problem()
+    s = pyoracle.OracleSystem(sub["params"])
+    P.setup(s, sub)
+    bonds = s.neighbor_stats()[1]
+    t0 = time.perf_counter()
+    s.run(1)
+    t1 = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, target_seconds / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    s.run(steps)
+    dt = time.perf_counter() - t0
+    return {"value": bonds * steps / dt, "unit": "bond-updates/s", "cores": threads,
+            "kind": "port", "steps": steps, "seconds": dt, "bonds_per_step": bonds,
+            "particles": s.n,
+            "sample": (f"first {CPU_SLAB_X} of {PLATE_CELLS[0]} x-columns of the plate "
+                       f"({s.n} particles, {bonds} bonds), {steps} timed steps after 1 "
+                       f"warm-up step, CPU oracle (C++17/OpenMP port of the reference "
+                       f"kernels), {threads} threads")}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    threads = os.cpu_count() or 1
+    pyoracle.set_num_threads(threads)
+    sub = cpu_sample_problem()
+    s = pyoracle.OracleSystem(sub["params"])
+    P.setup(s, sub)
+    bonds = s.neighbor_stats()[1]
+    s.run(args.warmup)
+    t0 = time.perf_counter()
+    s.run(args.steps)
+    dt = time.perf_counter() - t0
+    value = bonds * args.steps / dt
+    sample = (f"each step: one time step of the first {CPU_SLAB_X} of {PLATE_CELLS[0]} "
+              f"x-columns of the plate ({s.n} particles, {bonds} bonds); CPU oracle "
+              f"(C++17/OpenMP restatement of the reference kernels; the reference "
+              f"needs Kokkos/Cabana/MPI and is not buildable here), {threads} threads")
+    line = {
+        "impl": "reference", "metric": "bond-updates/s", "value": value,
+        "unit": "bond-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "pmb_fracture_notched_plate_impact",
+                   "plate_cells": list(PLATE_CELLS), "sample_particles": s.n,
+                   "sample_bonds": bonds},
+        "cpu_baseline": {"value": value, "unit": "bond-updates/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "bond-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_gpu(args, world, rank, local, pg):
+    import torch
+
+    import cabanapd_b200
+    device = local
+    torch.cuda.set_device(device)
+    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
+    stream = torch.cuda.Stream(device=device)
+
+    sys_ = cabanapd_b200.System(dict(prob["params"], device=device))
+    sys_.set_stream(stream.cuda_stream)
+    P.setup(sys_, prob)
+    _, bonds = sys_.neighbor_stats()
+    n = sys_.n
+
+    # Warm-up.
+    sys_.step(args.warmup)
+    sys_.synchronize()
+    sys_.set_kernel_timing(True)
+    launches0 = sys_.kernel_launches()
+
+    sampler = ClockSampler(visible_index(local)) if rank == 0 else None
+    barrier(pg, device)
+    torch.cuda.synchronize(device)
+    if sampler:
+        sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sys_.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize(device)
+    clocks = sampler.stop() if sampler else None
+    barrier(pg, device)
+    ms_local = ev0.elapsed_time(ev1)
+    launches = sys_.kernel_launches() - launches0
+    k_ms, k_n, k_bytes = sys_.kernel_time()
+    sys_.set_kernel_timing(False)
+
+    value, ms, total_bonds = aggregate(pg, device, ms_local, bonds, args.steps)
+    particle_steps = reduce_sum(pg, float(n), device) * args.steps / (ms / 1e3)
+
+    # End to end through the C ABI from pinned host buffers: upload, neighbour
+    # build, pre-notch, BCs, init, K steps with energy/damage read back every
+    # 10 steps, download of the displacement field.
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.int32,
+                        pin_memory=True)
+        arr = t.numpy()
+        arr[...] = a
+        return arr
+
+    hx, hvol, hrho = pinned(prob["x"]), pinned(prob["vol"]), pinned(prob["rho"])
+    hnf = pinned(prob["nofail"].astype(np.int32))
+    hv0 = pinned(prob["v0"])
+    hu = pinned(np.zeros_like(prob["x"]))
+    del sys_
+    torch.cuda.synchronize(device)
+    barrier(pg, device)
+    t0 = time.perf_counter()
+    e2 = cabanapd_b200.System(dict(prob["params"], device=device))
+    e2.set_stream(stream.cuda_stream)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    e2.set_particles(hx, hvol, hrho, hnf)
+    e2.set_state(None, hv0)
+    e2.build_neighbors()
+    e2.prenotch(*prob["notches"])
+    for kind, comp, idx, vals in prob["bcs"]:
+        e2.add_bc(kind, idx, vals, component=comp)
+    e2.init()
+    done = 0
+    reads = 0
+    while done < args.steps:
+        k = min(10, args.steps - done)
+        e2.step(k)
+        done += k
+        e2.compute_energy()
+        reads += 1
+    e2.get("u", out=hu)
+    s1.record(stream)
+    torch.cuda.synchronize(device)
+    wall = time.perf_counter() - t0
+    e2e_ms = max(s0.elapsed_time(s1), 1e3 * wall)
+    e2e_ms = reduce_max(pg, e2e_ms, device)
+    del e2
+    h2d = (hx.nbytes + hvol.nbytes + hrho.nbytes + hnf.nbytes + hv0.nbytes) / args.steps
+    d2h = (hu.nbytes + 16 * reads) / args.steps
+    e2e_value = total_bonds * args.steps / (e2e_ms / 1e3)
+
+    if rank != 0:
+        return
+    hbm, hbm_kind = peaks()
+    avg_ms = k_ms / max(k_n, 1)
+    achieved = k_bytes / (avg_ms / 1e3) / 1e9
+    tpb = traffic_per_bond()
+    line = {
+        "metric": "bond-updates/s", "value": value, "unit": "bond-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "pmb_fracture_notched_plate_impact",
+                   "plate_cells": list(PLATE_CELLS), "particles_per_gpu": n,
+                   "bonds_per_gpu": bonds, "precision": "fp64_exact",
+                   "l2": "inputs larger than L2 (neighbour list %.1f GB)" % (4 * bonds / 1e9),
+                   "particle_steps_per_s": particle_steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": hbm_kind,
+                     "kernel": "k_pd_force<PMB, fracture>",
+                     "kernel_ms_avg": avg_ms, "kernel_launches": k_n,
+                     "algorithmic_bytes_per_launch": k_bytes,
+                     "traffic": (tpb * bonds if tpb else None)},
+        "e2e": {"value": e2e_value, "unit": "bond-updates/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "job": "upload+neighbour build+prenotch+init+steps+energy every 10 steps+download u"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.skip_cpu:
+        line["cpu_baseline"] = time_cpu_sample()
+        cb = line["cpu_baseline"]
+        cb.pop("steps", None)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local, pg = (int(os.environ.get("WORLD_SIZE", "1")),
+                              int(os.environ.get("RANK", "0")),
+                              int(os.environ.get("LOCAL_RANK", "0")), None)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    world, rank, local, pg = dist_setup()
+    try:
+        run_gpu(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,924 @@
+// C ABI of the cabanapd_b200 library: system lifetime, host<->device
+// transfers and the Solver orchestration of the per-timestep hot path
+// (CabanaPD_Solver.hpp:229-477), issued asynchronously on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cpd_internal.cuh"
+
+using namespace cpd;
+
+namespace {
+thread_local std::string g_last_error;
+
+cpd_status set_error(cpd_status code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+}  // namespace
+
+#define CPD_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess)                                                      \
+            return set_error(e_ == cudaErrorMemoryAllocation ? CPD_ERR_OUT_OF_MEMORY \
+                                                             : CPD_ERR_CUDA,        \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+#define CPD_LAUNCHED(count_expr)                                                    \
+    do {                                                                            \
+        s->launches += (count_expr);                                                \
+        cudaError_t e_ = cudaGetLastError();                                        \
+        if (e_ != cudaSuccess)                                                      \
+            return set_error(CPD_ERR_CUDA, std::string("kernel launch: ") +         \
+                                               cudaGetErrorString(e_));             \
+    } while (0)
+
+#define CPD_OK_OR_RETURN(expr)                                                      \
+    do {                                                                            \
+        cpd_status s_ = (expr);                                                     \
+        if (s_ != CPD_OK) return s_;                                                \
+    } while (0)
+
+struct cpd_system {
+    cpd_params params{};
+    Model md;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int64_t n = 0, frozen = 0, npad = 0;
+    // Particle fields (component-major SoA, [3][npad] or [npad]).
+    double *x = nullptr, *u = nullptr, *v = nullptr, *f = nullptr;
+    double *vol = nullptr, *rho = nullptr, *m = nullptr, *theta = nullptr;
+    double *lps_a = nullptr, *lps_b = nullptr, *W = nullptr, *phi = nullptr;
+    double *radius = nullptr, *u_neigh = nullptr;
+    uint8_t* nofail = nullptr;
+    int32_t* perm = nullptr;  // internal -> caller index; nullptr = identity
+    std::vector<int32_t> h_inv;  // caller -> internal
+    double* staging = nullptr;   // [3 n] transfer buffer
+    double* red = nullptr;       // reduction partials
+    int red_cap = 0;
+    double* red_out = nullptr;   // small result slots
+    double* h_red = nullptr;     // pinned host mirror of red_out
+    NeighborList pd, contact;
+    std::vector<BoundaryCondition> bcs;
+    bool neighbors_built = false;
+    bool initialized = false;
+    double max_disp = 0.0;
+    int64_t steps_since_rebuild = 0;
+    int64_t rebuilds = 0;
+    int64_t launches = 0;
+    // Kernel timing.
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double timed_ms = 0.0;
+    int64_t timed_launches = 0;
+};
+
+namespace {
+
+bool has_pd(const cpd_system* s) { return s->md.pd != CPD_PD_NONE; }
+bool is_lps(const cpd_system* s)
+{
+    return s->md.pd == CPD_PD_LPS || s->md.pd == CPD_PD_LINEAR_LPS;
+}
+bool has_contact(const cpd_system* s) { return s->md.contact != CPD_CONTACT_NONE; }
+
+ParticleView view(const cpd_system* s)
+{
+    ParticleView p;
+    p.n = s->n;
+    p.frozen = s->frozen;
+    p.npad = s->npad;
+    p.x = s->x;
+    p.u = s->u;
+    p.v = s->v;
+    p.f = s->f;
+    p.vol = s->vol;
+    p.rho = s->rho;
+    p.nofail = s->nofail;
+    p.m = s->m;
+    p.theta = s->theta;
+    p.lps_a = s->lps_a;
+    p.lps_b = s->lps_b;
+    p.W = s->W;
+    p.phi = s->phi;
+    p.radius = s->radius;
+    p.u_neigh = s->u_neigh;
+    return p;
+}
+
+EllView pd_view(const cpd_system* s)
+{
+    EllView v = s->pd.view();
+    if (!s->md.fracture) v.mu = nullptr;
+    return v;
+}
+
+void free_particles(cpd_system* s)
+{
+    double** arrays[] = {&s->x,     &s->u,     &s->v,     &s->f,     &s->vol,
+                         &s->rho,   &s->m,     &s->theta, &s->lps_a, &s->lps_b,
+                         &s->W,     &s->phi,   &s->radius, &s->u_neigh, &s->staging,
+                         &s->red,   &s->red_out};
+    for (double** a : arrays)
+        if (*a) {
+            cudaFree(*a);
+            *a = nullptr;
+        }
+    if (s->nofail) cudaFree(s->nofail);
+    s->nofail = nullptr;
+    if (s->perm) cudaFree(s->perm);
+    s->perm = nullptr;
+    for (auto& bc : s->bcs) {
+        if (bc.idx) cudaFree(bc.idx);
+        if (bc.values) cudaFree(bc.values);
+    }
+    s->bcs.clear();
+    free_neighbor_list(s->pd);
+    free_neighbor_list(s->contact);
+    s->n = s->npad = s->frozen = 0;
+    s->red_cap = 0;
+    s->neighbors_built = false;
+    s->initialized = false;
+}
+
+cudaEvent_t take_event(cpd_system* s)
+{
+    if (!s->event_pool.empty()) {
+        cudaEvent_t e = s->event_pool.back();
+        s->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+cpd_status harvest_timing(cpd_system* s)
+{
+    for (auto& pr : s->pending) {
+        CPD_CUDA(cudaEventSynchronize(pr.second));
+        float ms = 0.f;
+        CPD_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        s->timed_ms += ms;
+        s->timed_launches++;
+        s->event_pool.push_back(pr.first);
+        s->event_pool.push_back(pr.second);
+    }
+    s->pending.clear();
+    return CPD_OK;
+}
+
+// Morton code of the particle's cell (21 bits per axis).
+uint64_t spread3(uint64_t v)
+{
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+}
+
+std::vector<int32_t> morton_order(const double* x, int64_t n, int64_t frozen, double cell)
+{
+    double lo[3] = {x[0], x[1], x[2]};
+    for (int64_t p = 0; p < n; p++)
+        for (int d = 0; d < 3; d++) lo[d] = std::min(lo[d], x[3 * p + d]);
+    std::vector<uint64_t> code(n);
+    for (int64_t p = 0; p < n; p++) {
+        uint64_t c[3];
+        for (int d = 0; d < 3; d++) c[d] = (uint64_t)std::floor((x[3 * p + d] - lo[d]) / cell);
+        code[p] = spread3(c[0]) | spread3(c[1]) << 1 | spread3(c[2]) << 2;
+    }
+    std::vector<int32_t> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    auto cmp = [&](int32_t a, int32_t b) { return code[a] < code[b]; };
+    // Frozen particles stay in front (they are never integrated).
+    std::stable_sort(order.begin(), order.begin() + frozen, cmp);
+    std::stable_sort(order.begin() + frozen, order.end(), cmp);
+    return order;
+}
+
+cpd_status upload_vector(cpd_system* s, const double* host, double* dst)
+{
+    CPD_CUDA(cudaMemcpyAsync(s->staging, host, sizeof(double) * 3 * s->n,
+                             cudaMemcpyHostToDevice, s->stream));
+    s->launches += launch_aos_to_soa(s->staging, dst, s->n, s->npad, 3, s->perm, s->stream);
+    CPD_CUDA(cudaGetLastError());
+    return CPD_OK;
+}
+
+cpd_status upload_scalar(cpd_system* s, const double* host, double* dst)
+{
+    CPD_CUDA(cudaMemcpyAsync(s->staging, host, sizeof(double) * s->n,
+                             cudaMemcpyHostToDevice, s->stream));
+    s->launches += launch_aos_to_soa(s->staging, dst, s->n, s->npad, 1, s->perm, s->stream);
+    CPD_CUDA(cudaGetLastError());
+    return CPD_OK;
+}
+
+cpd_status ensure_reduction(cpd_system* s, int blocks)
+{
+    if (blocks * 2 <= s->red_cap) return CPD_OK;
+    if (s->red) CPD_CUDA(cudaFree(s->red));
+    s->red = nullptr;
+    CPD_CUDA(cudaMalloc(&s->red, sizeof(double) * 2 * blocks));
+    s->red_cap = 2 * blocks;
+    return CPD_OK;
+}
+
+cpd_status rebuild_contact(cpd_system* s, double cutoff)
+{
+    std::string err;
+    int l = build_neighbor_list(s->x, s->u, s->n, s->npad, s->frozen, cutoff, s->perm,
+                                false, s->contact, s->stream, err);
+    if (l < 0) return set_error(CPD_ERR_CUDA, "contact neighbour build: " + err);
+    s->launches += l;
+    // CabanaPD_Neighbor.hpp:127-130: displacement at the last build.
+    CPD_CUDA(cudaMemcpyAsync(s->u_neigh, s->u, sizeof(double) * 3 * s->npad,
+                             cudaMemcpyDeviceToDevice, s->stream));
+    s->rebuilds++;
+    s->steps_since_rebuild = 0;
+    return CPD_OK;
+}
+
+// CabanaPD_Neighbor.hpp:107-132 Neighbor::update, or every rebuild_every steps.
+cpd_status contact_update(cpd_system* s)
+{
+    bool rebuild;
+    if (s->params.rebuild_every > 0) {
+        rebuild = s->steps_since_rebuild >= s->params.rebuild_every;
+    } else {
+        CPD_CUDA(cudaMemcpyAsync(s->h_red, s->red_out, sizeof(double), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
+        s->max_disp = s->h_red[0];
+        rebuild = s->max_disp > s->md.radius_extend;
+    }
+    if (rebuild) return rebuild_contact(s, 2.0 * s->md.radius + s->md.radius_extend);
+    return CPD_OK;
+}
+
+cpd_status timed_begin(cpd_system* s, cudaEvent_t& e0)
+{
+    e0 = nullptr;
+    if (!s->timing) return CPD_OK;
+    e0 = take_event(s);
+    CPD_CUDA(cudaEventRecord(e0, s->stream));
+    return CPD_OK;
+}
+
+cpd_status timed_end(cpd_system* s, cudaEvent_t e0)
+{
+    if (!e0) return CPD_OK;
+    cudaEvent_t e1 = take_event(s);
+    CPD_CUDA(cudaEventRecord(e1, s->stream));
+    s->pending.emplace_back(e0, e1);
+    if (s->pending.size() > 4096) return harvest_timing(s);
+    return CPD_OK;
+}
+
+cpd_status pd_force(cpd_system* s)
+{
+    const ParticleView p = view(s);
+    cudaEvent_t e0;
+    CPD_OK_OR_RETURN(timed_begin(s, e0));
+    CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
+    return timed_end(s, e0);
+}
+
+cpd_status contact_force(cpd_system* s, bool reset)
+{
+    const ParticleView p = view(s);
+    cudaEvent_t e0 = nullptr;
+    if (!has_pd(s)) CPD_OK_OR_RETURN(timed_begin(s, e0));
+    CPD_LAUNCHED(launch_hertz_force(p, s->contact.view(), s->md, reset, s->stream));
+    return timed_end(s, e0);
+}
+
+cpd_status apply_force_bcs(cpd_system* s)
+{
+    const ParticleView p = view(s);
+    for (const auto& bc : s->bcs) CPD_LAUNCHED(launch_force_bc(p, bc, s->stream));
+    return CPD_OK;
+}
+
+// CabanaPD_Solver.hpp:462-477 updateForce, then the contact force.
+cpd_status update_force(cpd_system* s)
+{
+    const ParticleView p = view(s);
+    if (has_pd(s)) {
+        if (is_lps(s)) {
+            if (s->md.fracture)
+                CPD_LAUNCHED(launch_lps_weighted_volume(p, pd_view(s), s->md, s->stream));
+            CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
+        }
+        CPD_OK_OR_RETURN(pd_force(s));
+    }
+    if (has_contact(s)) {
+        CPD_OK_OR_RETURN(contact_update(s));
+        CPD_OK_OR_RETURN(contact_force(s, !has_pd(s)));
+    }
+    return CPD_OK;
+}
+
+cpd_status vv_initial(cpd_system* s)
+{
+    const ParticleView p = view(s);
+    const bool track = has_contact(s);
+    const int nb = vv_blocks(s->n - s->frozen);
+    if (track) CPD_OK_OR_RETURN(ensure_reduction(s, nb));
+    CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->stream));
+    if (track && s->n > s->frozen)
+        CPD_LAUNCHED(launch_max_partials(s->red, nb, s->red_out, s->stream));
+    s->steps_since_rebuild++;
+    return CPD_OK;
+}
+
+cpd_status check_ready(const cpd_system* s, bool need_neighbors)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    if (s->n == 0) return set_error(CPD_ERR_STATE, "no particles uploaded");
+    if (need_neighbors && !s->neighbors_built)
+        return set_error(CPD_ERR_STATE, "neighbour list not built");
+    return CPD_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int32_t cpd_abi_version(void) { return CPD_ABI_VERSION; }
+const char* cpd_last_error(void) { return g_last_error.c_str(); }
+
+cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
+{
+    if (!params || !out) return set_error(CPD_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    const cpd_params& P = *params;
+    if (P.pd_model < CPD_PD_NONE || P.pd_model > CPD_PD_LINEAR_LPS)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown pd_model");
+    if (P.contact_model != CPD_CONTACT_NONE && P.contact_model != CPD_CONTACT_HERTZ)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown contact_model");
+    if (P.pd_model == CPD_PD_NONE && P.contact_model == CPD_CONTACT_NONE)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "need a PD model or a contact model");
+    if ((P.pd_model == CPD_PD_LINEAR_PMB || P.pd_model == CPD_PD_LINEAR_LPS) && P.fracture)
+        return set_error(CPD_ERR_UNSUPPORTED, "linearized models have no fracture variant");
+    if (P.pd_model != CPD_PD_NONE && !(P.horizon > 0))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "horizon must be > 0");
+    if (P.contact_model == CPD_CONTACT_HERTZ && !(P.contact_radius > 0))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "contact_radius must be > 0");
+    if (P.precision != CPD_FP64_EXACT)
+        return set_error(CPD_ERR_UNSUPPORTED, "unknown precision mode");
+    if (P.ordering != CPD_ORDER_INPUT && P.ordering != CPD_ORDER_MORTON)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown ordering");
+    const bool lps = P.pd_model == CPD_PD_LPS || P.pd_model == CPD_PD_LINEAR_LPS;
+    const int infl = P.influence_type >= 0 ? P.influence_type : (lps ? 0 : 1);
+    if (infl != 0 && infl != 1)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "Influence function type must be 0 or 1.");
+
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_error(CPD_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (P.device < 0 || P.device >= ndev)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    CPD_CUDA(cudaSetDevice(P.device));
+
+    cpd_system* s = new cpd_system();
+    s->params = P;
+    s->device = P.device;
+    Model& md = s->md;
+    md.pd = P.pd_model;
+    md.fracture = P.fracture ? 1 : 0;
+    md.contact = P.contact_model;
+    md.influence = infl;
+    md.horizon = P.horizon;
+    md.K = P.K;
+    md.G = P.G;
+    md.G0 = P.G0;
+    if (md.pd != CPD_PD_NONE) {
+        const double h = md.horizon;
+        // force_models/CabanaPD_PMB.hpp:44-46
+        md.c = 18.0 * md.K / (kPi * h * h * h * h);
+        // force_models/CabanaPD_LPS.hpp:66-67
+        md.theta_coeff = 3.0 * md.K - 5.0 * md.G;
+        md.s_coeff = 15.0 * md.G;
+        if (md.fracture) {
+            // CabanaPD_ForceModels.hpp:97-101 (LPS ctor :209-223 agrees)
+            md.s0 = std::sqrt(5.0 * md.G0 / 9.0 / md.K / h);
+            if (md.influence == 0) md.s0 = std::sqrt(8.0 * md.G0 / 15.0 / md.K / h);
+            md.bond_break_coeff = (1.0 + md.s0) * (1.0 + md.s0);
+        }
+    }
+    if (md.contact == CPD_CONTACT_HERTZ) {
+        // force_models/CabanaPD_Hertzian.hpp:40-56
+        md.radius = P.contact_radius;
+        md.radius_extend = P.radius_extend;
+        md.nu = P.nu;
+        md.E = P.E;
+        md.e = P.restitution;
+        md.Rs = 0.5 * md.radius;
+        md.Es = md.E / (2.0 * (1.0 - std::pow(md.nu, 2.0)));
+        const double ln_e = std::log(md.e);
+        md.beta = -ln_e / std::sqrt(std::pow(ln_e, 2.0) + std::pow(kPi, 2.0));
+        md.coeff_h_n = 4.0 / 3.0 * md.Es * std::sqrt(md.Rs);
+        md.coeff_h_d = -2.0 * std::sqrt(5.0 / 6.0) * md.beta;
+        md.per_particle_radius = P.per_particle_radius ? 1 : 0;
+    }
+    e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return set_error(CPD_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    }
+    s->stream = s->own_stream;
+    e = cudaMallocHost(&s->h_red, sizeof(double) * 8);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s->own_stream);
+        delete s;
+        return set_error(CPD_ERR_CUDA, std::string("pinned: ") + cudaGetErrorString(e));
+    }
+    *out = s;
+    return CPD_OK;
+}
+
+cpd_status cpd_system_destroy(cpd_system* s)
+{
+    if (!s) return CPD_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_particles(s);
+    for (auto& pr : s->pending) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
+    if (s->h_red) cudaFreeHost(s->h_red);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+    return CPD_OK;
+}
+
+cpd_status cpd_set_stream(cpd_system* s, void* stream)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return CPD_OK;
+}
+
+cpd_status cpd_get_stream(cpd_system* s, void** stream)
+{
+    if (!s || !stream) return set_error(CPD_ERR_INVALID_ARGUMENT, "null argument");
+    *stream = (void*)s->stream;
+    return CPD_OK;
+}
+
+cpd_status cpd_model_constants(const cpd_system* s, double* o)
+{
+    if (!s || !o) return set_error(CPD_ERR_INVALID_ARGUMENT, "null argument");
+    const Model& m = s->md;
+    const double v[10] = {m.c,  m.s0, m.bond_break_coeff, m.theta_coeff, m.s_coeff,
+                          m.Rs, m.Es, m.beta,             m.coeff_h_n,   m.coeff_h_d};
+    std::memcpy(o, v, sizeof(v));
+    return CPD_OK;
+}
+
+cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, const double* x,
+                                const double* vol, const double* rho, const int32_t* nofail,
+                                const double* radius)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    if (n <= 0 || n >= (int64_t)1 << 31 || n_frozen < 0 || n_frozen > n || !x || !vol)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_upload_particles: bad arguments");
+    if (s->md.per_particle_radius && !radius)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "per-particle radius model needs radius");
+    CPD_CUDA(cudaSetDevice(s->device));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    free_particles(s);
+    s->n = n;
+    s->frozen = n_frozen;
+    s->npad = std::max<int64_t>(128, (n + 127) / 128 * 128);
+    const size_t sv = sizeof(double) * 3 * s->npad, ss = sizeof(double) * s->npad;
+    double** vec[] = {&s->x, &s->u, &s->v, &s->f, &s->u_neigh};
+    for (double** a : vec) {
+        CPD_CUDA(cudaMalloc(a, sv));
+        CPD_CUDA(cudaMemsetAsync(*a, 0, sv, s->stream));
+    }
+    double** sca[] = {&s->vol, &s->rho, &s->m, &s->theta, &s->lps_a, &s->lps_b,
+                      &s->W,   &s->phi, &s->radius};
+    for (double** a : sca) {
+        CPD_CUDA(cudaMalloc(a, ss));
+        CPD_CUDA(cudaMemsetAsync(*a, 0, ss, s->stream));
+    }
+    CPD_CUDA(cudaMalloc(&s->nofail, s->npad));
+    CPD_CUDA(cudaMemsetAsync(s->nofail, 0, s->npad, s->stream));
+    CPD_CUDA(cudaMalloc(&s->staging, sizeof(double) * 3 * n));
+    CPD_CUDA(cudaMalloc(&s->red_out, sizeof(double) * 8));
+    CPD_CUDA(cudaMemsetAsync(s->red_out, 0, sizeof(double) * 8, s->stream));
+
+    // Internal order.
+    std::vector<int32_t> order;
+    if (s->params.ordering == CPD_ORDER_MORTON) {
+        double cell = has_pd(s) ? s->md.horizon : 2.0 * s->md.radius + s->md.radius_extend;
+        order = morton_order(x, n, n_frozen, cell);
+        CPD_CUDA(cudaMalloc(&s->perm, sizeof(int32_t) * n));
+        CPD_CUDA(cudaMemcpyAsync(s->perm, order.data(), sizeof(int32_t) * n,
+                                 cudaMemcpyHostToDevice, s->stream));
+    } else {
+        order.resize(n);
+        std::iota(order.begin(), order.end(), 0);
+    }
+    s->h_inv.assign(n, 0);
+    for (int64_t k = 0; k < n; k++) s->h_inv[order[k]] = (int32_t)k;
+
+    CPD_OK_OR_RETURN(upload_vector(s, x, s->x));
+    CPD_OK_OR_RETURN(upload_scalar(s, vol, s->vol));
+    std::vector<double> tmp;
+    if (rho) {
+        CPD_OK_OR_RETURN(upload_scalar(s, rho, s->rho));
+    } else {
+        tmp.assign(n, 1.0);
+        CPD_OK_OR_RETURN(upload_scalar(s, tmp.data(), s->rho));
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    if (radius) {
+        CPD_OK_OR_RETURN(upload_scalar(s, radius, s->radius));
+    } else {
+        tmp.assign(n, s->md.radius);
+        CPD_OK_OR_RETURN(upload_scalar(s, tmp.data(), s->radius));
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    std::vector<uint8_t> nf(n, 0);
+    if (nofail)
+        for (int64_t k = 0; k < n; k++) nf[k] = nofail[order[k]] != 0;
+    CPD_CUDA(cudaMemcpyAsync(s->nofail, nf.data(), n, cudaMemcpyHostToDevice, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_set_state(cpd_system* s, const double* u, const double* v)
+{
+    CPD_OK_OR_RETURN(check_ready(s, false));
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (u) CPD_OK_OR_RETURN(upload_vector(s, u, s->u));
+    if (v) CPD_OK_OR_RETURN(upload_vector(s, v, s->v));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_build_neighbors(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, false));
+    CPD_CUDA(cudaSetDevice(s->device));
+    std::string err;
+    if (has_pd(s)) {
+        // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
+        int l = build_neighbor_list(s->x, nullptr, s->n, s->npad, s->frozen,
+                                    s->md.horizon + 1e-14, s->perm, s->md.fracture != 0,
+                                    s->pd, s->stream, err);
+        if (l < 0) return set_error(CPD_ERR_CUDA, "neighbour build: " + err);
+        s->launches += l;
+    }
+    if (has_contact(s)) {
+        // CabanaPD_Neighbor.hpp:60-63: current positions, cutoff + 1e-14.
+        CPD_OK_OR_RETURN(rebuild_contact(s, 2.0 * s->md.radius + s->md.radius_extend + 1e-14));
+        s->rebuilds = 0;
+    }
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    s->neighbors_built = true;
+    s->initialized = false;
+    return CPD_OK;
+}
+
+cpd_status cpd_neighbor_stats(const cpd_system* s, int32_t* max_n, int64_t* total)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
+    if (max_n) *max_n = nl.max_n;
+    if (total) *total = nl.total;
+    return CPD_OK;
+}
+
+cpd_status cpd_download_neighbors(cpd_system* s, int32_t* counts, int32_t* indices,
+                                  int32_t* mu)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
+    const size_t cells = (size_t)s->n * std::max(nl.max_n, 1);
+    int32_t *dc = nullptr, *di = nullptr, *dm = nullptr;
+    CPD_CUDA(cudaMalloc(&dc, sizeof(int32_t) * s->n));
+    CPD_CUDA(cudaMalloc(&di, sizeof(int32_t) * cells));
+    CPD_CUDA(cudaMalloc(&dm, sizeof(int32_t) * cells));
+    NeighborList tmp = nl;
+    if (!(has_pd(s) && s->md.fracture)) tmp.mu = nullptr;
+    s->launches += launch_ell_to_rows(tmp, s->n, s->npad, s->perm, s->perm, dc, di, dm, s->stream);
+    CPD_CUDA(cudaGetLastError());
+    if (counts)
+        CPD_CUDA(cudaMemcpyAsync(counts, dc, sizeof(int32_t) * s->n, cudaMemcpyDeviceToHost,
+                                 s->stream));
+    if (indices && nl.max_n > 0)
+        CPD_CUDA(cudaMemcpyAsync(indices, di, sizeof(int32_t) * cells, cudaMemcpyDeviceToHost,
+                                 s->stream));
+    if (mu && nl.max_n > 0)
+        CPD_CUDA(cudaMemcpyAsync(mu, dm, sizeof(int32_t) * cells, cudaMemcpyDeviceToHost,
+                                 s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    cudaFree(dc);
+    cudaFree(di);
+    cudaFree(dm);
+    return CPD_OK;
+}
+
+cpd_status cpd_prenotch(cpd_system* s, int32_t count, const double* v1, const double* v2,
+                        const double* p0)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!has_pd(s) || !s->md.fracture)
+        return set_error(CPD_ERR_STATE, "Cannot create prenotch in system without fracture.");
+    if (count < 0 || (count > 0 && (!v1 || !v2 || !p0)))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_prenotch: bad arguments");
+    CPD_CUDA(cudaSetDevice(s->device));
+    const ParticleView p = view(s);
+    const double cutoff = s->md.horizon + 1e-14;
+    for (int32_t q = 0; q < count; q++) {
+        const double* a = v1 + 3 * q;
+        const double* b = v2 + 3 * q;
+        const double na = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        const double nb = std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+        const double cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2],
+                     cz = a[0] * b[1] - a[1] * b[0];
+        const double sin_ab = std::sqrt(cx * cx + cy * cy + cz * cz) / (na * nb);
+        if (!(sin_ab > 1e-12))
+            return set_error(CPD_ERR_INVALID_ARGUMENT, "notch vectors are parallel");
+        // A bond (length <= cutoff) that can meet the notch within the
+        // reference's 1e-10 parametric tolerances starts no farther than this
+        // from the notch's bounding box (coplanar case: parametric extents
+        // of the bond are bounded by |l| / sin(angle(v1, v2))).
+        const double margin = cutoff * (2.0 + 2.0 / sin_ab) + 1e-6 * (na + nb + cutoff);
+        CPD_LAUNCHED(launch_prenotch(p, s->pd.view(), a, b, p0 + 3 * q, margin, s->stream));
+    }
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t component,
+                                      int64_t count, const int64_t* indices,
+                                      const double* values)
+{
+    CPD_OK_OR_RETURN(check_ready(s, false));
+    if (kind < CPD_BC_FORCE_VALUE || kind > CPD_BC_FORCE_ADD || count < 0 || !values ||
+        (count > 0 && !indices))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_add_boundary_condition: bad arguments");
+    if (kind == CPD_BC_FORCE_ADD && (component < 0 || component > 2))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "component must be 0, 1 or 2");
+    CPD_CUDA(cudaSetDevice(s->device));
+    BoundaryCondition bc;
+    bc.kind = kind;
+    bc.component = component;
+    bc.count = count;
+    bc.value = values[0];
+    std::vector<int32_t> idx(count);
+    for (int64_t b = 0; b < count; b++) {
+        if (indices[b] < 0 || indices[b] >= s->n)
+            return set_error(CPD_ERR_INVALID_ARGUMENT, "boundary index out of range");
+        idx[b] = s->h_inv[indices[b]];
+    }
+    if (count > 0) {
+        CPD_CUDA(cudaMalloc(&bc.idx, sizeof(int32_t) * count));
+        CPD_CUDA(cudaMemcpy(bc.idx, idx.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+        if (kind == CPD_BC_FORCE_ADD) {
+            CPD_CUDA(cudaMalloc(&bc.values, sizeof(double) * count));
+            CPD_CUDA(cudaMemcpy(bc.values, values, sizeof(double) * count,
+                                cudaMemcpyHostToDevice));
+        }
+    }
+    s->bcs.push_back(bc);
+    return CPD_OK;
+}
+
+cpd_status cpd_clear_boundary_conditions(cpd_system* s)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto& bc : s->bcs) {
+        if (bc.idx) cudaFree(bc.idx);
+        if (bc.values) cudaFree(bc.values);
+    }
+    s->bcs.clear();
+    return CPD_OK;
+}
+
+cpd_status cpd_compute_weighted_volume(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (is_lps(s)) CPD_LAUNCHED(launch_lps_weighted_volume(view(s), pd_view(s), s->md, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_compute_dilatation(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (is_lps(s)) CPD_LAUNCHED(launch_lps_dilatation(view(s), pd_view(s), s->md, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_compute_force(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (has_pd(s)) CPD_OK_OR_RETURN(pd_force(s));
+    if (has_contact(s)) CPD_OK_OR_RETURN(contact_force(s, !has_pd(s)));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    double Wt = 0.0, Dt = 0.0;
+    if (has_pd(s)) {
+        const int nb = energy_blocks(s->n - s->frozen);
+        CPD_OK_OR_RETURN(ensure_reduction(s, nb));
+        CPD_LAUNCHED(launch_pd_energy(view(s), pd_view(s), s->md, s->red, nb, s->stream));
+        CPD_LAUNCHED(launch_sum_partials(s->red, nb, 2, s->red_out + 2, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
+                                 cudaMemcpyDeviceToHost, s->stream));
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
+        Wt = s->h_red[2];
+        Dt = s->h_red[3];
+    }
+    if (total_W) *total_W = Wt;
+    if (total_D) *total_D = Dt;
+    return CPD_OK;
+}
+
+// CabanaPD_Solver.hpp:229-279 init(bc): weighted volume once without
+// fracture, updateForce (no contact force unless the contact model is the
+// force model), energy, force BCs at t = 0.
+cpd_status cpd_init(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    const ParticleView p = view(s);
+    if (has_pd(s)) {
+        if (is_lps(s)) {
+            // Once here without fracture (Solver.hpp:235-239), inside
+            // updateForce with fracture (Solver.hpp:466-470): once either way.
+            CPD_LAUNCHED(launch_lps_weighted_volume(p, pd_view(s), s->md, s->stream));
+            CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
+        }
+        CPD_OK_OR_RETURN(pd_force(s));
+    } else if (has_contact(s)) {
+        CPD_OK_OR_RETURN(contact_force(s, true));
+    }
+    if (has_pd(s)) CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
+    CPD_OK_OR_RETURN(apply_force_bcs(s));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    s->initialized = true;
+    return CPD_OK;
+}
+
+// CabanaPD_Solver.hpp:332-375 runStep(step, bc), num_steps times.
+cpd_status cpd_step(cpd_system* s, int32_t num_steps)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step");
+    if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
+    CPD_CUDA(cudaSetDevice(s->device));
+    const ParticleView p = view(s);
+    for (int32_t k = 0; k < num_steps; k++) {
+        CPD_OK_OR_RETURN(vv_initial(s));
+        CPD_OK_OR_RETURN(update_force(s));
+        CPD_OK_OR_RETURN(apply_force_bcs(s));
+        CPD_LAUNCHED(launch_vv_final(p, s->params.dt, s->stream));
+    }
+    return CPD_OK;
+}
+
+cpd_status cpd_synchronize(cpd_system* s)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    CPD_CUDA(cudaSetDevice(s->device));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_download(cpd_system* s, int32_t field, double* out)
+{
+    CPD_OK_OR_RETURN(check_ready(s, false));
+    if (!out) return set_error(CPD_ERR_INVALID_ARGUMENT, "null output");
+    CPD_CUDA(cudaSetDevice(s->device));
+    const double* src = nullptr;
+    int comps = 1;
+    switch (field) {
+    case CPD_FIELD_X: src = s->x; comps = 3; break;
+    case CPD_FIELD_U: src = s->u; comps = 3; break;
+    case CPD_FIELD_V: src = s->v; comps = 3; break;
+    case CPD_FIELD_F: src = s->f; comps = 3; break;
+    case CPD_FIELD_VOL: src = s->vol; break;
+    case CPD_FIELD_RHO: src = s->rho; break;
+    case CPD_FIELD_M: src = s->m; break;
+    case CPD_FIELD_THETA: src = s->theta; break;
+    case CPD_FIELD_W: src = s->W; break;
+    case CPD_FIELD_PHI: src = s->phi; break;
+    case CPD_FIELD_RADIUS: src = s->radius; break;
+    default: return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown field");
+    }
+    s->launches += launch_soa_to_aos(src, s->staging, s->n, s->npad, comps, s->perm, s->stream);
+    CPD_CUDA(cudaGetLastError());
+    CPD_CUDA(cudaMemcpyAsync(out, s->staging, sizeof(double) * comps * s->n,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+double cpd_max_displacement(const cpd_system* s) { return s ? s->max_disp : 0.0; }
+int64_t cpd_contact_rebuilds(const cpd_system* s) { return s ? s->rebuilds : 0; }
+
+cpd_status cpd_device_field(cpd_system* s, int32_t field, void** ptr, int64_t* stride)
+{
+    CPD_OK_OR_RETURN(check_ready(s, false));
+    if (!ptr) return set_error(CPD_ERR_INVALID_ARGUMENT, "null output");
+    void* p = nullptr;
+    switch (field) {
+    case CPD_FIELD_X: p = s->x; break;
+    case CPD_FIELD_U: p = s->u; break;
+    case CPD_FIELD_V: p = s->v; break;
+    case CPD_FIELD_F: p = s->f; break;
+    case CPD_FIELD_VOL: p = s->vol; break;
+    case CPD_FIELD_RHO: p = s->rho; break;
+    case CPD_FIELD_M: p = s->m; break;
+    case CPD_FIELD_THETA: p = s->theta; break;
+    case CPD_FIELD_W: p = s->W; break;
+    case CPD_FIELD_PHI: p = s->phi; break;
+    case CPD_FIELD_RADIUS: p = s->radius; break;
+    default: return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown field");
+    }
+    *ptr = p;
+    if (stride) *stride = s->npad;
+    return CPD_OK;
+}
+
+cpd_status cpd_set_kernel_timing(cpd_system* s, int32_t enable)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    CPD_OK_OR_RETURN(harvest_timing(s));
+    s->timing = enable != 0;
+    s->timed_ms = 0.0;
+    s->timed_launches = 0;
+    return CPD_OK;
+}
+
+cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
+                           double* bytes_per_launch)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    CPD_OK_OR_RETURN(harvest_timing(s));
+    if (total_ms) *total_ms = s->timed_ms;
+    if (launches) *launches = s->timed_launches;
+    if (bytes_per_launch) {
+        // Compulsory traffic of one bond-kernel launch: per row, read x, u
+        // (48 B), vol (8 B), count (4 B), write f (24 B); per bond the 4-byte
+        // neighbour index; with fracture the 1-bit bond state read and
+        // written (0.25 B) and the 1-byte no-fail flag per row; LPS adds the
+        // two per-particle coefficient arrays (16 B). Neighbour gathers are
+        // counted once (ideal reuse).
+        const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
+        const double rows = (double)(s->n - s->frozen);
+        double per_row = 48.0 + 8.0 + 4.0 + 24.0;
+        double per_bond = 4.0;
+        if (has_pd(s) && s->md.fracture) {
+            per_row += 1.0;
+            per_bond += 0.25;
+        }
+        if (is_lps(s)) per_row += 16.0;
+        if (!has_pd(s)) per_row += 24.0 + 16.0;  // Hertz: v, rho (+vol already)
+        *bytes_per_launch = per_row * rows + per_bond * (double)nl.total;
+    }
+    return CPD_OK;
+}
+
+int64_t cpd_kernel_launches(const cpd_system* s) { return s ? s->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+// Internal data structures of the cabanapd_b200 library.
+//
+// HBM layout (one cpd_system):
+//   particle fields   structure-of-arrays, component-major: a vector field is
+//                     three contiguous double arrays of `npad` entries
+//                     (x0[0..npad), x1[...], x2[...]); scalars are [npad].
+//   PD neighbour list padded ELL, column-major: idx[k * npad + i] is the k-th
+//                     neighbour of particle i (internal index), k < count[i].
+//                     Row order is ascending caller index of the neighbour.
+//   broken bonds      one bit per bond: mu[w * npad + i] bit b covers bond
+//                     k = 32 w + b of particle i (1 = intact).
+// Column-major ELL makes the k-th loads of a warp's 32 consecutive particles
+// contiguous, and for particles on a lattice stored x-fastest the k-th
+// neighbours of consecutive particles are consecutive too, so neighbour
+// gathers coalesce.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cabanapd_b200.h"
+
+namespace cpd {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Model constants, derived on the host with the reference constructors'
+// expressions (force_models/CabanaPD_PMB.hpp:41-47, CabanaPD_LPS.hpp:64-75,
+// CabanaPD_ForceModels.hpp:93-102, CabanaPD_Hertzian.hpp:40-56).
+struct Model {
+    int pd = CPD_PD_NONE;
+    int fracture = 0;
+    int influence = 1;
+    int contact = CPD_CONTACT_NONE;
+    int per_particle_radius = 0;
+    double horizon = 0, K = 0, G = 0, G0 = 0;
+    double c = 0;
+    double theta_coeff = 0, s_coeff = 0;
+    double s0 = 0, bond_break_coeff = 0;
+    double radius = 0, radius_extend = 0, nu = 0, E = 0, e = 0;
+    double Rs = 0, Es = 0, beta = 0, coeff_h_n = 0, coeff_h_d = 0;
+};
+
+// Device view of one neighbour list.
+struct EllView {
+    const int32_t* count;
+    const int32_t* idx;
+    uint32_t* mu;  // nullptr for lists without bond state
+    int32_t max_n;
+};
+
+// Everything a particle kernel needs, passed by value.
+struct ParticleView {
+    int64_t n, frozen, npad;
+    const double* x;  // [3][npad]
+    double* u;        // [3][npad]
+    double* v;
+    double* f;
+    const double* vol;
+    const double* rho;
+    const uint8_t* nofail;
+    double* m;
+    double* theta;
+    double* lps_a;  // theta_coeff * theta / m per particle
+    double* lps_b;  // s_coeff / m per particle
+    double* W;
+    double* phi;
+    const double* radius;
+    double* u_neigh;
+};
+
+struct NeighborList {
+    int32_t max_n = 0;
+    int64_t total = 0;
+    int32_t nwords = 0;
+    int32_t* count = nullptr;
+    int32_t* idx = nullptr;
+    uint32_t* mu = nullptr;
+    EllView view() const { return EllView{count, idx, mu, max_n}; }
+};
+
+struct BoundaryCondition {
+    int kind = 0;
+    int component = 0;
+    int64_t count = 0;
+    int32_t* idx = nullptr;      // internal indices
+    double* values = nullptr;    // device, [count] for FORCE_ADD
+    double value = 0;            // scalar kinds
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (definitions in cpd_kernels_exact.cu / cpd_neighbor.cu).
+// Each returns the number of kernels it launched.
+int launch_vv_initial(const ParticleView& p, double dt, bool track_max,
+                      double* block_max, int max_blocks, cudaStream_t st);
+int launch_vv_final(const ParticleView& p, double dt, cudaStream_t st);
+int launch_lps_weighted_volume(const ParticleView& p, const EllView& nl,
+                               const Model& md, cudaStream_t st);
+int launch_lps_dilatation(const ParticleView& p, const EllView& nl,
+                          const Model& md, cudaStream_t st);
+int launch_pd_force(const ParticleView& p, const EllView& nl, const Model& md,
+                    cudaStream_t st);
+int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
+                     double* partials, int nblocks, cudaStream_t st);
+int launch_hertz_force(const ParticleView& p, const EllView& nl,
+                       const Model& md, bool reset, cudaStream_t st);
+int launch_force_bc(const ParticleView& p, const BoundaryCondition& bc,
+                    cudaStream_t st);
+int launch_prenotch(const ParticleView& p, const EllView& nl, const double* v1,
+                    const double* v2, const double* p0, double margin,
+                    cudaStream_t st);
+int launch_sum_partials(const double* partials, int nblocks, int ncols,
+                        double* out, cudaStream_t st);
+int launch_max_partials(const double* partials, int nblocks, double* out,
+                        cudaStream_t st);
+int energy_blocks(int64_t nrows);
+int vv_blocks(int64_t nrows);
+
+// Neighbour build (cpd_neighbor.cu). Builds rows for [begin, n) from
+// positions pos (+ optional displacement disp) with squared distance
+// <= cutoff^2; rows sorted by ascending user_id of the neighbour.
+struct BuildScratch;
+int build_neighbor_list(const double* pos, const double* disp, int64_t n,
+                        int64_t npad, int64_t begin, double cutoff,
+                        const int32_t* user_id, bool with_mu,
+                        NeighborList& out, cudaStream_t st, std::string& err);
+void free_neighbor_list(NeighborList& nl);
+
+// Layout kernels.
+int launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t npad,
+                      int comps, const int32_t* perm, cudaStream_t st);
+int launch_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t npad,
+                      int comps, const int32_t* perm, cudaStream_t st);
+int launch_ell_to_rows(const NeighborList& nl, int64_t n, int64_t npad,
+                       const int32_t* perm, const int32_t* user_id,
+                       int32_t* counts, int32_t* indices, int32_t* mu,
+                       cudaStream_t st);
+
+}  // namespace cpd

@@ -1,0 +1,274 @@
+"""Python binding of the C ABI (include/cabanapd_b200.h) via ctypes.
+
+The CUDA library is the only compute path: if libcabanapd_b200.so is
+missing, or no CUDA device is present, System() raises. There is no CPU
+fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcabanapd_b200.so")
+
+FIELDS = {"x": 0, "u": 1, "v": 2, "f": 3, "vol": 4, "rho": 5, "m": 6,
+          "theta": 7, "W": 8, "phi": 9, "radius": 10}
+VECTOR_FIELDS = {"x", "u", "v", "f"}
+FP64_EXACT = 0
+ORDER_INPUT, ORDER_MORTON = 0, 1
+
+_lib = None
+
+
+class CpdParams(ctypes.Structure):
+    _fields_ = [
+        ("pd_model", ctypes.c_int32),
+        ("fracture", ctypes.c_int32),
+        ("influence_type", ctypes.c_int32),
+        ("contact_model", ctypes.c_int32),
+        ("horizon", ctypes.c_double),
+        ("K", ctypes.c_double),
+        ("G", ctypes.c_double),
+        ("G0", ctypes.c_double),
+        ("contact_radius", ctypes.c_double),
+        ("radius_extend", ctypes.c_double),
+        ("nu", ctypes.c_double),
+        ("E", ctypes.c_double),
+        ("restitution", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("rebuild_every", ctypes.c_int32),
+        ("per_particle_radius", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("ordering", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class CpdError(RuntimeError):
+    pass
+
+
+# Every symbol the header declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "cpd_abi_version": (_I32, []),
+    "cpd_last_error": (ctypes.c_char_p, []),
+    "cpd_system_create": (_I32, [ctypes.POINTER(CpdParams), ctypes.POINTER(_P)]),
+    "cpd_system_destroy": (_I32, [_P]),
+    "cpd_set_stream": (_I32, [_P, _P]),
+    "cpd_get_stream": (_I32, [_P, ctypes.POINTER(_P)]),
+    "cpd_model_constants": (_I32, [_P, _DP]),
+    "cpd_upload_particles": (_I32, [_P, _I64, _I64, _P, _P, _P, _P, _P]),
+    "cpd_set_state": (_I32, [_P, _P, _P]),
+    "cpd_build_neighbors": (_I32, [_P]),
+    "cpd_neighbor_stats": (_I32, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
+    "cpd_download_neighbors": (_I32, [_P, _P, _P, _P]),
+    "cpd_prenotch": (_I32, [_P, _I32, _P, _P, _P]),
+    "cpd_add_boundary_condition": (_I32, [_P, _I32, _I32, _I64, _P, _P]),
+    "cpd_clear_boundary_conditions": (_I32, [_P]),
+    "cpd_compute_weighted_volume": (_I32, [_P]),
+    "cpd_compute_dilatation": (_I32, [_P]),
+    "cpd_compute_force": (_I32, [_P]),
+    "cpd_compute_energy": (_I32, [_P, _DP, _DP]),
+    "cpd_init": (_I32, [_P]),
+    "cpd_step": (_I32, [_P, _I32]),
+    "cpd_synchronize": (_I32, [_P]),
+    "cpd_download": (_I32, [_P, _I32, _P]),
+    "cpd_max_displacement": (_D, [_P]),
+    "cpd_contact_rebuilds": (_I64, [_P]),
+    "cpd_device_field": (_I32, [_P, _I32, ctypes.POINTER(_P), ctypes.POINTER(_I64)]),
+    "cpd_set_kernel_timing": (_I32, [_P, _I32]),
+    "cpd_kernel_time": (_I32, [_P, _DP, ctypes.POINTER(_I64), _DP]),
+    "cpd_kernel_launches": (_I64, [_P]),
+}
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CpdError(
+            f"{path} not found: build the CUDA library first "
+            "(python -c 'import __graft_entry__ as g; g.build()' or make -C "
+            "cabanapd_b200/csrc)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class System:
+    """One simulation on the GPU (a cpd_system handle)."""
+
+    backend = "cuda"
+
+    def __init__(self, params, device=0, precision=FP64_EXACT, ordering=ORDER_INPUT):
+        lib = load()
+        p = CpdParams()
+        p.influence_type = -1
+        for k, _ in CpdParams._fields_:
+            if k in params:
+                setattr(p, k, params[k])
+        p.precision = params.get("precision", precision)
+        p.ordering = params.get("ordering", ordering)
+        p.device = params.get("device", device)
+        self._lib = lib
+        h = _P()
+        self._check(lib.cpd_system_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.n = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CpdError(f"cabanapd_b200 error {rc}: {self._lib.cpd_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cpd_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def model_constants(self):
+        out = np.zeros(10)
+        self._check(self._lib.cpd_model_constants(self._h, out.ctypes.data_as(_DP)))
+        keys = ["c", "s0", "bond_break_coeff", "theta_coeff", "s_coeff", "Rs",
+                "Es", "beta", "coeff_h_n", "coeff_h_d"]
+        return dict(zip(keys, out.tolist()))
+
+    def set_particles(self, x, vol, rho=None, nofail=None, radius=None, n_frozen=0):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        n = x.shape[0]
+        vol = np.ascontiguousarray(vol, dtype=np.float64)
+        rho = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        nofail = None if nofail is None else np.ascontiguousarray(nofail, dtype=np.int32)
+        radius = None if radius is None else np.ascontiguousarray(radius, dtype=np.float64)
+        self._check(self._lib.cpd_upload_particles(
+            self._h, n, int(n_frozen), _ptr(x), _ptr(vol), _ptr(rho), _ptr(nofail),
+            _ptr(radius)))
+        self.n = n
+
+    def set_state(self, u=None, v=None):
+        u = None if u is None else np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
+        v = None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        self._check(self._lib.cpd_set_state(self._h, _ptr(u), _ptr(v)))
+
+    def build_neighbors(self):
+        self._check(self._lib.cpd_build_neighbors(self._h))
+
+    def neighbor_stats(self):
+        mx, tot = _I32(), _I64()
+        self._check(self._lib.cpd_neighbor_stats(self._h, ctypes.byref(mx), ctypes.byref(tot)))
+        return mx.value, tot.value
+
+    def neighbors(self):
+        mx, _ = self.neighbor_stats()
+        counts = np.zeros(self.n, dtype=np.int32)
+        idx = np.zeros((self.n, max(mx, 1)), dtype=np.int32)
+        mu = np.zeros((self.n, max(mx, 1)), dtype=np.int32)
+        self._check(self._lib.cpd_download_neighbors(self._h, _ptr(counts), _ptr(idx), _ptr(mu)))
+        return counts, idx[:, :mx], mu[:, :mx]
+
+    def prenotch(self, v1, v2, p0):
+        v1 = np.ascontiguousarray(v1, dtype=np.float64).reshape(-1, 3)
+        v2 = np.ascontiguousarray(v2, dtype=np.float64).reshape(-1, 3)
+        p0 = np.ascontiguousarray(p0, dtype=np.float64).reshape(-1, 3)
+        self._check(self._lib.cpd_prenotch(self._h, p0.shape[0], _ptr(v1), _ptr(v2), _ptr(p0)))
+
+    def add_bc(self, kind, indices, values, component=0):
+        idx = np.ascontiguousarray(indices, dtype=np.int64)
+        vals = np.ascontiguousarray(np.atleast_1d(values), dtype=np.float64)
+        self._check(self._lib.cpd_add_boundary_condition(
+            self._h, int(kind), int(component), idx.size, _ptr(idx), _ptr(vals)))
+
+    def clear_bcs(self):
+        self._check(self._lib.cpd_clear_boundary_conditions(self._h))
+
+    def compute_weighted_volume(self):
+        self._check(self._lib.cpd_compute_weighted_volume(self._h))
+
+    def compute_dilatation(self):
+        self._check(self._lib.cpd_compute_dilatation(self._h))
+
+    def compute_force(self):
+        self._check(self._lib.cpd_compute_force(self._h))
+
+    def compute_energy(self):
+        w, d = _D(), _D()
+        self._check(self._lib.cpd_compute_energy(self._h, ctypes.byref(w), ctypes.byref(d)))
+        return w.value, d.value
+
+    def init(self):
+        self._check(self._lib.cpd_init(self._h))
+
+    def step(self, num_steps):
+        """Queue num_steps steps (asynchronous)."""
+        self._check(self._lib.cpd_step(self._h, int(num_steps)))
+
+    def run(self, num_steps):
+        self.step(num_steps)
+        self.synchronize()
+
+    def synchronize(self):
+        self._check(self._lib.cpd_synchronize(self._h))
+
+    def get(self, field, out=None):
+        shape = (self.n, 3) if field in VECTOR_FIELDS else (self.n,)
+        if out is None:
+            out = np.zeros(shape)
+        self._check(self._lib.cpd_download(self._h, FIELDS[field], out.ctypes.data))
+        return out
+
+    def max_displacement(self):
+        return self._lib.cpd_max_displacement(self._h)
+
+    def contact_rebuilds(self):
+        return self._lib.cpd_contact_rebuilds(self._h)
+
+    def device_field(self, field):
+        ptr, stride = _P(), _I64()
+        self._check(self._lib.cpd_device_field(self._h, FIELDS[field], ctypes.byref(ptr),
+                                               ctypes.byref(stride)))
+        return ptr.value, stride.value
+
+    def set_stream(self, stream_handle):
+        self._check(self._lib.cpd_set_stream(self._h, stream_handle))
+
+    def get_stream(self):
+        s = _P()
+        self._check(self._lib.cpd_get_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+    def set_kernel_timing(self, enable=True):
+        self._check(self._lib.cpd_set_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_time(self):
+        ms, n, b = _D(), _I64(), _D()
+        self._check(self._lib.cpd_kernel_time(self._h, ctypes.byref(ms), ctypes.byref(n),
+                                              ctypes.byref(b)))
+        return ms.value, n.value, b.value
+
+    def kernel_launches(self):
+        return self._lib.cpd_kernel_launches(self._h)

@@ -1,0 +1,225 @@
+/*
+ * cabanapd_b200 — C ABI of the B200-native CabanaPD per-timestep hot path.
+ *
+ * One opaque handle (cpd_system) owns every device buffer of one simulation:
+ * particle fields in structure-of-arrays layout, the padded-ELL neighbour
+ * list with 1-bit-per-bond broken-bond masks, the contact list, boundary
+ * condition index lists and reduction scratch. Host arrays passed in or out
+ * are owned by the caller and are copied; no pointer is retained after a
+ * call returns. Calls are synchronous with respect to the host unless they
+ * say otherwise; work is issued on the system's CUDA stream.
+ *
+ * The entry points replace the reference's template interface as follows
+ * (paths relative to the CabanaPD source tree):
+ *
+ *   cpd_system_create        ForceModel(...) constructors
+ *                            (force_models/CabanaPD_PMB.hpp:165-231,
+ *                             force_models/CabanaPD_LPS.hpp:151-253,
+ *                             force_models/CabanaPD_Hertzian.hpp:40-56),
+ *                            VelocityVerlet(dt) (CabanaPD_Integrate.hpp:80-86)
+ *   cpd_upload_particles     Particles::create + Particles::update
+ *                            (CabanaPD_Particles.hpp:242-307, 429-443)
+ *   cpd_set_state            Particles::update of u / v (same lines)
+ *   cpd_build_neighbors      Neighbor ctor (CabanaPD_Neighbor.hpp:44-66,
+ *                            199-210): full list, cutoff + 1e-14, mu = 1
+ *   cpd_neighbor_stats       Neighbor::getStatistics (Neighbor.hpp:80-102)
+ *   cpd_prenotch             Prenotch<N>::create (CabanaPD_Prenotch.hpp:215-263)
+ *   cpd_add_boundary_condition  createBoundaryCondition / BodyTerm
+ *                            (CabanaPD_Boundary.hpp:34-204, CabanaPD_BodyTerm.hpp:25-69)
+ *   cpd_compute_weighted_volume / cpd_compute_dilatation / cpd_compute_force /
+ *   cpd_compute_energy       Force<...>::computeWeightedVolume /
+ *                            computeDilatation / computeForceFull /
+ *                            computeEnergyFull and the free functions
+ *                            computeForce / computeEnergy (CabanaPD_Force.hpp:176-219)
+ *   cpd_init                 Solver::init(bc[, prenotch]) (CabanaPD_Solver.hpp:229-297)
+ *   cpd_step                 Solver::runStep(step, bc) x num_steps
+ *                            (CabanaPD_Solver.hpp:332-375)
+ *   cpd_download             Particles::slice*() + deep_copy to host
+ *
+ * Errors: every call returns a cpd_status; cpd_last_error() gives the
+ * message of the last failure on the calling thread. The reference throws
+ * std::runtime_error in the same situations (e.g. Solver.hpp:172-174).
+ * Handles are not thread-safe: drive one handle from one host thread.
+ */
+#ifndef CABANAPD_B200_H
+#define CABANAPD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPD_ABI_VERSION 1
+
+typedef struct cpd_system cpd_system;
+typedef int32_t cpd_status;
+
+enum {
+    CPD_OK = 0,
+    CPD_ERR_INVALID_ARGUMENT = 1,
+    CPD_ERR_OUT_OF_MEMORY = 2,
+    CPD_ERR_CUDA = 3,
+    CPD_ERR_STATE = 4,       /* call out of order (e.g. step before init) */
+    CPD_ERR_UNSUPPORTED = 5
+};
+
+/* Peridynamic force models (CabanaPD_Types.hpp:145-163). */
+enum {
+    CPD_PD_NONE = 0,
+    CPD_PD_PMB = 1,
+    CPD_PD_LPS = 2,
+    CPD_PD_LINEAR_PMB = 3,
+    CPD_PD_LINEAR_LPS = 4
+};
+
+/* Contact models (force_models/CabanaPD_Hertzian.hpp). */
+enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1 };
+
+/* Kernel arithmetic. EXACT evaluates every per-bond expression with IEEE
+ * double operations in the reference's operand order (no FMA contraction),
+ * so per-particle results equal a scalar CPU evaluation bit for bit. */
+enum { CPD_FP64_EXACT = 0 };
+
+/* Internal particle order: INPUT keeps the caller's order; MORTON sorts by
+ * the Morton code of the particle's cell (results are returned in the
+ * caller's order either way). */
+enum { CPD_ORDER_INPUT = 0, CPD_ORDER_MORTON = 1 };
+
+/* Force boundary conditions, applied after the force every step and once at
+ * init (Solver.hpp:270-273, 365-367), in the order they were added. */
+enum {
+    CPD_BC_FORCE_VALUE = 0,  /* f(p, d) = values[0], d = 0..2 (ForceValueBCTag) */
+    CPD_BC_FORCE_UPDATE = 1, /* f(p, d) += values[0], d = 0..2 (ForceUpdateBCTag) */
+    CPD_BC_FORCE_ADD = 2     /* f(p, component) += values[b]: the custom-functor
+                                traction / body-force form f(p, d) += g(p) */
+};
+
+/* Fields for cpd_download / cpd_device_field. Vector fields are returned as
+ * [n][3] (x, y, z interleaved, the reference's slice layout). */
+enum {
+    CPD_FIELD_X = 0,      /* reference position */
+    CPD_FIELD_U = 1,      /* displacement */
+    CPD_FIELD_V = 2,      /* velocity */
+    CPD_FIELD_F = 3,      /* force density */
+    CPD_FIELD_VOL = 4,
+    CPD_FIELD_RHO = 5,
+    CPD_FIELD_M = 6,      /* LPS weighted volume */
+    CPD_FIELD_THETA = 7,  /* LPS dilatation */
+    CPD_FIELD_W = 8,      /* strain energy density */
+    CPD_FIELD_PHI = 9,    /* damage */
+    CPD_FIELD_RADIUS = 10 /* contact radius (per-particle model) */
+};
+
+typedef struct cpd_params {
+    int32_t pd_model;            /* CPD_PD_* */
+    int32_t fracture;            /* 1: critical-stretch bond breaking */
+    int32_t influence_type;      /* LPS/fracture influence: -1 model default
+                                    (PMB 1, LPS 0), else 0 or 1 */
+    int32_t contact_model;       /* CPD_CONTACT_* */
+    double horizon;              /* PD force horizon delta */
+    double K, G, G0;             /* bulk modulus, shear modulus, fracture energy */
+    double contact_radius;       /* Hertz particle radius (largest radius when
+                                    per_particle_radius = 1) */
+    double radius_extend;        /* contact search-radius extension (skin) */
+    double nu, E, restitution;   /* Hertz material */
+    double dt;                   /* time step */
+    int32_t rebuild_every;       /* contact list: 0 = rebuild when the largest
+                                    displacement since the last build exceeds
+                                    radius_extend (Neighbor.hpp:118-119);
+                                    k > 0 = rebuild every k steps */
+    int32_t per_particle_radius; /* 1: Hertz with per-particle radii */
+    int32_t precision;           /* CPD_FP64_EXACT */
+    int32_t ordering;            /* CPD_ORDER_* */
+    int32_t device;              /* CUDA device ordinal */
+} cpd_params;
+
+int32_t cpd_abi_version(void);
+const char* cpd_last_error(void);
+
+cpd_status cpd_system_create(const cpd_params* params, cpd_system** out);
+cpd_status cpd_system_destroy(cpd_system* sys);
+
+/* Use a caller-owned CUDA stream (a cudaStream_t passed as void*) instead of
+ * the system's own. NULL restores the system's own stream. */
+cpd_status cpd_set_stream(cpd_system* sys, void* cuda_stream);
+cpd_status cpd_get_stream(cpd_system* sys, void** cuda_stream);
+
+/* Model constants derived by the reference constructors:
+ * out[0]=c, [1]=s0, [2]=bond_break_coeff, [3]=theta_coeff, [4]=s_coeff,
+ * [5]=Rs, [6]=Es, [7]=beta, [8]=coeff_h_n, [9]=coeff_h_d. */
+cpd_status cpd_model_constants(const cpd_system* sys, double* out10);
+
+/* Particles [0, n_frozen) are frozen: never integrated, no neighbour rows,
+ * but still neighbours of others (CabanaPD_Particles.hpp:543-556).
+ * x: [n][3]; vol: [n]; rho, nofail, radius may be NULL (1.0, 0, contact_radius).
+ * Resets u, v, f to zero. */
+cpd_status cpd_upload_particles(cpd_system* sys, int64_t n, int64_t n_frozen,
+                                const double* x, const double* vol,
+                                const double* rho, const int32_t* nofail,
+                                const double* radius);
+/* u, v: [n][3] or NULL to leave unchanged. */
+cpd_status cpd_set_state(cpd_system* sys, const double* u, const double* v);
+
+cpd_status cpd_build_neighbors(cpd_system* sys);
+cpd_status cpd_neighbor_stats(const cpd_system* sys, int32_t* max_neighbors,
+                              int64_t* total_neighbors);
+/* Row i (caller's order) lists neighbours in ascending caller index:
+ * counts [n]; indices and mu [n][max_neighbors] (padding -1 / 0).
+ * mu[i][k] = 1 while bond k of particle i is intact. Any pointer may be NULL.
+ * Returns the PD list, or the contact list for a DEM-only system. */
+cpd_status cpd_download_neighbors(cpd_system* sys, int32_t* counts,
+                                  int32_t* indices, int32_t* mu);
+
+/* v1, v2, p0: [count][3] (plane vectors and corner of each notch). */
+cpd_status cpd_prenotch(cpd_system* sys, int32_t count, const double* v1,
+                        const double* v2, const double* p0);
+
+/* indices: caller particle indices [count]; values: 1 scalar for
+ * FORCE_VALUE / FORCE_UPDATE, [count] for FORCE_ADD. */
+cpd_status cpd_add_boundary_condition(cpd_system* sys, int32_t kind,
+                                      int32_t component, int64_t count,
+                                      const int64_t* indices,
+                                      const double* values);
+cpd_status cpd_clear_boundary_conditions(cpd_system* sys);
+
+/* Kernel-level seam, as the reference's unit tests call Force directly. */
+cpd_status cpd_compute_weighted_volume(cpd_system* sys);
+cpd_status cpd_compute_dilatation(cpd_system* sys);
+cpd_status cpd_compute_force(cpd_system* sys);
+/* W_i, damage phi_i and the totals sum(W_i vol_i), sum(phi_i). */
+cpd_status cpd_compute_energy(cpd_system* sys, double* total_strain_energy,
+                              double* total_damage);
+
+cpd_status cpd_init(cpd_system* sys);
+/* num_steps velocity-Verlet steps. Asynchronous: returns once the work is
+ * queued on the stream (cpd_synchronize or any download waits for it). */
+cpd_status cpd_step(cpd_system* sys, int32_t num_steps);
+cpd_status cpd_synchronize(cpd_system* sys);
+
+/* Copy a field to host memory in the caller's particle order. */
+cpd_status cpd_download(cpd_system* sys, int32_t field, double* host_out);
+double cpd_max_displacement(const cpd_system* sys);
+int64_t cpd_contact_rebuilds(const cpd_system* sys);
+
+/* Device pointer of a field in the internal order, component-major
+ * ([3][stride] for vectors), for user kernels between steps. */
+cpd_status cpd_device_field(cpd_system* sys, int32_t field, void** ptr,
+                            int64_t* stride);
+
+/* Per-kernel device time: when enabled, the bond kernels of every step are
+ * bracketed by CUDA events on the system stream.
+ * cpd_kernel_time returns the summed milliseconds and launch count of the
+ * main bond kernel since timing was enabled, and the bytes it is
+ * algorithmically required to move per launch. */
+cpd_status cpd_set_kernel_timing(cpd_system* sys, int32_t enable);
+cpd_status cpd_kernel_time(cpd_system* sys, double* total_ms,
+                           int64_t* launches, double* bytes_per_launch);
+/* Number of kernels this library launched on the system since creation. */
+int64_t cpd_kernel_launches(const cpd_system* sys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

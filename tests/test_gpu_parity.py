@@ -1,0 +1,208 @@
+"""Parity of the CUDA path (called through the C ABI) against the CPU oracle
+on the same seeded inputs, plus the reference's own checks run on the GPU.
+
+Tolerances: the plain-FP64 path evaluates every per-bond expression with
+the reference's IEEE operation order and sums each neighbour row in the
+oracle's order, so per-particle fields (u, v, f, W, phi, m, theta) and the
+broken-bond sets must be BIT-IDENTICAL. Global totals are tree reductions on
+the GPU vs serial sums on the CPU: relative difference <= 1e-12. Hertz
+contact evaluates pow(|d|, 1.5), which CUDA and glibc may round differently
+in the last place: <= 1e-12 relative, norm-wise.
+"""
+import numpy as np
+import pytest
+
+import force_checks
+from cabanapd_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    import cabanapd_b200
+    return cabanapd_b200
+
+
+def _pair(cuda, oracle, prob, init=True, ordering=0):
+    params = dict(prob["params"], ordering=ordering)
+    g = cuda.System(params)
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(g, prob, init=init)
+    P.setup(o, prob, init=init)
+    return g, o
+
+
+def _assert_same(g, o, fields=("u", "v", "f")):
+    for fld in fields:
+        a, b = g.get(fld), o.get(fld)
+        assert np.array_equal(a, b), (fld, np.max(np.abs(a - b)))
+
+
+def _rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+@pytest.mark.parametrize("case,kind,coeff", [
+    ("pmb", "linear", 0.1), ("pmb", "quadratic", 0.01),
+    ("pmb_damage", "quadratic", 0.01), ("linear_pmb", "linear", 0.1),
+    ("lps", "linear", 0.1), ("lps", "quadratic", 0.01),
+    ("lps_damage", "quadratic", 0.01), ("linear_lps", "linear", 0.1),
+])
+def test_force_cases_match_reference_and_oracle(cuda, oracle, case, kind, coeff):
+    """unit_test/tstForce.hpp checks on the GPU, and bit-identity with the
+    oracle for every particle."""
+    res_g, _ = force_checks.run_case(lambda p: cuda.System(p), case, kind, coeff)
+    force_checks.check_case(res_g, case, kind, coeff, max_checked=40)
+    res_o, _ = force_checks.run_case(lambda p: oracle.OracleSystem(p), case, kind, coeff)
+    for fld in ("f", "W", "theta"):
+        assert np.array_equal(res_g[fld], res_o[fld]), fld
+    assert _rel(res_g["Phi"], res_o["Phi"]) <= 1e-12
+    assert res_g["constants"] == res_o["constants"]
+    assert res_g["max_neighbors"] == res_o["max_neighbors"] == 122
+
+
+@pytest.mark.parametrize("ordering", [0, 1])
+def test_neighbor_sets_identical(cuda, oracle, ordering):
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, size=(3000, 3))
+    params = dict(pd_model=P.PD_PMB, fracture=1, horizon=0.2, K=1.0, G0=1.0, dt=1.0)
+    g = cuda.System(dict(params, ordering=ordering))
+    o = oracle.OracleSystem(params)
+    for s in (g, o):
+        s.set_particles(x, np.ones(3000), n_frozen=100)
+        s.build_neighbors()
+    assert g.neighbor_stats() == o.neighbor_stats()
+    cg, ig, mg = g.neighbors()
+    co, io, mo = o.neighbors()
+    assert np.array_equal(cg, co)
+    assert np.array_equal(ig, io)
+    assert np.array_equal(mg, mo)
+    assert np.all(cg[:100] == 0)
+
+
+def test_elastic_wave_pmb_bit_exact(cuda, oracle):
+    """Config 0 (41^3 PMB elastic wave, 100 steps): displacements bit-identical
+    at every checked step, total strain energy within 1e-12."""
+    prob = P.elastic_wave_pmb(n=41, steps=100)
+    g, o = _pair(cuda, oracle, prob)
+    assert g.neighbor_stats() == o.neighbor_stats()
+    done = 0
+    for target in (1, 10, 100):
+        g.run(target - done)
+        o.run(target - done)
+        done = target
+        _assert_same(g, o)
+        wg, _ = g.compute_energy()
+        wo, _ = o.compute_energy()
+        assert _rel(wg, wo) <= 1e-12
+        assert np.array_equal(g.get("W"), o.get("W"))
+
+
+@pytest.mark.parametrize("ordering", [0, 1])
+def test_plate_impact_fracture_bit_exact(cuda, oracle, ordering):
+    """Config 1 layout at reduced size: identical broken-bond sets, forces,
+    displacements and damage after each block of steps."""
+    prob = P.plate_impact(num_cells=(96, 48, 6), steps=240, v0=60.0)
+    g, o = _pair(cuda, oracle, prob, ordering=ordering)
+    _, _, mu0 = o.neighbors()
+    _, _, mg0 = g.neighbors()
+    assert np.array_equal(mg0, mu0)
+    assert (mu0 == 0).sum() > 0  # the notches cut bonds
+    for _ in range(3):
+        g.run(80)
+        o.run(80)
+        _assert_same(g, o)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        wg, dg = g.compute_energy()
+        wo, do = o.compute_energy()
+        assert np.array_equal(g.get("phi"), o.get("phi"))
+        assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+    assert (o.neighbors()[2] == 0).sum() > (mu0 == 0).sum()  # bonds broke
+
+
+def test_lps_random_notches_bit_exact(cuda, oracle):
+    """Config 2 layout at reduced size (LPS, fracture, 20 seeded notches,
+    traction BC, no-fail zone): m, theta, u, f, mu identical."""
+    prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
+    prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
+    g, o = _pair(cuda, oracle, prob)
+    for _ in range(3):
+        g.run(20)
+        o.run(20)
+        _assert_same(g, o, ("u", "v", "f", "m", "theta"))
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+    wg, dg = g.compute_energy()
+    wo, do = o.compute_energy()
+    assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+    assert np.array_equal(g.get("W"), o.get("W"))
+
+
+@pytest.mark.parametrize("model", [P.PD_LINEAR_PMB, P.PD_LINEAR_LPS, P.PD_LPS])
+def test_elastic_models_bit_exact(cuda, oracle, model):
+    prob = P.elastic_wave_pmb(n=21, steps=30)
+    prob["params"] = dict(prob["params"], pd_model=model, G=0.5)
+    g, o = _pair(cuda, oracle, prob)
+    g.run(30)
+    o.run(30)
+    _assert_same(g, o, ("u", "v", "f", "theta", "m"))
+
+
+def test_kalthoff_winkler_regression_on_gpu(cuda, golden):
+    from test_oracle_regression import kw_max_crack_y
+    g_ = golden["kalthoff_winkler"]
+    prob = P.kalthoff_winkler_regression()
+    s = cuda.System(prob["params"])
+    P.setup(s, prob)
+    y = kw_max_crack_y(s, prob)
+    assert abs(y - g_["max_crack_y"]) <= g_["tolerance"], y
+
+
+def test_hertz_regression_on_gpu(cuda, oracle, golden):
+    from test_oracle_regression import hertz_restitution
+    prob = P.hertz_two_spheres()
+    s = cuda.System(prob["params"])
+    P.setup(s, prob)
+    r = hertz_restitution(s, prob)
+    e = golden["hertz"]["input"]["restitution"]["value"]
+    assert abs(r - e) <= golden["hertz"]["tolerance"], r
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(o, prob)
+    o.run(prob["num_steps"])
+    v_g, v_o = s.get("v"), o.get("v")
+    assert np.linalg.norm(v_g - v_o) <= 1e-12 * np.linalg.norm(v_o)
+    assert s.contact_rebuilds() == o.contact_rebuilds()
+
+
+def test_dem_packing_parity(cuda, oracle):
+    """Config 3 layout at reduced size: polydisperse Hertz, rebuild every 10
+    steps; contact sets identical at each rebuild, fields within 1e-12."""
+    prob = P.dem_packing(lattice_dims=(16, 16, 8), steps=100, dt=2e-6)
+    g, o = _pair(cuda, oracle, prob)
+    for _ in range(4):
+        g.run(25)
+        o.run(25)
+        assert g.contact_rebuilds() == o.contact_rebuilds()
+        assert np.array_equal(g.neighbors()[1], o.neighbors()[1])
+        for fld in ("u", "v"):
+            a, b = g.get(fld), o.get(fld)
+            assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), fld
+
+
+def test_errors_are_reported(cuda):
+    s = cuda.System(dict(pd_model=P.PD_PMB, horizon=0.1, K=1.0, dt=1.0))
+    with pytest.raises(cuda.CpdError):
+        s.init()  # no particles
+    with pytest.raises(cuda.CpdError):
+        cuda.System(dict(pd_model=P.PD_LINEAR_PMB, fracture=1, horizon=0.1, K=1.0))
+    x, vol, _ = P.lattice([0, 0, 0], [1, 1, 1], [4, 4, 4])
+    s.set_particles(x, vol)
+    with pytest.raises(cuda.CpdError):
+        s.step(1)  # neighbour list not built
+    s.build_neighbors()
+    with pytest.raises(cuda.CpdError):
+        s.step(1)  # init not called
+    with pytest.raises(cuda.CpdError):
+        s.prenotch([[1, 0, 0]], [[0, 1, 0]], [[0, 0, 0]])  # no fracture model
+    with pytest.raises(cuda.CpdError):
+        s.add_bc(P.BC_FORCE_VALUE, [10 ** 6], [0.0])
