@@ -266,7 +266,8 @@ def run_gpu(args, world, rank, local, pg):
     prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
     stream = torch.cuda.Stream(device=device)
 
-    sys_ = cabanapd_b200.System(dict(prob["params"], device=device))
+    prec = {"fp64": 1, "exact": 0}[args.precision]
+    sys_ = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
     sys_.set_stream(stream.cuda_stream)
     P.setup(sys_, prob)
     _, bonds = sys_.neighbor_stats()
@@ -299,6 +300,52 @@ def run_gpu(args, world, rank, local, pg):
     value, ms, total_bonds = aggregate(pg, device, ms_local, bonds, args.steps)
     particle_steps = reduce_sum(pg, float(n), device) * args.steps / (ms / 1e3)
 
+    if args.skip_e2e:
+        e2e_value, h2d, d2h = None, None, None
+    else:
+        e2e_value, h2d, d2h = run_e2e(args, prob, device, stream, pg, total_bonds, sys_)
+        sys_ = None
+    if rank != 0:
+        return
+    hbm, hbm_kind = peaks()
+    avg_ms = k_ms / max(k_n, 1)
+    achieved = k_bytes / (avg_ms / 1e3) / 1e9
+    tpb = traffic_per_bond()
+    line = {
+        "metric": "bond-updates/s", "value": value, "unit": "bond-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "pmb_fracture_notched_plate_impact",
+                   "plate_cells": list(PLATE_CELLS), "particles_per_gpu": n,
+                   "bonds_per_gpu": bonds, "precision": args.precision,
+                   "l2": "inputs larger than L2 (neighbour list %.1f GB)" % (4 * bonds / 1e9),
+                   "particle_steps_per_s": particle_steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": hbm_kind,
+                     "kernel": ("k_pmb_force_fast<fracture>" if args.precision == "fp64"
+                                else "k_pd_force<PMB, fracture> (exact)"),
+                     "kernel_ms_avg": avg_ms, "kernel_launches": k_n,
+                     "algorithmic_bytes_per_launch": k_bytes,
+                     "traffic": (tpb * bonds if tpb else None)},
+        "e2e": ({"value": e2e_value, "unit": "bond-updates/s",
+                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                 "job": ("upload + neighbour build + prenotch + init + steps + "
+                         "energy/damage read every 10 steps + download u")}
+                if e2e_value is not None else None),
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.skip_cpu:
+        line["cpu_baseline"] = time_cpu_sample()
+        line["cpu_baseline"].pop("steps", None)
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, prob, device, stream, pg, total_bonds, old_system):
+    import torch
+
+    import cabanapd_b200
     # End to end through the C ABI from pinned host buffers: upload, neighbour
     # build, pre-notch, BCs, init, K steps with energy/damage read back every
     # 10 steps, download of the displacement field.
@@ -313,11 +360,12 @@ def run_gpu(args, world, rank, local, pg):
     hnf = pinned(prob["nofail"].astype(np.int32))
     hv0 = pinned(prob["v0"])
     hu = pinned(np.zeros_like(prob["x"]))
-    del sys_
+    old_system.close()
     torch.cuda.synchronize(device)
     barrier(pg, device)
     t0 = time.perf_counter()
-    e2 = cabanapd_b200.System(dict(prob["params"], device=device))
+    prec = {"fp64": 1, "exact": 0}[args.precision]
+    e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
     e2.set_stream(stream.cuda_stream)
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
@@ -348,39 +396,7 @@ def run_gpu(args, world, rank, local, pg):
     d2h = (hu.nbytes + 16 * reads) / args.steps
     e2e_value = total_bonds * args.steps / (e2e_ms / 1e3)
 
-    if rank != 0:
-        return
-    hbm, hbm_kind = peaks()
-    avg_ms = k_ms / max(k_n, 1)
-    achieved = k_bytes / (avg_ms / 1e3) / 1e9
-    tpb = traffic_per_bond()
-    line = {
-        "metric": "bond-updates/s", "value": value, "unit": "bond-updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "pmb_fracture_notched_plate_impact",
-                   "plate_cells": list(PLATE_CELLS), "particles_per_gpu": n,
-                   "bonds_per_gpu": bonds, "precision": "fp64_exact",
-                   "l2": "inputs larger than L2 (neighbour list %.1f GB)" % (4 * bonds / 1e9),
-                   "particle_steps_per_s": particle_steps},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": hbm_kind,
-                     "kernel": "k_pd_force<PMB, fracture>",
-                     "kernel_ms_avg": avg_ms, "kernel_launches": k_n,
-                     "algorithmic_bytes_per_launch": k_bytes,
-                     "traffic": (tpb * bonds if tpb else None)},
-        "e2e": {"value": e2e_value, "unit": "bond-updates/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "job": "upload+neighbour build+prenotch+init+steps+energy every 10 steps+download u"},
-        "gpu_launches": launches,
-        "clocks": clocks,
-    }
-    if world == 1 and not args.skip_cpu:
-        line["cpu_baseline"] = time_cpu_sample()
-        cb = line["cpu_baseline"]
-        cb.pop("steps", None)
-    print(json.dumps(line), flush=True)
+    return e2e_value, h2d, d2h
 
 
 def main():
@@ -390,9 +406,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact"],
+                    help="fp64: throughput FP64 kernels (default); exact: bit-exact kernels")
+    ap.add_argument("--cells", default=None,
+                    help="plate cells nx,ny,nz (profiling on a smaller plate)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    global PLATE_CELLS
+    if args.cells:
+        PLATE_CELLS = tuple(int(c) for c in args.cells.split(","))
     world, rank, local, pg = (int(os.environ.get("WORLD_SIZE", "1")),
                               int(os.environ.get("RANK", "0")),
                               int(os.environ.get("LOCAL_RANK", "0")), None)

@@ -291,13 +291,34 @@ cpd_status timed_end(cpd_system* s, cudaEvent_t e0)
     return CPD_OK;
 }
 
+bool use_fast(const cpd_system* s)
+{
+    return s->params.precision == CPD_FP64 && fast_supported(s->md);
+}
+
 cpd_status pd_force(cpd_system* s)
 {
     const ParticleView p = view(s);
     cudaEvent_t e0;
     CPD_OK_OR_RETURN(timed_begin(s, e0));
-    CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
+    if (use_fast(s))
+        CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, s->stream));
+    else
+        CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
     return timed_end(s, e0);
+}
+
+// LPS weighted volume (when compute_m) and dilatation.
+cpd_status lps_prepare(cpd_system* s, bool compute_m)
+{
+    const ParticleView p = view(s);
+    if (use_fast(s)) {
+        CPD_LAUNCHED(launch_lps_m_theta_fast(p, pd_view(s), s->md, compute_m, s->stream));
+        return CPD_OK;
+    }
+    if (compute_m) CPD_LAUNCHED(launch_lps_weighted_volume(p, pd_view(s), s->md, s->stream));
+    CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
+    return CPD_OK;
 }
 
 cpd_status contact_force(cpd_system* s, bool reset)
@@ -319,13 +340,8 @@ cpd_status apply_force_bcs(cpd_system* s)
 // CabanaPD_Solver.hpp:462-477 updateForce, then the contact force.
 cpd_status update_force(cpd_system* s)
 {
-    const ParticleView p = view(s);
     if (has_pd(s)) {
-        if (is_lps(s)) {
-            if (s->md.fracture)
-                CPD_LAUNCHED(launch_lps_weighted_volume(p, pd_view(s), s->md, s->stream));
-            CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
-        }
+        if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force(s));
     }
     if (has_contact(s)) {
@@ -382,7 +398,7 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "horizon must be > 0");
     if (P.contact_model == CPD_CONTACT_HERTZ && !(P.contact_radius > 0))
         return set_error(CPD_ERR_INVALID_ARGUMENT, "contact_radius must be > 0");
-    if (P.precision != CPD_FP64_EXACT)
+    if (P.precision != CPD_FP64_EXACT && P.precision != CPD_FP64)
         return set_error(CPD_ERR_UNSUPPORTED, "unknown precision mode");
     if (P.ordering != CPD_ORDER_INPUT && P.ordering != CPD_ORDER_MORTON)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown ordering");
@@ -737,7 +753,7 @@ cpd_status cpd_compute_dilatation(cpd_system* s)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
-    if (is_lps(s)) CPD_LAUNCHED(launch_lps_dilatation(view(s), pd_view(s), s->md, s->stream));
+    if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, false));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     return CPD_OK;
 }
@@ -780,14 +796,10 @@ cpd_status cpd_init(cpd_system* s)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
-    const ParticleView p = view(s);
     if (has_pd(s)) {
-        if (is_lps(s)) {
-            // Once here without fracture (Solver.hpp:235-239), inside
-            // updateForce with fracture (Solver.hpp:466-470): once either way.
-            CPD_LAUNCHED(launch_lps_weighted_volume(p, pd_view(s), s->md, s->stream));
-            CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
-        }
+        // Weighted volume once here without fracture (Solver.hpp:235-239),
+        // inside updateForce with fracture (Solver.hpp:466-470): once either way.
+        if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, true));
         CPD_OK_OR_RETURN(pd_force(s));
     } else if (has_contact(s)) {
         CPD_OK_OR_RETURN(contact_force(s, true));

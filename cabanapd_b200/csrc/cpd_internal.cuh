@@ -105,6 +105,12 @@ int launch_pd_force(const ParticleView& p, const EllView& nl, const Model& md,
                     cudaStream_t st);
 int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
                      double* partials, int nblocks, cudaStream_t st);
+// Throughput-form FP64 kernels (cpd_kernels_fast.cu): PMB and LPS.
+bool fast_supported(const Model& md);
+int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                         cudaStream_t st);
+int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                            bool with_m, cudaStream_t st);
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
                        const Model& md, bool reset, cudaStream_t st);
 int launch_force_bc(const ParticleView& p, const BoundaryCondition& bc,

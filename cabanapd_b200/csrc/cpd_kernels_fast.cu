@@ -1,0 +1,338 @@
+// Plain-FP64 particle kernels, throughput form.
+//
+// Same physics and the same double precision as cpd_kernels_exact.cu, but
+// each bond length costs one reciprocal square root and one correction step
+// instead of an IEEE square root, and the divisions by xi and r become
+// multiplications by the reciprocal square roots:
+//   r2, xi2 summed in the reference's order without FMA (as the reference)
+//   r  = sqrt(r2)  from y = rsqrt(r2): g = r2 y, e = r2 - g g (exact FMA
+//        residual), r = g + e y / 2 -- the Newton-Raphson / Markstein
+//        correction of the square root, which returns the correctly rounded
+//        root except in rare hard cases (then within one ulp)
+//   s  = (r - xi) * rsqrt(xi2)     (r - xi is exact, as in the reference)
+//   f += (c s vol_j rsqrt(r2)) * r_vec
+// Because r and xi carry the reference's rounding, s differs from the
+// reference's (r - xi) / xi by a few ulps of s itself -- no 1/s growth -- and
+// forces agree with the bit-exact path to ~1e-15 relative.
+//
+// Bond breaking stays exact: the reference's test is r * r >=
+// (bond_break_coeff * xi) * xi (CabanaPD_ForceModels.hpp:123-128). Inside a
+// relative guard band of 1e-12 the test is re-evaluated with correctly
+// rounded intrinsics, so broken-bond sets are identical.
+#include <cuda_runtime.h>
+
+#include "cpd_internal.cuh"
+
+namespace cpd {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr double kGuard = 1e-12;
+
+inline int blocks_for(int64_t rows) { return (int)((rows + kBlock - 1) / kBlock); }
+
+struct FastModel {
+    double c, theta_coeff, s_coeff, bond_break_coeff;
+};
+
+// The reference's break test for bond vector xi = (xx, xy, xz) and deformed
+// vector r = (rx, ry, rz), with every operation rounded separately.
+__device__ __noinline__ bool critical_exact(double xx, double xy, double xz, double rx,
+                                            double ry, double rz, double bbc)
+{
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)),
+                                __dmul_rn(rz, rz));
+    const double x2 = __dadd_rn(__dadd_rn(__dmul_rn(xx, xx), __dmul_rn(xy, xy)),
+                                __dmul_rn(xz, xz));
+    const double r = __dsqrt_rn(r2);
+    const double xi = __dsqrt_rn(x2);
+    return __dmul_rn(r, r) >= __dmul_rn(__dmul_rn(bbc, xi), xi);
+}
+
+// Squared length summed as the reference sums it: (a*a + b*b) + c*c, each
+// product and sum rounded (no FMA).
+__device__ __forceinline__ double norm2_ref(double a, double b, double c)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+}
+
+// sqrt(a) from y ~ 1/sqrt(a): one Newton-Raphson step on g = a y with the
+// residual a - g^2 formed exactly by FMA (Markstein's correction).
+__device__ __forceinline__ double sqrt_from_rsqrt(double a, double y)
+{
+    const double g = a * y;
+    const double e = fma(-g, g, a);
+    return fma(e, 0.5 * y, g);
+}
+
+struct Bond {
+    double xx, xy, xz, rx, ry, rz;
+    double r, xi, rinv, xiinv, s;
+};
+
+__device__ __forceinline__ void bond_fast(const double* __restrict__ X,
+                                          const double* __restrict__ U, int64_t np,
+                                          int64_t j, double xi0, double xi1, double xi2,
+                                          double ui0, double ui1, double ui2, Bond& b)
+{
+    b.xx = __ldg(X + j) - xi0;
+    b.xy = __ldg(X + np + j) - xi1;
+    b.xz = __ldg(X + 2 * np + j) - xi2;
+    b.rx = b.xx + (__ldg(U + j) - ui0);
+    b.ry = b.xy + (__ldg(U + np + j) - ui1);
+    b.rz = b.xz + (__ldg(U + 2 * np + j) - ui2);
+    const double r2 = norm2_ref(b.rx, b.ry, b.rz);
+    const double x2 = norm2_ref(b.xx, b.xy, b.xz);
+    b.rinv = rsqrt(r2);
+    b.xiinv = rsqrt(x2);
+    b.r = sqrt_from_rsqrt(r2, b.rinv);
+    b.xi = sqrt_from_rsqrt(x2, b.xiinv);
+    b.s = (b.r - b.xi) * b.xiinv;
+}
+
+__device__ __forceinline__ bool critical_fast(const Bond& b, double bbc)
+{
+    const double lhs = __dmul_rn(b.r, b.r);
+    const double rhs = __dmul_rn(__dmul_rn(bbc, b.xi), b.xi);
+    if (fabs(lhs - rhs) <= kGuard * rhs)
+        return critical_exact(b.xx, b.xy, b.xz, b.rx, b.ry, b.rz, bbc);
+    return lhs >= rhs;
+}
+
+// PMB force (force/CabanaPD_PMB.hpp:89-125, :222-287).
+template <bool FRACTURE>
+__global__ void __launch_bounds__(kBlock)
+    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double* __restrict__ X = p.x;
+    const double* __restrict__ U = p.u;
+    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
+    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
+    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
+    const int cnt = nl.count[i];
+    const int32_t* __restrict__ idx = nl.idx + i;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    uint32_t word = 0;
+    bool dirty = false;
+    for (int k = 0; k < cnt; ++k) {
+        if (FRACTURE && (k & 31) == 0) {
+            if (dirty) nl.mu[(int64_t)((k >> 5) - 1) * np + i] = word;
+            dirty = false;
+            word = nl.mu[(int64_t)(k >> 5) * np + i];
+        }
+        const int64_t j = __ldg(idx + (int64_t)k * np);
+        Bond b;
+        bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+        bool intact = true;
+        if (FRACTURE) {
+            const uint32_t bit = 1u << (k & 31);
+            const bool nofail_j = __ldg(p.nofail + j) != 0;
+            if (!nofail_i && !nofail_j && critical_fast(b, md.bond_break_coeff)) {
+                if (word & bit) {
+                    word &= ~bit;
+                    dirty = true;
+                }
+                intact = false;
+            } else {
+                intact = (word & bit) != 0;
+            }
+        }
+        if (intact) {
+            const double kf = md.c * b.s * __ldg(p.vol + j) * b.rinv;
+            fx = fma(kf, b.rx, fx);
+            fy = fma(kf, b.ry, fy);
+            fz = fma(kf, b.rz, fz);
+        }
+    }
+    if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
+    p.f[i] = fx;
+    p.f[np + i] = fy;
+    p.f[2 * np + i] = fz;
+}
+
+// LPS weighted volume and dilatation fused (force/CabanaPD_LPS.hpp:89-141,
+// :287-378): m_i first, then theta_i with the just-computed m_i, in one
+// pass over the row (two loops; the second re-reads the row from L1/L2).
+// Stores a = theta_coeff theta / m and b = s_coeff / m for the force loop.
+template <int INFL, bool FRACTURE, bool WITH_M>
+__global__ void __launch_bounds__(kBlock)
+    k_lps_m_theta_fast(ParticleView p, EllView nl, FastModel md)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double* __restrict__ X = p.x;
+    const double* __restrict__ U = p.u;
+    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
+    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
+    const int cnt = nl.count[i];
+    const int32_t* __restrict__ idx = nl.idx + i;
+    double mi;
+    if (WITH_M) {
+        mi = 0.0;
+        uint32_t word = 0;
+        for (int k = 0; k < cnt; ++k) {
+            if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+            if (FRACTURE && !((word >> (k & 31)) & 1u)) continue;
+            const int64_t j = __ldg(idx + (int64_t)k * np);
+            const double xx = __ldg(X + j) - xi0;
+            const double xy = __ldg(X + np + j) - xi1;
+            const double xz = __ldg(X + 2 * np + j) - xi2v;
+            const double x2 = norm2_ref(xx, xy, xz);
+            const double y = rsqrt(x2);
+            const double xi = sqrt_from_rsqrt(x2, y);
+            // omega xi^2 (force_models/CabanaPD_LPS.hpp:100-106)
+            const double w = INFL == 1 ? xi : xi * xi;
+            mi = fma(w, __ldg(p.vol + j), mi);
+        }
+        p.m[i] = mi;
+    } else {
+        mi = p.m[i];
+    }
+    double th = 0.0;
+    if (!FRACTURE || mi > 0) {
+        uint32_t word = 0;
+        for (int k = 0; k < cnt; ++k) {
+            if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+            if (FRACTURE && !((word >> (k & 31)) & 1u)) continue;
+            const int64_t j = __ldg(idx + (int64_t)k * np);
+            Bond b;
+            bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+            // omega s xi^2 vol_j (force_models/CabanaPD_LPS.hpp:108-116)
+            const double w = INFL == 1 ? b.s * b.xi : b.s * b.xi * b.xi;
+            th = fma(w, __ldg(p.vol + j), th);
+        }
+        th = 3.0 * th / mi;
+    }
+    p.theta[i] = th;
+    p.lps_a[i] = md.theta_coeff * th / mi;
+    p.lps_b[i] = md.s_coeff / mi;
+}
+
+// LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447).
+template <int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock)
+    k_lps_force_fast(ParticleView p, EllView nl, FastModel md)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double* __restrict__ X = p.x;
+    const double* __restrict__ U = p.u;
+    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
+    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
+    const double a_i = p.lps_a[i], b_i = p.lps_b[i];
+    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
+    const int cnt = nl.count[i];
+    const int32_t* __restrict__ idx = nl.idx + i;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    uint32_t word = 0;
+    bool dirty = false;
+    for (int k = 0; k < cnt; ++k) {
+        if (FRACTURE && (k & 31) == 0) {
+            if (dirty) nl.mu[(int64_t)((k >> 5) - 1) * np + i] = word;
+            dirty = false;
+            word = nl.mu[(int64_t)(k >> 5) * np + i];
+        }
+        const int64_t j = __ldg(idx + (int64_t)k * np);
+        Bond b;
+        bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+        bool intact = true;
+        if (FRACTURE) {
+            // nofail(i) tested twice by the reference (force/CabanaPD_LPS.hpp:417-418).
+            const uint32_t bit = 1u << (k & 31);
+            if (!nofail_i && critical_fast(b, md.bond_break_coeff)) {
+                if (word & bit) {
+                    word &= ~bit;
+                    dirty = true;
+                }
+                intact = false;
+            } else {
+                intact = (word & bit) != 0;
+            }
+        }
+        if (intact) {
+            const double a_j = __ldg(p.lps_a + j), b_j = __ldg(p.lps_b + j);
+            // (force_models/CabanaPD_LPS.hpp:118-134) omega xi vol_j / r
+            const double oxi = INFL == 1 ? 1.0 : b.xi;
+            const double kf = (a_i + a_j + b.s * (b_i + b_j)) * oxi * __ldg(p.vol + j) * b.rinv;
+            fx = fma(kf, b.rx, fx);
+            fy = fma(kf, b.ry, fy);
+            fz = fma(kf, b.rz, fz);
+        }
+    }
+    if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
+    p.f[i] = fx;
+    p.f[np + i] = fy;
+    p.f[2 * np + i] = fz;
+}
+
+FastModel to_fast(const Model& m)
+{
+    return FastModel{m.c, m.theta_coeff, m.s_coeff, m.bond_break_coeff};
+}
+
+}  // namespace
+
+bool fast_supported(const Model& md)
+{
+    return md.pd == CPD_PD_PMB || md.pd == CPD_PD_LPS;
+}
+
+int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                         cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    const int g = blocks_for(rows);
+    const FastModel fm = to_fast(md);
+    if (md.pd == CPD_PD_PMB) {
+        if (md.fracture)
+            k_pmb_force_fast<true><<<g, kBlock, 0, st>>>(p, nl, fm);
+        else
+            k_pmb_force_fast<false><<<g, kBlock, 0, st>>>(p, nl, fm);
+    } else {
+        if (md.influence == 1) {
+            if (md.fracture)
+                k_lps_force_fast<1, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+            else
+                k_lps_force_fast<1, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+        } else {
+            if (md.fracture)
+                k_lps_force_fast<0, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+            else
+                k_lps_force_fast<0, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+        }
+    }
+    return 1;
+}
+
+int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                            bool with_m, cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    const int g = blocks_for(rows);
+    const FastModel fm = to_fast(md);
+#define CPD_MT(I, F, W) k_lps_m_theta_fast<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm)
+    if (md.influence == 1) {
+        if (md.fracture) {
+            if (with_m) CPD_MT(1, true, true); else CPD_MT(1, true, false);
+        } else {
+            if (with_m) CPD_MT(1, false, true); else CPD_MT(1, false, false);
+        }
+    } else {
+        if (md.fracture) {
+            if (with_m) CPD_MT(0, true, true); else CPD_MT(0, true, false);
+        } else {
+            if (with_m) CPD_MT(0, false, true); else CPD_MT(0, false, false);
+        }
+    }
+#undef CPD_MT
+    return 1;
+}
+
+}  // namespace cpd

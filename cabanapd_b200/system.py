@@ -16,6 +16,7 @@ FIELDS = {"x": 0, "u": 1, "v": 2, "f": 3, "vol": 4, "rho": 5, "m": 6,
           "theta": 7, "W": 8, "phi": 9, "radius": 10}
 VECTOR_FIELDS = {"x", "u", "v", "f"}
 FP64_EXACT = 0
+FP64 = 1
 ORDER_INPUT, ORDER_MORTON = 0, 1
 
 _lib = None

@@ -79,8 +79,14 @@ enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1 };
 
 /* Kernel arithmetic. EXACT evaluates every per-bond expression with IEEE
  * double operations in the reference's operand order (no FMA contraction),
- * so per-particle results equal a scalar CPU evaluation bit for bit. */
-enum { CPD_FP64_EXACT = 0 };
+ * so per-particle results equal a scalar CPU evaluation bit for bit.
+ * FP64 is the throughput form of the same double-precision model: one
+ * reciprocal square root per bond length instead of two square roots and
+ * four divisions, FMA allowed; forces agree with EXACT to ~1e-13 relative
+ * (norm-wise) and the broken-bond decision is re-evaluated exactly inside a
+ * 1e-12 guard band, so broken-bond sets are identical. PMB and LPS use it;
+ * the linearized models and Hertz contact always run EXACT. */
+enum { CPD_FP64_EXACT = 0, CPD_FP64 = 1 };
 
 /* Internal particle order: INPUT keeps the caller's order; MORTON sorts by
  * the Morton code of the particle's cell (results are returned in the
@@ -130,7 +136,7 @@ typedef struct cpd_params {
                                     radius_extend (Neighbor.hpp:118-119);
                                     k > 0 = rebuild every k steps */
     int32_t per_particle_radius; /* 1: Hertz with per-particle radii */
-    int32_t precision;           /* CPD_FP64_EXACT */
+    int32_t precision;           /* CPD_FP64_EXACT or CPD_FP64 */
     int32_t ordering;            /* CPD_ORDER_* */
     int32_t device;              /* CUDA device ordinal */
 } cpd_params;

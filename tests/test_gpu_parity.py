@@ -206,3 +206,82 @@ def test_errors_are_reported(cuda):
         s.prenotch([[1, 0, 0]], [[0, 1, 0]], [[0, 0, 0]])  # no fracture model
     with pytest.raises(cuda.CpdError):
         s.add_bc(P.BC_FORCE_VALUE, [10 ** 6], [0.0])
+
+
+# ---------------------------------------------------------------------------
+# Throughput-form FP64 path (precision = CPD_FP64): the same double model
+# with rsqrt-based bond lengths and FMA. Tolerance: norm-wise relative
+# difference <= 1e-12 for every field (the reference's own rounding of
+# s = (r - xi)/xi is ~1e-16/s relative per bond); broken-bond sets identical.
+FAST = 1
+
+
+def _nrel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def _pair_fast(cuda, oracle, prob, ordering=0):
+    g = cuda.System(dict(prob["params"], precision=FAST, ordering=ordering))
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(g, prob)
+    P.setup(o, prob)
+    return g, o
+
+
+@pytest.mark.parametrize("case,kind,coeff", [
+    ("pmb", "linear", 0.1), ("pmb", "quadratic", 0.01),
+    ("pmb_damage", "quadratic", 0.01),
+    ("lps", "linear", 0.1), ("lps", "quadratic", 0.01),
+    ("lps_damage", "linear", 0.1),
+])
+def test_fast_force_cases(cuda, oracle, case, kind, coeff):
+    res_g, _ = force_checks.run_case(lambda p: cuda.System(dict(p, precision=FAST)),
+                                     case, kind, coeff)
+    force_checks.check_case(res_g, case, kind, coeff, max_checked=40)
+    res_o, _ = force_checks.run_case(lambda p: oracle.OracleSystem(p), case, kind, coeff)
+    for fld in ("f", "theta"):
+        assert _nrel(res_g[fld], res_o[fld]) <= 1e-12, fld
+
+
+def test_fast_elastic_wave(cuda, oracle):
+    prob = P.elastic_wave_pmb(n=41, steps=100)
+    g, o = _pair_fast(cuda, oracle, prob)
+    done = 0
+    for target in (1, 10, 100):
+        g.run(target - done)
+        o.run(target - done)
+        done = target
+        for fld in ("u", "v", "f"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-12, (target, fld)
+        wg, _ = g.compute_energy()
+        wo, _ = o.compute_energy()
+        assert _rel(wg, wo) <= 1e-12
+
+
+@pytest.mark.parametrize("ordering", [0, 1])
+def test_fast_plate_impact(cuda, oracle, ordering):
+    prob = P.plate_impact(num_cells=(96, 48, 6), steps=240, v0=60.0)
+    g, o = _pair_fast(cuda, oracle, prob, ordering=ordering)
+    for _ in range(3):
+        g.run(80)
+        o.run(80)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        for fld in ("u", "v", "f"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-12, fld
+        wg, dg = g.compute_energy()
+        wo, do = o.compute_energy()
+        assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+
+
+def test_fast_lps_random_notches(cuda, oracle):
+    prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
+    prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
+    g, o = _pair_fast(cuda, oracle, prob)
+    for _ in range(3):
+        g.run(20)
+        o.run(20)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        for fld in ("u", "v", "f", "m", "theta"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-12, fld
+    assert (o.neighbors()[2] == 0).sum() > 0
