@@ -934,3 +934,77 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
 int64_t cpd_kernel_launches(const cpd_system* s) { return s ? s->launches : 0; }
 
 }  // extern "C"
+
+// ===========================================================================
+// Energy and damage without any device allocation.
+//
+// cpd_compute_energy lazily cudaMallocs its reduction scratch on first use.
+// Some callers cannot allow that: a job server that reserves each
+// simulation's device memory when it admits the job and must never allocate
+// while jobs are running (an allocation mid-run can fail under the budget or
+// fragment the pool), or a host framework that owns all device memory
+// through its own allocator and forbids raw cudaMalloc. For them this entry
+// point keeps its scratch -- one pair of partial sums per 256-row block -- in
+// the file-scope array below, which exists on every GPU that loads this
+// library until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 16384;  // 256-row blocks: 4,194,304 rows
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks];
+
+constexpr int kMaxDevices = 64;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+// Host code may not use g_noalloc_scratch's name as a device address; the
+// address is fetched once per device, with that device current.
+cpd_status noalloc_scratch(int device, double** out)
+{
+    if (device < 0 || device >= kMaxDevices)
+        return set_error(CPD_ERR_UNSUPPORTED, "device ordinal above the no-allocation table");
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return set_error(CPD_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation "
+                                                       "scratch): ") +
+                                               cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return CPD_OK;
+}
+
+}  // namespace
+
+extern "C" cpd_status cpd_compute_energy_noalloc(cpd_system* s, double* W_out,
+                                                 double* phi_out, double* totals_out)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!W_out || !phi_out || !totals_out)
+        return set_error(CPD_ERR_INVALID_ARGUMENT,
+                         "cpd_compute_energy_noalloc: W, phi and totals must be device pointers");
+    const int64_t rows = s->n - s->frozen;
+    const int nb = energy_blocks(rows);
+    if (nb > kNoAllocMaxBlocks)
+        return set_error(CPD_ERR_INVALID_ARGUMENT,
+                         "cpd_compute_energy_noalloc: " + std::to_string(rows) +
+                             " particle rows exceed the no-allocation scratch limit of " +
+                             std::to_string((int64_t)kNoAllocMaxBlocks * 256) + " rows");
+    CPD_CUDA(cudaSetDevice(s->device));
+    double* scratch = nullptr;
+    CPD_OK_OR_RETURN(noalloc_scratch(s->device, &scratch));
+    if (!has_pd(s)) {
+        // A DEM-only system has no strain energy or damage (cpd_compute_energy
+        // returns zeros as well).
+        CPD_CUDA(cudaMemsetAsync(totals_out, 0, 2 * sizeof(double), s->stream));
+        return CPD_OK;
+    }
+    ParticleView p = view(s);
+    p.W = W_out;
+    p.phi = phi_out;
+    // Every partial slot the sum reads is written by this launch first, so
+    // nothing left in the scratch by an earlier call reaches the result.
+    CPD_LAUNCHED(launch_pd_energy(p, pd_view(s), s->md, scratch, nb, s->stream));
+    CPD_LAUNCHED(launch_sum_partials(scratch, nb, 2, totals_out, s->stream));
+    return CPD_OK;
+}

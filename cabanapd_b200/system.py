@@ -76,6 +76,7 @@ SIGNATURES = {
     "cpd_compute_dilatation": (_I32, [_P]),
     "cpd_compute_force": (_I32, [_P]),
     "cpd_compute_energy": (_I32, [_P, _DP, _DP]),
+    "cpd_compute_energy_noalloc": (_I32, [_P, _P, _P, _P]),
     "cpd_init": (_I32, [_P]),
     "cpd_step": (_I32, [_P, _I32]),
     "cpd_synchronize": (_I32, [_P]),

@@ -197,6 +197,22 @@ cpd_status cpd_compute_force(cpd_system* sys);
 /* W_i, damage phi_i and the totals sum(W_i vol_i), sum(phi_i). */
 cpd_status cpd_compute_energy(cpd_system* sys, double* total_strain_energy,
                               double* total_damage);
+/* No counterpart in the reference. The same energy and damage computation
+ * for callers that may not allocate device memory after set-up (a job
+ * server that reserved each job's memory at admission, or a framework that
+ * owns all device memory through its own pool). W_out and phi_out are caller
+ * device buffers of at least the system's stride (cpd_device_field) doubles,
+ * filled in the internal particle order; totals_out is a caller device
+ * buffer of 2 doubles (sum W_i vol_i, sum phi_i). Queued on the system's
+ * stream without waiting. Scratch is a fixed 256 KB array inside the library
+ * (held on every GPU that loads it until exit), which limits a call to
+ * 4,194,304 particle rows; larger systems are rejected with
+ * CPD_ERR_INVALID_ARGUMENT. The first call on a device looks up that array's
+ * device address, so make it before any stream capture. All calls share the
+ * one array: calls whose work overlaps on the GPU (other streams, other
+ * systems on the same device) race; calls queued on one stream do not. */
+cpd_status cpd_compute_energy_noalloc(cpd_system* sys, double* W_out, double* phi_out,
+                                      double* totals_out);
 
 cpd_status cpd_init(cpd_system* sys);
 /* num_steps velocity-Verlet steps. Asynchronous: returns once the work is
