@@ -21,6 +21,8 @@
 // rounded intrinsics, so broken-bond sets are identical.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "cpd_internal.cuh"
 
 namespace cpd {
@@ -99,21 +101,71 @@ __device__ __forceinline__ bool critical_fast(const Bond& b, double bbc)
     return lhs >= rhs;
 }
 
-// PMB force (force/CabanaPD_PMB.hpp:89-125, :222-287).
+// Bond geometry from already-gathered neighbour data.
+__device__ __forceinline__ void bond_from(double xj0, double xj1, double xj2, double uj0,
+                                          double uj1, double uj2, double xi0, double xi1,
+                                          double xi2, double ui0, double ui1, double ui2,
+                                          Bond& b)
+{
+    b.xx = xj0 - xi0;
+    b.xy = xj1 - xi1;
+    b.xz = xj2 - xi2;
+    b.rx = b.xx + (uj0 - ui0);
+    b.ry = b.xy + (uj1 - ui1);
+    b.rz = b.xz + (uj2 - ui2);
+    const double r2 = norm2_ref(b.rx, b.ry, b.rz);
+    const double x2 = norm2_ref(b.xx, b.xy, b.xz);
+    b.rinv = rsqrt(r2);
+    b.xiinv = rsqrt(x2);
+    b.r = sqrt_from_rsqrt(r2, b.rinv);
+    b.xi = sqrt_from_rsqrt(x2, b.xiinv);
+    b.s = (b.r - b.xi) * b.xiinv;
+}
+
+// Neighbour data a bond needs, gathered ahead of its arithmetic.
+struct Gather {
+    double x0, x1, x2, u0, u1, u2, vol;
+    bool nofail;
+};
+
 template <bool FRACTURE>
+__device__ __forceinline__ void gather(const ParticleView& p, int64_t np, int64_t j, Gather& g)
+{
+    g.x0 = __ldg(p.x + j);
+    g.x1 = __ldg(p.x + np + j);
+    g.x2 = __ldg(p.x + 2 * np + j);
+    g.u0 = __ldg(p.u + j);
+    g.u1 = __ldg(p.u + np + j);
+    g.u2 = __ldg(p.u + 2 * np + j);
+    g.vol = __ldg(p.vol + j);
+    g.nofail = FRACTURE ? (__ldg(p.nofail + j) != 0) : false;
+}
+
+// PMB force (force/CabanaPD_PMB.hpp:89-125, :222-287).
+//
+// Latency hiding: each bond's work hangs off its neighbour index, which
+// streams from HBM. The indices of the next PF bonds are loaded PF
+// iterations ahead (a shift register in registers), and with GP the
+// neighbour's position / displacement / volume are gathered one bond ahead,
+// so a warp keeps several independent loads in flight while it computes.
+template <bool FRACTURE, int PF, bool GP>
 __global__ void __launch_bounds__(kBlock)
     k_pmb_force_fast(ParticleView p, EllView nl, FastModel md)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const int64_t np = p.npad;
-    const double* __restrict__ X = p.x;
-    const double* __restrict__ U = p.u;
-    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
-    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
     const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
     const int cnt = nl.count[i];
     const int32_t* __restrict__ idx = nl.idx + i;
+    constexpr int Q = PF > 0 ? PF : 1;
+    int32_t q[Q];
+#pragma unroll
+    for (int a = 0; a < Q; ++a) q[a] = (PF > 0 && a < cnt) ? __ldg(idx + (int64_t)a * np) : 0;
+    Gather g_next;
+    if (GP && cnt > 0) gather<FRACTURE>(p, np, PF > 0 ? q[0] : __ldg(idx), g_next);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     uint32_t word = 0;
     bool dirty = false;
@@ -123,14 +175,30 @@ __global__ void __launch_bounds__(kBlock)
             dirty = false;
             word = nl.mu[(int64_t)(k >> 5) * np + i];
         }
-        const int64_t j = __ldg(idx + (int64_t)k * np);
+        int64_t j;
+        if (PF > 0) {
+            j = q[0];
+#pragma unroll
+            for (int a = 0; a + 1 < Q; ++a) q[a] = q[a + 1];
+            q[Q - 1] = (k + Q < cnt) ? __ldg(idx + (int64_t)(k + Q) * np) : 0;
+        } else {
+            j = __ldg(idx + (int64_t)k * np);
+        }
+        Gather g;
+        if (GP) {
+            g = g_next;
+            if (k + 1 < cnt)
+                gather<FRACTURE>(p, np, PF > 0 ? q[0] : __ldg(idx + (int64_t)(k + 1) * np),
+                                 g_next);
+        } else {
+            gather<FRACTURE>(p, np, j, g);
+        }
         Bond b;
-        bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+        bond_from(g.x0, g.x1, g.x2, g.u0, g.u1, g.u2, xi0, xi1, xi2v, ui0, ui1, ui2, b);
         bool intact = true;
         if (FRACTURE) {
             const uint32_t bit = 1u << (k & 31);
-            const bool nofail_j = __ldg(p.nofail + j) != 0;
-            if (!nofail_i && !nofail_j && critical_fast(b, md.bond_break_coeff)) {
+            if (!nofail_i && !g.nofail && critical_fast(b, md.bond_break_coeff)) {
                 if (word & bit) {
                     word &= ~bit;
                     dirty = true;
@@ -141,7 +209,7 @@ __global__ void __launch_bounds__(kBlock)
             }
         }
         if (intact) {
-            const double kf = md.c * b.s * __ldg(p.vol + j) * b.rinv;
+            const double kf = md.c * b.s * g.vol * b.rinv;
             fx = fma(kf, b.rx, fx);
             fy = fma(kf, b.ry, fy);
             fz = fma(kf, b.rz, fz);
@@ -270,6 +338,20 @@ __global__ void __launch_bounds__(kBlock)
     p.f[2 * np + i] = fz;
 }
 
+// Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-4):
+// 0 no prefetch, 1 indices 2 bonds ahead, 2 indices 4 ahead, 3 / 4 the same
+// plus neighbour gathers one bond ahead. Measured on the full plate (B200):
+// 11.3 / 8.2 / 9.0 / 11.9 / 11.8 ms per launch, so 1 is the default.
+int fast_variant()
+{
+    static int v = [] {
+        const char* e = getenv("CPD_FORCE_VARIANT");
+        int x = e ? atoi(e) : 1;
+        return (x < 0 || x > 4) ? 1 : x;
+    }();
+    return v;
+}
+
 FastModel to_fast(const Model& m)
 {
     return FastModel{m.c, m.theta_coeff, m.s_coeff, m.bond_break_coeff};
@@ -290,10 +372,19 @@ int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& 
     const int g = blocks_for(rows);
     const FastModel fm = to_fast(md);
     if (md.pd == CPD_PD_PMB) {
-        if (md.fracture)
-            k_pmb_force_fast<true><<<g, kBlock, 0, st>>>(p, nl, fm);
-        else
-            k_pmb_force_fast<false><<<g, kBlock, 0, st>>>(p, nl, fm);
+        // Variant: index prefetch distance and neighbour-gather pipelining.
+        switch (md.fracture ? fast_variant() : 100 + fast_variant()) {
+        case 0: k_pmb_force_fast<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 1: k_pmb_force_fast<true, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 2: k_pmb_force_fast<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 3: k_pmb_force_fast<true, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 4: k_pmb_force_fast<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 100: k_pmb_force_fast<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 101: k_pmb_force_fast<false, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 102: k_pmb_force_fast<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 103: k_pmb_force_fast<false, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        }
     } else {
         if (md.influence == 1) {
             if (md.fracture)
