@@ -266,7 +266,7 @@ def run_gpu(args, world, rank, local, pg):
     prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
     stream = torch.cuda.Stream(device=device)
 
-    prec = {"fp64": 1, "exact": 0}[args.precision]
+    prec = {"fp64": 1, "exact": 0, "mixed": 2}[args.precision]
     sys_ = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
     sys_.set_stream(stream.cuda_stream)
     P.setup(sys_, prob)
@@ -323,8 +323,9 @@ def run_gpu(args, world, rank, local, pg):
                    "particle_steps_per_s": particle_steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": hbm_kind,
-                     "kernel": ("k_pmb_force_fast<fracture>" if args.precision == "fp64"
-                                else "k_pd_force<PMB, fracture> (exact)"),
+                     "kernel": {"fp64": "k_pmb_force_fast<fracture>",
+                                "mixed": "k_pmb_force_mixed<fracture>",
+                                "exact": "k_pd_force<PMB, fracture> (exact)"}[args.precision],
                      "kernel_ms_avg": avg_ms, "kernel_launches": k_n,
                      "algorithmic_bytes_per_launch": k_bytes,
                      "traffic": (tpb * bonds if tpb else None)},
@@ -364,7 +365,7 @@ def run_e2e(args, prob, device, stream, pg, total_bonds, old_system):
     torch.cuda.synchronize(device)
     barrier(pg, device)
     t0 = time.perf_counter()
-    prec = {"fp64": 1, "exact": 0}[args.precision]
+    prec = {"fp64": 1, "exact": 0, "mixed": 2}[args.precision]
     e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
     e2.set_stream(stream.cuda_stream)
     s0 = torch.cuda.Event(enable_timing=True)
@@ -407,8 +408,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact"],
-                    help="fp64: throughput FP64 kernels (default); exact: bit-exact kernels")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"],
+                    help="fp64: throughput FP64 kernels (default); exact: bit-exact; "
+                         "mixed: FP32 bonds / FP64 integration")
     ap.add_argument("--cells", default=None,
                     help="plate cells nx,ny,nz (profiling on a smaller plate)")
     args = ap.parse_args()

@@ -70,6 +70,7 @@ struct cpd_system {
     double* red_out = nullptr;   // small result slots
     double* h_red = nullptr;     // pinned host mirror of red_out
     NeighborList pd, contact;
+    MixedState mixed;  // CPD_MIXED: FP32 split copies and bond stencil codes
     std::vector<BoundaryCondition> bcs;
     bool neighbors_built = false;
     bool initialized = false;
@@ -147,6 +148,7 @@ void free_particles(cpd_system* s)
     s->bcs.clear();
     free_neighbor_list(s->pd);
     free_neighbor_list(s->contact);
+    free_mixed(s->mixed);
     s->n = s->npad = s->frozen = 0;
     s->red_cap = 0;
     s->neighbors_built = false;
@@ -291,9 +293,19 @@ cpd_status timed_end(cpd_system* s, cudaEvent_t e0)
     return CPD_OK;
 }
 
+bool use_mixed(const cpd_system* s)
+{
+    return s->params.precision == CPD_MIXED && s->md.pd == CPD_PD_PMB &&
+           s->md.contact == CPD_CONTACT_NONE;
+}
+
+// The throughput FP64 kernels serve CPD_FP64, and CPD_MIXED for the models
+// the mixed kernel does not cover (LPS).
 bool use_fast(const cpd_system* s)
 {
-    return s->params.precision == CPD_FP64 && fast_supported(s->md);
+    return (s->params.precision == CPD_FP64 ||
+            (s->params.precision == CPD_MIXED && !use_mixed(s))) &&
+           fast_supported(s->md);
 }
 
 cpd_status pd_force(cpd_system* s)
@@ -301,7 +313,9 @@ cpd_status pd_force(cpd_system* s)
     const ParticleView p = view(s);
     cudaEvent_t e0;
     CPD_OK_OR_RETURN(timed_begin(s, e0));
-    if (use_fast(s))
+    if (use_mixed(s))
+        CPD_LAUNCHED(launch_pd_force_mixed(p, pd_view(s), s->md, s->mixed, s->stream));
+    else if (use_fast(s))
         CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, s->stream));
     else
         CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
@@ -357,7 +371,10 @@ cpd_status vv_initial(cpd_system* s)
     const bool track = has_contact(s);
     const int nb = vv_blocks(s->n - s->frozen);
     if (track) CPD_OK_OR_RETURN(ensure_reduction(s, nb));
-    CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->stream));
+    if (use_mixed(s))
+        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->params.dt, s->mixed, s->stream));
+    else
+        CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->stream));
     if (track && s->n > s->frozen)
         CPD_LAUNCHED(launch_max_partials(s->red, nb, s->red_out, s->stream));
     s->steps_since_rebuild++;
@@ -398,7 +415,7 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "horizon must be > 0");
     if (P.contact_model == CPD_CONTACT_HERTZ && !(P.contact_radius > 0))
         return set_error(CPD_ERR_INVALID_ARGUMENT, "contact_radius must be > 0");
-    if (P.precision != CPD_FP64_EXACT && P.precision != CPD_FP64)
+    if (P.precision != CPD_FP64_EXACT && P.precision != CPD_FP64 && P.precision != CPD_MIXED)
         return set_error(CPD_ERR_UNSUPPORTED, "unknown precision mode");
     if (P.ordering != CPD_ORDER_INPUT && P.ordering != CPD_ORDER_MORTON)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown ordering");
@@ -593,6 +610,7 @@ cpd_status cpd_set_state(cpd_system* s, const double* u, const double* v)
     CPD_CUDA(cudaSetDevice(s->device));
     if (u) CPD_OK_OR_RETURN(upload_vector(s, u, s->u));
     if (v) CPD_OK_OR_RETURN(upload_vector(s, v, s->v));
+    if (use_mixed(s) && s->mixed.uh) s->launches += launch_split_u(view(s), s->mixed, s->stream);
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     return CPD_OK;
 }
@@ -609,6 +627,11 @@ cpd_status cpd_build_neighbors(cpd_system* s)
                                     s->pd, s->stream, err);
         if (l < 0) return set_error(CPD_ERR_CUDA, "neighbour build: " + err);
         s->launches += l;
+        if (use_mixed(s)) {
+            l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, s->mixed, s->stream, err);
+            if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
+            s->launches += l;
+        }
     }
     if (has_contact(s)) {
         // CabanaPD_Neighbor.hpp:60-63: current positions, cutoff + 1e-14.
@@ -758,10 +781,19 @@ cpd_status cpd_compute_dilatation(cpd_system* s)
     return CPD_OK;
 }
 
+// The mixed kernel reads the FP32 split of u; refresh it where u may have
+// changed outside the integrator (set_state, init, kernel-level calls).
+cpd_status refresh_mixed_u(cpd_system* s)
+{
+    if (use_mixed(s) && s->mixed.uh) CPD_LAUNCHED(launch_split_u(view(s), s->mixed, s->stream));
+    return CPD_OK;
+}
+
 cpd_status cpd_compute_force(cpd_system* s)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
+    CPD_OK_OR_RETURN(refresh_mixed_u(s));
     if (has_pd(s)) CPD_OK_OR_RETURN(pd_force(s));
     if (has_contact(s)) CPD_OK_OR_RETURN(contact_force(s, !has_pd(s)));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
@@ -796,6 +828,7 @@ cpd_status cpd_init(cpd_system* s)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
+    CPD_OK_OR_RETURN(refresh_mixed_u(s));
     if (has_pd(s)) {
         // Weighted volume once here without fracture (Solver.hpp:235-239),
         // inside updateForce with fracture (Solver.hpp:466-470): once either way.
@@ -918,6 +951,13 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
         // counted once (ideal reuse).
         const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
         const double rows = (double)(s->n - s->frozen);
+        if (use_mixed(s)) {
+            // Mixed kernel: per row the FP32 hi/lo displacement with volume and
+            // no-fail (32 B), count (4 B), force write (24 B); per bond the
+            // 1-byte stencil code and the bond bit read + write.
+            *bytes_per_launch = 60.0 * rows + (1.0 + (s->md.fracture ? 0.25 : 0.0)) * (double)nl.total;
+            return CPD_OK;
+        }
         double per_row = 48.0 + 8.0 + 4.0 + 24.0;
         double per_bond = 4.0;
         if (has_pd(s) && s->md.fracture) {

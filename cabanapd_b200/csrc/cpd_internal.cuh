@@ -125,6 +125,46 @@ int launch_max_partials(const double* partials, int nblocks, double* out,
 int energy_blocks(int64_t nrows);
 int vv_blocks(int64_t nrows);
 
+// Mixed-precision PMB path (cpd_kernels_mixed.cu).
+constexpr int kMixedGeneric = 254;  // bond code: no lattice stencil entry
+struct __align__(16) MixedStencil {
+    float x, y, z, xi;  // FP32 bond reference vector and its length
+    float xiinv;        // 1 / length
+    int32_t delta;      // neighbour index - particle index
+    int32_t pad[2];
+};
+struct MixedView {
+    const float4* xh;  // positions, FP32 hi part
+    const float4* xl;  // positions, FP32 lo part (x - hi)
+    const float4* uh;  // displacement hi part; w = volume
+    const float4* ul;  // displacement lo part; w = no-fail flag
+    const uint8_t* code;  // [max_n][npad] stencil code per bond slot
+    const MixedStencil* table;
+    const uint8_t* warp_kind;  // per warp of rows: 2 all rows full stencil, 1 all rows
+                               // stencil subsets, 0 otherwise (per-bond codes)
+    const uint32_t* pmask;     // [ceil(ntab/32)][npad] stencil entries present per row
+};
+struct MixedState {
+    float4* xh = nullptr;
+    float4* xl = nullptr;
+    float4* uh = nullptr;
+    float4* ul = nullptr;
+    uint8_t* code = nullptr;
+    MixedStencil* table = nullptr;
+    uint8_t* warp_kind = nullptr;
+    uint32_t* pmask = nullptr;
+    int ntab = 0;
+    double h[3] = {0, 0, 0};
+};
+int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
+                  MixedState& m, cudaStream_t st, std::string& err);
+void free_mixed(MixedState& m);
+int launch_split_u(const ParticleView& p, MixedState& m, cudaStream_t st);
+int launch_vv_initial_mixed(const ParticleView& p, double dt, MixedState& m,
+                            cudaStream_t st);
+int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                          const MixedState& m, cudaStream_t st);
+
 // Neighbour build (cpd_neighbor.cu). Builds rows for [begin, n) from
 // positions pos (+ optional displacement disp) with squared distance
 // <= cutoff^2; rows sorted by ascending user_id of the neighbour.

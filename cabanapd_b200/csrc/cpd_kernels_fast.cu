@@ -148,8 +148,8 @@ __device__ __forceinline__ void gather(const ParticleView& p, int64_t np, int64_
 // iterations ahead (a shift register in registers), and with GP the
 // neighbour's position / displacement / volume are gathered one bond ahead,
 // so a warp keeps several independent loads in flight while it computes.
-template <bool FRACTURE, int PF, bool GP>
-__global__ void __launch_bounds__(kBlock)
+template <bool FRACTURE, int PF, bool GP, int MINB = 1>
+__global__ void __launch_bounds__(kBlock, MINB)
     k_pmb_force_fast(ParticleView p, EllView nl, FastModel md)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -338,16 +338,17 @@ __global__ void __launch_bounds__(kBlock)
     p.f[2 * np + i] = fz;
 }
 
-// Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-4):
+// Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-5):
 // 0 no prefetch, 1 indices 2 bonds ahead, 2 indices 4 ahead, 3 / 4 the same
-// plus neighbour gathers one bond ahead. Measured on the full plate (B200):
-// 11.3 / 8.2 / 9.0 / 11.9 / 11.8 ms per launch, so 1 is the default.
+// plus neighbour gathers one bond ahead, 5 = 1 compiled for 4 blocks of 256
+// per SM (64 registers). Full plate on B200, ms per launch: 11.3 / 11.3 /
+// 9.0 / 11.9 / 11.8 / 7.3, so 5 is the default.
 int fast_variant()
 {
     static int v = [] {
         const char* e = getenv("CPD_FORCE_VARIANT");
-        int x = e ? atoi(e) : 1;
-        return (x < 0 || x > 4) ? 1 : x;
+        int x = e ? atoi(e) : 5;
+        return (x < 0 || x > 5) ? 5 : x;
     }();
     return v;
 }
@@ -379,10 +380,12 @@ int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& 
         case 2: k_pmb_force_fast<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 3: k_pmb_force_fast<true, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 4: k_pmb_force_fast<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 5: k_pmb_force_fast<true, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 100: k_pmb_force_fast<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 101: k_pmb_force_fast<false, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 102: k_pmb_force_fast<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         case 103: k_pmb_force_fast<false, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 105: k_pmb_force_fast<false, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         }
     } else {

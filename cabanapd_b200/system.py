@@ -17,6 +17,7 @@ FIELDS = {"x": 0, "u": 1, "v": 2, "f": 3, "vol": 4, "rho": 5, "m": 6,
 VECTOR_FIELDS = {"x", "u", "v", "f"}
 FP64_EXACT = 0
 FP64 = 1
+MIXED = 2
 ORDER_INPUT, ORDER_MORTON = 0, 1
 
 _lib = None

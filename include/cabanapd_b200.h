@@ -85,8 +85,13 @@ enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1 };
  * four divisions, FMA allowed; forces agree with EXACT to ~1e-13 relative
  * (norm-wise) and the broken-bond decision is re-evaluated exactly inside a
  * 1e-12 guard band, so broken-bond sets are identical. PMB and LPS use it;
- * the linearized models and Hertz contact always run EXACT. */
-enum { CPD_FP64_EXACT = 0, CPD_FP64 = 1 };
+ * the linearized models and Hertz contact always run EXACT.
+ * MIXED (PMB without contact): FP32 bond arithmetic with FP32 bond reference
+ * vectors precomputed in FP64, Kahan-compensated per-particle force sums,
+ * FP64 integration and reductions, and an FP64 re-test of every bond whose
+ * stretch is within 1e-4 s0 of s0, so broken-bond sets match FP64; other
+ * models run the FP64 kernels under MIXED. */
+enum { CPD_FP64_EXACT = 0, CPD_FP64 = 1, CPD_MIXED = 2 };
 
 /* Internal particle order: INPUT keeps the caller's order; MORTON sorts by
  * the Morton code of the particle's cell (results are returned in the
@@ -136,7 +141,7 @@ typedef struct cpd_params {
                                     radius_extend (Neighbor.hpp:118-119);
                                     k > 0 = rebuild every k steps */
     int32_t per_particle_radius; /* 1: Hertz with per-particle radii */
-    int32_t precision;           /* CPD_FP64_EXACT or CPD_FP64 */
+    int32_t precision;           /* CPD_FP64_EXACT, CPD_FP64 or CPD_MIXED */
     int32_t ordering;            /* CPD_ORDER_* */
     int32_t device;              /* CUDA device ordinal */
 } cpd_params;
