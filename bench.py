@@ -8,6 +8,11 @@ break test + PMB force over every directed bond, force BC, both half-step
 updates. Metric: bond-updates/s = (directed neighbour entries, broken ones
 included, since the kernel visits them) x steps / device time.
 
+Default run: the mixed-precision path (FP32 bonds, FP64 state) is the
+headline `value`; the plain FP64 path runs the same steps from the same
+start and is reported beside it (`plain_fp64`, `mixed_vs_plain`), with the
+per-field error of mixed vs FP64 (`mixed_error_vs_fp64`).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 N > 1 (torchrun, one rank per GPU): every rank advances its own plate
@@ -48,10 +53,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_bond():
-    """DRAM bytes per directed bond of the force kernel from the committed ncu
-    summary (profiles/pmb_force_plate.txt), or None."""
-    path = os.path.join(ROOT, "profiles", "pmb_force_plate.txt")
+def traffic_per_bond(name):
+    """DRAM bytes per directed bond of a bond kernel from its committed ncu
+    summary under profiles/, or None."""
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     with open(path) as fh:
@@ -257,29 +262,21 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------------------
-def run_gpu(args, world, rank, local, pg):
+PRECISION = {"exact": 0, "fp64": 1, "mixed": 2}
+KERNEL = {"fp64": "k_pmb_force_fast<fracture>", "mixed": "k_pmb_force_mixed<fracture>",
+          "exact": "k_pd_force<PMB, fracture> (bit-exact)"}
+PROFILE = {"fp64": "pmb_force_plate.txt", "mixed": "pmb_force_mixed_plate.txt",
+           "exact": "pmb_force_exact_plate.txt"}
+
+
+def timed_steps(sys_, stream, args, device, pg, sampler):
+    """Warm-up, then exactly args.steps device-timed steps (CUDA events on
+    the launching stream, barrier + synchronize on both sides)."""
     import torch
-
-    import cabanapd_b200
-    device = local
-    torch.cuda.set_device(device)
-    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
-    stream = torch.cuda.Stream(device=device)
-
-    prec = {"fp64": 1, "exact": 0, "mixed": 2}[args.precision]
-    sys_ = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
-    sys_.set_stream(stream.cuda_stream)
-    P.setup(sys_, prob)
-    _, bonds = sys_.neighbor_stats()
-    n = sys_.n
-
-    # Warm-up.
     sys_.step(args.warmup)
     sys_.synchronize()
     sys_.set_kernel_timing(True)
     launches0 = sys_.kernel_launches()
-
-    sampler = ClockSampler(visible_index(local)) if rank == 0 else None
     barrier(pg, device)
     torch.cuda.synchronize(device)
     if sampler:
@@ -292,58 +289,106 @@ def run_gpu(args, world, rank, local, pg):
     torch.cuda.synchronize(device)
     clocks = sampler.stop() if sampler else None
     barrier(pg, device)
-    ms_local = ev0.elapsed_time(ev1)
-    launches = sys_.kernel_launches() - launches0
     k_ms, k_n, k_bytes = sys_.kernel_time()
     sys_.set_kernel_timing(False)
+    return {"ms": ev0.elapsed_time(ev1), "launches": sys_.kernel_launches() - launches0,
+            "k_ms": k_ms, "k_n": k_n, "k_bytes": k_bytes, "clocks": clocks}
 
-    value, ms, total_bonds = aggregate(pg, device, ms_local, bonds, args.steps)
+
+def roofline(prec, r, bonds):
+    hbm, hbm_kind = peaks()
+    avg_ms = r["k_ms"] / max(r["k_n"], 1)
+    achieved = r["k_bytes"] / (avg_ms / 1e3) / 1e9
+    tpb = traffic_per_bond(PROFILE[prec])
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": hbm_kind, "kernel": KERNEL[prec],
+            "kernel_ms_avg": avg_ms, "kernel_launches": r["k_n"],
+            "algorithmic_bytes_per_launch": r["k_bytes"],
+            "traffic": (tpb * bonds if tpb else None)}
+
+
+def run_gpu(args, world, rank, local, pg):
+    import torch
+
+    import cabanapd_b200
+    device = local
+    torch.cuda.set_device(device)
+    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
+    stream = torch.cuda.Stream(device=device)
+    precs = [args.precision] if args.precision != "mixed" or args.only else ["mixed", "fp64"]
+    systems, res = {}, {}
+    for prec in precs:
+        sys_ = cabanapd_b200.System(dict(prob["params"], device=device,
+                                         precision=PRECISION[prec]))
+        sys_.set_stream(stream.cuda_stream)
+        P.setup(sys_, prob)
+        sampler = ClockSampler(visible_index(local)) if rank == 0 else None
+        res[prec] = timed_steps(sys_, stream, args, device, pg, sampler)
+        systems[prec] = sys_
+    head = precs[0]
+    _, bonds = systems[head].neighbor_stats()
+    n = systems[head].n
+    value, ms, total_bonds = aggregate(pg, device, res[head]["ms"], bonds, args.steps)
     particle_steps = reduce_sum(pg, float(n), device) * args.steps / (ms / 1e3)
+    plain = None
+    if "fp64" in res and head != "fp64":
+        pv, pms, _ = aggregate(pg, device, res["fp64"]["ms"], bonds, args.steps)
+        # Same start, same number of steps: error of the headline path vs FP64.
+        a, b = systems[head], systems["fp64"]
+        err = {}
+        for fld in ("u", "v", "f"):
+            x, y = a.get(fld), b.get(fld)
+            err[fld] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        wa, da = a.compute_energy()
+        wb, db = b.compute_energy()
+        err["strain_energy"] = abs(wa - wb) / abs(wb)
+        err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
+        err["total_damage"] = [da, db]
+        plain = {"value": pv, "ms_per_step": pms / args.steps,
+                 "roofline": roofline("fp64", res["fp64"], bonds),
+                 "gpu_launches": res["fp64"]["launches"]}
+    for sys_ in systems.values():
+        sys_.close()
+    systems.clear()
 
     if args.skip_e2e:
         e2e_value, h2d, d2h = None, None, None
     else:
-        e2e_value, h2d, d2h = run_e2e(args, prob, device, stream, pg, total_bonds, sys_)
-        sys_ = None
+        e2e_value, h2d, d2h = run_e2e(args, prob, device, stream, pg, total_bonds, head)
     if rank != 0:
         return
-    hbm, hbm_kind = peaks()
-    avg_ms = k_ms / max(k_n, 1)
-    achieved = k_bytes / (avg_ms / 1e3) / 1e9
-    tpb = traffic_per_bond()
     line = {
         "metric": "bond-updates/s", "value": value, "unit": "bond-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": {"mixed": "f32 bonds + f64 state", "fp64": "f64", "exact": "f64"}[head],
+        "data": "synthetic",
         "config": {"workload": "pmb_fracture_notched_plate_impact",
                    "plate_cells": list(PLATE_CELLS), "particles_per_gpu": n,
-                   "bonds_per_gpu": bonds, "precision": args.precision,
+                   "bonds_per_gpu": bonds, "precision": head,
                    "l2": "inputs larger than L2 (neighbour list %.1f GB)" % (4 * bonds / 1e9),
                    "particle_steps_per_s": particle_steps},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": hbm_kind,
-                     "kernel": {"fp64": "k_pmb_force_fast<fracture>",
-                                "mixed": "k_pmb_force_mixed<fracture>",
-                                "exact": "k_pd_force<PMB, fracture> (exact)"}[args.precision],
-                     "kernel_ms_avg": avg_ms, "kernel_launches": k_n,
-                     "algorithmic_bytes_per_launch": k_bytes,
-                     "traffic": (tpb * bonds if tpb else None)},
+        "roofline": roofline(head, res[head], bonds),
         "e2e": ({"value": e2e_value, "unit": "bond-updates/s",
                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                  "job": ("upload + neighbour build + prenotch + init + steps + "
                          "energy/damage read every 10 steps + download u")}
                 if e2e_value is not None else None),
-        "gpu_launches": launches,
-        "clocks": clocks,
+        "gpu_launches": res[head]["launches"],
+        "clocks": res[head]["clocks"],
     }
+    if plain is not None:
+        line["plain_fp64"] = plain
+        line["mixed_vs_plain"] = value / plain["value"]
+        line["mixed_error_vs_fp64"] = err
     if world == 1 and not args.skip_cpu:
         line["cpu_baseline"] = time_cpu_sample()
         line["cpu_baseline"].pop("steps", None)
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, prob, device, stream, pg, total_bonds, old_system):
+def run_e2e(args, prob, device, stream, pg, total_bonds, prec):
     import torch
 
     import cabanapd_b200
@@ -361,12 +406,10 @@ def run_e2e(args, prob, device, stream, pg, total_bonds, old_system):
     hnf = pinned(prob["nofail"].astype(np.int32))
     hv0 = pinned(prob["v0"])
     hu = pinned(np.zeros_like(prob["x"]))
-    old_system.close()
     torch.cuda.synchronize(device)
     barrier(pg, device)
     t0 = time.perf_counter()
-    prec = {"fp64": 1, "exact": 0, "mixed": 2}[args.precision]
-    e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=prec))
+    e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
     e2.set_stream(stream.cuda_stream)
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
@@ -408,9 +451,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"],
-                    help="fp64: throughput FP64 kernels (default); exact: bit-exact; "
-                         "mixed: FP32 bonds / FP64 integration")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "exact", "mixed"],
+                    help="mixed (default): FP32 bonds / FP64 state, measured beside the "
+                         "plain FP64 path; fp64: throughput FP64 only; exact: bit-exact")
+    ap.add_argument("--only", action="store_true",
+                    help="with mixed: skip the plain FP64 comparison run")
     ap.add_argument("--cells", default=None,
                     help="plate cells nx,ny,nz (profiling on a smaller plate)")
     args = ap.parse_args()

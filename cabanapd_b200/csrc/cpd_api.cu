@@ -943,7 +943,9 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
     if (total_ms) *total_ms = s->timed_ms;
     if (launches) *launches = s->timed_launches;
     if (bytes_per_launch) {
-        // Compulsory traffic of one bond-kernel launch: per row, read x, u
+        // Compulsory traffic of one plain-FP64 bond-kernel launch (the same
+        // denominator for every precision mode, so fractions compare the
+        // modes on the same work): per row, read x, u
         // (48 B), vol (8 B), count (4 B), write f (24 B); per bond the 4-byte
         // neighbour index; with fracture the 1-bit bond state read and
         // written (0.25 B) and the 1-byte no-fail flag per row; LPS adds the
@@ -951,13 +953,6 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
         // counted once (ideal reuse).
         const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
         const double rows = (double)(s->n - s->frozen);
-        if (use_mixed(s)) {
-            // Mixed kernel: per row the FP32 hi/lo displacement with volume and
-            // no-fail (32 B), count (4 B), force write (24 B); per bond the
-            // 1-byte stencil code and the bond bit read + write.
-            *bytes_per_launch = 60.0 * rows + (1.0 + (s->md.fracture ? 0.25 : 0.0)) * (double)nl.total;
-            return CPD_OK;
-        }
         double per_row = 48.0 + 8.0 + 4.0 + 24.0;
         double per_bond = 4.0;
         if (has_pd(s) && s->md.fracture) {

@@ -238,8 +238,9 @@ cpd_status cpd_device_field(cpd_system* sys, int32_t field, void** ptr,
 /* Per-kernel device time: when enabled, the bond kernels of every step are
  * bracketed by CUDA events on the system stream.
  * cpd_kernel_time returns the summed milliseconds and launch count of the
- * main bond kernel since timing was enabled, and the bytes it is
- * algorithmically required to move per launch. */
+ * main bond kernel since timing was enabled, and the bytes the plain-FP64
+ * bond algorithm is required to move per launch (the same denominator in
+ * every precision mode). */
 cpd_status cpd_set_kernel_timing(cpd_system* sys, int32_t enable);
 cpd_status cpd_kernel_time(cpd_system* sys, double* total_ms,
                            int64_t* launches, double* bytes_per_launch);
