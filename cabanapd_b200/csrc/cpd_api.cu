@@ -91,7 +91,7 @@ namespace {
 bool has_pd(const cpd_system* s) { return s->md.pd != CPD_PD_NONE; }
 bool is_lps(const cpd_system* s)
 {
-    return s->md.pd == CPD_PD_LPS || s->md.pd == CPD_PD_LINEAR_LPS;
+    return s->md.pd == CPD_PD_LPS;
 }
 bool has_contact(const cpd_system* s) { return s->md.contact != CPD_CONTACT_NONE; }
 
@@ -409,8 +409,9 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown contact_model");
     if (P.pd_model == CPD_PD_NONE && P.contact_model == CPD_CONTACT_NONE)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "need a PD model or a contact model");
-    if ((P.pd_model == CPD_PD_LINEAR_PMB || P.pd_model == CPD_PD_LINEAR_LPS) && P.fracture)
-        return set_error(CPD_ERR_UNSUPPORTED, "linearized models have no fracture variant");
+    // Force<LinearPMB, Fracture> is not defined (force/CabanaPD_PMB.hpp:407).
+    if (P.pd_model == CPD_PD_LINEAR_PMB && P.fracture)
+        return set_error(CPD_ERR_UNSUPPORTED, "LinearPMB has no fracture variant");
     if (P.pd_model != CPD_PD_NONE && !(P.horizon > 0))
         return set_error(CPD_ERR_INVALID_ARGUMENT, "horizon must be > 0");
     if (P.contact_model == CPD_CONTACT_HERTZ && !(P.contact_radius > 0))
@@ -436,7 +437,12 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
     s->params = P;
     s->device = P.device;
     Model& md = s->md;
-    md.pd = P.pd_model;
+    // LinearLPS computes with the LPS kernels: ForceModel<LinearLPS>
+    // (force_models/CabanaPD_LPS.hpp:255-272) keeps the base model's
+    // force_tag = LPS (:32), and the Solver instantiates
+    // Force<memory_space, force_tag, fracture_type> (CabanaPD_Solver.hpp:96-99),
+    // so the linearised Force<LinearLPS> is never selected.
+    md.pd = P.pd_model == CPD_PD_LINEAR_LPS ? CPD_PD_LPS : P.pd_model;
     md.fracture = P.fracture ? 1 : 0;
     md.contact = P.contact_model;
     md.influence = infl;
@@ -859,6 +865,26 @@ cpd_status cpd_step(cpd_system* s, int32_t num_steps)
         CPD_LAUNCHED(launch_vv_final(p, s->params.dt, s->stream));
     }
     return CPD_OK;
+}
+
+cpd_status cpd_step_stage(cpd_system* s, int32_t stage)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step_stage");
+    CPD_CUDA(cudaSetDevice(s->device));
+    switch (stage) {
+    case CPD_STAGE_INITIAL_HALF: return vv_initial(s);
+    case CPD_STAGE_FORCE:
+        // Device code run between stages may have written u: re-split it for
+        // the mixed kernels (a no-op in the FP64 modes).
+        CPD_OK_OR_RETURN(refresh_mixed_u(s));
+        return update_force(s);
+    case CPD_STAGE_FORCE_BC: return apply_force_bcs(s);
+    case CPD_STAGE_FINAL_HALF:
+        CPD_LAUNCHED(launch_vv_final(view(s), s->params.dt, s->stream));
+        return CPD_OK;
+    default: return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown step stage");
+    }
 }
 
 cpd_status cpd_synchronize(cpd_system* s)

@@ -151,10 +151,10 @@ __global__ void __launch_bounds__(kBlock)
 // ---------------------------------------------------------------------------
 // PD force. PMB: force/CabanaPD_PMB.hpp:89-125 (NoFracture), :222-287
 // (Fracture); LinearPMB :406-455; LPS: force/CabanaPD_LPS.hpp:143-181
-// (NoFracture), :380-447 (Fracture); LinearLPS :577-627.
+// (NoFracture), :380-447 (Fracture). LinearLPS systems run as LPS.
 // The force is written (not accumulated): CabanaPD_Force.hpp:187-189 zeroes
 // f before the kernel, and 0.0 + t == t.
-enum { M_PMB = 0, M_LPS = 1, M_LINEAR_PMB = 2, M_LINEAR_LPS = 3 };
+enum { M_PMB = 0, M_LPS = 1, M_LINEAR_PMB = 2 };
 
 template <int MODEL, int INFL, bool FRACTURE>
 __global__ void __launch_bounds__(kBlock)
@@ -165,8 +165,8 @@ __global__ void __launch_bounds__(kBlock)
     const int64_t np = p.npad;
     const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
     const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
-    constexpr bool lps = MODEL == M_LPS || MODEL == M_LINEAR_LPS;
-    constexpr bool linear = MODEL == M_LINEAR_PMB || MODEL == M_LINEAR_LPS;
+    constexpr bool lps = MODEL == M_LPS;
+    constexpr bool linear = MODEL == M_LINEAR_PMB;
     double a_i = 0.0, b_i = 0.0;
     if (lps) {
         a_i = p.lps_a[i];
@@ -189,13 +189,7 @@ __global__ void __launch_bounds__(kBlock)
             double xi, ls, xx, xy, xz;
             bond_linearized(p.x, p.u, np, j, xi0, xi1, xi2, ui0, ui1, ui2, xi, ls,
                             xx, xy, xz);
-            double coeff;
-            if (lps) {
-                const double a_j = __ldg(p.lps_a + j), b_j = __ldg(p.lps_b + j);
-                coeff = (a_i + a_j + ls * (b_i + b_j)) * influence<INFL>(xi) * xi * vol_j;
-            } else {
-                coeff = md.c * ls * vol_j;
-            }
+            const double coeff = md.c * ls * vol_j;
             fx += coeff * xx / xi;
             fy += coeff * xy / xi;
             fz += coeff * xz / xi;
@@ -244,7 +238,7 @@ __global__ void __launch_bounds__(kBlock)
 // ---------------------------------------------------------------------------
 // Strain energy density and damage: force/CabanaPD_PMB.hpp:127-155
 // (NoFracture), :289-339 (Fracture), :458-491 (LinearPMB);
-// force/CabanaPD_LPS.hpp:183-219, :449-504, :629-670.
+// force/CabanaPD_LPS.hpp:183-219, :449-504.
 // Per particle W_i and phi_i are exact; the block partial sums of
 // (sum_k w_k vol_i or W_i vol_i, phi_i) are reduced in a fixed tree order.
 template <int MODEL, int INFL, bool FRACTURE>
@@ -259,8 +253,8 @@ __global__ void __launch_bounds__(kBlock)
         const int64_t np = p.npad;
         const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
         const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
-        constexpr bool lps = MODEL == M_LPS || MODEL == M_LINEAR_LPS;
-        constexpr bool linear = MODEL == M_LINEAR_PMB || MODEL == M_LINEAR_LPS;
+        constexpr bool lps = MODEL == M_LPS;
+        constexpr bool linear = MODEL == M_LINEAR_PMB;
         const int cnt = nl.count[i];
         const double vol_i = p.vol[i];
         double m_i = 0.0, th_i = 0.0;
@@ -706,12 +700,6 @@ int launch_lps_dilatation(const ParticleView& p, const EllView& nl,
                 else                                                                \
                     KERNEL<M_LPS, 0, false><<<GRID, kBlock, 0, st>>>(__VA_ARGS__);  \
             }                                                                       \
-            break;                                                                  \
-        case CPD_PD_LINEAR_LPS:                                                     \
-            if (infl)                                                               \
-                KERNEL<M_LINEAR_LPS, 1, false><<<GRID, kBlock, 0, st>>>(__VA_ARGS__); \
-            else                                                                    \
-                KERNEL<M_LINEAR_LPS, 0, false><<<GRID, kBlock, 0, st>>>(__VA_ARGS__); \
             break;                                                                  \
         default:                                                                    \
             return 0;                                                               \

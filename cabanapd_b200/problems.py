@@ -122,6 +122,50 @@ def elastic_wave_pmb(n=41, steps=100):
                     dx=h)
 
 
+def elastic_wave_lps(deck):
+    """The LinearLPS spherical-wave program of the reference's
+    examples/mechanics/elastic_wave.cpp:57-100 for an input deck (dict in
+    the JSON input format): cell-centre lattice from system_size and
+    num_cells, horizon + 1e-10, u0 = 1e-3 exp(-((|x| - 0.25) / 0.07)^2) x/|x|
+    (exp from the C library, through math.exp), v0 = 0, num_steps =
+    int(final_time / timestep)."""
+    n = deck["num_cells"]["value"]
+    size = deck["system_size"]["value"]
+    low = [-0.5 * s for s in size]
+    high = [0.5 * s for s in size]
+    x, vol, h = lattice(low, high, n)
+    u0 = np.zeros_like(x)
+    for p in range(x.shape[0]):
+        r = math.sqrt(x[p, 0] * x[p, 0] + x[p, 1] * x[p, 1] + x[p, 2] * x[p, 2])
+        d = r - 0.25
+        arg = d * d / 0.07 / 0.07
+        for c in range(3):
+            direction = x[p, c] / r if r > 0.0 else 0.0
+            u0[p, c] = 0.001 * math.exp(-arg) * direction
+    dt = deck["timestep"]["value"]
+    steps = int(deck["final_time"]["value"] / dt)
+    params = dict(pd_model=PD_LINEAR_LPS, fracture=0,
+                  horizon=deck["horizon"]["value"] + 1e-10,
+                  K=deck["bulk_modulus"]["value"], G=deck["shear_modulus"]["value"], dt=dt)
+    return _problem("elastic_wave_lps", params, x, vol,
+                    rho=np.full(x.shape[0], float(deck["density"]["value"])), u0=u0,
+                    num_steps=steps, dx=h,
+                    output_frequency=int(deck["output_frequency"]["value"]))
+
+
+def displacement_profile(prob, u, profile_dim=0, displacement_dim=None):
+    """createDisplacementProfile (CabanaPD_OutputProfiles.hpp:27-84): the
+    particles strictly within half a cell of the line through the origin
+    along profile_dim, in index order, as (x[profile_dim], u[disp_dim])."""
+    if displacement_dim is None:
+        displacement_dim = profile_dim
+    x, h = prob["x"], prob["dx"]
+    d1, d2 = (profile_dim + 1) % 3, (profile_dim + 2) % 3
+    on = np.nonzero((x[:, d1] < h[d1] / 2) & (x[:, d1] > -h[d1] / 2) &
+                    (x[:, d2] < h[d2] / 2) & (x[:, d2] > -h[d2] / 2))[0]
+    return x[on, profile_dim], u[on, displacement_dim]
+
+
 def plate_impact(num_cells=(800, 400, 36), steps=2000, v0=16.5):
     """PMB brittle fracture, double-notched plate impact (Kalthoff-Winkler
     layout of examples/mechanics/kalthoff_winkler.cpp): plate

@@ -81,6 +81,7 @@ SIGNATURES = {
     "cpd_init": (_I32, [_P]),
     "cpd_step": (_I32, [_P, _I32]),
     "cpd_synchronize": (_I32, [_P]),
+    "cpd_step_stage": (_I32, [_P, _I32]),
     "cpd_download": (_I32, [_P, _I32, _P]),
     "cpd_max_displacement": (_D, [_P]),
     "cpd_contact_rebuilds": (_I64, [_P]),
@@ -236,6 +237,11 @@ class System:
 
     def synchronize(self):
         self._check(self._lib.cpd_synchronize(self._h))
+
+    def step_stage(self, stage):
+        """One stage of a time step (0 initial half, 1 force, 2 force BCs,
+        3 final half), queued asynchronously."""
+        self._check(self._lib.cpd_step_stage(self._h, int(stage)))
 
     def get(self, field, out=None):
         shape = (self.n, 3) if field in VECTOR_FIELDS else (self.n,)

@@ -65,7 +65,12 @@ enum {
     CPD_ERR_UNSUPPORTED = 5
 };
 
-/* Peridynamic force models (CabanaPD_Types.hpp:145-163). */
+/* Peridynamic force models (CabanaPD_Types.hpp:145-163). LINEAR_PMB uses the
+ * linearised bond stretch (force/CabanaPD_PMB.hpp:406-538) and has no
+ * fracture variant. LINEAR_LPS computes exactly like LPS, with or without
+ * fracture, as the reference's Solver does: ForceModel<LinearLPS> keeps
+ * force_tag = LPS (force_models/CabanaPD_LPS.hpp:32, 255-272) and the Solver
+ * selects Force<force_tag, ...> (CabanaPD_Solver.hpp:96-99). */
 enum {
     CPD_PD_NONE = 0,
     CPD_PD_PMB = 1,
@@ -224,6 +229,21 @@ cpd_status cpd_init(cpd_system* sys);
  * queued on the stream (cpd_synchronize or any download waits for it). */
 cpd_status cpd_step(cpd_system* sys, int32_t num_steps);
 cpd_status cpd_synchronize(cpd_system* sys);
+/* One stage of one time step, for callers that run their own device code
+ * between stages (CabanaPD_Solver.hpp:332-375 order): INITIAL_HALF is the
+ * first velocity-Verlet half step, FORCE the weighted volume / dilatation /
+ * bond force / contact force, FORCE_BC the boundary conditions added with
+ * cpd_add_boundary_condition, FINAL_HALF the second half step. Running the
+ * four stages in order equals cpd_step(sys, 1). Device code between stages
+ * may write the fields of cpd_device_field on the system's stream (FORCE
+ * re-reads u for the MIXED kernels). Asynchronous. */
+enum {
+    CPD_STAGE_INITIAL_HALF = 0,
+    CPD_STAGE_FORCE = 1,
+    CPD_STAGE_FORCE_BC = 2,
+    CPD_STAGE_FINAL_HALF = 3
+};
+cpd_status cpd_step_stage(cpd_system* sys, int32_t stage);
 
 /* Copy a field to host memory in the caller's particle order. */
 cpd_status cpd_download(cpd_system* sys, int32_t field, double* host_out);

@@ -319,16 +319,16 @@ void lps_dilatation(orc_system& s)
 
 // force/CabanaPD_PMB.hpp:89-125 (NoFracture), :222-287 (Fracture),
 // :406-455 (LinearPMB); force/CabanaPD_LPS.hpp:143-181 (NoFracture),
-// :380-447 (Fracture), :577-627 (LinearLPS). f is zeroed first
-// (CabanaPD_Force.hpp:187-189).
+// :380-447 (Fracture). f is zeroed first (CabanaPD_Force.hpp:187-189).
+// LinearLPS systems reach here as LPS (see orc_create).
 void pd_force(orc_system& s)
 {
     const Model& md = s.model;
     const NList& nl = s.pd_list;
     const double* x = s.x.data();
     const double* u = s.u.data();
-    const bool linear = md.pd == ORC_PD_LINEAR_PMB || md.pd == ORC_PD_LINEAR_LPS;
-    const bool lps = md.pd == ORC_PD_LPS || md.pd == ORC_PD_LINEAR_LPS;
+    const bool linear = md.pd == ORC_PD_LINEAR_PMB;
+    const bool lps = md.pd == ORC_PD_LPS;
     std::fill(s.f.begin(), s.f.end(), 0.0);
 #pragma omp parallel for schedule(static)
     for (int64_t i = s.frozen; i < s.n; i++) {
@@ -338,12 +338,7 @@ void pd_force(orc_system& s)
             if (linear) {
                 double xi, ls, xx, xy, xz;
                 get_linearized_distance(x, u, i, j, xi, ls, xx, xy, xz);
-                double coeff;
-                if (lps)
-                    coeff = lps_force_coeff(md, ls, xi, s.vol[j], s.m[i],
-                                            s.m[j], s.theta[i], s.theta[j]);
-                else
-                    coeff = md.c * ls * s.vol[j];
+                const double coeff = md.c * ls * s.vol[j];
                 fx += coeff * xx / xi;
                 fy += coeff * xy / xi;
                 fz += coeff * xz / xi;
@@ -391,7 +386,7 @@ void pd_force(orc_system& s)
 }
 
 // force/CabanaPD_PMB.hpp:127-155, :289-339, :458-491;
-// force/CabanaPD_LPS.hpp:183-219, :449-504, :629-670.
+// force/CabanaPD_LPS.hpp:183-219, :449-504.
 // W is reset first (CabanaPD_Force.hpp:213-214). Per-particle W_i and phi_i
 // are exact restatements; the totals are summed serially over i.
 void pd_energy(orc_system& s, double& total_W, double& total_D)
@@ -400,8 +395,8 @@ void pd_energy(orc_system& s, double& total_W, double& total_D)
     const NList& nl = s.pd_list;
     const double* x = s.x.data();
     const double* u = s.u.data();
-    const bool linear = md.pd == ORC_PD_LINEAR_PMB || md.pd == ORC_PD_LINEAR_LPS;
-    const bool lps = md.pd == ORC_PD_LPS || md.pd == ORC_PD_LINEAR_LPS;
+    const bool linear = md.pd == ORC_PD_LINEAR_PMB;
+    const bool lps = md.pd == ORC_PD_LPS;
     std::fill(s.W.begin(), s.W.end(), 0.0);
     std::vector<double> phi_contrib(s.n, 0.0);
 #pragma omp parallel for schedule(static)
@@ -422,11 +417,7 @@ void pd_energy(orc_system& s, double& total_W, double& total_D)
             if (linear) {
                 double xi, ls, xx, xy, xz;
                 get_linearized_distance(x, u, i, j, xi, ls, xx, xy, xz);
-                if (lps)
-                    w = lps_energy(md, ls, xi, s.vol[j], s.m[i], s.theta[i],
-                                   num_bonds);
-                else
-                    w = 0.25 * md.c * ls * ls * xi * s.vol[j];
+                w = 0.25 * md.c * ls * ls * xi * s.vol[j];
             } else {
                 double xi, r, st, rx, ry, rz, xx, xy, xz;
                 get_distance(x, u, i, j, xi, r, st, rx, ry, rz, xx, xy, xz);
@@ -614,7 +605,7 @@ void apply_force_bcs(orc_system& s)
 bool has_pd(const orc_system& s) { return s.model.pd != ORC_PD_NONE; }
 bool is_lps(const orc_system& s)
 {
-    return s.model.pd == ORC_PD_LPS || s.model.pd == ORC_PD_LINEAR_LPS;
+    return s.model.pd == ORC_PD_LPS;
 }
 
 // CabanaPD_Solver.hpp:462-477 updateForce, plus the contact force
@@ -728,22 +719,26 @@ orc_system* orc_create(const orc_params* p)
         fail("need a PD model or a contact model");
         return nullptr;
     }
-    if ((p->pd_model == ORC_PD_LINEAR_PMB || p->pd_model == ORC_PD_LINEAR_LPS) &&
-        p->fracture) {
-        // The reference defines Force<LinearPMB|LinearLPS, NoFracture> only.
-        fail("linearized models have no fracture variant");
+    if (p->pd_model == ORC_PD_LINEAR_PMB && p->fracture) {
+        // Force<LinearPMB, Fracture> is not defined (force/CabanaPD_PMB.hpp:407).
+        fail("LinearPMB has no fracture variant");
         return nullptr;
     }
     orc_system* s = new orc_system();
     Model& md = s->model;
-    md.pd = p->pd_model;
+    // LinearLPS computes with the LPS kernels: ForceModel<LinearLPS>
+    // (force_models/CabanaPD_LPS.hpp:255-272) keeps the base model's
+    // force_tag = LPS (:32), and the Solver and the unit tests instantiate
+    // Force<memory_space, force_tag, fracture_type> (CabanaPD_Solver.hpp:96-99,
+    // unit_test/tstForce.hpp:927), so Force<LinearLPS> is never selected.
+    md.pd = p->pd_model == ORC_PD_LINEAR_LPS ? ORC_PD_LPS : p->pd_model;
     md.fracture = p->fracture;
     md.contact = p->contact_model;
     md.horizon = p->horizon;
     md.K = p->K;
     md.G = p->G;
     md.G0 = p->G0;
-    const bool lps = md.pd == ORC_PD_LPS || md.pd == ORC_PD_LINEAR_LPS;
+    const bool lps = md.pd == ORC_PD_LPS;
     md.influence = p->influence_type >= 0 ? p->influence_type : (lps ? 0 : 1);
     if (md.pd != ORC_PD_NONE) {
         const double h = md.horizon;

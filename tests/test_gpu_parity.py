@@ -189,6 +189,21 @@ def test_dem_packing_parity(cuda, oracle):
             assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), fld
 
 
+def test_linear_lps_fracture_is_lps(cuda, oracle):
+    """LinearLPS with fracture runs the LPS fracture kernels (the
+    reference's Solver selects Force<LPS> for it): bit-identical to the
+    oracle and to an LPS system."""
+    prob = P.lps_random_notches(num_cells=(80, 32, 4), steps=30)
+    lin = dict(prob, params=dict(prob["params"], pd_model=P.PD_LINEAR_LPS))
+    g, o = _pair(cuda, oracle, lin)
+    ref = P.setup(cuda.System(prob["params"]), prob)
+    for s in (g, o, ref):
+        s.run(prob["num_steps"])
+    _assert_same(g, o, ("u", "v", "f", "theta", "m"))
+    _assert_same(g, ref, ("u", "v", "f", "theta", "m"))
+    assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+
+
 def test_errors_are_reported(cuda):
     s = cuda.System(dict(pd_model=P.PD_PMB, horizon=0.1, K=1.0, dt=1.0))
     with pytest.raises(cuda.CpdError):

@@ -33,6 +33,53 @@ def hertz_restitution(system, prob):
     return np.sqrt(ke() / ke_i)
 
 
+def elastic_wave_profile_errors(golden, xs, us):
+    """regression_test/tstElasticWave.hpp:54-96: relative error of each
+    profile point against the fitted polynomial (skipping |x| > 0.425 and
+    |x| < 0.025) and the l2 norm of the differences."""
+    coeff = golden["elastic_wave"]["poly_coeff_descending"]
+    rel, total = [], 0.0
+    for xx, u in zip(xs, us):
+        if xx > 0.425 or xx < -0.425 or (-0.025 < xx < 0.025):
+            continue
+        fit = 0.0
+        for c in coeff:
+            fit = fit * xx + c
+        rel.append(abs((u - fit) / fit))
+        total += (u - fit) ** 2
+    return max(rel), total ** 0.5
+
+
+def test_elastic_wave_profile(oracle, golden):
+    """The LinearLPS elastic-wave regression on the oracle (41^3, 60 steps):
+    the displacement profile along x within 3.5 % of the fitted polynomial
+    and l2 < 3e-5. Passing it needs LinearLPS to compute as LPS."""
+    g = golden["elastic_wave"]
+    prob = P.elastic_wave_lps(g["input"])
+    s = oracle.OracleSystem(prob["params"])
+    P.setup(s, prob)
+    s.run(prob["num_steps"])
+    xs, us = P.displacement_profile(prob, s.get("u"))
+    assert len(xs) == 41
+    rel, l2 = elastic_wave_profile_errors(golden, xs, us)
+    assert rel < g["rel_tol"] and l2 < g["l2_tol"], (rel, l2)
+
+
+def test_linear_lps_computes_as_lps(oracle):
+    """ForceModel<LinearLPS> selects Force<LPS> in the reference, with or
+    without fracture: identical fields."""
+    prob = P.lps_random_notches(num_cells=(60, 24, 2), steps=5)
+    out = []
+    for model in (P.PD_LPS, P.PD_LINEAR_LPS):
+        s = oracle.OracleSystem(dict(prob["params"], pd_model=model))
+        P.setup(s, prob)
+        s.run(prob["num_steps"])
+        out.append([s.get(f) for f in ("u", "f", "theta", "m")] + [s.compute_energy()])
+    for a, b in zip(out[0][:4], out[1][:4]):
+        assert np.array_equal(a, b)
+    assert out[0][4] == out[1][4]
+
+
 def test_kalthoff_winkler_crack_extent(oracle, golden):
     g = golden["kalthoff_winkler"]
     prob = P.kalthoff_winkler_regression()
