@@ -5,7 +5,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <utility>
@@ -16,6 +18,49 @@
 using namespace cpd;
 
 namespace {
+constexpr int kPoolDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pool[kPoolDevices] = {};
+int g_live_systems[kPoolDevices] = {};
+
+cudaError_t device_pool(int dev, cudaMemPool_t* out)
+{
+    if (dev < 0 || dev >= kPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaError_t e = cudaMemPoolCreate(&g_pool[dev], &props);
+        if (e != cudaSuccess) {
+            g_pool[dev] = nullptr;
+            return e;
+        }
+        // Keep freed blocks for the next system instead of returning them
+        // at every synchronisation; trimmed when no system is live.
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    *out = g_pool[dev];
+    return cudaSuccess;
+}
+
+void system_opened(int dev)
+{
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    g_live_systems[dev]++;
+}
+
+// Called after the closing system's frees have completed.
+void system_closed(int dev)
+{
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (--g_live_systems[dev] == 0 && g_pool[dev]) cudaMemPoolTrimTo(g_pool[dev], 0);
+}
+
 thread_local std::string g_last_error;
 
 cpd_status set_error(cpd_status code, const std::string& msg)
@@ -24,6 +69,25 @@ cpd_status set_error(cpd_status code, const std::string& msg)
     return code;
 }
 }  // namespace
+
+namespace cpd {
+
+cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t st)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = nullptr;
+    e = device_pool(dev, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(ptr, bytes > 0 ? bytes : 16, pool, st);
+}
+
+cudaError_t dev_free(void* ptr, cudaStream_t st) { return cudaFreeAsync(ptr, st); }
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+}  // namespace cpd
 
 #define CPD_CUDA(call)                                                              \
     do {                                                                            \
@@ -134,21 +198,21 @@ void free_particles(cpd_system* s)
                          &s->red,   &s->red_out};
     for (double** a : arrays)
         if (*a) {
-            cudaFree(*a);
+            dev_free(*a, s->stream);
             *a = nullptr;
         }
-    if (s->nofail) cudaFree(s->nofail);
+    if (s->nofail) dev_free(s->nofail, s->stream);
     s->nofail = nullptr;
-    if (s->perm) cudaFree(s->perm);
+    if (s->perm) dev_free(s->perm, s->stream);
     s->perm = nullptr;
     for (auto& bc : s->bcs) {
-        if (bc.idx) cudaFree(bc.idx);
-        if (bc.values) cudaFree(bc.values);
+        if (bc.idx) dev_free(bc.idx, s->stream);
+        if (bc.values) dev_free(bc.values, s->stream);
     }
     s->bcs.clear();
-    free_neighbor_list(s->pd);
-    free_neighbor_list(s->contact);
-    free_mixed(s->mixed);
+    free_neighbor_list(s->pd, s->stream);
+    free_neighbor_list(s->contact, s->stream);
+    free_mixed(s->mixed, s->stream);
     s->n = s->npad = s->frozen = 0;
     s->red_cap = 0;
     s->neighbors_built = false;
@@ -235,9 +299,9 @@ cpd_status upload_scalar(cpd_system* s, const double* host, double* dst)
 cpd_status ensure_reduction(cpd_system* s, int blocks)
 {
     if (blocks * 2 <= s->red_cap) return CPD_OK;
-    if (s->red) CPD_CUDA(cudaFree(s->red));
+    if (s->red) CPD_CUDA(dev_free(s->red, s->stream));
     s->red = nullptr;
-    CPD_CUDA(cudaMalloc(&s->red, sizeof(double) * 2 * blocks));
+    CPD_CUDA(dev_alloc(&s->red, sizeof(double) * 2 * blocks, s->stream));
     s->red_cap = 2 * blocks;
     return CPD_OK;
 }
@@ -491,6 +555,7 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         delete s;
         return set_error(CPD_ERR_CUDA, std::string("pinned: ") + cudaGetErrorString(e));
     }
+    system_opened(s->device);
     *out = s;
     return CPD_OK;
 }
@@ -501,6 +566,7 @@ cpd_status cpd_system_destroy(cpd_system* s)
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     free_particles(s);
+    if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& pr : s->pending) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
@@ -508,6 +574,7 @@ cpd_status cpd_system_destroy(cpd_system* s)
     for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
     if (s->h_red) cudaFreeHost(s->h_red);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    system_closed(s->device);
     delete s;
     return CPD_OK;
 }
@@ -555,19 +622,19 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
     const size_t sv = sizeof(double) * 3 * s->npad, ss = sizeof(double) * s->npad;
     double** vec[] = {&s->x, &s->u, &s->v, &s->f, &s->u_neigh};
     for (double** a : vec) {
-        CPD_CUDA(cudaMalloc(a, sv));
+        CPD_CUDA(dev_alloc(a, sv, s->stream));
         CPD_CUDA(cudaMemsetAsync(*a, 0, sv, s->stream));
     }
     double** sca[] = {&s->vol, &s->rho, &s->m, &s->theta, &s->lps_a, &s->lps_b,
                       &s->W,   &s->phi, &s->radius};
     for (double** a : sca) {
-        CPD_CUDA(cudaMalloc(a, ss));
+        CPD_CUDA(dev_alloc(a, ss, s->stream));
         CPD_CUDA(cudaMemsetAsync(*a, 0, ss, s->stream));
     }
-    CPD_CUDA(cudaMalloc(&s->nofail, s->npad));
+    CPD_CUDA(dev_alloc(&s->nofail, s->npad, s->stream));
     CPD_CUDA(cudaMemsetAsync(s->nofail, 0, s->npad, s->stream));
-    CPD_CUDA(cudaMalloc(&s->staging, sizeof(double) * 3 * n));
-    CPD_CUDA(cudaMalloc(&s->red_out, sizeof(double) * 8));
+    CPD_CUDA(dev_alloc(&s->staging, sizeof(double) * 3 * n, s->stream));
+    CPD_CUDA(dev_alloc(&s->red_out, sizeof(double) * 8, s->stream));
     CPD_CUDA(cudaMemsetAsync(s->red_out, 0, sizeof(double) * 8, s->stream));
 
     // Internal order.
@@ -575,7 +642,7 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
     if (s->params.ordering == CPD_ORDER_MORTON) {
         double cell = has_pd(s) ? s->md.horizon : 2.0 * s->md.radius + s->md.radius_extend;
         order = morton_order(x, n, n_frozen, cell);
-        CPD_CUDA(cudaMalloc(&s->perm, sizeof(int32_t) * n));
+        CPD_CUDA(dev_alloc(&s->perm, sizeof(int32_t) * n, s->stream));
         CPD_CUDA(cudaMemcpyAsync(s->perm, order.data(), sizeof(int32_t) * n,
                                  cudaMemcpyHostToDevice, s->stream));
     } else {
@@ -667,9 +734,9 @@ cpd_status cpd_download_neighbors(cpd_system* s, int32_t* counts, int32_t* indic
     const NeighborList& nl = has_pd(s) ? s->pd : s->contact;
     const size_t cells = (size_t)s->n * std::max(nl.max_n, 1);
     int32_t *dc = nullptr, *di = nullptr, *dm = nullptr;
-    CPD_CUDA(cudaMalloc(&dc, sizeof(int32_t) * s->n));
-    CPD_CUDA(cudaMalloc(&di, sizeof(int32_t) * cells));
-    CPD_CUDA(cudaMalloc(&dm, sizeof(int32_t) * cells));
+    CPD_CUDA(dev_alloc(&dc, sizeof(int32_t) * s->n, s->stream));
+    CPD_CUDA(dev_alloc(&di, sizeof(int32_t) * cells, s->stream));
+    CPD_CUDA(dev_alloc(&dm, sizeof(int32_t) * cells, s->stream));
     NeighborList tmp = nl;
     if (!(has_pd(s) && s->md.fracture)) tmp.mu = nullptr;
     s->launches += launch_ell_to_rows(tmp, s->n, s->npad, s->perm, s->perm, dc, di, dm, s->stream);
@@ -683,10 +750,10 @@ cpd_status cpd_download_neighbors(cpd_system* s, int32_t* counts, int32_t* indic
     if (mu && nl.max_n > 0)
         CPD_CUDA(cudaMemcpyAsync(mu, dm, sizeof(int32_t) * cells, cudaMemcpyDeviceToHost,
                                  s->stream));
+    dev_free(dc, s->stream);
+    dev_free(di, s->stream);
+    dev_free(dm, s->stream);
     CPD_CUDA(cudaStreamSynchronize(s->stream));
-    cudaFree(dc);
-    cudaFree(di);
-    cudaFree(dm);
     return CPD_OK;
 }
 
@@ -745,13 +812,15 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
         idx[b] = s->h_inv[indices[b]];
     }
     if (count > 0) {
-        CPD_CUDA(cudaMalloc(&bc.idx, sizeof(int32_t) * count));
-        CPD_CUDA(cudaMemcpy(bc.idx, idx.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+        CPD_CUDA(dev_alloc(&bc.idx, sizeof(int32_t) * count, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(bc.idx, idx.data(), sizeof(int32_t) * count,
+                                 cudaMemcpyHostToDevice, s->stream));
         if (kind == CPD_BC_FORCE_ADD) {
-            CPD_CUDA(cudaMalloc(&bc.values, sizeof(double) * count));
-            CPD_CUDA(cudaMemcpy(bc.values, values, sizeof(double) * count,
-                                cudaMemcpyHostToDevice));
+            CPD_CUDA(dev_alloc(&bc.values, sizeof(double) * count, s->stream));
+            CPD_CUDA(cudaMemcpyAsync(bc.values, values, sizeof(double) * count,
+                                     cudaMemcpyHostToDevice, s->stream));
         }
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
     }
     s->bcs.push_back(bc);
     return CPD_OK;
@@ -762,8 +831,8 @@ cpd_status cpd_clear_boundary_conditions(cpd_system* s)
     if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     for (auto& bc : s->bcs) {
-        if (bc.idx) cudaFree(bc.idx);
-        if (bc.values) cudaFree(bc.values);
+        if (bc.idx) dev_free(bc.idx, s->stream);
+        if (bc.values) dev_free(bc.values, s->stream);
     }
     s->bcs.clear();
     return CPD_OK;
@@ -993,6 +1062,22 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
 }
 
 int64_t cpd_kernel_launches(const cpd_system* s) { return s ? s->launches : 0; }
+
+cpd_status cpd_device_bytes(const cpd_system* s, uint64_t* bytes)
+{
+    if (!s || !bytes) return set_error(CPD_ERR_INVALID_ARGUMENT, "null argument");
+    const uint64_t np = (uint64_t)s->npad, n = (uint64_t)s->n;
+    uint64_t b = 0;
+    if (s->x) {
+        b += 5 * 24 * np + 9 * 8 * np + np;  // vectors, scalars, nofail
+        b += 24 * n + 64 + 8 * (uint64_t)s->red_cap;  // staging, reduction
+        if (s->perm) b += 4 * n;
+    }
+    for (const auto& bc : s->bcs) b += (uint64_t)bc.count * (bc.values ? 12 : 4);
+    b += s->pd.bytes + s->contact.bytes + s->mixed.bytes;
+    *bytes = b;
+    return CPD_OK;
+}
 
 }  // extern "C"
 

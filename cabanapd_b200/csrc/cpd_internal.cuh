@@ -27,6 +27,23 @@ namespace cpd {
 
 constexpr double kPi = 3.14159265358979323846;
 
+// Device memory of the library comes from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the owning system's stream),
+// so setting up or releasing a system never synchronises the device: a job
+// admitted or retired while others run does not stall them. Freed blocks
+// stay in the pool for the next system and are returned to the driver when
+// the last live system on the device is destroyed.
+// Message returned by cpd_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
+
+cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t st);
+cudaError_t dev_free(void* ptr, cudaStream_t st);
+template <class T>
+inline cudaError_t dev_alloc(T** ptr, size_t bytes, cudaStream_t st)
+{
+    return dev_alloc(reinterpret_cast<void**>(ptr), bytes, st);
+}
+
 // Model constants, derived on the host with the reference constructors'
 // expressions (force_models/CabanaPD_PMB.hpp:41-47, CabanaPD_LPS.hpp:64-75,
 // CabanaPD_ForceModels.hpp:93-102, CabanaPD_Hertzian.hpp:40-56).
@@ -74,6 +91,8 @@ struct ParticleView {
 
 struct NeighborList {
     int32_t max_n = 0;
+    int32_t cap = 0;      // allocated row capacity (>= max_n)
+    size_t bytes = 0;     // device bytes held
     int64_t total = 0;
     int32_t nwords = 0;
     int32_t* count = nullptr;
@@ -155,10 +174,11 @@ struct MixedState {
     uint32_t* pmask = nullptr;
     int ntab = 0;
     double h[3] = {0, 0, 0};
+    size_t bytes = 0;     // device bytes held
 };
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                   MixedState& m, cudaStream_t st, std::string& err);
-void free_mixed(MixedState& m);
+void free_mixed(MixedState& m, cudaStream_t st);
 int launch_split_u(const ParticleView& p, MixedState& m, cudaStream_t st);
 int launch_vv_initial_mixed(const ParticleView& p, double dt, MixedState& m,
                             cudaStream_t st);
@@ -173,7 +193,7 @@ int build_neighbor_list(const double* pos, const double* disp, int64_t n,
                         int64_t npad, int64_t begin, double cutoff,
                         const int32_t* user_id, bool with_mu,
                         NeighborList& out, cudaStream_t st, std::string& err);
-void free_neighbor_list(NeighborList& nl);
+void free_neighbor_list(NeighborList& nl, cudaStream_t st);
 
 // Layout kernels.
 int launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t npad,

@@ -481,11 +481,11 @@ int mixed_variant()
 
 }  // namespace
 
-void free_mixed(MixedState& m)
+void free_mixed(MixedState& m, cudaStream_t st)
 {
     void* ptrs[] = {m.xh, m.xl, m.uh, m.ul, m.code, m.table, m.warp_kind, m.pmask};
     for (void* q : ptrs)
-        if (q) cudaFree(q);
+        if (q) dev_free(q, st);
     m = MixedState{};
 }
 
@@ -493,16 +493,18 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                   MixedState& m, cudaStream_t st, std::string& err)
 {
     int launches = 0;
-    free_mixed(m);
+    free_mixed(m, st);
     const int64_t np = p.npad;
-    CPD_TRY(cudaMalloc(&m.xh, sizeof(float4) * np));
-    CPD_TRY(cudaMalloc(&m.xl, sizeof(float4) * np));
-    CPD_TRY(cudaMalloc(&m.uh, sizeof(float4) * np));
-    CPD_TRY(cudaMalloc(&m.ul, sizeof(float4) * np));
-    CPD_TRY(cudaMalloc(&m.table, sizeof(MixedStencil) * kMixedGeneric));
-    CPD_TRY(cudaMalloc(&m.code, (size_t)std::max(pd.max_n, 1) * np));
+    CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
+    CPD_TRY(dev_alloc(&m.xl, sizeof(float4) * np, st));
+    CPD_TRY(dev_alloc(&m.uh, sizeof(float4) * np, st));
+    CPD_TRY(dev_alloc(&m.ul, sizeof(float4) * np, st));
+    CPD_TRY(dev_alloc(&m.table, sizeof(MixedStencil) * kMixedGeneric, st));
+    CPD_TRY(dev_alloc(&m.code, (size_t)std::max(pd.max_n, 1) * np, st));
     const int64_t nwarps = (np + 31) / 32 + 8;
-    CPD_TRY(cudaMalloc(&m.warp_kind, nwarps));
+    CPD_TRY(dev_alloc(&m.warp_kind, nwarps, st));
+    m.bytes = 4 * sizeof(float4) * np + sizeof(MixedStencil) * kMixedGeneric +
+              (size_t)std::max(pd.max_n, 1) * np + nwarps;
     CPD_TRY(cudaMemsetAsync(m.warp_kind, 0, nwarps, st));
     CPD_TRY(cudaMemsetAsync(m.code, kMixedGeneric, (size_t)std::max(pd.max_n, 1) * np, st));
     k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, nullptr, nullptr, m.xh, m.xl);
@@ -511,14 +513,14 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
     const int64_t rows = p.n - p.frozen;
     if (rows > 0 && pd.max_n > 0) {
         unsigned long long* d_min = nullptr;
-        CPD_TRY(cudaMallocAsync(&d_min, 3 * sizeof(unsigned long long), st));
+        CPD_TRY(dev_alloc(&d_min, 3 * sizeof(unsigned long long), st));
         CPD_TRY(cudaMemsetAsync(d_min, 0x7f, 3 * sizeof(unsigned long long), st));
         k_min_spacing<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_min);
         launches++;
         unsigned long long hmin[3];
         CPD_TRY(cudaMemcpyAsync(hmin, d_min, sizeof(hmin), cudaMemcpyDeviceToHost, st));
         CPD_TRY(cudaStreamSynchronize(st));
-        CPD_TRY(cudaFreeAsync(d_min, st));
+        CPD_TRY(dev_free(d_min, st));
         double h[3];
         bool lattice = true;
         for (int d = 0; d < 3; ++d) {
@@ -557,8 +559,8 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
             if (lattice && !tab.empty()) {
                 int16_t* d_lut = nullptr;
                 unsigned long long* d_delta = nullptr;
-                CPD_TRY(cudaMallocAsync(&d_lut, sizeof(int16_t) * lut.size(), st));
-                CPD_TRY(cudaMallocAsync(&d_delta, sizeof(unsigned long long) * kMixedGeneric, st));
+                CPD_TRY(dev_alloc(&d_lut, sizeof(int16_t) * lut.size(), st));
+                CPD_TRY(dev_alloc(&d_delta, sizeof(unsigned long long) * kMixedGeneric, st));
                 CPD_TRY(cudaMemcpyAsync(d_lut, lut.data(), sizeof(int16_t) * lut.size(),
                                         cudaMemcpyHostToDevice, st));
                 CPD_TRY(cudaMemsetAsync(d_delta, 0xff, sizeof(unsigned long long) * kMixedGeneric, st));
@@ -581,12 +583,13 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                 CPD_TRY(cudaMemcpyAsync(m.table, tab.data(), sizeof(MixedStencil) * tab.size(),
                                         cudaMemcpyHostToDevice, st));
                 CPD_TRY(cudaStreamSynchronize(st));
-                CPD_TRY(cudaFreeAsync(d_lut, st));
-                CPD_TRY(cudaFreeAsync(d_delta, st));
+                CPD_TRY(dev_free(d_lut, st));
+                CPD_TRY(dev_free(d_delta, st));
                 m.ntab = (int)tab.size();
                 for (int d = 0; d < 3; ++d) m.h[d] = h[d];
                 const int nmask = (m.ntab + 31) / 32;
-                CPD_TRY(cudaMalloc(&m.pmask, sizeof(uint32_t) * nmask * np));
+                CPD_TRY(dev_alloc(&m.pmask, sizeof(uint32_t) * nmask * np, st));
+                m.bytes += sizeof(uint32_t) * nmask * np;
                 k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), m.code, m.ntab,
                                                                  m.pmask, m.warp_kind);
                 launches++;

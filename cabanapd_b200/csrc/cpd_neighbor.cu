@@ -288,11 +288,11 @@ __global__ void k_ell_to_rows(const int32_t* count, const int32_t* idx, const ui
 
 }  // namespace
 
-void free_neighbor_list(NeighborList& nl)
+void free_neighbor_list(NeighborList& nl, cudaStream_t st)
 {
-    if (nl.count) cudaFree(nl.count);
-    if (nl.idx) cudaFree(nl.idx);
-    if (nl.mu) cudaFree(nl.mu);
+    if (nl.count) dev_free(nl.count, st);
+    if (nl.idx) dev_free(nl.idx, st);
+    if (nl.mu) dev_free(nl.mu, st);
     nl = NeighborList{};
 }
 
@@ -305,7 +305,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     const double* pos = x;
     double* y = nullptr;
     if (disp) {
-        CPD_TRY(cudaMallocAsync(&y, sizeof(double) * 3 * npad, st));
+        CPD_TRY(dev_alloc(&y, sizeof(double) * 3 * npad, st));
         k_positions<<<blocks_for(n), kBlock, 0, st>>>(x, disp, y, n, npad);
         launches++;
         pos = y;
@@ -313,14 +313,14 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     // Bounding box.
     const int nb = blocks_for(n);
     double* d_part = nullptr;
-    CPD_TRY(cudaMallocAsync(&d_part, sizeof(double) * 6 * nb, st));
+    CPD_TRY(dev_alloc(&d_part, sizeof(double) * 6 * nb, st));
     k_bbox<<<nb, kBlock, 0, st>>>(pos, n, npad, d_part);
     launches++;
     std::vector<double> part(6 * (size_t)nb);
     CPD_TRY(cudaMemcpyAsync(part.data(), d_part, sizeof(double) * 6 * nb,
                             cudaMemcpyDeviceToHost, st));
     CPD_TRY(cudaStreamSynchronize(st));
-    CPD_TRY(cudaFreeAsync(d_part, st));
+    CPD_TRY(dev_free(d_part, st));
     double lo[3], hi[3];
     for (int d = 0; d < 3; d++) {
         lo[d] = part[d];
@@ -348,10 +348,10 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     const int64_t ncell = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
 
     int32_t *cellid = nullptr, *cell_count = nullptr, *cell_start = nullptr, *order = nullptr;
-    CPD_TRY(cudaMallocAsync(&cellid, sizeof(int32_t) * n, st));
-    CPD_TRY(cudaMallocAsync(&cell_count, sizeof(int32_t) * (ncell + 1), st));
-    CPD_TRY(cudaMallocAsync(&cell_start, sizeof(int32_t) * (ncell + 1), st));
-    CPD_TRY(cudaMallocAsync(&order, sizeof(int32_t) * n, st));
+    CPD_TRY(dev_alloc(&cellid, sizeof(int32_t) * n, st));
+    CPD_TRY(dev_alloc(&cell_count, sizeof(int32_t) * (ncell + 1), st));
+    CPD_TRY(dev_alloc(&cell_start, sizeof(int32_t) * (ncell + 1), st));
+    CPD_TRY(dev_alloc(&order, sizeof(int32_t) * n, st));
     CPD_TRY(cudaMemsetAsync(cell_count, 0, sizeof(int32_t) * (ncell + 1), st));
     k_cell_index<<<blocks_for(n), kBlock, 0, st>>>(pos, n, npad, g, cellid, cell_count);
     launches++;
@@ -359,7 +359,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     CPD_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cell_count, cell_start,
                                           (int)(ncell + 1), st));
     void* tmp = nullptr;
-    CPD_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+    CPD_TRY(dev_alloc(&tmp, tmp_bytes, st));
     CPD_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cell_count, cell_start,
                                           (int)(ncell + 1), st));
     launches++;
@@ -368,7 +368,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     launches++;
 
     // Row counts.
-    if (!out.count) CPD_TRY(cudaMalloc(&out.count, sizeof(int32_t) * npad));
+    if (!out.count) CPD_TRY(dev_alloc(&out.count, sizeof(int32_t) * npad, st));
     const double rsqr = cutoff * cutoff;
     k_count<<<blocks_for(npad), kBlock, 0, st>>>(pos, n, npad, begin, g, cell_start, order,
                                                  rsqr, out.count);
@@ -376,8 +376,8 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     const int nbc = blocks_for(npad);
     int32_t* d_bmax = nullptr;
     long long* d_bsum = nullptr;
-    CPD_TRY(cudaMallocAsync(&d_bmax, sizeof(int32_t) * nbc, st));
-    CPD_TRY(cudaMallocAsync(&d_bsum, sizeof(long long) * nbc, st));
+    CPD_TRY(dev_alloc(&d_bmax, sizeof(int32_t) * nbc, st));
+    CPD_TRY(dev_alloc(&d_bsum, sizeof(long long) * nbc, st));
     k_count_stats<<<nbc, kBlock, 0, st>>>(out.count, npad, d_bmax, d_bsum);
     launches++;
     std::vector<int32_t> bmax(nbc);
@@ -387,8 +387,8 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     CPD_TRY(cudaMemcpyAsync(bsum.data(), d_bsum, sizeof(long long) * nbc,
                             cudaMemcpyDeviceToHost, st));
     CPD_TRY(cudaStreamSynchronize(st));
-    CPD_TRY(cudaFreeAsync(d_bmax, st));
-    CPD_TRY(cudaFreeAsync(d_bsum, st));
+    CPD_TRY(dev_free(d_bmax, st));
+    CPD_TRY(dev_free(d_bsum, st));
     int32_t max_n = 0;
     long long total = 0;
     for (int b = 0; b < nbc; b++) {
@@ -397,15 +397,18 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     }
     // (Re)allocate the padded list when it grows.
     const int32_t cap = std::max(max_n, 1);
-    if (!out.idx || cap > out.max_n) {
-        if (out.idx) CPD_TRY(cudaFree(out.idx));
+    if (!out.idx || cap > out.cap) {
+        if (out.idx) CPD_TRY(dev_free(out.idx, st));
         out.idx = nullptr;
-        CPD_TRY(cudaMalloc(&out.idx, sizeof(int32_t) * (size_t)cap * npad));
+        CPD_TRY(dev_alloc(&out.idx, sizeof(int32_t) * (size_t)cap * npad, st));
+        out.cap = cap;
+        out.bytes = sizeof(int32_t) * (size_t)npad * (1 + (size_t)cap);
         if (with_mu) {
-            if (out.mu) CPD_TRY(cudaFree(out.mu));
+            if (out.mu) CPD_TRY(dev_free(out.mu, st));
             out.mu = nullptr;
             const int32_t nw = (cap + 31) / 32;
-            CPD_TRY(cudaMalloc(&out.mu, sizeof(uint32_t) * (size_t)nw * npad));
+            CPD_TRY(dev_alloc(&out.mu, sizeof(uint32_t) * (size_t)nw * npad, st));
+            out.bytes += sizeof(uint32_t) * (size_t)nw * npad;
         }
     }
     out.max_n = max_n;
@@ -422,12 +425,12 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
         launches++;
     }
     CPD_TRY(cudaGetLastError());
-    CPD_TRY(cudaFreeAsync(tmp, st));
-    CPD_TRY(cudaFreeAsync(cellid, st));
-    CPD_TRY(cudaFreeAsync(cell_count, st));
-    CPD_TRY(cudaFreeAsync(cell_start, st));
-    CPD_TRY(cudaFreeAsync(order, st));
-    if (y) CPD_TRY(cudaFreeAsync(y, st));
+    CPD_TRY(dev_free(tmp, st));
+    CPD_TRY(dev_free(cellid, st));
+    CPD_TRY(dev_free(cell_count, st));
+    CPD_TRY(dev_free(cell_start, st));
+    CPD_TRY(dev_free(order, st));
+    if (y) CPD_TRY(dev_free(y, st));
     return launches;
 }
 

@@ -372,3 +372,35 @@ def unit_cube(model, dx, s0, kind, K=1.0, G=0.5, G0=None, influence_type=None):
     if influence_type is not None:
         params["influence_type"] = influence_type
     return _problem("unit_cube", params, x, vol, u0=u0, dx=h)
+
+
+# ---------------------------------------------------------------------------
+# Served stream of independent jobs.
+
+def served_jobs(count=512, n_range=(1e3, 2e6), steps_range=(200, 2000), seed=20261203):
+    """Independent jobs for the job server: half PMB (alternately the
+    elastic-wave cube and the double-notched plate), half LPS (random-notch
+    box), particle counts log-uniform in n_range (grids keep each geometry's
+    aspect ratio), step counts uniform in steps_range, all seeded.
+    Returns a list of problem dicts (see setup())."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lo, hi = math.log(n_range[0]), math.log(n_range[1])
+    jobs = []
+    for k in range(count):
+        target = math.exp(rng.uniform(lo, hi))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        kind = ("wave", "plate", "lps", "lps")[k % 4]
+        if kind == "wave":
+            side = max(8, int(round(target ** (1.0 / 3.0))))
+            prob = elastic_wave_pmb(n=side, steps=steps)
+        elif kind == "plate":
+            a = max(16, int(round((target / (0.5 * 0.045)) ** (1.0 / 3.0))))
+            cells = (a, max(8, a // 2), max(1, int(round(0.045 * a))))
+            prob = plate_impact(num_cells=cells, steps=steps)
+        else:
+            a = max(30, int(round((target / (0.4 * 0.02)) ** (1.0 / 3.0))))
+            cells = (a, max(12, int(round(0.4 * a))), max(1, int(round(0.02 * a))))
+            prob = lps_random_notches(num_cells=cells, steps=steps, seed=seed + k)
+        prob["kind"] = kind
+        jobs.append(prob)
+    return jobs

@@ -51,6 +51,52 @@ class CpdError(RuntimeError):
     pass
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_active", ctypes.c_int32),
+        ("steps_per_launch", ctypes.c_int32),
+        ("use_graphs", ctypes.c_int32),
+        ("hbm_budget_bytes", ctypes.c_uint64),
+    ]
+
+
+class JobStatus(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("steps_done", ctypes.c_int32),
+        ("priority", ctypes.c_int32),
+        ("n", ctypes.c_int64),
+        ("bonds", ctypes.c_int64),
+        ("device_bytes", ctypes.c_uint64),
+        ("submit_time", ctypes.c_double),
+        ("admit_time", ctypes.c_double),
+        ("start_time", ctypes.c_double),
+        ("finish_time", ctypes.c_double),
+        ("total_strain_energy", ctypes.c_double),
+        ("total_damage", ctypes.c_double),
+        ("kernel_launches", ctypes.c_int64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64),
+        ("done", ctypes.c_int64),
+        ("failed", ctypes.c_int64),
+        ("resident", ctypes.c_int64),
+        ("queued", ctypes.c_int64),
+        ("resident_bytes", ctypes.c_uint64),
+        ("peak_resident_bytes", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_int64),
+        ("bond_updates", ctypes.c_double),
+    ]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
 # Every symbol the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -89,6 +135,25 @@ SIGNATURES = {
     "cpd_set_kernel_timing": (_I32, [_P, _I32]),
     "cpd_kernel_time": (_I32, [_P, _DP, ctypes.POINTER(_I64), _DP]),
     "cpd_kernel_launches": (_I64, [_P]),
+    "cpd_device_bytes": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "cpd_job_create": (_I32, [ctypes.POINTER(CpdParams), _I32, ctypes.POINTER(_P)]),
+    "cpd_job_destroy": (_I32, [_P]),
+    "cpd_job_set_particles": (_I32, [_P, _I64, _I64, _P, _P, _P, _P, _P]),
+    "cpd_job_set_state": (_I32, [_P, _P, _P]),
+    "cpd_job_prenotch": (_I32, [_P, _I32, _P, _P, _P]),
+    "cpd_job_add_boundary_condition": (_I32, [_P, _I32, _I32, _I64, _P, _P]),
+    "cpd_job_keep_fields": (_I32, [_P, ctypes.c_uint32]),
+    "cpd_server_create": (_I32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    "cpd_server_destroy": (_I32, [_P]),
+    "cpd_server_submit": (_I32, [_P, _P, ctypes.POINTER(_I64)]),
+    "cpd_server_clock": (_D, [_P]),
+    "cpd_server_wait": (_I32, [_P, _I64, _D]),
+    "cpd_server_drain": (_I32, [_P, _D]),
+    "cpd_server_job_status": (_I32, [_P, _I64, ctypes.POINTER(JobStatus)]),
+    "cpd_server_job_error": (_I32, [_P, _I64, ctypes.c_char_p, _I64]),
+    "cpd_server_download": (_I32, [_P, _I64, _I32, _P]),
+    "cpd_server_release": (_I32, [_P, _I64]),
+    "cpd_server_stats_get": (_I32, [_P, ctypes.POINTER(ServerStats)]),
 }
 
 
@@ -122,14 +187,7 @@ class System:
 
     def __init__(self, params, device=0, precision=FP64_EXACT, ordering=ORDER_INPUT):
         lib = load()
-        p = CpdParams()
-        p.influence_type = -1
-        for k, _ in CpdParams._fields_:
-            if k in params:
-                setattr(p, k, params[k])
-        p.precision = params.get("precision", precision)
-        p.ordering = params.get("ordering", ordering)
-        p.device = params.get("device", device)
+        p = _params_struct(params, precision, ordering, device)
         self._lib = lib
         h = _P()
         self._check(lib.cpd_system_create(ctypes.byref(p), ctypes.byref(h)))
@@ -281,3 +339,129 @@ class System:
 
     def kernel_launches(self):
         return self._lib.cpd_kernel_launches(self._h)
+
+
+def _params_struct(params, precision=FP64_EXACT, ordering=ORDER_INPUT, device=0):
+    p = CpdParams()
+    p.influence_type = -1
+    for k, _ in CpdParams._fields_:
+        if k in params:
+            setattr(p, k, params[k])
+    p.precision = params.get("precision", precision)
+    p.ordering = params.get("ordering", ordering)
+    p.device = params.get("device", device)
+    return p
+
+
+class Server:
+    """Job server (cpd_server): continuous batching of independent
+    simulations on one GPU with admission against a device-memory budget.
+
+    submit() takes a problem dict as built by cabanapd_b200.problems
+    (params, x, vol, rho, nofail, radius, u0, v0, notches, bcs, num_steps)
+    and returns a job id; results stay on the host until release()."""
+
+    def __init__(self, device=0, max_active=16, steps_per_launch=32, use_graphs=True,
+                 hbm_budget_bytes=150 * 10**9):
+        lib = load()
+        self._lib = lib
+        cfg = ServerConfig(device, max_active, steps_per_launch, 1 if use_graphs else 0,
+                           int(hbm_budget_bytes))
+        h = _P()
+        self._check(lib.cpd_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._n = {}
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CpdError(f"cabanapd_b200 error {rc}: {self._lib.cpd_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cpd_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clock(self):
+        return self._lib.cpd_server_clock(self._h)
+
+    def submit(self, prob, precision=FP64_EXACT, keep=("u",)):
+        lib = self._lib
+        p = _params_struct(prob["params"], precision=precision)
+        job = _P()
+        self._check(lib.cpd_job_create(ctypes.byref(p), int(prob["num_steps"]), ctypes.byref(job)))
+        submitted = False
+        try:
+            x = np.ascontiguousarray(prob["x"], dtype=np.float64).reshape(-1, 3)
+            vol = np.ascontiguousarray(prob["vol"], dtype=np.float64)
+            arrays = {}
+            for key, dt in (("rho", np.float64), ("nofail", np.int32), ("radius", np.float64)):
+                arrays[key] = (None if prob.get(key) is None
+                               else np.ascontiguousarray(prob[key], dtype=dt))
+            self._check(lib.cpd_job_set_particles(
+                job, x.shape[0], int(prob.get("n_frozen", 0)), _ptr(x), _ptr(vol),
+                _ptr(arrays["rho"]), _ptr(arrays["nofail"]), _ptr(arrays["radius"])))
+            u0, v0 = prob.get("u0"), prob.get("v0")
+            if u0 is not None or v0 is not None:
+                u0 = None if u0 is None else np.ascontiguousarray(u0, dtype=np.float64)
+                v0 = None if v0 is None else np.ascontiguousarray(v0, dtype=np.float64)
+                self._check(lib.cpd_job_set_state(job, _ptr(u0), _ptr(v0)))
+            if prob.get("notches") is not None:
+                v1, v2, p0 = (np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 3)
+                              for a in prob["notches"])
+                self._check(lib.cpd_job_prenotch(job, v1.shape[0], _ptr(v1), _ptr(v2), _ptr(p0)))
+            for kind, comp, idx, vals in prob.get("bcs", []):
+                idx = np.ascontiguousarray(idx, dtype=np.int64)
+                vals = np.ascontiguousarray(np.atleast_1d(vals), dtype=np.float64)
+                self._check(lib.cpd_job_add_boundary_condition(
+                    job, int(kind), int(comp), idx.shape[0], _ptr(idx), _ptr(vals)))
+            mask = 0
+            for f in keep:
+                mask |= 1 << FIELDS[f]
+            self._check(lib.cpd_job_keep_fields(job, mask))
+            jid = _I64()
+            submitted = True
+            self._check(lib.cpd_server_submit(self._h, job, ctypes.byref(jid)))
+        finally:
+            if not submitted:
+                lib.cpd_job_destroy(job)
+        self._n[jid.value] = x.shape[0]
+        return jid.value
+
+    def wait(self, job_id, timeout=600.0):
+        self._check(self._lib.cpd_server_wait(self._h, int(job_id), float(timeout)))
+        return self.status(job_id)
+
+    def drain(self, timeout=3600.0):
+        self._check(self._lib.cpd_server_drain(self._h, float(timeout)))
+
+    def status(self, job_id):
+        st = JobStatus()
+        self._check(self._lib.cpd_server_job_status(self._h, int(job_id), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in JobStatus._fields_}
+
+    def error(self, job_id):
+        buf = ctypes.create_string_buffer(1024)
+        self._check(self._lib.cpd_server_job_error(self._h, int(job_id), buf, 1024))
+        return buf.value.decode()
+
+    def get(self, job_id, field):
+        n = self._n[job_id]
+        out = np.empty((n, 3) if field in VECTOR_FIELDS else (n,), dtype=np.float64)
+        self._check(self._lib.cpd_server_download(self._h, int(job_id), FIELDS[field],
+                                                  out.ctypes.data))
+        return out
+
+    def release(self, job_id):
+        self._check(self._lib.cpd_server_release(self._h, int(job_id)))
+        self._n.pop(job_id, None)
+
+    def stats(self):
+        st = ServerStats()
+        self._check(self._lib.cpd_server_stats_get(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}

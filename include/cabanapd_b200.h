@@ -266,6 +266,94 @@ cpd_status cpd_kernel_time(cpd_system* sys, double* total_ms,
                            int64_t* launches, double* bytes_per_launch);
 /* Number of kernels this library launched on the system since creation. */
 int64_t cpd_kernel_launches(const cpd_system* sys);
+/* No counterpart in the reference. Device bytes the system holds (particle
+ * fields, neighbour and contact lists, mixed-precision copies, boundary
+ * lists), for admission against a memory budget. */
+cpd_status cpd_device_bytes(const cpd_system* sys, uint64_t* bytes);
+
+/* ===========================================================================
+ * Job server. No counterpart in the reference, which runs one simulation per
+ * process. Continuous batching of independent simulations on one GPU: jobs
+ * are described on the host (cpd_job_*: the same inputs as a cpd_system),
+ * submitted at any time, admitted in arrival order while the device bytes of
+ * the resident jobs stay within a budget, advanced concurrently (each on its
+ * own CUDA stream, in k-step chunks replayed from a CUDA graph, jobs with less
+ * work on higher-priority streams) and retired when done; their totals and
+ * the fields asked for stay on the host until released. A job's results do
+ * not depend on what else runs: it owns its arrays and stream, and every
+ * kernel is deterministic. Thread-safe: any host thread may submit, wait,
+ * query, download or release while the server's two threads run the jobs.
+ * Contact (DEM) jobs run too, without graphs (their neighbour rebuilds are
+ * decided on the host between steps).
+ */
+typedef struct cpd_job cpd_job;
+typedef struct cpd_server cpd_server;
+
+enum { CPD_JOB_QUEUED = 0, CPD_JOB_RUNNING = 1, CPD_JOB_DONE = 2, CPD_JOB_FAILED = 3 };
+
+typedef struct cpd_server_config {
+    int32_t device;
+    int32_t max_active;         /* resident jobs at once (one stream each) */
+    int32_t steps_per_launch;   /* k: steps per launched chunk */
+    int32_t use_graphs;         /* 1: replay the k-step chunk as a CUDA graph */
+    uint64_t hbm_budget_bytes;  /* admission budget on resident device bytes */
+} cpd_server_config;
+
+typedef struct cpd_job_status {
+    int32_t state;              /* CPD_JOB_* */
+    int32_t steps;              /* requested */
+    int32_t steps_done;
+    int32_t priority;           /* CUDA stream priority of the job */
+    int64_t n;                  /* particles */
+    int64_t bonds;              /* directed neighbour entries at admission */
+    uint64_t device_bytes;      /* held while resident */
+    double submit_time, admit_time, start_time, finish_time; /* server clock, s */
+    double total_strain_energy, total_damage;                 /* at the end */
+    int64_t kernel_launches;    /* kernels run (graph replays count each node) */
+} cpd_job_status;
+
+typedef struct cpd_server_stats {
+    int64_t submitted, done, failed, resident, queued;
+    uint64_t resident_bytes, peak_resident_bytes;
+    int64_t kernel_launches;
+    double bond_updates;        /* sum over finished jobs of bonds x steps */
+} cpd_server_stats;
+
+cpd_status cpd_job_create(const cpd_params* params, int32_t num_steps, cpd_job** out);
+/* Only for a job that was never submitted (submission takes ownership). */
+cpd_status cpd_job_destroy(cpd_job* job);
+cpd_status cpd_job_set_particles(cpd_job* job, int64_t n, int64_t n_frozen, const double* x,
+                                 const double* vol, const double* rho, const int32_t* nofail,
+                                 const double* radius);
+cpd_status cpd_job_set_state(cpd_job* job, const double* u, const double* v);
+cpd_status cpd_job_prenotch(cpd_job* job, int32_t count, const double* v1, const double* v2,
+                            const double* p0);
+cpd_status cpd_job_add_boundary_condition(cpd_job* job, int32_t kind, int32_t component,
+                                          int64_t count, const int64_t* indices,
+                                          const double* values);
+/* Fields (bit 1 << CPD_FIELD_*) copied to the host when the job finishes;
+ * default: U only. */
+cpd_status cpd_job_keep_fields(cpd_job* job, uint32_t field_mask);
+
+cpd_status cpd_server_create(const cpd_server_config* config, cpd_server** out);
+/* Fails queued jobs, lets resident ones finish, then stops the threads. */
+cpd_status cpd_server_destroy(cpd_server* server);
+/* Takes ownership of job, also when it returns an error. */
+cpd_status cpd_server_submit(cpd_server* server, cpd_job* job, int64_t* job_id);
+/* Seconds since the server was created (the clock of cpd_job_status). */
+double cpd_server_clock(const cpd_server* server);
+/* Block until the job is DONE or FAILED; CPD_ERR_STATE after timeout_s. */
+cpd_status cpd_server_wait(cpd_server* server, int64_t job_id, double timeout_s);
+/* Block until every submitted job is DONE or FAILED. */
+cpd_status cpd_server_drain(cpd_server* server, double timeout_s);
+cpd_status cpd_server_job_status(cpd_server* server, int64_t job_id, cpd_job_status* out);
+/* Error message of a FAILED job (empty otherwise), NUL-terminated. */
+cpd_status cpd_server_job_error(cpd_server* server, int64_t job_id, char* buf, int64_t size);
+/* A kept field of a DONE job, in the caller's particle order. */
+cpd_status cpd_server_download(cpd_server* server, int64_t job_id, int32_t field,
+                               double* host_out);
+cpd_status cpd_server_release(cpd_server* server, int64_t job_id);
+cpd_status cpd_server_stats_get(cpd_server* server, cpd_server_stats* out);
 
 #ifdef __cplusplus
 }
