@@ -13,6 +13,12 @@ headline `value`; the plain FP64 path runs the same steps from the same
 start and is reported beside it (`plain_fp64`, `mixed_vs_plain`), with the
 per-field error of mixed vs FP64 (`mixed_error_vs_fp64`).
 
+`serving` (N = 1): a served stream of independent PMB/LPS jobs through the
+job server (continuous batching, mixed precision): capacity from a
+saturated pass, then Poisson arrivals at 0.8 x capacity with p50/p99 job
+latency, beside the same jobs run one at a time on the plain FP64 path
+(--serve-jobs 512 --serve-n 1e3 2e6 for the full 512-job stream).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 N > 1 (torchrun, one rank per GPU): every rank advances its own plate
@@ -382,10 +388,117 @@ def run_gpu(args, world, rank, local, pg):
         line["plain_fp64"] = plain
         line["mixed_vs_plain"] = value / plain["value"]
         line["mixed_error_vs_fp64"] = err
+    if world == 1 and not args.skip_serve:
+        line["serving"] = run_serving(args, device)
     if world == 1 and not args.skip_cpu:
         line["cpu_baseline"] = time_cpu_sample()
         line["cpu_baseline"].pop("steps", None)
     print(json.dumps(line), flush=True)
+
+
+def _percentile(values, q):
+    v = sorted(values)
+    if not v:
+        return None
+    k = (len(v) - 1) * q
+    lo, hi = int(math.floor(k)), int(math.ceil(k))
+    return v[lo] + (v[hi] - v[lo]) * (k - lo)
+
+
+def _latency_summary(lat):
+    return {"p50": _percentile(lat, 0.50), "p99": _percentile(lat, 0.99),
+            "mean": sum(lat) / len(lat), "max": max(lat)}
+
+
+def run_serving(args, device):
+    """Served stream: independent PMB/LPS jobs through the job server
+    (mixed precision), beside the same jobs run one at a time on the plain
+    FP64 path. Three passes over the same seeded jobs:
+    1. saturated: all jobs submitted at t = 0; capacity = jobs / makespan;
+    2. served: Poisson arrivals at 0.8 x capacity (seeded), latency =
+       finish - arrival for every job;
+    3. one at a time, plain FP64: each job alone (set-up, steps, energy,
+       u read back), timed; its FIFO latencies under the same arrivals
+       follow from those measured service times (a single server that takes
+       jobs in order: start = max(arrival, previous finish))."""
+    import cabanapd_b200
+    n_lo, n_hi = args.serve_n
+    jobs = P.served_jobs(count=args.serve_jobs, n_range=(n_lo, n_hi),
+                         steps_range=tuple(args.serve_steps), seed=args.serve_seed)
+    budget = int(args.serve_budget_gb * 1e9)
+
+    def serve(arrivals):
+        srv = cabanapd_b200.Server(device=device, max_active=args.serve_active,
+                                   steps_per_launch=args.serve_k, hbm_budget_bytes=budget)
+        ids = []
+        t0 = time.perf_counter()
+        for prob, at in zip(jobs, arrivals):
+            delay = at - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(prob, precision=PRECISION["mixed"]))
+        srv.drain(timeout=7200)
+        sts = [srv.status(i) for i in ids]
+        stats = srv.stats()
+        srv.close()
+        failed = [i for i, st in zip(ids, sts) if st["state"] != cabanapd_b200.system.JOB_DONE]
+        if failed:
+            raise RuntimeError(f"serving: {len(failed)} jobs failed")
+        first = min(st["submit_time"] for st in sts)
+        span = max(st["finish_time"] for st in sts) - first
+        bonds = sum(st["bonds"] * st["steps"] for st in sts)
+        lat = [st["finish_time"] - st["submit_time"] for st in sts]
+        wait = [st["start_time"] - st["submit_time"] for st in sts]
+        return {"makespan_s": span, "bond_updates": bonds,
+                "throughput_bond_updates_per_s": bonds / span,
+                "jobs_per_s": len(sts) / span, "latency_s": _latency_summary(lat),
+                "queue_wait_s": _latency_summary(wait),
+                "peak_resident_bytes": stats["peak_resident_bytes"],
+                "gpu_launches": stats["kernel_launches"]}
+
+    saturated = serve([0.0] * len(jobs))
+    capacity = saturated["jobs_per_s"]
+    rate = 0.8 * capacity
+    rng = np.random.Generator(np.random.PCG64(args.serve_seed + 1))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs))).tolist()
+    served = serve(arrivals)
+
+    service, bonds_total = [], 0
+    for prob in jobs:
+        t0 = time.perf_counter()
+        s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION["fp64"]))
+        P.setup(s, prob)
+        s.run(prob["num_steps"])
+        s.compute_energy()
+        s.get("u")
+        service.append(time.perf_counter() - t0)
+        bonds_total += s.neighbor_stats()[1] * prob["num_steps"]
+        s.close()
+    finish, lat = 0.0, []
+    for at, sv in zip(arrivals, service):
+        finish = max(at, finish) + sv
+        lat.append(finish - at)
+    one_at_a_time = {"service_time_sum_s": sum(service),
+                     "throughput_bond_updates_per_s": bonds_total / sum(service),
+                     "latency_s": _latency_summary(lat)}
+    kinds = {k: sum(1 for j in jobs if j["kind"] == k) for k in ("wave", "plate", "lps")}
+    return {
+        "workload": (f"{len(jobs)} independent jobs: {kinds['wave']} PMB elastic-wave cubes, "
+                     f"{kinds['plate']} PMB notched plates, {kinds['lps']} LPS random-notch "
+                     f"boxes; particles log-uniform in [{n_lo:.0f}, {n_hi:.0f}], steps "
+                     f"uniform in [{args.serve_steps[0]}, {args.serve_steps[1]}], seed "
+                     f"{args.serve_seed}"),
+        "precision": "mixed (PMB: FP32 bonds / FP64 state; LPS: FP64 kernels)",
+        "server": {"max_active": args.serve_active, "steps_per_launch": args.serve_k,
+                   "cuda_graphs": True, "hbm_budget_bytes": budget},
+        "capacity_jobs_per_s": capacity,
+        "saturated": saturated,
+        "arrival_rate_jobs_per_s": rate,
+        "served": served,
+        "one_at_a_time_fp64": one_at_a_time,
+        "throughput_vs_one_at_a_time": (served["throughput_bond_updates_per_s"] /
+                                        one_at_a_time["throughput_bond_updates_per_s"]),
+    }
 
 
 def run_e2e(args, prob, device, stream, pg, total_bonds, prec):
@@ -458,6 +571,16 @@ def main():
                     help="with mixed: skip the plain FP64 comparison run")
     ap.add_argument("--cells", default=None,
                     help="plate cells nx,ny,nz (profiling on a smaller plate)")
+    ap.add_argument("--skip-serve", action="store_true", help="omit the served-stream leg")
+    ap.add_argument("--serve-jobs", type=int, default=96,
+                    help="served stream: number of jobs (512 for the full stream)")
+    ap.add_argument("--serve-n", type=float, nargs=2, default=[1e3, 2e5],
+                    help="served stream: particle-count range (1e3 2e6 for the full stream)")
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[200, 2000])
+    ap.add_argument("--serve-seed", type=int, default=20261203)
+    ap.add_argument("--serve-active", type=int, default=16)
+    ap.add_argument("--serve-k", type=int, default=32, help="steps per CUDA-graph chunk")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
