@@ -429,7 +429,8 @@ def run_serving(args, device):
 
     def serve(arrivals):
         srv = cabanapd_b200.Server(device=device, max_active=args.serve_active,
-                                   steps_per_launch=args.serve_k, hbm_budget_bytes=budget)
+                                   steps_per_launch=args.serve_k, hbm_budget_bytes=budget,
+                                   setup_threads=args.serve_setup_threads)
         ids = []
         t0 = time.perf_counter()
         for prob, at in zip(jobs, arrivals):
@@ -449,10 +450,12 @@ def run_serving(args, device):
         bonds = sum(st["bonds"] * st["steps"] for st in sts)
         lat = [st["finish_time"] - st["submit_time"] for st in sts]
         wait = [st["start_time"] - st["submit_time"] for st in sts]
+        setup = [st["ready_time"] - st["admit_time"] for st in sts]
         return {"makespan_s": span, "bond_updates": bonds,
                 "throughput_bond_updates_per_s": bonds / span,
                 "jobs_per_s": len(sts) / span, "latency_s": _latency_summary(lat),
                 "queue_wait_s": _latency_summary(wait),
+                "setup_s": dict(_latency_summary(setup), total=sum(setup)),
                 "peak_resident_bytes": stats["peak_resident_bytes"],
                 "gpu_launches": stats["kernel_launches"]}
 
@@ -490,6 +493,7 @@ def run_serving(args, device):
                      f"{args.serve_seed}"),
         "precision": "mixed (PMB: FP32 bonds / FP64 state; LPS: FP64 kernels)",
         "server": {"max_active": args.serve_active, "steps_per_launch": args.serve_k,
+                   "setup_threads": args.serve_setup_threads,
                    "cuda_graphs": True, "hbm_budget_bytes": budget},
         "capacity_jobs_per_s": capacity,
         "saturated": saturated,
@@ -581,6 +585,7 @@ def main():
     ap.add_argument("--serve-active", type=int, default=16)
     ap.add_argument("--serve-k", type=int, default=32, help="steps per CUDA-graph chunk")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-setup-threads", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

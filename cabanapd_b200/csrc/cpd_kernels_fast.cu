@@ -338,6 +338,138 @@ __global__ void __launch_bounds__(kBlock)
     p.f[2 * np + i] = fz;
 }
 
+// Neighbour indices of one ELL row read PF bonds ahead of use (a shift
+// register), so the index load of bond k + PF overlaps the work of bond k.
+template <int PF>
+struct IndexStream {
+    const int32_t* __restrict__ idx;
+    int64_t np;
+    int cnt;
+    int32_t q[PF];
+    __device__ __forceinline__ IndexStream(const int32_t* row, int64_t stride, int count)
+        : idx(row), np(stride), cnt(count)
+    {
+#pragma unroll
+        for (int a = 0; a < PF; ++a) q[a] = a < cnt ? __ldg(idx + (int64_t)a * np) : 0;
+    }
+    // Index of bond k (called for k = 0, 1, ... in order).
+    __device__ __forceinline__ int64_t next(int k)
+    {
+        const int64_t j = q[0];
+#pragma unroll
+        for (int a = 0; a + 1 < PF; ++a) q[a] = q[a + 1];
+        q[PF - 1] = (k + PF < cnt) ? __ldg(idx + (int64_t)(k + PF) * np) : 0;
+        return j;
+    }
+};
+
+// LPS weighted volume and dilatation in ONE pass over the row
+// (force/CabanaPD_LPS.hpp:89-141, :287-378): both sums accumulate per bond,
+// theta_i = 3 sum(omega s xi^2 vol_j) / m_i at the end (the reference divides
+// each term by m_i; the factored division differs by rounding only). With
+// WITH_M false, m_i is read (the elastic model computes it once).
+template <int INFL, bool FRACTURE, bool WITH_M>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_m_theta_1pass(ParticleView p, EllView nl, FastModel md)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+    const int cnt = nl.count[i];
+    IndexStream<2> js(nl.idx + i, np, cnt);
+    double mi = WITH_M ? 0.0 : p.m[i];
+    double th = 0.0;
+    uint32_t word = 0;
+    for (int k = 0; k < cnt; ++k) {
+        if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+        const int64_t j = js.next(k);
+        if (FRACTURE && !((word >> (k & 31)) & 1u)) continue;
+        Bond b;
+        bond_fast(p.x, p.u, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+        const double vol_j = __ldg(p.vol + j);
+        // omega xi^2 (force_models/CabanaPD_LPS.hpp:100-106)
+        const double w = INFL == 1 ? b.xi : b.xi * b.xi;
+        if (WITH_M) mi = fma(w, vol_j, mi);
+        // omega s xi^2 vol_j (force_models/CabanaPD_LPS.hpp:108-116)
+        th = fma(w * b.s, vol_j, th);
+    }
+    if (WITH_M) p.m[i] = mi;
+    th = (!FRACTURE || mi > 0) ? 3.0 * th / mi : 0.0;
+    p.theta[i] = th;
+    p.lps_a[i] = md.theta_coeff * th / mi;
+    p.lps_b[i] = md.s_coeff / mi;
+}
+
+// LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447) with the row's
+// indices streamed two bonds ahead, compiled for 4 blocks of 256 per SM.
+template <int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_force_pf(ParticleView p, EllView nl, FastModel md)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+    const double a_i = p.lps_a[i], b_i = p.lps_b[i];
+    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
+    const int cnt = nl.count[i];
+    IndexStream<2> js(nl.idx + i, np, cnt);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    uint32_t word = 0;
+    bool dirty = false;
+    for (int k = 0; k < cnt; ++k) {
+        if (FRACTURE && (k & 31) == 0) {
+            if (dirty) nl.mu[(int64_t)((k >> 5) - 1) * np + i] = word;
+            dirty = false;
+            word = nl.mu[(int64_t)(k >> 5) * np + i];
+        }
+        const int64_t j = js.next(k);
+        Bond b;
+        bond_fast(p.x, p.u, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
+        bool intact = true;
+        if (FRACTURE) {
+            // nofail(i) tested twice by the reference (force/CabanaPD_LPS.hpp:417-418).
+            const uint32_t bit = 1u << (k & 31);
+            if (!nofail_i && critical_fast(b, md.bond_break_coeff)) {
+                if (word & bit) {
+                    word &= ~bit;
+                    dirty = true;
+                }
+                intact = false;
+            } else {
+                intact = (word & bit) != 0;
+            }
+        }
+        if (intact) {
+            const double a_j = __ldg(p.lps_a + j), b_j = __ldg(p.lps_b + j);
+            const double oxi = INFL == 1 ? 1.0 : b.xi;
+            const double kf = (a_i + a_j + b.s * (b_i + b_j)) * oxi * __ldg(p.vol + j) * b.rinv;
+            fx = fma(kf, b.rx, fx);
+            fy = fma(kf, b.ry, fy);
+            fz = fma(kf, b.rz, fz);
+        }
+    }
+    if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
+    p.f[i] = fx;
+    p.f[np + i] = fy;
+    p.f[2 * np + i] = fz;
+}
+
+// LPS kernel form, from CPD_LPS_VARIANT: 0 two-pass m / theta and plain
+// loops; 1 (default) one-pass m / theta, index streaming, 4 blocks per SM.
+int lps_variant()
+{
+    static int v = [] {
+        const char* e = getenv("CPD_LPS_VARIANT");
+        const int x = e ? atoi(e) : 1;
+        return (x < 0 || x > 1) ? 1 : x;
+    }();
+    return v;
+}
+
 // Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-5):
 // 0 no prefetch, 1 indices 2 bonds ahead, 2 indices 4 ahead, 3 / 4 the same
 // plus neighbour gathers one bond ahead, 5 = 1 compiled for 4 blocks of 256
@@ -388,6 +520,18 @@ int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& 
         case 105: k_pmb_force_fast<false, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
         }
+    } else if (lps_variant() == 1) {
+        if (md.influence == 1) {
+            if (md.fracture)
+                k_lps_force_pf<1, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+            else
+                k_lps_force_pf<1, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+        } else {
+            if (md.fracture)
+                k_lps_force_pf<0, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+            else
+                k_lps_force_pf<0, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+        }
     } else {
         if (md.influence == 1) {
             if (md.fracture)
@@ -411,7 +555,13 @@ int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Mode
     if (rows <= 0) return 0;
     const int g = blocks_for(rows);
     const FastModel fm = to_fast(md);
-#define CPD_MT(I, F, W) k_lps_m_theta_fast<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm)
+#define CPD_MT(I, F, W)                                                          \
+    do {                                                                         \
+        if (lps_variant() == 1)                                                  \
+            k_lps_m_theta_1pass<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm);       \
+        else                                                                     \
+            k_lps_m_theta_fast<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm);        \
+    } while (0)
     if (md.influence == 1) {
         if (md.fracture) {
             if (with_m) CPD_MT(1, true, true); else CPD_MT(1, true, false);

@@ -4,7 +4,8 @@
 // A job is a host-side description (the same calls that set up a cpd_system:
 // particles, state, pre-notches, boundary conditions, step count). The server
 // runs two threads:
-//   worker   -- admits queued jobs in arrival order while the device bytes of
+//   workers  -- (setup_threads of them) admit queued jobs in arrival order
+//               while the device bytes of
 //               the resident jobs stay within the budget (builds the job's
 //               system on its own stream, captures its k-step chunk as a
 //               CUDA graph), and retires finished jobs (energy, result
@@ -89,7 +90,7 @@ struct Job {
     int64_t n = 0, bonds = 0;
     uint64_t est_bytes = 0, bytes = 0;
     int32_t priority = 0;
-    double t_submit = 0, t_admit = 0, t_finish = 0;
+    double t_submit = 0, t_admit = 0, t_ready = 0, t_finish = 0;
     std::atomic<double> t_start{-1.0};
     double W = 0, D = 0;
     bool contact = false;
@@ -166,7 +167,8 @@ struct cpd_server {
     int64_t n_submitted = 0, n_done = 0, n_failed = 0, launches = 0;
     double bond_updates = 0;
 
-    std::thread worker, launcher;
+    std::vector<std::thread> workers;
+    std::thread launcher;
 
     double now() const
     {
@@ -374,9 +376,10 @@ struct cpd_server {
                 resident_bytes += std::max(j->bytes, j->est_bytes) - j->est_bytes;
                 peak_bytes = std::max(peak_bytes, resident_bytes);
                 j->state = CPD_JOB_RUNNING;
+                j->t_ready = now();
                 admitted.push_back(j);
                 cv_launcher.notify_one();
-                // Let the launcher start it before setting up the next one.
+                // Retire finished jobs before setting up the next one.
                 if (!retire.empty()) break;
             }
         }
@@ -425,7 +428,9 @@ struct cpd_server {
                                          [&] { return stopping || !admitted.empty(); });
                 for (Job* j : admitted) running.push_back(j);
                 admitted.clear();
-                if (stopping && running.empty() && resident == 0 && queue.empty()) break;
+                if (stopping && running.empty() && resident == 0 && queue.empty() &&
+                    admitted.empty())
+                    break;
             }
             bool progressed = false;
             std::vector<Job*> finished, failed;
@@ -567,7 +572,8 @@ cpd_status cpd_server_create(const cpd_server_config* cfg, cpd_server** out)
 {
     if (!cfg || !out) return fail(CPD_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
-    if (cfg->max_active < 1 || cfg->steps_per_launch < 1 || cfg->hbm_budget_bytes == 0)
+    if (cfg->max_active < 1 || cfg->steps_per_launch < 1 || cfg->hbm_budget_bytes == 0 ||
+        cfg->setup_threads < 0)
         return fail(CPD_ERR_INVALID_ARGUMENT,
                     "max_active, steps_per_launch and hbm_budget_bytes must be positive");
     int ndev = 0;
@@ -581,7 +587,9 @@ cpd_status cpd_server_create(const cpd_server_config* cfg, cpd_server** out)
     s->t0 = std::chrono::steady_clock::now();
     cudaSetDevice(cfg->device);
     cudaDeviceGetStreamPriorityRange(&s->prio_least, &s->prio_greatest);
-    s->worker = std::thread([p = s.get()] { p->worker_loop(); });
+    if (s->cfg.setup_threads == 0) s->cfg.setup_threads = 4;
+    for (int w = 0; w < s->cfg.setup_threads; w++)
+        s->workers.emplace_back([p = s.get()] { p->worker_loop(); });
     s->launcher = std::thread([p = s.get()] { p->launcher_loop(); });
     *out = s.release();
     return CPD_OK;
@@ -597,7 +605,7 @@ cpd_status cpd_server_destroy(cpd_server* s)
     }
     s->cv_worker.notify_all();
     s->cv_launcher.notify_all();
-    s->worker.join();
+    for (auto& w : s->workers) w.join();
     s->launcher.join();
     delete s;
     return CPD_OK;
@@ -668,6 +676,7 @@ cpd_status cpd_server_job_status(cpd_server* s, int64_t id, cpd_job_status* out)
     st.device_bytes = std::max(j.bytes, j.est_bytes);
     st.submit_time = j.t_submit;
     st.admit_time = j.t_admit;
+    st.ready_time = j.t_ready;
     st.start_time = j.t_start;
     st.finish_time = j.t_finish;
     st.total_strain_energy = j.W;

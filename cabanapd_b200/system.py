@@ -58,6 +58,8 @@ class ServerConfig(ctypes.Structure):
         ("steps_per_launch", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
         ("hbm_budget_bytes", ctypes.c_uint64),
+        ("setup_threads", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -72,6 +74,7 @@ class JobStatus(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64),
         ("submit_time", ctypes.c_double),
         ("admit_time", ctypes.c_double),
+        ("ready_time", ctypes.c_double),
         ("start_time", ctypes.c_double),
         ("finish_time", ctypes.c_double),
         ("total_strain_energy", ctypes.c_double),
@@ -362,11 +365,11 @@ class Server:
     and returns a job id; results stay on the host until release()."""
 
     def __init__(self, device=0, max_active=16, steps_per_launch=32, use_graphs=True,
-                 hbm_budget_bytes=150 * 10**9):
+                 hbm_budget_bytes=150 * 10**9, setup_threads=4):
         lib = load()
         self._lib = lib
         cfg = ServerConfig(device, max_active, steps_per_launch, 1 if use_graphs else 0,
-                           int(hbm_budget_bytes))
+                           int(hbm_budget_bytes), int(setup_threads), 0)
         h = _P()
         self._check(lib.cpd_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -297,6 +297,9 @@ typedef struct cpd_server_config {
     int32_t steps_per_launch;   /* k: steps per launched chunk */
     int32_t use_graphs;         /* 1: replay the k-step chunk as a CUDA graph */
     uint64_t hbm_budget_bytes;  /* admission budget on resident device bytes */
+    int32_t setup_threads;      /* host threads that admit / set up / retire
+                                   jobs concurrently; 0 = 4 */
+    int32_t reserved;
 } cpd_server_config;
 
 typedef struct cpd_job_status {
@@ -307,7 +310,9 @@ typedef struct cpd_job_status {
     int64_t n;                  /* particles */
     int64_t bonds;              /* directed neighbour entries at admission */
     uint64_t device_bytes;      /* held while resident */
-    double submit_time, admit_time, start_time, finish_time; /* server clock, s */
+    /* server clock, s: submitted, admitted (set-up begins), set up, first
+     * chunk launched, finished */
+    double submit_time, admit_time, ready_time, start_time, finish_time;
     double total_strain_energy, total_damage;                 /* at the end */
     int64_t kernel_launches;    /* kernels run (graph replays count each node) */
 } cpd_job_status;
