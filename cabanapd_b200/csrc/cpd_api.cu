@@ -436,7 +436,7 @@ cpd_status vv_initial(cpd_system* s)
     const int nb = vv_blocks(s->n - s->frozen);
     if (track) CPD_OK_OR_RETURN(ensure_reduction(s, nb));
     if (use_mixed(s))
-        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->params.dt, s->mixed, s->stream));
+        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, s->mixed, s->stream));
     else
         CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->stream));
     if (track && s->n > s->frozen)
@@ -683,7 +683,8 @@ cpd_status cpd_set_state(cpd_system* s, const double* u, const double* v)
     CPD_CUDA(cudaSetDevice(s->device));
     if (u) CPD_OK_OR_RETURN(upload_vector(s, u, s->u));
     if (v) CPD_OK_OR_RETURN(upload_vector(s, v, s->v));
-    if (use_mixed(s) && s->mixed.uh) s->launches += launch_split_u(view(s), s->mixed, s->stream);
+    if (use_mixed(s) && s->mixed.u2)
+        s->launches += launch_split_u(view(s), s->md, s->mixed, s->stream);
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     return CPD_OK;
 }
@@ -860,7 +861,8 @@ cpd_status cpd_compute_dilatation(cpd_system* s)
 // changed outside the integrator (set_state, init, kernel-level calls).
 cpd_status refresh_mixed_u(cpd_system* s)
 {
-    if (use_mixed(s) && s->mixed.uh) CPD_LAUNCHED(launch_split_u(view(s), s->mixed, s->stream));
+    if (use_mixed(s) && s->mixed.u2)
+        CPD_LAUNCHED(launch_split_u(view(s), s->md, s->mixed, s->stream));
     return CPD_OK;
 }
 

@@ -152,11 +152,16 @@ struct __align__(16) MixedStencil {
     int32_t delta;      // neighbour index - particle index
     int32_t pad[2];
 };
+// FP32 split of one particle's displacement, hi and lo together so one
+// address serves both loads: u = hi.xyz + lo.xyz; hi.w = c vol (the PMB
+// micromodulus times the particle volume), lo.w = no-fail flag.
+struct __align__(32) MixedU {
+    float4 hi, lo;
+};
 struct MixedView {
     const float4* xh;  // positions, FP32 hi part
     const float4* xl;  // positions, FP32 lo part (x - hi)
-    const float4* uh;  // displacement hi part; w = volume
-    const float4* ul;  // displacement lo part; w = no-fail flag
+    const MixedU* u2;  // displacement split
     const uint8_t* code;  // [max_n][npad] stencil code per bond slot
     const MixedStencil* table;
     const uint8_t* warp_kind;  // per warp of rows: 2 all rows full stencil, 1 all rows
@@ -166,8 +171,7 @@ struct MixedView {
 struct MixedState {
     float4* xh = nullptr;
     float4* xl = nullptr;
-    float4* uh = nullptr;
-    float4* ul = nullptr;
+    MixedU* u2 = nullptr;
     uint8_t* code = nullptr;
     MixedStencil* table = nullptr;
     uint8_t* warp_kind = nullptr;
@@ -179,8 +183,8 @@ struct MixedState {
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                   MixedState& m, cudaStream_t st, std::string& err);
 void free_mixed(MixedState& m, cudaStream_t st);
-int launch_split_u(const ParticleView& p, MixedState& m, cudaStream_t st);
-int launch_vv_initial_mixed(const ParticleView& p, double dt, MixedState& m,
+int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st);
+int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, MixedState& m,
                             cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, cudaStream_t st);

@@ -196,10 +196,9 @@ __global__ void __launch_bounds__(kBlock)
         kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = full ? 2 : (subset ? 1 : 0);
 }
 
-// FP64 SoA -> FP32 hi/lo float4 (w carries an extra scalar per array).
+// FP64 SoA positions -> FP32 hi/lo float4 (w = 0).
 __global__ void __launch_bounds__(kBlock)
-    k_split(const double* __restrict__ src, int64_t n, int64_t np, const double* w_hi,
-            const uint8_t* w_lo, float4* hi, float4* lo)
+    k_split(const double* __restrict__ src, int64_t n, int64_t np, float4* hi, float4* lo)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -209,30 +208,50 @@ __global__ void __launch_bounds__(kBlock)
         h[d] = __double2float_rn(v);
         l[d] = __double2float_rn(v - (double)h[d]);
     }
-    hi[i] = make_float4(h[0], h[1], h[2], w_hi ? __double2float_rn(w_hi[i]) : 0.f);
-    lo[i] = make_float4(l[0], l[1], l[2], w_lo ? (float)w_lo[i] : 0.f);
+    hi[i] = make_float4(h[0], h[1], h[2], 0.f);
+    lo[i] = make_float4(l[0], l[1], l[2], 0.f);
+}
+
+__device__ __forceinline__ MixedU split_u(double u0, double u1, double u2, double cvol,
+                                          uint8_t nofail)
+{
+    MixedU m;
+    m.hi = make_float4(__double2float_rn(u0), __double2float_rn(u1), __double2float_rn(u2),
+                       __double2float_rn(cvol));
+    m.lo = make_float4(__double2float_rn(u0 - (double)m.hi.x),
+                       __double2float_rn(u1 - (double)m.hi.y),
+                       __double2float_rn(u2 - (double)m.hi.z), (float)nofail);
+    return m;
+}
+
+// FP64 displacement -> MixedU for every particle.
+__global__ void __launch_bounds__(kBlock)
+    k_split_u(ParticleView p, double c, MixedU* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    out[i] = split_u(p.u[i], p.u[np + i], p.u[2 * np + i], c * p.vol[i], p.nofail[i]);
 }
 
 // Velocity Verlet first half (CabanaPD_Integrate.hpp:89-116) that also
-// refreshes the FP32 hi/lo copy of u with vol (w of hi) and nofail (w of lo).
+// refreshes the FP32 split of u.
 __global__ void __launch_bounds__(kBlock)
-    k_vv_initial_mixed(ParticleView p, double dt, double half_dt, float4* uh, float4* ul)
+    k_vv_initial_mixed(ParticleView p, double dt, double half_dt, double c,
+                       MixedU* __restrict__ out)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const int64_t np = p.npad;
     const double half_dt_m = half_dt / p.rho[i];
-    float h[3], l[3];
+    double u[3];
     for (int d = 0; d < 3; ++d) {
         const double v = p.v[d * np + i] + half_dt_m * p.f[d * np + i];
         p.v[d * np + i] = v;
-        const double u = p.u[d * np + i] + dt * v;
-        p.u[d * np + i] = u;
-        h[d] = __double2float_rn(u);
-        l[d] = __double2float_rn(u - (double)h[d]);
+        u[d] = p.u[d * np + i] + dt * v;
+        p.u[d * np + i] = u[d];
     }
-    uh[i] = make_float4(h[0], h[1], h[2], __double2float_rn(p.vol[i]));
-    ul[i] = make_float4(l[0], l[1], l[2], (float)p.nofail[i]);
+    out[i] = split_u(u[0], u[1], u[2], c * p.vol[i], p.nofail[i]);
 }
 
 struct MixedModel {
@@ -254,7 +273,193 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float term)
 // Bonds are walked one 32-bond mask word at a time (the word is loaded,
 // tested bit by bit and written back once); stencil codes stream two bonds
 // ahead. MINB is the occupancy target passed to __launch_bounds__.
-template <bool FRACTURE, int MINB, bool PIPE>
+// One bond of the mixed kernel: deformed bond vector r, FP32 stretch s and
+// 1/|r| from the FP32 reference vector e (|e| = xi) and the split
+// displacements of both ends.
+struct MixedBond {
+    float rx, ry, rz, s, rinv;
+};
+
+__device__ __forceinline__ void mixed_bond(float ex, float ey, float ez, float xi, float xiinv,
+                                           const float4& uhj, const float4& ulj,
+                                           const float4& uhi, const float4& uli, MixedBond& b)
+{
+    const float nx = (uhj.x - uhi.x) + (ulj.x - uli.x);
+    const float ny = (uhj.y - uhi.y) + (ulj.y - uli.y);
+    const float nz = (uhj.z - uhi.z) + (ulj.z - uli.z);
+    b.rx = ex + nx;
+    b.ry = ey + ny;
+    b.rz = ez + nz;
+    const float r2 = b.rx * b.rx + b.ry * b.ry + b.rz * b.rz;
+    b.rinv = rsqrtf(r2);
+    const float r = r2 * b.rinv;
+    // eta . (2 xi_vec + eta) = r^2 - xi^2 without cancellation.
+    const float num = nx * (2.f * ex + nx) + ny * (2.f * ey + ny) + nz * (2.f * ez + nz);
+    b.s = __fdividef(num * xiinv, r + xi);
+}
+
+// The same bond with the x and y components carried as one float2 in the
+// paired FP32 instructions of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn,
+// each lane an IEEE round-to-nearest operation). eta and r are formed as in
+// mixed_bond; the squared length and the stretch numerator group their
+// terms differently, so results differ from mixed_bond by rounding only.
+struct MixedBond2 {
+    float2 rxy;
+    float rz, s, rinv;
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ __forceinline__ void mixed_bond2(float2 exy, float ez, float xi, float xiinv,
+                                            const float4& uhj, const float4& ulj,
+                                            float2 nuhi_xy, float nuhi_z, float2 nuli_xy,
+                                            float nuli_z, MixedBond2& b)
+{
+    // u_j - u_i with the negated own displacement (hi and lo) held by the row.
+    const float2 nxy = __fadd2_rn(__fadd2_rn(f2(uhj.x, uhj.y), nuhi_xy),
+                                  __fadd2_rn(f2(ulj.x, ulj.y), nuli_xy));
+    const float nz = (uhj.z + nuhi_z) + (ulj.z + nuli_z);
+    b.rxy = __fadd2_rn(exy, nxy);
+    b.rz = ez + nz;
+    const float2 sq = __fmul2_rn(b.rxy, b.rxy);
+    const float r2 = fmaf(b.rz, b.rz, sq.x + sq.y);
+    b.rinv = rsqrtf(r2);
+    const float r = r2 * b.rinv;
+    const float2 a2 = __ffma2_rn(f2(2.f, 2.f), exy, nxy);
+    const float2 pq = __fmul2_rn(nxy, a2);
+    const float num = fmaf(nz, fmaf(2.f, ez, nz), pq.x + pq.y);
+    b.s = __fdividef(num * xiinv, r + xi);
+}
+
+// Kahan-compensated accumulation of a pair of terms (x, y lanes).
+__device__ __forceinline__ void kahan_add2(float2& sum, float2& comp, float2 term)
+{
+    const float2 m1 = f2(-1.f, -1.f);
+    const float2 y = __ffma2_rn(comp, m1, term);   // term - comp
+    const float2 t = __fadd2_rn(sum, y);
+    const float2 z = __ffma2_rn(sum, m1, t);       // t - sum
+    comp = __ffma2_rn(y, m1, z);                   // (t - sum) - y
+    sum = t;
+}
+
+// The break test of one bond (CabanaPD_ForceModels.hpp:123-128 with the
+// PMB no-fail rule, force/CabanaPD_PMB.hpp:260-261): FP32 stretch against
+// s0, re-tested in FP64 inside the guard band.
+__device__ __forceinline__ bool mixed_critical(float s, float nofail_j, bool nofail_i,
+                                               const MixedModel& md, const ParticleView& p,
+                                               int64_t i, int64_t j)
+{
+    if (nofail_i || nofail_j != 0.f) return false;
+    if (fabsf(s - md.s0) <= md.guard) return critical_exact64(p.x, p.u, p.npad, i, j, md.bbc);
+    return s >= md.s0;
+}
+
+// Full-stencil rows (every table entry present, bond slot k = entry k):
+// the table is walked in chunks of 8 bonds with the bond bits of a chunk
+// tested at constant positions, broken bonds contribute a zero term instead
+// of a branch, and the newly broken bits of a 32-bond word are cleared once.
+template <bool FRACTURE>
+__device__ __forceinline__ void mixed_full_rows(const ParticleView& p, const EllView& nl,
+                                                const MixedU* __restrict__ u2_i,
+                                                const MixedStencil* tab,
+                                                const MixedModel& md, int64_t i,
+                                                const float4& uhi, const float4& uli,
+                                                bool nofail_i, float (&sum)[3], float (&comp)[3])
+{
+    const int64_t np = p.npad;
+    for (int base = 0; base < md.ntab; base += 32) {
+        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+        uint32_t clr = 0;
+        const int lim = min(32, md.ntab - base);
+        int b = 0;
+        for (; b + 8 <= lim; b += 8) {
+            const uint32_t w8 = word >> b;
+            uint32_t c8 = 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const MixedStencil t = tab[base + b + u];
+                const MixedU uj = u2_i[t.delta];
+                MixedBond bd;
+                mixed_bond(t.x, t.y, t.z, t.xi, t.xiinv, uj.hi, uj.lo, uhi, uli, bd);
+                float kf = uj.hi.w * bd.s * bd.rinv;
+                if (FRACTURE) {
+                    const bool crit = mixed_critical(bd.s, uj.lo.w, nofail_i, md, p, i,
+                                                     i + t.delta);
+                    c8 |= (uint32_t)crit << u;
+                    kf = (((w8 >> u) & 1u) && !crit) ? kf : 0.f;
+                }
+                kahan_add(sum[0], comp[0], kf * bd.rx);
+                kahan_add(sum[1], comp[1], kf * bd.ry);
+                kahan_add(sum[2], comp[2], kf * bd.rz);
+            }
+            clr |= c8 << b;
+        }
+        for (; b < lim; ++b) {
+            const MixedStencil t = tab[base + b];
+            const MixedU uj = u2_i[t.delta];
+            MixedBond bd;
+            mixed_bond(t.x, t.y, t.z, t.xi, t.xiinv, uj.hi, uj.lo, uhi, uli, bd);
+            float kf = uj.hi.w * bd.s * bd.rinv;
+            if (FRACTURE) {
+                const bool crit = mixed_critical(bd.s, uj.lo.w, nofail_i, md, p, i, i + t.delta);
+                clr |= (uint32_t)crit << b;
+                kf = (((word >> b) & 1u) && !crit) ? kf : 0.f;
+            }
+            kahan_add(sum[0], comp[0], kf * bd.rx);
+            kahan_add(sum[1], comp[1], kf * bd.ry);
+            kahan_add(sum[2], comp[2], kf * bd.rz);
+        }
+        if (FRACTURE && (word & clr)) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+    }
+}
+
+// mixed_full_rows with the x / y lanes in paired FP32 instructions.
+template <bool FRACTURE>
+__device__ __forceinline__ void mixed_full_rows2(const ParticleView& p, const EllView& nl,
+                                                 const MixedU* __restrict__ u2_i,
+                                                 const MixedStencil* tab,
+                                                 const MixedModel& md, int64_t i,
+                                                 const float4& uhi, const float4& uli,
+                                                 bool nofail_i, float2& sxy, float2& cxy,
+                                                 float& sz, float& cz)
+{
+    const int64_t np = p.npad;
+    const float2 nuhi_xy = f2(-uhi.x, -uhi.y), nuli_xy = f2(-uli.x, -uli.y);
+    const float nuhi_z = -uhi.z, nuli_z = -uli.z;
+    for (int base = 0; base < md.ntab; base += 32) {
+        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+        uint32_t clr = 0;
+        const int lim = min(32, md.ntab - base);
+        for (int b = 0; b < lim; b += 8) {
+            const uint32_t w8 = word >> b;
+            uint32_t c8 = 0;
+            const int n8 = min(8, lim - b);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (u < n8) {
+                    const MixedStencil t = tab[base + b + u];
+                    const MixedU uj = u2_i[t.delta];
+                    MixedBond2 bd;
+                    mixed_bond2(f2(t.x, t.y), t.z, t.xi, t.xiinv, uj.hi, uj.lo, nuhi_xy, nuhi_z,
+                                nuli_xy, nuli_z, bd);
+                    float kf = uj.hi.w * bd.s * bd.rinv;
+                    if (FRACTURE) {
+                        const bool crit = mixed_critical(bd.s, uj.lo.w, nofail_i, md, p, i,
+                                                         i + t.delta);
+                        c8 |= (uint32_t)crit << u;
+                        kf = (((w8 >> u) & 1u) && !crit) ? kf : 0.f;
+                    }
+                    kahan_add2(sxy, cxy, __fmul2_rn(f2(kf, kf), bd.rxy));
+                    kahan_add(sz, cz, kf * bd.rz);
+                }
+            }
+            clr |= c8 << b;
+        }
+        if (FRACTURE && (word & clr)) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+    }
+}
+
+template <bool FRACTURE, int MINB, bool PIPE, int FULL = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
     k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md)
 {
@@ -264,21 +469,38 @@ __global__ void __launch_bounds__(kBlock, MINB)
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const int64_t np = p.npad;
-    const float4 uhi = mv.uh[i], uli = mv.ul[i];
+    const MixedU ui = mv.u2[i];
+    const float4 uhi = ui.hi, uli = ui.lo;
     const bool nofail_i = FRACTURE ? (uli.w != 0.f) : false;
     const int cnt = nl.count[i];
     const uint8_t* __restrict__ code = mv.code + i;
-    const float4* __restrict__ UH = mv.uh;
-    const float4* __restrict__ UL = mv.ul;
+    const MixedU* __restrict__ U2 = mv.u2;
     float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
     const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    if (kind == 2 && FULL == 2) {
+        float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
+        float sz = 0.f, cz = 0.f;
+        mixed_full_rows2<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sxy, cxy, sz,
+                                   cz);
+        p.f[i] = (double)sxy.x - (double)cxy.x;
+        p.f[np + i] = (double)sxy.y - (double)cxy.y;
+        p.f[2 * np + i] = (double)sz - (double)cz;
+        return;
+    }
+    if (kind == 2 && FULL == 1) {
+        float sum[3] = {0.f, 0.f, 0.f}, comp[3] = {0.f, 0.f, 0.f};
+        mixed_full_rows<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sum, comp);
+        p.f[i] = (double)sum[0] - (double)comp[0];
+        p.f[np + i] = (double)sum[1] - (double)comp[1];
+        p.f[2 * np + i] = (double)sum[2] - (double)comp[2];
+        return;
+    }
     if (kind == 2 && PIPE) {
         // Full-stencil warp, software-pipelined: the next entry's table row
         // and neighbour data are loaded before the current bond is computed.
-        const float4* __restrict__ uh_i = UH + i;
-        const float4* __restrict__ ul_i = UL + i;
+        const MixedU* __restrict__ u2_i = U2 + i;
         MixedStencil tn = tab[0];
-        float4 uhn = uh_i[tn.delta], uln = ul_i[tn.delta];
+        float4 uhn = u2_i[tn.delta].hi, uln = u2_i[tn.delta].lo;
         for (int base = 0; base < cnt; base += 32) {
             uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
             const uint32_t old = word;
@@ -289,8 +511,8 @@ __global__ void __launch_bounds__(kBlock, MINB)
                 const float4 uhj = uhn, ulj = uln;
                 if (k + 1 < cnt) {
                     tn = tab[k + 1];
-                    uhn = uh_i[tn.delta];
-                    uln = ul_i[tn.delta];
+                    uhn = u2_i[tn.delta].hi;
+                    uln = u2_i[tn.delta].lo;
                 }
                 const float nx = (uhj.x - uhi.x) + (ulj.x - uli.x);
                 const float ny = (uhj.y - uhi.y) + (ulj.y - uli.y);
@@ -314,7 +536,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     intact = (word >> b) & 1u;
                 }
                 if (intact) {
-                    const float kf = md.c * uhj.w * s * rinv;
+                    const float kf = uhj.w * s * rinv;
                     kahan_add(sx, cx, kf * rx);
                     kahan_add(sy, cy, kf * ry);
                     kahan_add(sz, cz, kf * rz);
@@ -331,8 +553,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
         // Stencil rows: bond slots are the row's table entries in table
         // order, so entry k is read at a warp-uniform address. Full rows
         // (kind 2) hold every entry; subset rows skip the absent ones.
-        const float4* __restrict__ uh_i = UH + i;
-        const float4* __restrict__ ul_i = UL + i;
+        const MixedU* __restrict__ u2_i = U2 + i;
         const int nmask = (md.ntab + 31) / 32;
         int slot = 0, cur_w = 0;
         uint32_t word = FRACTURE ? nl.mu[i] : 0xffffffffu;
@@ -351,7 +572,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                 const int sb = slot & 31;
                 ++slot;
                 const MixedStencil t = tab[32 * w + b];
-                const float4 uhj = uh_i[t.delta], ulj = ul_i[t.delta];
+                const float4 uhj = u2_i[t.delta].hi, ulj = u2_i[t.delta].lo;
                 const float nx = (uhj.x - uhi.x) + (ulj.x - uli.x);
                 const float ny = (uhj.y - uhi.y) + (ulj.y - uli.y);
                 const float nz = (uhj.z - uhi.z) + (ulj.z - uli.z);
@@ -374,7 +595,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                     intact = (word >> sb) & 1u;
                 }
                 if (intact) {
-                    const float kf = md.c * uhj.w * s * rinv;
+                    const float kf = uhj.w * s * rinv;
                     kahan_add(sx, cx, kf * rx);
                     kahan_add(sy, cy, kf * ry);
                     kahan_add(sz, cz, kf * rz);
@@ -419,7 +640,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                 xiinv = rsqrtf(x2);
                 xi = x2 * xiinv;
             }
-            const float4 uhj = UH[j], ulj = UL[j];
+            const float4 uhj = U2[j].hi, ulj = U2[j].lo;
             const float nx = (uhj.x - uhi.x) + (ulj.x - uli.x);
             const float ny = (uhj.y - uhi.y) + (ulj.y - uli.y);
             const float nz = (uhj.z - uhi.z) + (ulj.z - uli.z);
@@ -443,7 +664,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
                 intact = (word >> b) & 1u;
             }
             if (intact) {
-                const float kf = md.c * uhj.w * s * rinv;
+                const float kf = uhj.w * s * rinv;
                 kahan_add(sx, cx, kf * rx);
                 kahan_add(sy, cy, kf * ry);
                 kahan_add(sz, cz, kf * rz);
@@ -458,14 +679,18 @@ __global__ void __launch_bounds__(kBlock, MINB)
 
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
 // (64 registers), 1 -> 4 blocks with the full-stencil loop software
-// pipelined, 2 -> pipelined with 3 blocks (more registers). Full plate on
-// B200, ms per launch: 4.70 / 4.64 / 4.92; 0 is the default (no spills).
+// pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
+// rows in unrolled 8-bond chunks with branch-free bond bits, 4 -> 3 with the
+// x / y lanes in paired FP32 instructions (default). Full plate on B200, ms
+// per launch for 3 / 4: 4.15 / 4.12 (4 compiled for 3 or 2 blocks per SM:
+// 5.05).
+// Full plate on B200, ms per launch for 0 / 1 / 2: 4.70 / 4.64 / 4.92.
 int mixed_variant()
 {
     static int v = [] {
         const char* e = getenv("CPD_MIXED_VARIANT");
-        int x = e ? atoi(e) : 0;
-        return (x < 0 || x > 2) ? 0 : x;
+        int x = e ? atoi(e) : 4;
+        return (x < 0 || x > 4) ? 4 : x;
     }();
     return v;
 }
@@ -483,7 +708,7 @@ int mixed_variant()
 
 void free_mixed(MixedState& m, cudaStream_t st)
 {
-    void* ptrs[] = {m.xh, m.xl, m.uh, m.ul, m.code, m.table, m.warp_kind, m.pmask};
+    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
@@ -497,17 +722,16 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
     const int64_t np = p.npad;
     CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
     CPD_TRY(dev_alloc(&m.xl, sizeof(float4) * np, st));
-    CPD_TRY(dev_alloc(&m.uh, sizeof(float4) * np, st));
-    CPD_TRY(dev_alloc(&m.ul, sizeof(float4) * np, st));
+    CPD_TRY(dev_alloc(&m.u2, sizeof(MixedU) * np, st));
     CPD_TRY(dev_alloc(&m.table, sizeof(MixedStencil) * kMixedGeneric, st));
     CPD_TRY(dev_alloc(&m.code, (size_t)std::max(pd.max_n, 1) * np, st));
     const int64_t nwarps = (np + 31) / 32 + 8;
     CPD_TRY(dev_alloc(&m.warp_kind, nwarps, st));
-    m.bytes = 4 * sizeof(float4) * np + sizeof(MixedStencil) * kMixedGeneric +
+    m.bytes = (2 * sizeof(float4) + sizeof(MixedU)) * np + sizeof(MixedStencil) * kMixedGeneric +
               (size_t)std::max(pd.max_n, 1) * np + nwarps;
     CPD_TRY(cudaMemsetAsync(m.warp_kind, 0, nwarps, st));
     CPD_TRY(cudaMemsetAsync(m.code, kMixedGeneric, (size_t)std::max(pd.max_n, 1) * np, st));
-    k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, nullptr, nullptr, m.xh, m.xl);
+    k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, m.xh, m.xl);
     launches++;
     m.ntab = 0;
     const int64_t rows = p.n - p.frozen;
@@ -600,18 +824,19 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
     return launches;
 }
 
-int launch_split_u(const ParticleView& p, MixedState& m, cudaStream_t st)
+int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st)
 {
     if (p.n <= 0) return 0;
-    k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.u, p.n, p.npad, p.vol, p.nofail, m.uh, m.ul);
+    k_split_u<<<blocks_for(p.n), kBlock, 0, st>>>(p, md.c, m.u2);
     return 1;
 }
 
-int launch_vv_initial_mixed(const ParticleView& p, double dt, MixedState& m, cudaStream_t st)
+int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, MixedState& m,
+                            cudaStream_t st)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, m.uh, m.ul);
+    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, md.c, m.u2);
     return 1;
 }
 
@@ -620,7 +845,7 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    MixedView mv{m.xh, m.xl, m.uh, m.ul, m.code, m.table, m.warp_kind, m.pmask};
+    MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
     MixedModel mm;
     mm.c = (float)md.c;
     mm.s0 = (float)md.s0;
@@ -632,9 +857,13 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
     case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
     case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
     case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
     case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    default: k_pmb_force_mixed<false, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    default: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
     }
     return 1;
 }
