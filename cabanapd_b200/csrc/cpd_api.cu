@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -136,6 +137,23 @@ struct cpd_system {
     NeighborList pd, contact;
     MixedState mixed;  // CPD_MIXED: FP32 split copies and bond stencil codes
     std::vector<BoundaryCondition> bcs;
+    // Host copy of the boundary conditions (internal indices), and the
+    // per-row program the fused step applies (built on first use).
+    struct HostBC {
+        int kind, component;
+        std::vector<int32_t> idx;
+        std::vector<double> values;
+    };
+    std::vector<HostBC> hbcs;
+    int bc_prog = 0;  // 0 not built, 1 built, -1 the conditions cannot be fused
+    uint32_t* bc_bits = nullptr;
+    int32_t* bc_row = nullptr;
+    uint8_t* bc_keep = nullptr;
+    double* bc_add = nullptr;
+    int32_t nbc = 0;
+    // Second displacement buffers of the fused step.
+    double* u_alt = nullptr;
+    MixedU* u2_alt = nullptr;
     bool neighbors_built = false;
     bool initialized = false;
     double max_disp = 0.0;
@@ -190,6 +208,19 @@ EllView pd_view(const cpd_system* s)
     return v;
 }
 
+void free_bc_program(cpd_system* s)
+{
+    void* arrays[] = {s->bc_bits, s->bc_row, s->bc_keep, s->bc_add};
+    for (void* a : arrays)
+        if (a) dev_free(a, s->stream);
+    s->bc_bits = nullptr;
+    s->bc_row = nullptr;
+    s->bc_keep = nullptr;
+    s->bc_add = nullptr;
+    s->nbc = 0;
+    s->bc_prog = 0;
+}
+
 void free_particles(cpd_system* s)
 {
     double** arrays[] = {&s->x,     &s->u,     &s->v,     &s->f,     &s->vol,
@@ -210,6 +241,12 @@ void free_particles(cpd_system* s)
         if (bc.values) dev_free(bc.values, s->stream);
     }
     s->bcs.clear();
+    s->hbcs.clear();
+    free_bc_program(s);
+    if (s->u_alt) dev_free(s->u_alt, s->stream);
+    s->u_alt = nullptr;
+    if (s->u2_alt) dev_free(s->u2_alt, s->stream);
+    s->u2_alt = nullptr;
     free_neighbor_list(s->pd, s->stream);
     free_neighbor_list(s->contact, s->stream);
     free_mixed(s->mixed, s->stream);
@@ -372,24 +409,27 @@ bool use_fast(const cpd_system* s)
            fast_supported(s->md);
 }
 
-cpd_status pd_force(cpd_system* s)
+// The bond kernel on particle view p (displacement buffer p.u; on the
+// mixed path its split in m.u2), finishing each row as ep says.
+cpd_status pd_force_on(cpd_system* s, const ParticleView& p, const MixedState& m,
+                       const StepEpilogue& ep)
 {
-    const ParticleView p = view(s);
     cudaEvent_t e0;
     CPD_OK_OR_RETURN(timed_begin(s, e0));
     if (use_mixed(s))
-        CPD_LAUNCHED(launch_pd_force_mixed(p, pd_view(s), s->md, s->mixed, s->stream));
+        CPD_LAUNCHED(launch_pd_force_mixed(p, pd_view(s), s->md, m, ep, s->stream));
     else if (use_fast(s))
-        CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, s->stream));
+        CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, ep, s->stream));
     else
         CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
     return timed_end(s, e0);
 }
 
+cpd_status pd_force(cpd_system* s) { return pd_force_on(s, view(s), s->mixed, StepEpilogue{}); }
+
 // LPS weighted volume (when compute_m) and dilatation.
-cpd_status lps_prepare(cpd_system* s, bool compute_m)
+cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, bool compute_m)
 {
-    const ParticleView p = view(s);
     if (use_fast(s)) {
         CPD_LAUNCHED(launch_lps_m_theta_fast(p, pd_view(s), s->md, compute_m, s->stream));
         return CPD_OK;
@@ -398,6 +438,8 @@ cpd_status lps_prepare(cpd_system* s, bool compute_m)
     CPD_LAUNCHED(launch_lps_dilatation(p, pd_view(s), s->md, s->stream));
     return CPD_OK;
 }
+
+cpd_status lps_prepare(cpd_system* s, bool compute_m) { return lps_prepare_on(s, view(s), compute_m); }
 
 cpd_status contact_force(cpd_system* s, bool reset)
 {
@@ -436,12 +478,162 @@ cpd_status vv_initial(cpd_system* s)
     const int nb = vv_blocks(s->n - s->frozen);
     if (track) CPD_OK_OR_RETURN(ensure_reduction(s, nb));
     if (use_mixed(s))
-        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, s->mixed, s->stream));
+        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, s->u, s->mixed.u2,
+                                             s->stream));
     else
-        CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->stream));
+        CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, track, s->red, nb, s->u, s->stream));
     if (track && s->n > s->frozen)
         CPD_LAUNCHED(launch_max_partials(s->red, nb, s->red_out, s->stream));
     s->steps_since_rebuild++;
+    return CPD_OK;
+}
+
+// The boundary conditions as one program per row (see StepEpilogue):
+// possible when every row and component is touched by at most one
+// operation and no condition acts on a frozen particle; the program then
+// applies exactly the operations of the separate kernel.
+cpd_status build_bc_program(cpd_system* s)
+{
+    struct Row {
+        uint8_t keep = 0;  // bits 0-2 keep f, bits 4-6 component touched
+        double add[3] = {0.0, 0.0, 0.0};
+    };
+    std::vector<std::pair<int32_t, Row>> rows;
+    std::vector<int32_t> where(s->n, -1);
+    bool ok = true;
+    for (const auto& bc : s->hbcs) {
+        for (size_t b = 0; b < bc.idx.size() && ok; ++b) {
+            const int32_t q = bc.idx[b];
+            if (q < s->frozen) {
+                ok = false;
+                break;
+            }
+            if (where[q] < 0) {
+                where[q] = (int32_t)rows.size();
+                rows.push_back({q, Row{}});
+            }
+            Row& r = rows[where[q]].second;
+            for (int d = 0; d < 3; ++d) {
+                const bool touched = bc.kind != CPD_BC_FORCE_ADD || d == bc.component;
+                if (!touched) continue;
+                if (r.keep & (16u << d)) {
+                    ok = false;
+                    break;
+                }
+                r.keep |= (uint8_t)(16u << d);
+                if (bc.kind == CPD_BC_FORCE_VALUE) {
+                    r.add[d] = bc.values[0];
+                } else {
+                    r.keep |= (uint8_t)(1u << d);
+                    r.add[d] = bc.kind == CPD_BC_FORCE_UPDATE ? bc.values[0] : bc.values[b];
+                }
+            }
+        }
+        if (!ok) break;
+    }
+    if (!ok) {
+        s->bc_prog = -1;
+        return CPD_OK;
+    }
+    std::sort(rows.begin(), rows.end(),
+              [](const std::pair<int32_t, Row>& a, const std::pair<int32_t, Row>& b) {
+                  return a.first < b.first;
+              });
+    const int32_t m = (int32_t)rows.size();
+    s->nbc = m;
+    if (m > 0) {
+        const size_t nwords = (size_t)(s->npad + 31) / 32;
+        std::vector<uint32_t> bits(nwords, 0u);
+        std::vector<int32_t> row(m);
+        std::vector<uint8_t> keep(m);
+        std::vector<double> add(3 * (size_t)m);
+        for (int32_t k = 0; k < m; ++k) {
+            const int32_t q = rows[k].first;
+            bits[q >> 5] |= 1u << (q & 31);
+            row[k] = q;
+            keep[k] = rows[k].second.keep;
+            for (int d = 0; d < 3; ++d) add[(size_t)d * m + k] = rows[k].second.add[d];
+        }
+        CPD_CUDA(dev_alloc(&s->bc_bits, sizeof(uint32_t) * nwords, s->stream));
+        CPD_CUDA(dev_alloc(&s->bc_row, sizeof(int32_t) * m, s->stream));
+        CPD_CUDA(dev_alloc(&s->bc_keep, m, s->stream));
+        CPD_CUDA(dev_alloc(&s->bc_add, sizeof(double) * 3 * m, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(s->bc_bits, bits.data(), sizeof(uint32_t) * nwords,
+                                 cudaMemcpyHostToDevice, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(s->bc_row, row.data(), sizeof(int32_t) * m,
+                                 cudaMemcpyHostToDevice, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(s->bc_keep, keep.data(), m, cudaMemcpyHostToDevice, s->stream));
+        CPD_CUDA(cudaMemcpyAsync(s->bc_add, add.data(), sizeof(double) * 3 * m,
+                                 cudaMemcpyHostToDevice, s->stream));
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    s->bc_prog = 1;
+    return CPD_OK;
+}
+
+// Whether cpd_step may run the fused step: PD without contact on the
+// throughput kernels, with boundary conditions a row program can express.
+// CPD_FUSED_STEP=0 selects the separate kernels (for comparisons).
+bool fused_steps_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("CPD_FUSED_STEP");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+bool fusable(cpd_system* s)
+{
+    if (!has_pd(s) || has_contact(s) || !(use_fast(s) || use_mixed(s))) return false;
+    if (s->bc_prog == 0 && build_bc_program(s) != CPD_OK) return false;
+    return s->bc_prog == 1;
+}
+
+// num_steps steps as: first half step, then one bond kernel per step whose
+// epilogue applies the boundary conditions, the second half step and (but
+// for the last step) the next first half step, alternating displacement
+// buffers. The first half step writes to the buffer that makes the last
+// step end in the system's own arrays.
+cpd_status step_fused(cpd_system* s, int32_t num_steps)
+{
+    const bool mixed = use_mixed(s);
+    const size_t vb = sizeof(double) * 3 * s->npad;
+    if (!s->u_alt) CPD_CUDA(dev_alloc(&s->u_alt, vb, s->stream));
+    if (mixed && !s->u2_alt) CPD_CUDA(dev_alloc(&s->u2_alt, sizeof(MixedU) * s->npad, s->stream));
+    const bool start_alt = ((num_steps - 1) & 1) != 0;
+    double* ucur = start_alt ? s->u_alt : s->u;
+    double* unxt = start_alt ? s->u : s->u_alt;
+    MixedU* u2cur = mixed ? (start_alt ? s->u2_alt : s->mixed.u2) : nullptr;
+    MixedU* u2nxt = mixed ? (start_alt ? s->mixed.u2 : s->u2_alt) : nullptr;
+    const ParticleView p = view(s);
+    if (mixed)
+        CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, ucur, u2cur, s->stream));
+    else
+        CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, false, nullptr, 0, ucur, s->stream));
+    StepEpilogue ep;
+    ep.dt = s->params.dt;
+    ep.half_dt = 0.5 * s->params.dt;
+    ep.c = s->md.c;
+    ep.bc_bits = s->bc_bits;
+    ep.bc_row = s->bc_row;
+    ep.bc_keep = s->bc_keep;
+    ep.bc_add = s->bc_add;
+    ep.nbc = s->nbc;
+    for (int32_t k = 0; k < num_steps; ++k) {
+        ParticleView pk = p;
+        pk.u = ucur;
+        MixedState mk = s->mixed;
+        mk.u2 = u2cur;
+        ep.mode = k + 1 < num_steps ? 2 : 1;
+        ep.u_next = unxt;
+        ep.u2_next = u2nxt;
+        if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, s->md.fracture != 0));
+        CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
+        std::swap(ucur, unxt);
+        std::swap(u2cur, u2nxt);
+    }
+    s->steps_since_rebuild += num_steps;
     return CPD_OK;
 }
 
@@ -824,6 +1016,13 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
         CPD_CUDA(cudaStreamSynchronize(s->stream));
     }
     s->bcs.push_back(bc);
+    cpd_system::HostBC hb;
+    hb.kind = kind;
+    hb.component = component;
+    hb.idx = idx;
+    hb.values.assign(values, values + (kind == CPD_BC_FORCE_ADD ? count : 1));
+    s->hbcs.push_back(std::move(hb));
+    free_bc_program(s);
     return CPD_OK;
 }
 
@@ -836,6 +1035,8 @@ cpd_status cpd_clear_boundary_conditions(cpd_system* s)
         if (bc.values) dev_free(bc.values, s->stream);
     }
     s->bcs.clear();
+    s->hbcs.clear();
+    free_bc_program(s);
     return CPD_OK;
 }
 
@@ -928,6 +1129,7 @@ cpd_status cpd_step(cpd_system* s, int32_t num_steps)
     if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step");
     if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
     CPD_CUDA(cudaSetDevice(s->device));
+    if (num_steps > 0 && fused_steps_enabled() && fusable(s)) return step_fused(s, num_steps);
     const ParticleView p = view(s);
     for (int32_t k = 0; k < num_steps; k++) {
         CPD_OK_OR_RETURN(vv_initial(s));
@@ -1042,7 +1244,7 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
     if (bytes_per_launch) {
         // Compulsory traffic of one plain-FP64 bond-kernel launch (the same
         // denominator for every precision mode, so fractions compare the
-        // modes on the same work): per row, read x, u
+        // modes on the same work) in a step of cpd_step: per row, read x, u
         // (48 B), vol (8 B), count (4 B), write f (24 B); per bond the 4-byte
         // neighbour index; with fracture the 1-bit bond state read and
         // written (0.25 B) and the 1-byte no-fail flag per row; LPS adds the
@@ -1058,6 +1260,9 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
         }
         if (is_lps(s)) per_row += 16.0;
         if (!has_pd(s)) per_row += 24.0 + 16.0;  // Hertz: v, rho (+vol already)
+        // The fused step's bond kernel also integrates: read v and rho,
+        // write v and the next u (48 + 8 + 24 + 24 B) instead of writing f.
+        if (fused_steps_enabled() && fusable(s)) per_row += 48.0 + 8.0 + 24.0 + 24.0 - 24.0;
         *bytes_per_launch = per_row * rows + per_bond * (double)nl.total;
     }
     return CPD_OK;
@@ -1076,6 +1281,9 @@ cpd_status cpd_device_bytes(const cpd_system* s, uint64_t* bytes)
         if (s->perm) b += 4 * n;
     }
     for (const auto& bc : s->bcs) b += (uint64_t)bc.count * (bc.values ? 12 : 4);
+    if (s->u_alt) b += 24 * np;
+    if (s->u2_alt) b += sizeof(MixedU) * np;
+    if (s->bc_bits) b += 4 * ((np + 31) / 32) + 29 * (uint64_t)s->nbc;
     b += s->pd.bytes + s->contact.bytes + s->mixed.bytes;
     *bytes = b;
     return CPD_OK;

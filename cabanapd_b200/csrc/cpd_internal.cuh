@@ -110,11 +110,14 @@ struct BoundaryCondition {
     double value = 0;            // scalar kinds
 };
 
+struct StepEpilogue;
+
 // ---------------------------------------------------------------------------
 // Kernel launchers (definitions in cpd_kernels_exact.cu / cpd_neighbor.cu).
 // Each returns the number of kernels it launched.
+// u_out: where the new displacement goes (p.u for in place).
 int launch_vv_initial(const ParticleView& p, double dt, bool track_max,
-                      double* block_max, int max_blocks, cudaStream_t st);
+                      double* block_max, int max_blocks, double* u_out, cudaStream_t st);
 int launch_vv_final(const ParticleView& p, double dt, cudaStream_t st);
 int launch_lps_weighted_volume(const ParticleView& p, const EllView& nl,
                                const Model& md, cudaStream_t st);
@@ -127,7 +130,7 @@ int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
 // Throughput-form FP64 kernels (cpd_kernels_fast.cu): PMB and LPS.
 bool fast_supported(const Model& md);
 int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
-                         cudaStream_t st);
+                         const StepEpilogue& ep, cudaStream_t st);
 int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Model& md,
                             bool with_m, cudaStream_t st);
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
@@ -168,6 +171,25 @@ struct MixedView {
                                // stencil subsets, 0 otherwise (per-bond codes)
     const uint32_t* pmask;     // [ceil(ntab/32)][npad] stencil entries present per row
 };
+// What a throughput bond kernel does after summing row i's force
+// (cpd_epilogue.cuh): mode 0 stores f; mode 1 applies the row's force
+// boundary condition and the second half step (v); mode 2 also applies the
+// next step's first half step, writing the new displacement to u_next (and
+// its FP32 split to u2_next on the mixed path) instead of storing f.
+struct StepEpilogue {
+    int mode = 0;
+    double dt = 0, half_dt = 0;
+    double* u_next = nullptr;
+    MixedU* u2_next = nullptr;
+    double c = 0;                      // PMB micromodulus, for the mixed split
+    const uint32_t* bc_bits = nullptr; // [ceil(npad / 32)] rows with a condition
+    const int32_t* bc_row = nullptr;   // [nbc] their internal indices, ascending
+    const uint8_t* bc_keep = nullptr;  // [nbc] bit 4+d: component d touched;
+                                       // bit d: then f_d + add_d, else add_d
+    const double* bc_add = nullptr;    // [3][nbc]
+    int32_t nbc = 0;
+};
+
 struct MixedState {
     float4* xh = nullptr;
     float4* xl = nullptr;
@@ -184,10 +206,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                   MixedState& m, cudaStream_t st, std::string& err);
 void free_mixed(MixedState& m, cudaStream_t st);
 int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st);
-int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, MixedState& m,
-                            cudaStream_t st);
+int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, double* u_out,
+                            MixedU* u2_out, cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                          const MixedState& m, cudaStream_t st);
+                          const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 
 // Neighbour build (cpd_neighbor.cu). Builds rows for [begin, n) from
 // positions pos (+ optional displacement disp) with squared distance

@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kBlock)
 // (Contact: also the largest displacement since the last list build).
 template <bool TRACK>
 __global__ void __launch_bounds__(kBlock)
-    k_vv_initial(ParticleView p, double dt, double half_dt, double* block_max)
+    k_vv_initial(ParticleView p, double dt, double half_dt, double* block_max, double* u_out)
 {
     __shared__ double s_max[kBlock];
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -456,9 +456,9 @@ __global__ void __launch_bounds__(kBlock)
         const double u0 = p.u[i] + dt * v0;
         const double u1 = p.u[np + i] + dt * v1;
         const double u2 = p.u[2 * np + i] + dt * v2;
-        p.u[i] = u0;
-        p.u[np + i] = u1;
-        p.u[2 * np + i] = u2;
+        u_out[i] = u0;
+        u_out[np + i] = u1;
+        u_out[2 * np + i] = u2;
         if (TRACK)
             um = norm3d(u0 - p.u_neigh[i], u1 - p.u_neigh[np + i],
                         u2 - p.u_neigh[2 * np + i]);
@@ -613,15 +613,15 @@ int energy_blocks(int64_t nrows) { return nrows > 0 ? blocks_for(nrows) : 1; }
 int vv_blocks(int64_t nrows) { return nrows > 0 ? blocks_for(nrows) : 1; }
 
 int launch_vv_initial(const ParticleView& p, double dt, bool track_max,
-                      double* block_max, int, cudaStream_t st)
+                      double* block_max, int, double* u_out, cudaStream_t st)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
     const double half_dt = 0.5 * dt;
     if (track_max)
-        k_vv_initial<true><<<blocks_for(rows), kBlock, 0, st>>>(p, dt, half_dt, block_max);
+        k_vv_initial<true><<<blocks_for(rows), kBlock, 0, st>>>(p, dt, half_dt, block_max, u_out);
     else
-        k_vv_initial<false><<<blocks_for(rows), kBlock, 0, st>>>(p, dt, half_dt, nullptr);
+        k_vv_initial<false><<<blocks_for(rows), kBlock, 0, st>>>(p, dt, half_dt, nullptr, u_out);
     return 1;
 }
 

@@ -23,6 +23,7 @@
 
 #include <cstdlib>
 
+#include "cpd_epilogue.cuh"
 #include "cpd_internal.cuh"
 
 namespace cpd {
@@ -150,7 +151,7 @@ __device__ __forceinline__ void gather(const ParticleView& p, int64_t np, int64_
 // so a warp keeps several independent loads in flight while it computes.
 template <bool FRACTURE, int PF, bool GP, int MINB = 1>
 __global__ void __launch_bounds__(kBlock, MINB)
-    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md)
+    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -216,9 +217,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
         }
     }
     if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
-    p.f[i] = fx;
-    p.f[np + i] = fy;
-    p.f[2 * np + i] = fz;
+    step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
 // LPS weighted volume and dilatation fused (force/CabanaPD_LPS.hpp:89-141,
@@ -283,7 +282,7 @@ __global__ void __launch_bounds__(kBlock)
 // LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447).
 template <int INFL, bool FRACTURE>
 __global__ void __launch_bounds__(kBlock)
-    k_lps_force_fast(ParticleView p, EllView nl, FastModel md)
+    k_lps_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -333,9 +332,7 @@ __global__ void __launch_bounds__(kBlock)
         }
     }
     if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
-    p.f[i] = fx;
-    p.f[np + i] = fy;
-    p.f[2 * np + i] = fz;
+    step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
 // Neighbour indices of one ELL row read PF bonds ahead of use (a shift
@@ -406,7 +403,7 @@ __global__ void __launch_bounds__(kBlock, 4)
 // indices streamed two bonds ahead, compiled for 4 blocks of 256 per SM.
 template <int INFL, bool FRACTURE>
 __global__ void __launch_bounds__(kBlock, 4)
-    k_lps_force_pf(ParticleView p, EllView nl, FastModel md)
+    k_lps_force_pf(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -453,9 +450,7 @@ __global__ void __launch_bounds__(kBlock, 4)
         }
     }
     if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
-    p.f[i] = fx;
-    p.f[np + i] = fy;
-    p.f[2 * np + i] = fz;
+    step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
 // LPS kernel form, from CPD_LPS_VARIANT: 0 two-pass m / theta and plain
@@ -498,7 +493,7 @@ bool fast_supported(const Model& md)
 }
 
 int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
-                         cudaStream_t st)
+                         const StepEpilogue& ep, cudaStream_t st)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
@@ -507,42 +502,42 @@ int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& 
     if (md.pd == CPD_PD_PMB) {
         // Variant: index prefetch distance and neighbour-gather pipelining.
         switch (md.fracture ? fast_variant() : 100 + fast_variant()) {
-        case 0: k_pmb_force_fast<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 1: k_pmb_force_fast<true, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 2: k_pmb_force_fast<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 3: k_pmb_force_fast<true, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 4: k_pmb_force_fast<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 5: k_pmb_force_fast<true, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 100: k_pmb_force_fast<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 101: k_pmb_force_fast<false, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 102: k_pmb_force_fast<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 103: k_pmb_force_fast<false, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        case 105: k_pmb_force_fast<false, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm); break;
-        default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm); break;
+        case 0: k_pmb_force_fast<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 1: k_pmb_force_fast<true, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 2: k_pmb_force_fast<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 3: k_pmb_force_fast<true, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 4: k_pmb_force_fast<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 5: k_pmb_force_fast<true, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 100: k_pmb_force_fast<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 101: k_pmb_force_fast<false, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 102: k_pmb_force_fast<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 103: k_pmb_force_fast<false, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        case 105: k_pmb_force_fast<false, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
+        default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
         }
     } else if (lps_variant() == 1) {
         if (md.influence == 1) {
             if (md.fracture)
-                k_lps_force_pf<1, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_pf<1, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
             else
-                k_lps_force_pf<1, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_pf<1, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
         } else {
             if (md.fracture)
-                k_lps_force_pf<0, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_pf<0, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
             else
-                k_lps_force_pf<0, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_pf<0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
         }
     } else {
         if (md.influence == 1) {
             if (md.fracture)
-                k_lps_force_fast<1, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_fast<1, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
             else
-                k_lps_force_fast<1, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_fast<1, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
         } else {
             if (md.fracture)
-                k_lps_force_fast<0, true><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_fast<0, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
             else
-                k_lps_force_fast<0, false><<<g, kBlock, 0, st>>>(p, nl, fm);
+                k_lps_force_fast<0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
         }
     }
     return 1;

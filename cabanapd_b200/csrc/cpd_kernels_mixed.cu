@@ -39,6 +39,7 @@
 #include <string>
 #include <vector>
 
+#include "cpd_epilogue.cuh"
 #include "cpd_internal.cuh"
 
 namespace cpd {
@@ -212,18 +213,6 @@ __global__ void __launch_bounds__(kBlock)
     lo[i] = make_float4(l[0], l[1], l[2], 0.f);
 }
 
-__device__ __forceinline__ MixedU split_u(double u0, double u1, double u2, double cvol,
-                                          uint8_t nofail)
-{
-    MixedU m;
-    m.hi = make_float4(__double2float_rn(u0), __double2float_rn(u1), __double2float_rn(u2),
-                       __double2float_rn(cvol));
-    m.lo = make_float4(__double2float_rn(u0 - (double)m.hi.x),
-                       __double2float_rn(u1 - (double)m.hi.y),
-                       __double2float_rn(u2 - (double)m.hi.z), (float)nofail);
-    return m;
-}
-
 // FP64 displacement -> MixedU for every particle.
 __global__ void __launch_bounds__(kBlock)
     k_split_u(ParticleView p, double c, MixedU* __restrict__ out)
@@ -235,21 +224,22 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // Velocity Verlet first half (CabanaPD_Integrate.hpp:89-116) that also
-// refreshes the FP32 split of u.
+// refreshes the FP32 split of u; the new u goes to u_out (p.u: in place).
+// Each operation is rounded separately, as in k_vv_initial.
 __global__ void __launch_bounds__(kBlock)
     k_vv_initial_mixed(ParticleView p, double dt, double half_dt, double c,
-                       MixedU* __restrict__ out)
+                       double* __restrict__ u_out, MixedU* __restrict__ out)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const int64_t np = p.npad;
-    const double half_dt_m = half_dt / p.rho[i];
+    const double half_dt_m = __ddiv_rn(half_dt, p.rho[i]);
     double u[3];
     for (int d = 0; d < 3; ++d) {
-        const double v = p.v[d * np + i] + half_dt_m * p.f[d * np + i];
+        const double v = __dadd_rn(p.v[d * np + i], __dmul_rn(half_dt_m, p.f[d * np + i]));
         p.v[d * np + i] = v;
-        u[d] = p.u[d * np + i] + dt * v;
-        p.u[d * np + i] = u[d];
+        u[d] = __dadd_rn(p.u[d * np + i], __dmul_rn(dt, v));
+        u_out[d * np + i] = u[d];
     }
     out[i] = split_u(u[0], u[1], u[2], c * p.vol[i], p.nofail[i]);
 }
@@ -461,7 +451,7 @@ __device__ __forceinline__ void mixed_full_rows2(const ParticleView& p, const El
 
 template <bool FRACTURE, int MINB, bool PIPE, int FULL = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
-    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md)
+    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep)
 {
     __shared__ MixedStencil tab[kMixedGeneric];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
@@ -482,17 +472,15 @@ __global__ void __launch_bounds__(kBlock, MINB)
         float sz = 0.f, cz = 0.f;
         mixed_full_rows2<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sxy, cxy, sz,
                                    cz);
-        p.f[i] = (double)sxy.x - (double)cxy.x;
-        p.f[np + i] = (double)sxy.y - (double)cxy.y;
-        p.f[2 * np + i] = (double)sz - (double)cz;
+        step_epilogue<true>(p, ep, i, (double)sxy.x - (double)cxy.x,
+                            (double)sxy.y - (double)cxy.y, (double)sz - (double)cz);
         return;
     }
     if (kind == 2 && FULL == 1) {
         float sum[3] = {0.f, 0.f, 0.f}, comp[3] = {0.f, 0.f, 0.f};
         mixed_full_rows<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sum, comp);
-        p.f[i] = (double)sum[0] - (double)comp[0];
-        p.f[np + i] = (double)sum[1] - (double)comp[1];
-        p.f[2 * np + i] = (double)sum[2] - (double)comp[2];
+        step_epilogue<true>(p, ep, i, (double)sum[0] - (double)comp[0],
+                            (double)sum[1] - (double)comp[1], (double)sum[2] - (double)comp[2]);
         return;
     }
     if (kind == 2 && PIPE) {
@@ -544,9 +532,8 @@ __global__ void __launch_bounds__(kBlock, MINB)
             }
             if (FRACTURE && word != old) nl.mu[(int64_t)(base >> 5) * np + i] = word;
         }
-        p.f[i] = (double)sx - (double)cx;
-        p.f[np + i] = (double)sy - (double)cy;
-        p.f[2 * np + i] = (double)sz - (double)cz;
+        step_epilogue<true>(p, ep, i, (double)sx - (double)cx, (double)sy - (double)cy,
+                            (double)sz - (double)cz);
         return;
     }
     if (kind != 0) {
@@ -603,9 +590,8 @@ __global__ void __launch_bounds__(kBlock, MINB)
             }
         }
         if (FRACTURE && word != old) nl.mu[(int64_t)cur_w * np + i] = word;
-        p.f[i] = (double)sx - (double)cx;
-        p.f[np + i] = (double)sy - (double)cy;
-        p.f[2 * np + i] = (double)sz - (double)cz;
+        step_epilogue<true>(p, ep, i, (double)sx - (double)cx, (double)sy - (double)cy,
+                            (double)sz - (double)cz);
         return;
     }
     int c1 = cnt > 0 ? __ldg(code) : 0;
@@ -672,9 +658,8 @@ __global__ void __launch_bounds__(kBlock, MINB)
         }
         if (FRACTURE && word != old) nl.mu[(int64_t)(base >> 5) * np + i] = word;
     }
-    p.f[i] = (double)sx - (double)cx;
-    p.f[np + i] = (double)sy - (double)cy;
-    p.f[2 * np + i] = (double)sz - (double)cz;
+    step_epilogue<true>(p, ep, i, (double)sx - (double)cx, (double)sy - (double)cy,
+                        (double)sz - (double)cz);
 }
 
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
@@ -831,17 +816,17 @@ int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaSt
     return 1;
 }
 
-int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, MixedState& m,
-                            cudaStream_t st)
+int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, double* u_out,
+                            MixedU* u2_out, cudaStream_t st)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, md.c, m.u2);
+    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, md.c, u_out, u2_out);
     return 1;
 }
 
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                          const MixedState& m, cudaStream_t st)
+                          const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
@@ -854,16 +839,16 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     mm.ntab = m.ntab;
     const int g = blocks_for(rows);
     switch ((md.fracture ? 0 : 10) + mixed_variant()) {
-    case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
-    default: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm); break;
+    case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    default: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
     }
     return 1;
 }

@@ -226,7 +226,12 @@ cpd_status cpd_compute_energy_noalloc(cpd_system* sys, double* W_out, double* ph
 
 cpd_status cpd_init(cpd_system* sys);
 /* num_steps velocity-Verlet steps. Asynchronous: returns once the work is
- * queued on the stream (cpd_synchronize or any download waits for it). */
+ * queued on the stream (cpd_synchronize or any download waits for it).
+ * For PD systems without contact on the FP64 and MIXED kernels, each step is
+ * one bond-kernel launch that also applies the force boundary conditions and
+ * both half steps (when every particle and force component has at most one
+ * boundary-condition operation); results are bit-identical to the separate
+ * stages of cpd_step_stage. */
 cpd_status cpd_step(cpd_system* sys, int32_t num_steps);
 cpd_status cpd_synchronize(cpd_system* sys);
 /* One stage of one time step, for callers that run their own device code

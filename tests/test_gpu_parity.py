@@ -204,6 +204,32 @@ def test_linear_lps_fracture_is_lps(cuda, oracle):
     assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
 
 
+@pytest.mark.parametrize("precision", [1, 2])
+@pytest.mark.parametrize("problem", ["plate", "lps"])
+def test_fused_step_equals_separate_stages(cuda, precision, problem):
+    """cpd_step runs one bond kernel per step with the boundary conditions
+    and both half steps in its epilogue (alternating displacement buffers);
+    the four separate stages of cpd_step_stage give the same bits, for odd and
+    even chunk lengths (ForceValue BC on the plate, per-particle ForceAdd
+    traction on the LPS box)."""
+    if problem == "plate":
+        prob = P.plate_impact(num_cells=(96, 48, 6), steps=60, v0=60.0)
+    else:
+        prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
+        prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
+    a = P.setup(cuda.System(dict(prob["params"], precision=precision)), prob)
+    b = P.setup(cuda.System(dict(prob["params"], precision=precision)), prob)
+    for chunk in (1, 2, 7, 50):
+        a.run(chunk)
+        for _ in range(chunk):
+            for stage in range(4):
+                b.step_stage(stage)
+        for fld in ("u", "v", "f"):
+            assert np.array_equal(a.get(fld), b.get(fld)), (chunk, fld)
+        assert np.array_equal(a.neighbors()[2], b.neighbors()[2])
+    assert a.compute_energy() == b.compute_energy()
+
+
 def test_errors_are_reported(cuda):
     s = cuda.System(dict(pd_model=P.PD_PMB, horizon=0.1, K=1.0, dt=1.0))
     with pytest.raises(cuda.CpdError):
