@@ -668,7 +668,9 @@ __global__ void __launch_bounds__(kBlock, MINB)
 // rows in unrolled 8-bond chunks with branch-free bond bits, 4 -> 3 with the
 // x / y lanes in paired FP32 instructions (default). Full plate on B200, ms
 // per launch for 3 / 4: 4.15 / 4.12 (4 compiled for 3 or 2 blocks per SM:
-// 5.05).
+// 5.05; 4 with the neighbour gathers as cp.async copies into shared memory
+// three bonds ahead: 8.28; a shared-memory tile of the lattice with its
+// halo: 5.86).
 // Full plate on B200, ms per launch for 0 / 1 / 2: 4.70 / 4.64 / 4.92.
 int mixed_variant()
 {
