@@ -13,6 +13,9 @@ headline `value`; the plain FP64 path runs the same steps from the same
 start and is reported beside it (`plain_fp64`, `mixed_vs_plain`), with the
 per-field error of mixed vs FP64 (`mixed_error_vs_fp64`).
 
+`other_workloads` (N = 1): short full-size runs of the LPS fracture box
+(8.0 M particles) and the Hertzian DEM packing (4.0 M spheres).
+
 `serving` (N = 1): a served stream of independent PMB/LPS jobs through the
 job server (continuous batching, mixed precision): capacity from a
 saturated pass, then Poisson arrivals at 0.8 x capacity with p50/p99 job
@@ -47,6 +50,8 @@ import numpy as np  # noqa: E402
 from cabanapd_b200 import problems as P  # noqa: E402
 
 PLATE_CELLS = (800, 400, 36)
+LPS_CELLS = (1000, 400, 20)   # LPS random-notch box, dx = 1e-4: 8.0 M particles
+DEM_DIMS = (200, 200, 100)    # Hertz packing: 4.0 M spheres
 CPU_SLAB_X = 50  # bounded CPU sample: the first 50 x-columns of the plate
 
 
@@ -313,6 +318,50 @@ def roofline(prec, r, bonds):
             "traffic": (tpb * bonds if tpb else None)}
 
 
+def measure_other(name, device, stream, steps, warmup):
+    """A short full-size measurement of another hot-path workload: the LPS
+    fracture box (8.0 M particles; the LPS kernels have no FP32 form, so
+    this is the FP64 path) or the Hertzian DEM packing (4.0 M spheres,
+    contact list rebuilt every 10 steps inside the timed steps)."""
+    import torch
+
+    import cabanapd_b200
+    if name == "lps":
+        prob = P.lps_random_notches(num_cells=LPS_CELLS, steps=steps)
+        prec, kernel = "fp64", "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"
+        wl = {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)}
+    else:
+        prob = P.dem_packing(lattice_dims=DEM_DIMS, steps=steps)
+        prec, kernel = "exact", "k_hertz_force<per-particle radius>"
+        wl = {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10}
+    s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
+    s.set_stream(stream.cuda_stream)
+    P.setup(s, prob)
+    s.step(warmup)
+    s.synchronize()
+    s.set_kernel_timing(True)
+    _, bonds0 = s.neighbor_stats()
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
+    k_ms, k_n, _ = s.kernel_time()
+    _, bonds1 = s.neighbor_stats()
+    bonds = bonds0 if name == "lps" else 0.5 * (bonds0 + bonds1)
+    out = dict(wl, particles=s.n, bonds=bonds, steps=steps, warmup=warmup,
+               precision=prec, ms_per_step=ms / steps,
+               value=bonds * steps / (ms / 1e3), unit="bond-updates/s",
+               kernel=kernel, kernel_ms_avg=k_ms / max(k_n, 1))
+    if name == "dem":
+        out["contact_rebuilds"] = s.contact_rebuilds()
+    s.close()
+    return out
+
+
 def run_gpu(args, world, rank, local, pg):
     import torch
 
@@ -388,6 +437,9 @@ def run_gpu(args, world, rank, local, pg):
         line["plain_fp64"] = plain
         line["mixed_vs_plain"] = value / plain["value"]
         line["mixed_error_vs_fp64"] = err
+    if world == 1 and not args.skip_others:
+        line["other_workloads"] = [measure_other("lps", device, stream, 20, 3),
+                                   measure_other("dem", device, stream, 50, 3)]
     if world == 1 and not args.skip_serve:
         line["serving"] = run_serving(args, device)
     if world == 1 and not args.skip_cpu:
@@ -574,8 +626,13 @@ def main():
     ap.add_argument("--only", action="store_true",
                     help="with mixed: skip the plain FP64 comparison run")
     ap.add_argument("--cells", default=None,
-                    help="plate cells nx,ny,nz (profiling on a smaller plate)")
+                    help="cells nx,ny,nz of the plate (or, with --only-other, of that "
+                         "workload) for profiling on a smaller case")
     ap.add_argument("--skip-serve", action="store_true", help="omit the served-stream leg")
+    ap.add_argument("--skip-others", action="store_true",
+                    help="omit the LPS-box and DEM-packing measurements")
+    ap.add_argument("--only-other", choices=["lps", "dem"], default=None,
+                    help="measure only that workload (for profiling) and print it")
     ap.add_argument("--serve-jobs", type=int, default=96,
                     help="served stream: number of jobs (512 for the full stream)")
     ap.add_argument("--serve-n", type=float, nargs=2, default=[1e3, 2e5],
@@ -589,14 +646,27 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    global PLATE_CELLS
+    global PLATE_CELLS, LPS_CELLS, DEM_DIMS
     if args.cells:
-        PLATE_CELLS = tuple(int(c) for c in args.cells.split(","))
+        cells = tuple(int(c) for c in args.cells.split(","))
+        if args.only_other == "lps":
+            LPS_CELLS = cells
+        elif args.only_other == "dem":
+            DEM_DIMS = cells
+        else:
+            PLATE_CELLS = cells
     world, rank, local, pg = (int(os.environ.get("WORLD_SIZE", "1")),
                               int(os.environ.get("RANK", "0")),
                               int(os.environ.get("LOCAL_RANK", "0")), None)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.only_other:
+        import torch
+        torch.cuda.set_device(local)
+        stream = torch.cuda.Stream(device=local)
+        print(json.dumps(measure_other(args.only_other, local, stream, args.steps, args.warmup)),
+              flush=True)
         return
     world, rank, local, pg = dist_setup()
     try:

@@ -583,11 +583,31 @@ bool fused_steps_enabled()
     return on;
 }
 
-bool fusable(cpd_system* s)
+bool fusable_kind(const cpd_system* s)
 {
-    if (!has_pd(s) || has_contact(s) || !(use_fast(s) || use_mixed(s))) return false;
-    if (s->bc_prog == 0 && build_bc_program(s) != CPD_OK) return false;
-    return s->bc_prog == 1;
+    return has_pd(s) && !has_contact(s) && (use_fast(s) || use_mixed(s));
+}
+
+// Builds what the fused step needs (second displacement buffers, the row
+// program of the boundary conditions); allocates and synchronises, so it
+// runs at init or when the conditions change, never inside a step.
+cpd_status prepare_fused(cpd_system* s)
+{
+    if (!fusable_kind(s) || !fused_steps_enabled()) return CPD_OK;
+    if (s->bc_prog == 0) CPD_OK_OR_RETURN(build_bc_program(s));
+    if (s->bc_prog != 1) return CPD_OK;
+    if (!s->u_alt) CPD_CUDA(dev_alloc(&s->u_alt, sizeof(double) * 3 * s->npad, s->stream));
+    if (use_mixed(s) && !s->u2_alt)
+        CPD_CUDA(dev_alloc(&s->u2_alt, sizeof(MixedU) * s->npad, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+// Whether cpd_step runs the fused step now (everything prepared).
+bool fused_ready(const cpd_system* s)
+{
+    return fused_steps_enabled() && fusable_kind(s) && s->bc_prog == 1 && s->u_alt &&
+           (!use_mixed(s) || s->u2_alt);
 }
 
 // num_steps steps as: first half step, then one bond kernel per step whose
@@ -598,9 +618,6 @@ bool fusable(cpd_system* s)
 cpd_status step_fused(cpd_system* s, int32_t num_steps)
 {
     const bool mixed = use_mixed(s);
-    const size_t vb = sizeof(double) * 3 * s->npad;
-    if (!s->u_alt) CPD_CUDA(dev_alloc(&s->u_alt, vb, s->stream));
-    if (mixed && !s->u2_alt) CPD_CUDA(dev_alloc(&s->u2_alt, sizeof(MixedU) * s->npad, s->stream));
     const bool start_alt = ((num_steps - 1) & 1) != 0;
     double* ucur = start_alt ? s->u_alt : s->u;
     double* unxt = start_alt ? s->u : s->u_alt;
@@ -1023,6 +1040,7 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
     hb.values.assign(values, values + (kind == CPD_BC_FORCE_ADD ? count : 1));
     s->hbcs.push_back(std::move(hb));
     free_bc_program(s);
+    if (s->initialized) CPD_OK_OR_RETURN(prepare_fused(s));
     return CPD_OK;
 }
 
@@ -1037,6 +1055,7 @@ cpd_status cpd_clear_boundary_conditions(cpd_system* s)
     s->bcs.clear();
     s->hbcs.clear();
     free_bc_program(s);
+    if (s->initialized) CPD_OK_OR_RETURN(prepare_fused(s));
     return CPD_OK;
 }
 
@@ -1117,6 +1136,7 @@ cpd_status cpd_init(cpd_system* s)
     }
     if (has_pd(s)) CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
     CPD_OK_OR_RETURN(apply_force_bcs(s));
+    CPD_OK_OR_RETURN(prepare_fused(s));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     s->initialized = true;
     return CPD_OK;
@@ -1129,7 +1149,14 @@ cpd_status cpd_step(cpd_system* s, int32_t num_steps)
     if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step");
     if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
     CPD_CUDA(cudaSetDevice(s->device));
-    if (num_steps > 0 && fused_steps_enabled() && fusable(s)) return step_fused(s, num_steps);
+    if (num_steps > 0 && !fused_ready(s)) {
+        // Prepare now unless the stream is being captured (then the steps
+        // run as separate kernels, which need nothing prepared).
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CPD_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+        if (cs == cudaStreamCaptureStatusNone) CPD_OK_OR_RETURN(prepare_fused(s));
+    }
+    if (num_steps > 0 && fused_ready(s)) return step_fused(s, num_steps);
     const ParticleView p = view(s);
     for (int32_t k = 0; k < num_steps; k++) {
         CPD_OK_OR_RETURN(vv_initial(s));
@@ -1262,7 +1289,7 @@ cpd_status cpd_kernel_time(cpd_system* s, double* total_ms, int64_t* launches,
         if (!has_pd(s)) per_row += 24.0 + 16.0;  // Hertz: v, rho (+vol already)
         // The fused step's bond kernel also integrates: read v and rho,
         // write v and the next u (48 + 8 + 24 + 24 B) instead of writing f.
-        if (fused_steps_enabled() && fusable(s)) per_row += 48.0 + 8.0 + 24.0 + 24.0 - 24.0;
+        if (fused_ready(s)) per_row += 48.0 + 8.0 + 24.0 + 24.0 - 24.0;
         *bytes_per_launch = per_row * rows + per_bond * (double)nl.total;
     }
     return CPD_OK;

@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kBlock)
 // m* = m_i (m_j / (m_i + m_j)), which round to the single-radius values when
 // R_i == R_j.
 template <bool PER_PARTICLE>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 3)
     k_hertz_force(ParticleView p, EllView nl, ModelDev md, bool reset)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

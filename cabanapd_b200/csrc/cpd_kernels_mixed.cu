@@ -110,43 +110,61 @@ struct LatticeLut {
     const int16_t* lut;  // [(2 half_x + 1)(2 half_y + 1)(2 half_z + 1)] -> code or -1
 };
 
+// Codes every bond and records, per code, the smallest index delta j - i
+// among its bonds (deterministic; on an x-fastest lattice all are equal),
+// biased by 2^31 so signed order survives the unsigned minimum. The minimum
+// is reduced in the warp (lanes holding the same code), then per block in
+// shared memory, and a block updates the global value only to lower it.
 __global__ void __launch_bounds__(kBlock)
-    k_code_bonds(ParticleView p, EllView nl, LatticeLut L, uint8_t* code,
-                 unsigned long long* delta)
+    k_code_bonds(ParticleView p, EllView nl, LatticeLut L, uint8_t* code, unsigned int* delta)
 {
+    __shared__ unsigned int s_min[kMixedGeneric];
+    for (int t = threadIdx.x; t < kMixedGeneric; t += blockDim.x) s_min[t] = 0xffffffffu;
+    __syncthreads();
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+    const bool row = i < p.n;
     const int64_t np = p.npad;
-    const int cnt = nl.count[i];
+    const int cnt = row ? nl.count[i] : 0;
+    const int kmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     const int nx = 2 * L.half[0] + 1, ny = 2 * L.half[1] + 1;
-    for (int k = 0; k < cnt; ++k) {
-        const int64_t j = nl.idx[(int64_t)k * np + i];
+    for (int k = 0; k < kmax; ++k) {
         int c = kMixedGeneric;
-        int o[3];
-        bool ok = true;
-        for (int d = 0; d < 3; ++d) {
-            const double dd = p.x[d * np + j] - p.x[d * np + i];
-            const double a = rint(dd / L.h[d]);
-            if (fabs(dd - a * L.h[d]) > 1e-6 * L.h[d] || fabs(a) > L.half[d]) ok = false;
-            o[d] = (int)a;
-        }
-        if (ok) {
-            const int e = L.lut[(o[0] + L.half[0]) + nx * ((o[1] + L.half[1]) + ny * (o[2] + L.half[2]))];
-            if (e >= 0) {
-                c = e;
-                // The code's index delta: the smallest j - i among its bonds
-                // (deterministic; on an x-fastest lattice all are equal).
-                // Stored biased by 2^62 so signed order survives the
-                // unsigned atomic.
-                atomicMin(delta + c, (unsigned long long)((long long)(j - i) + (1LL << 62)));
+        unsigned int v = 0xffffffffu;
+        if (k < cnt) {
+            const int64_t j = nl.idx[(int64_t)k * np + i];
+            int o[3];
+            bool ok = true;
+            for (int d = 0; d < 3; ++d) {
+                const double dd = p.x[d * np + j] - p.x[d * np + i];
+                const double a = rint(dd / L.h[d]);
+                if (fabs(dd - a * L.h[d]) > 1e-6 * L.h[d] || fabs(a) > L.half[d]) ok = false;
+                o[d] = (int)a;
             }
+            if (ok) {
+                const int e = L.lut[(o[0] + L.half[0]) +
+                                    nx * ((o[1] + L.half[1]) + ny * (o[2] + L.half[2]))];
+                if (e >= 0) {
+                    c = e;
+                    v = (unsigned int)((long long)(j - i) + (1LL << 31));
+                }
+            }
+            code[(int64_t)k * np + i] = (uint8_t)c;
         }
-        code[(int64_t)k * np + i] = (uint8_t)c;
+        // Every lane of the warp takes part (inactive and generic lanes with
+        // the generic code, which records nothing).
+        const unsigned int grp = __match_any_sync(0xffffffffu, c);
+        const unsigned int m = __reduce_min_sync(grp, v);
+        if (c != kMixedGeneric && (int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicMin(&s_min[c], m);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kMixedGeneric; t += blockDim.x) {
+        const unsigned int m = s_min[t];
+        if (m != 0xffffffffu && m < *(volatile unsigned int*)(delta + t)) atomicMin(delta + t, m);
     }
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_verify_delta(ParticleView p, EllView nl, const unsigned long long* delta, uint8_t* code)
+    k_verify_delta(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -157,7 +175,7 @@ __global__ void __launch_bounds__(kBlock)
         const int c = code[o];
         if (c == kMixedGeneric) continue;
         const int64_t j = nl.idx[o];
-        if ((long long)delta[c] - (1LL << 62) != (long long)(j - i)) code[o] = (uint8_t)kMixedGeneric;
+        if ((long long)delta[c] - (1LL << 31) != (long long)(j - i)) code[o] = (uint8_t)kMixedGeneric;
     }
 }
 
@@ -769,12 +787,12 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                     }
             if (lattice && !tab.empty()) {
                 int16_t* d_lut = nullptr;
-                unsigned long long* d_delta = nullptr;
+                unsigned int* d_delta = nullptr;
                 CPD_TRY(dev_alloc(&d_lut, sizeof(int16_t) * lut.size(), st));
-                CPD_TRY(dev_alloc(&d_delta, sizeof(unsigned long long) * kMixedGeneric, st));
+                CPD_TRY(dev_alloc(&d_delta, sizeof(unsigned int) * kMixedGeneric, st));
                 CPD_TRY(cudaMemcpyAsync(d_lut, lut.data(), sizeof(int16_t) * lut.size(),
                                         cudaMemcpyHostToDevice, st));
-                CPD_TRY(cudaMemsetAsync(d_delta, 0xff, sizeof(unsigned long long) * kMixedGeneric, st));
+                CPD_TRY(cudaMemsetAsync(d_delta, 0xff, sizeof(unsigned int) * kMixedGeneric, st));
                 LatticeLut L;
                 for (int d = 0; d < 3; ++d) {
                     L.h[d] = h[d];
@@ -784,13 +802,12 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                 k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
                 k_verify_delta<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code);
                 launches += 2;
-                std::vector<unsigned long long> delta(kMixedGeneric);
-                CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta,
-                                        sizeof(unsigned long long) * kMixedGeneric,
+                std::vector<unsigned int> delta(kMixedGeneric);
+                CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
                                         cudaMemcpyDeviceToHost, st));
                 CPD_TRY(cudaStreamSynchronize(st));
                 for (size_t t = 0; t < tab.size(); ++t)
-                    tab[t].delta = (int32_t)((long long)delta[t] - (1LL << 62));
+                    tab[t].delta = (int32_t)((long long)delta[t] - (1LL << 31));
                 CPD_TRY(cudaMemcpyAsync(m.table, tab.data(), sizeof(MixedStencil) * tab.size(),
                                         cudaMemcpyHostToDevice, st));
                 CPD_TRY(cudaStreamSynchronize(st));
