@@ -394,14 +394,22 @@ cpd_status timed_end(cpd_system* s, cudaEvent_t e0)
     return CPD_OK;
 }
 
-bool use_mixed(const cpd_system* s)
+// CPD_MIXED set-up applies to PMB and LPS without contact; the LPS kernels
+// then need every row to be a stencil row (mixed.lps_ok), else LPS keeps the
+// FP64 kernels.
+bool wants_mixed(const cpd_system* s)
 {
-    return s->params.precision == CPD_MIXED && s->md.pd == CPD_PD_PMB &&
-           s->md.contact == CPD_CONTACT_NONE;
+    return s->params.precision == CPD_MIXED && s->md.contact == CPD_CONTACT_NONE &&
+           (s->md.pd == CPD_PD_PMB || s->md.pd == CPD_PD_LPS);
 }
 
-// The throughput FP64 kernels serve CPD_FP64, and CPD_MIXED for the models
-// the mixed kernel does not cover (LPS).
+bool use_mixed(const cpd_system* s)
+{
+    return wants_mixed(s) && (s->md.pd == CPD_PD_PMB || s->mixed.lps_ok);
+}
+
+// The throughput FP64 kernels serve CPD_FP64, and CPD_MIXED where the mixed
+// kernels do not apply.
 bool use_fast(const cpd_system* s)
 {
     return (s->params.precision == CPD_FP64 ||
@@ -427,9 +435,15 @@ cpd_status pd_force_on(cpd_system* s, const ParticleView& p, const MixedState& m
 
 cpd_status pd_force(cpd_system* s) { return pd_force_on(s, view(s), s->mixed, StepEpilogue{}); }
 
-// LPS weighted volume (when compute_m) and dilatation.
-cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, bool compute_m)
+// LPS weighted volume (when compute_m) and dilatation; on the mixed path m
+// carries the displacement split of p.u.
+cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, const MixedState& m,
+                          bool compute_m)
 {
+    if (use_mixed(s)) {
+        CPD_LAUNCHED(launch_lps_mtheta_mixed(p, pd_view(s), s->md, m, compute_m, s->stream));
+        return CPD_OK;
+    }
     if (use_fast(s)) {
         CPD_LAUNCHED(launch_lps_m_theta_fast(p, pd_view(s), s->md, compute_m, s->stream));
         return CPD_OK;
@@ -439,7 +453,10 @@ cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, bool compute_m)
     return CPD_OK;
 }
 
-cpd_status lps_prepare(cpd_system* s, bool compute_m) { return lps_prepare_on(s, view(s), compute_m); }
+cpd_status lps_prepare(cpd_system* s, bool compute_m)
+{
+    return lps_prepare_on(s, view(s), s->mixed, compute_m);
+}
 
 cpd_status contact_force(cpd_system* s, bool reset)
 {
@@ -631,7 +648,7 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps)
     StepEpilogue ep;
     ep.dt = s->params.dt;
     ep.half_dt = 0.5 * s->params.dt;
-    ep.c = s->md.c;
+    ep.c = mixed_wscale(s->md);
     ep.bc_bits = s->bc_bits;
     ep.bc_row = s->bc_row;
     ep.bc_keep = s->bc_keep;
@@ -645,7 +662,7 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps)
         ep.mode = k + 1 < num_steps ? 2 : 1;
         ep.u_next = unxt;
         ep.u2_next = u2nxt;
-        if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, s->md.fracture != 0));
+        if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, mk, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
         std::swap(ucur, unxt);
         std::swap(u2cur, u2nxt);
@@ -910,8 +927,9 @@ cpd_status cpd_build_neighbors(cpd_system* s)
                                     s->pd, s->stream, err);
         if (l < 0) return set_error(CPD_ERR_CUDA, "neighbour build: " + err);
         s->launches += l;
-        if (use_mixed(s)) {
-            l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, s->mixed, s->stream, err);
+        if (wants_mixed(s)) {
+            l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
+                              s->stream, err);
             if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
             s->launches += l;
         }

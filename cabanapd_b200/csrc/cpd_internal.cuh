@@ -201,9 +201,15 @@ struct MixedState {
     int ntab = 0;
     double h[3] = {0, 0, 0};
     size_t bytes = 0;     // device bytes held
+    float2* ab = nullptr; // LPS: per-particle FP32 (theta_coeff theta / m, s_coeff / m)
+    int lps_ok = 0;       // LPS: every row is a stencil row (the mixed LPS kernels apply)
 };
-int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
+// lps: set up the LPS mixed kernels too (lps_ok, ab).
+int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err);
+int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                            const MixedState& m, bool with_m, cudaStream_t st);
+double mixed_wscale(const Model& md);
 void free_mixed(MixedState& m, cudaStream_t st);
 int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st);
 int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, double* u_out,

@@ -188,9 +188,10 @@ __global__ void __launch_bounds__(kBlock)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int nmask = (ntab + 31) / 32;
-    bool subset = i < p.n;
-    bool full = subset;
-    if (subset) {
+    // Lanes past the last row do not vote against their warp.
+    bool subset = true;
+    bool full = true;
+    if (i < p.n) {
         const int64_t np = p.npad;
         const int cnt = nl.count[i];
         full = cnt == ntab;
@@ -680,6 +681,218 @@ __global__ void __launch_bounds__(kBlock, MINB)
                         (double)sz - (double)cz);
 }
 
+// ---------------------------------------------------------------------------
+// LPS, mixed precision (force/CabanaPD_LPS.hpp:287-447 with the model of
+// force_models/CabanaPD_LPS.hpp:85-134). Stencil rows only: jobs with an
+// irregular row keep the FP64 LPS kernels. FP32 bond arithmetic as in the
+// PMB kernel (split displacements, stretch without cancellation), Kahan-
+// compensated FP32 sums; m, theta and the per-particle force factors
+// a = theta_coeff theta / m and b = s_coeff / m are formed in FP64 from the
+// sums and kept as FP32 pairs for the neighbours' force loop. The break test
+// follows the LPS rule (no-fail of the row only, tested twice by the
+// reference) with the FP64 re-test inside the guard band.
+struct MixedLps {
+    float s0, guard;
+    double bbc;
+    double theta_coeff, s_coeff;
+    int ntab;
+};
+
+// omega xi^2 of a stencil entry (force_models/CabanaPD_LPS.hpp:85-106) and
+// the omega xi factor of the force coefficient (:118-134).
+template <int INFL>
+__device__ __forceinline__ float lps_w(const MixedStencil& t)
+{
+    return INFL == 1 ? t.xi : t.xi * t.xi;
+}
+template <int INFL>
+__device__ __forceinline__ float lps_oxi(const MixedStencil& t)
+{
+    return INFL == 1 ? 1.f : t.xi;
+}
+
+// Weighted volume (when WITH_M) and dilatation of one row, one pass.
+template <bool FRACTURE, int INFL, bool WITH_M>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_mtheta_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                       float2* __restrict__ ab)
+{
+    __shared__ MixedStencil tab[kMixedGeneric];
+    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
+    __syncthreads();
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const MixedU ui = mv.u2[i];
+    const float4 uhi = ui.hi, uli = ui.lo;
+    const float2 nuhi_xy = f2(-uhi.x, -uhi.y), nuli_xy = f2(-uli.x, -uli.y);
+    const float nuhi_z = -uhi.z, nuli_z = -uli.z;
+    const MixedU* __restrict__ u2_i = mv.u2 + i;
+    const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    float ms = 0.f, mc = 0.f, ts = 0.f, tc = 0.f;
+    if (kind == 2) {
+        for (int base = 0; base < md.ntab; base += 32) {
+            const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+            const int lim = min(32, md.ntab - base);
+            for (int b = 0; b < lim; b += 8) {
+                const uint32_t w8 = word >> b;
+                const int n8 = min(8, lim - b);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (u < n8) {
+                        const MixedStencil t = tab[base + b + u];
+                        const MixedU uj = u2_i[t.delta];
+                        MixedBond2 bd;
+                        mixed_bond2(f2(t.x, t.y), t.z, t.xi, t.xiinv, uj.hi, uj.lo, nuhi_xy,
+                                    nuhi_z, nuli_xy, nuli_z, bd);
+                        const float on = ((w8 >> u) & 1u) ? 1.f : 0.f;
+                        const float wv = on * lps_w<INFL>(t) * uj.hi.w;
+                        if (WITH_M) kahan_add(ms, mc, wv);
+                        kahan_add(ts, tc, wv * bd.s);
+                    }
+                }
+            }
+        }
+    } else {
+        // Subset rows: bond slot = rank of the entry among the present ones.
+        const int nmask = (md.ntab + 31) / 32;
+        int slot = 0;
+        uint32_t word = FRACTURE ? nl.mu[i] : 0xffffffffu;
+        for (int w = 0; w < nmask; ++w) {
+            const uint32_t pm = mv.pmask[(int64_t)w * np + i];
+            const int kend = min(32, md.ntab - 32 * w);
+            for (int b = 0; b < kend; ++b) {
+                if (!((pm >> b) & 1u)) continue;
+                if (FRACTURE && (slot & 31) == 0 && slot > 0)
+                    word = nl.mu[(int64_t)(slot >> 5) * np + i];
+                const bool on = (word >> (slot & 31)) & 1u;
+                ++slot;
+                if (!on) continue;
+                const MixedStencil t = tab[32 * w + b];
+                const MixedU uj = u2_i[t.delta];
+                MixedBond2 bd;
+                mixed_bond2(f2(t.x, t.y), t.z, t.xi, t.xiinv, uj.hi, uj.lo, nuhi_xy, nuhi_z,
+                            nuli_xy, nuli_z, bd);
+                const float wv = lps_w<INFL>(t) * uj.hi.w;
+                if (WITH_M) kahan_add(ms, mc, wv);
+                kahan_add(ts, tc, wv * bd.s);
+            }
+        }
+    }
+    const double m = WITH_M ? (double)ms - (double)mc : p.m[i];
+    const double th = (!FRACTURE || m > 0) ? 3.0 * ((double)ts - (double)tc) / m : 0.0;
+    if (WITH_M) p.m[i] = m;
+    p.theta[i] = th;
+    const double a = md.theta_coeff * th / m, b = md.s_coeff / m;
+    p.lps_a[i] = a;
+    p.lps_b[i] = b;
+    ab[i] = make_float2((float)a, (float)b);
+}
+
+__device__ __forceinline__ bool lps_critical(float s, bool nofail_i, const MixedLps& md,
+                                             const ParticleView& p, int64_t i, int64_t j)
+{
+    // force/CabanaPD_LPS.hpp:417-418: only the row's no-fail flag counts.
+    if (nofail_i) return false;
+    if (fabsf(s - md.s0) <= md.guard) return critical_exact64(p.x, p.u, p.npad, i, j, md.bbc);
+    return s >= md.s0;
+}
+
+template <bool FRACTURE, int INFL>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                      const float2* __restrict__ ab, StepEpilogue ep)
+{
+    __shared__ MixedStencil tab[kMixedGeneric];
+    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
+    __syncthreads();
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const MixedU ui = mv.u2[i];
+    const float4 uhi = ui.hi, uli = ui.lo;
+    const bool nofail_i = FRACTURE ? (uli.w != 0.f) : false;
+    const float2 nuhi_xy = f2(-uhi.x, -uhi.y), nuli_xy = f2(-uli.x, -uli.y);
+    const float nuhi_z = -uhi.z, nuli_z = -uli.z;
+    const float2 abi = ab[i];
+    const MixedU* __restrict__ u2_i = mv.u2 + i;
+    const float2* __restrict__ ab_i = ab + i;
+    const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
+    float sz = 0.f, cz = 0.f;
+    if (kind == 2) {
+        for (int base = 0; base < md.ntab; base += 32) {
+            const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+            uint32_t clr = 0;
+            const int lim = min(32, md.ntab - base);
+            for (int b = 0; b < lim; b += 8) {
+                const uint32_t w8 = word >> b;
+                uint32_t c8 = 0;
+                const int n8 = min(8, lim - b);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (u < n8) {
+                        const MixedStencil t = tab[base + b + u];
+                        const MixedU uj = u2_i[t.delta];
+                        const float2 abj = ab_i[t.delta];
+                        MixedBond2 bd;
+                        mixed_bond2(f2(t.x, t.y), t.z, t.xi, t.xiinv, uj.hi, uj.lo, nuhi_xy,
+                                    nuhi_z, nuli_xy, nuli_z, bd);
+                        float kf = (abi.x + abj.x + bd.s * (abi.y + abj.y)) * lps_oxi<INFL>(t) *
+                                   uj.hi.w * bd.rinv;
+                        if (FRACTURE) {
+                            const bool crit = lps_critical(bd.s, nofail_i, md, p, i, i + t.delta);
+                            c8 |= (uint32_t)crit << u;
+                            kf = (((w8 >> u) & 1u) && !crit) ? kf : 0.f;
+                        }
+                        kahan_add2(sxy, cxy, __fmul2_rn(f2(kf, kf), bd.rxy));
+                        kahan_add(sz, cz, kf * bd.rz);
+                    }
+                }
+                clr |= c8 << b;
+            }
+            if (FRACTURE && (word & clr)) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+        }
+    } else {
+        const int nmask = (md.ntab + 31) / 32;
+        int slot = 0, cur_w = 0;
+        uint32_t word = FRACTURE ? nl.mu[i] : 0xffffffffu;
+        uint32_t old = word;
+        for (int w = 0; w < nmask; ++w) {
+            const uint32_t pm = mv.pmask[(int64_t)w * np + i];
+            const int kend = min(32, md.ntab - 32 * w);
+            for (int b = 0; b < kend; ++b) {
+                if (!((pm >> b) & 1u)) continue;
+                if (FRACTURE && (slot >> 5) != cur_w) {
+                    if (word != old) nl.mu[(int64_t)cur_w * np + i] = word;
+                    cur_w = slot >> 5;
+                    word = nl.mu[(int64_t)cur_w * np + i];
+                    old = word;
+                }
+                const int sb = slot & 31;
+                ++slot;
+                const MixedStencil t = tab[32 * w + b];
+                const MixedU uj = u2_i[t.delta];
+                const float2 abj = ab_i[t.delta];
+                MixedBond2 bd;
+                mixed_bond2(f2(t.x, t.y), t.z, t.xi, t.xiinv, uj.hi, uj.lo, nuhi_xy, nuhi_z,
+                            nuli_xy, nuli_z, bd);
+                float kf = (abi.x + abj.x + bd.s * (abi.y + abj.y)) * lps_oxi<INFL>(t) * uj.hi.w *
+                           bd.rinv;
+                if (FRACTURE) {
+                    if (lps_critical(bd.s, nofail_i, md, p, i, i + t.delta)) word &= ~(1u << sb);
+                    kf = ((word >> sb) & 1u) ? kf : 0.f;
+                }
+                kahan_add2(sxy, cxy, __fmul2_rn(f2(kf, kf), bd.rxy));
+                kahan_add(sz, cz, kf * bd.rz);
+            }
+        }
+        if (FRACTURE && word != old) nl.mu[(int64_t)cur_w * np + i] = word;
+    }
+    step_epilogue<true>(p, ep, i, (double)sxy.x - (double)cxy.x, (double)sxy.y - (double)cxy.y,
+                        (double)sz - (double)cz);
+}
+
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
 // (64 registers), 1 -> 4 blocks with the full-stencil loop software
 // pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
@@ -713,13 +926,13 @@ int mixed_variant()
 
 void free_mixed(MixedState& m, cudaStream_t st)
 {
-    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.ab};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
 }
 
-int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
+int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err)
 {
     int launches = 0;
@@ -821,6 +1034,21 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
                 k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), m.code, m.ntab,
                                                                  m.pmask, m.warp_kind);
                 launches++;
+                if (lps) {
+                    // The LPS kernels take stencil rows only: every warp of rows
+                    // must be kind 1 or 2.
+                    const int64_t nw = (rows + 31) / 32;
+                    std::vector<uint8_t> kinds(nw);
+                    CPD_TRY(cudaMemcpyAsync(kinds.data(), m.warp_kind, nw, cudaMemcpyDeviceToHost,
+                                            st));
+                    CPD_TRY(cudaStreamSynchronize(st));
+                    m.lps_ok = std::all_of(kinds.begin(), kinds.end(),
+                                           [](uint8_t k) { return k != 0; }) ? 1 : 0;
+                    if (m.lps_ok) {
+                        CPD_TRY(dev_alloc(&m.ab, sizeof(float2) * np, st));
+                        m.bytes += sizeof(float2) * np;
+                    }
+                }
             }
         }
     }
@@ -828,10 +1056,14 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff,
     return launches;
 }
 
+// Scale of the volume in the w lane of the displacement split: the PMB
+// micromodulus (its force is c s vol_j / r), 1 for LPS.
+double mixed_wscale(const Model& md) { return md.pd == CPD_PD_PMB ? md.c : 1.0; }
+
 int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st)
 {
     if (p.n <= 0) return 0;
-    k_split_u<<<blocks_for(p.n), kBlock, 0, st>>>(p, md.c, m.u2);
+    k_split_u<<<blocks_for(p.n), kBlock, 0, st>>>(p, mixed_wscale(md), m.u2);
     return 1;
 }
 
@@ -840,13 +1072,66 @@ int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, d
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, md.c, u_out, u2_out);
+    k_vv_initial_mixed<<<blocks_for(rows), kBlock, 0, st>>>(p, dt, 0.5 * dt, mixed_wscale(md),
+                                                            u_out, u2_out);
+    return 1;
+}
+
+MixedLps to_mixed_lps(const Model& md, const MixedState& m)
+{
+    MixedLps l;
+    l.s0 = (float)md.s0;
+    l.guard = (float)(1e-4 * md.s0);
+    l.bbc = md.bond_break_coeff;
+    l.theta_coeff = md.theta_coeff;
+    l.s_coeff = md.s_coeff;
+    l.ntab = m.ntab;
+    return l;
+}
+
+int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                            const MixedState& m, bool with_m, cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    const MixedLps l = to_mixed_lps(md, m);
+    const int g = blocks_for(rows);
+    const int key = (md.fracture ? 4 : 0) + (md.influence == 1 ? 2 : 0) + (with_m ? 1 : 0);
+    switch (key) {
+    case 0: k_lps_mtheta_mixed<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 1: k_lps_mtheta_mixed<false, 0, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 2: k_lps_mtheta_mixed<false, 1, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 3: k_lps_mtheta_mixed<false, 1, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 4: k_lps_mtheta_mixed<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 5: k_lps_mtheta_mixed<true, 0, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    case 6: k_lps_mtheta_mixed<true, 1, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    default: k_lps_mtheta_mixed<true, 1, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    }
+    return 1;
+}
+
+int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    const MixedLps l = to_mixed_lps(md, m);
+    const int g = blocks_for(rows);
+    switch ((md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0)) {
+    case 0: k_lps_force_mixed<false, 0><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
+    case 1: k_lps_force_mixed<false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
+    case 2: k_lps_force_mixed<true, 0><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
+    default: k_lps_force_mixed<true, 1><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
+    }
     return 1;
 }
 
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
 {
+    if (md.pd == CPD_PD_LPS) return launch_lps_force_mixed(p, nl, md, m, ep, st);
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
     MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};

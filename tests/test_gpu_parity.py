@@ -377,9 +377,41 @@ def test_mixed_elastic_wave(cuda, oracle):
     assert _nrel(g.get("f"), o.get("f")) <= 1e-5
 
 
-def test_mixed_falls_back_to_fp64_for_lps(cuda, oracle):
-    prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=40)
+def test_mixed_lps_random_notches(cuda, oracle):
+    """LPS fracture on the mixed kernels (stencil rows, FP32 bonds, Kahan
+    sums, FP64 re-test in the guard band): same bars as the PMB mixed path."""
+    prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
+    prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
     g, o = _pair_mixed(cuda, oracle, prob)
+    for _ in range(3):
+        g.run(20)
+        o.run(20)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        assert _nrel(g.get("u"), o.get("u")) <= 1e-6
+        for fld in ("v", "f", "m", "theta"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-5, fld
+        dg = g.compute_energy()[1]
+        do = o.compute_energy()[1]
+        assert _rel(dg, do) <= 1e-12
+    assert (o.neighbors()[2] == 0).sum() > 0
+
+
+def test_mixed_lps_elastic_wave(cuda, oracle, golden):
+    """The LinearLPS (= LPS) elastic wave of the regression test on the mixed
+    kernels, against the FP64 oracle."""
+    prob = P.elastic_wave_lps(golden["elastic_wave"]["input"])
+    g, o = _pair_mixed(cuda, oracle, prob)
+    g.run(prob["num_steps"])
+    o.run(prob["num_steps"])
+    assert _nrel(g.get("u"), o.get("u")) <= 1e-6
+    assert _nrel(g.get("theta"), o.get("theta")) <= 1e-5
+
+
+def test_mixed_lps_irregular_rows_keep_fp64(cuda, oracle):
+    """Morton order breaks the lattice index deltas, so rows are irregular
+    and LPS under CPD_MIXED keeps the FP64 kernels (<= 1e-12)."""
+    prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=40)
+    g, o = _pair_mixed(cuda, oracle, prob, ordering=1)
     g.run(40)
     o.run(40)
     assert _nrel(g.get("u"), o.get("u")) <= 1e-12
