@@ -14,7 +14,8 @@ start and is reported beside it (`plain_fp64`, `mixed_vs_plain`), with the
 per-field error of mixed vs FP64 (`mixed_error_vs_fp64`).
 
 `other_workloads` (N = 1): short full-size runs of the LPS fracture box
-(8.0 M particles) and the Hertzian DEM packing (4.0 M spheres).
+(8.0 M particles; mixed beside plain FP64 with the error between them) and
+the Hertzian DEM packing (4.0 M spheres).
 
 `serving` (N = 1): a served stream of independent PMB/LPS jobs through the
 job server (continuous batching, mixed precision): capacity from a
@@ -318,29 +319,11 @@ def roofline(prec, r, bonds):
             "traffic": (tpb * bonds if tpb else None)}
 
 
-def measure_other(name, device, stream, steps, warmup):
-    """A short full-size measurement of another hot-path workload: the LPS
-    fracture box (8.0 M particles; the LPS kernels have no FP32 form, so
-    this is the FP64 path) or the Hertzian DEM packing (4.0 M spheres,
-    contact list rebuilt every 10 steps inside the timed steps)."""
+def _time_system(s, stream, device, steps, warmup):
     import torch
-
-    import cabanapd_b200
-    if name == "lps":
-        prob = P.lps_random_notches(num_cells=LPS_CELLS, steps=steps)
-        prec, kernel = "fp64", "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"
-        wl = {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)}
-    else:
-        prob = P.dem_packing(lattice_dims=DEM_DIMS, steps=steps)
-        prec, kernel = "exact", "k_hertz_force<per-particle radius>"
-        wl = {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10}
-    s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
-    s.set_stream(stream.cuda_stream)
-    P.setup(s, prob)
     s.step(warmup)
     s.synchronize()
     s.set_kernel_timing(True)
-    _, bonds0 = s.neighbor_stats()
     torch.cuda.synchronize(device)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -348,17 +331,58 @@ def measure_other(name, device, stream, steps, warmup):
     s.step(steps)
     ev1.record(stream)
     torch.cuda.synchronize(device)
-    ms = ev0.elapsed_time(ev1)
     k_ms, k_n, _ = s.kernel_time()
-    _, bonds1 = s.neighbor_stats()
-    bonds = bonds0 if name == "lps" else 0.5 * (bonds0 + bonds1)
-    out = dict(wl, particles=s.n, bonds=bonds, steps=steps, warmup=warmup,
-               precision=prec, ms_per_step=ms / steps,
-               value=bonds * steps / (ms / 1e3), unit="bond-updates/s",
-               kernel=kernel, kernel_ms_avg=k_ms / max(k_n, 1))
-    if name == "dem":
-        out["contact_rebuilds"] = s.contact_rebuilds()
-    s.close()
+    return ev0.elapsed_time(ev1), k_ms / max(k_n, 1)
+
+
+def measure_other(name, device, stream, steps, warmup):
+    """A short full-size measurement of another hot-path workload: the LPS
+    fracture box (8.0 M particles), mixed precision beside plain FP64 from
+    the same start with the error of mixed vs FP64, or the Hertzian DEM
+    packing (4.0 M spheres, contact list rebuilt every 10 steps inside the
+    timed steps; Hertz runs in FP64)."""
+    import cabanapd_b200
+    if name == "lps":
+        prob = P.lps_random_notches(num_cells=LPS_CELLS, steps=steps)
+        precs = ["mixed", "fp64"]
+        kernel = {"mixed": "k_lps_mtheta_mixed + k_lps_force_mixed<fracture> (fused step)",
+                  "fp64": "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"}
+        wl = {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)}
+    else:
+        prob = P.dem_packing(lattice_dims=DEM_DIMS, steps=steps)
+        precs = ["exact"]
+        kernel = {"exact": "k_hertz_force<per-particle radius>"}
+        wl = {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10}
+    res, systems = {}, {}
+    for prec in precs:
+        s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
+        s.set_stream(stream.cuda_stream)
+        P.setup(s, prob)
+        _, bonds0 = s.neighbor_stats()
+        ms, k_avg = _time_system(s, stream, device, steps, warmup)
+        _, bonds1 = s.neighbor_stats()
+        bonds = bonds0 if name == "lps" else 0.5 * (bonds0 + bonds1)
+        res[prec] = dict(precision=prec, ms_per_step=ms / steps,
+                         value=bonds * steps / (ms / 1e3), kernel=kernel[prec],
+                         kernel_ms_avg=k_avg)
+        if name == "dem":
+            res[prec]["contact_rebuilds"] = s.contact_rebuilds()
+        systems[prec] = s
+    head = precs[0]
+    out = dict(wl, particles=systems[head].n, bonds=bonds, steps=steps, warmup=warmup,
+               unit="bond-updates/s", **res[head])
+    if "fp64" in res and head != "fp64":
+        a, b = systems[head], systems["fp64"]
+        err = {}
+        for fld in ("u", "v", "f", "theta"):
+            x, y = a.get(fld), b.get(fld)
+            err[fld] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
+        out["plain_fp64"] = res["fp64"]
+        out["mixed_vs_plain"] = res["fp64"]["ms_per_step"] / res[head]["ms_per_step"]
+        out["mixed_error_vs_fp64"] = err
+    for s in systems.values():
+        s.close()
     return out
 
 
@@ -543,7 +567,7 @@ def run_serving(args, device):
                      f"boxes; particles log-uniform in [{n_lo:.0f}, {n_hi:.0f}], steps "
                      f"uniform in [{args.serve_steps[0]}, {args.serve_steps[1]}], seed "
                      f"{args.serve_seed}"),
-        "precision": "mixed (PMB: FP32 bonds / FP64 state; LPS: FP64 kernels)",
+        "precision": "mixed (FP32 bonds / FP64 state, PMB and LPS)",
         "server": {"max_active": args.serve_active, "steps_per_launch": args.serve_k,
                    "setup_threads": args.serve_setup_threads,
                    "cuda_graphs": True, "hbm_budget_bytes": budget},
