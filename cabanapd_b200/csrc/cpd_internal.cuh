@@ -153,7 +153,8 @@ struct __align__(16) MixedStencil {
     float x, y, z, xi;  // FP32 bond reference vector and its length
     float xiinv;        // 1 / length
     int32_t delta;      // neighbour index - particle index
-    int32_t pad[2];
+    float xi2;          // squared length
+    int32_t pad;
 };
 // FP32 split of one particle's displacement, hi and lo together so one
 // address serves both loads: u = hi.xyz + lo.xyz; hi.w = c vol (the PMB
@@ -167,9 +168,11 @@ struct MixedView {
     const MixedU* u2;  // displacement split
     const uint8_t* code;  // [max_n][npad] stencil code per bond slot
     const MixedStencil* table;
-    const uint8_t* warp_kind;  // per warp of rows: 2 all rows full stencil, 1 all rows
-                               // stencil subsets, 0 otherwise (per-bond codes)
+    const uint8_t* warp_kind;  // per warp of rows: 2 all rows full stencil, 3 all rows
+                               // the same stencil subset, 1 all rows stencil subsets,
+                               // 0 otherwise (per-bond codes)
     const uint32_t* pmask;     // [ceil(ntab/32)][npad] stencil entries present per row
+    const uint32_t* warp_pmask;  // [warp][ceil(ntab/32)] the common subset of a kind-3 warp
 };
 // What a throughput bond kernel does after summing row i's force
 // (cpd_epilogue.cuh): mode 0 stores f; mode 1 applies the row's force
@@ -198,7 +201,9 @@ struct MixedState {
     MixedStencil* table = nullptr;
     uint8_t* warp_kind = nullptr;
     uint32_t* pmask = nullptr;
+    uint32_t* warp_pmask = nullptr;
     int ntab = 0;
+    int64_t row_pitch = 0;  // index delta of the (0, 1, 0) lattice offset (0: none)
     double h[3] = {0, 0, 0};
     size_t bytes = 0;     // device bytes held
     float2* ab = nullptr; // LPS: per-particle FP32 (theta_coeff theta / m, s_coeff / m)

@@ -181,21 +181,22 @@ __global__ void __launch_bounds__(kBlock)
 
 // Per row: presence bits of the stencil entries it holds (its codes are a
 // strictly increasing subset of the table); per warp: 2 if every row is the
-// whole table, 1 if every row is a table subset, else 0.
+// whole table, 3 if every row is the same table subset (the subset is
+// recorded for the warp), 1 if every row is a table subset, else 0.
 __global__ void __launch_bounds__(kBlock)
     k_row_masks(ParticleView p, EllView nl, const uint8_t* code, int ntab, uint32_t* pmask,
-                uint8_t* kind)
+                uint8_t* kind, uint32_t* warp_pmask)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int nmask = (ntab + 31) / 32;
     // Lanes past the last row do not vote against their warp.
     bool subset = true;
     bool full = true;
+    uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (i < p.n) {
         const int64_t np = p.npad;
         const int cnt = nl.count[i];
         full = cnt == ntab;
-        uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         int prev = -1;
         for (int k = 0; k < cnt; ++k) {
             const int c = code[(int64_t)k * np + i];
@@ -210,10 +211,24 @@ __global__ void __launch_bounds__(kBlock)
         if (!subset) full = false;
         for (int w = 0; w < nmask; ++w) pmask[(int64_t)w * np + i] = subset ? m[w] : 0u;
     }
+    // Lane 0 holds a row whenever any lane of the warp does (rows are
+    // contiguous from the warp's first lane).
+    bool same = true;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const uint32_t lead = __shfl_sync(0xffffffffu, m[w], 0);
+        if (i < p.n && m[w] != lead) same = false;
+    }
     full = __all_sync(0xffffffffu, full);
     subset = __all_sync(0xffffffffu, subset);
-    if ((threadIdx.x & 31) == 0)
-        kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5] = full ? 2 : (subset ? 1 : 0);
+    same = __all_sync(0xffffffffu, same);
+    if ((threadIdx.x & 31) == 0) {
+        const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int k = full ? 2 : (subset ? (same ? 3 : 1) : 0);
+        kind[warp] = (uint8_t)k;
+        if (k == 3)
+            for (int w = 0; w < nmask; ++w) warp_pmask[warp * nmask + w] = m[w];
+    }
 }
 
 // FP64 SoA positions -> FP32 hi/lo float4 (w = 0).
@@ -265,8 +280,11 @@ __global__ void __launch_bounds__(kBlock)
 
 struct MixedModel {
     float c, s0, guard;
+    float s_lo, s_hi;  // s0 - guard, s0 + guard
     double bbc;
     int ntab;
+    int wstride;      // lean form: warps of a block are wstride row chunks apart
+    int64_t nchunks;  // row chunks of 32 rows
 };
 
 // Kahan-compensated accumulation of one FP32 term.
@@ -468,14 +486,146 @@ __device__ __forceinline__ void mixed_full_rows2(const ParticleView& p, const El
     }
 }
 
+// Row i's own displacement split, negated, and its no-fail flag.
+struct RowSplit {
+    float2 nuh_xy, nul_xy;
+    float nuh_z, nul_z;
+    bool nofail;
+};
+
+// One bond of a stencil row in the lean form: adds the pair force to
+// (cxy, cz). The break test branches only for an intact bond whose FP32
+// stretch reaches s0 - guard: between s0 - guard and s0 + guard the
+// reference's FP64 expression decides, above it the bond breaks (unless an
+// end is no-fail); a bond that breaks sets its bit in clr.
+// Bond geometry of the lean form: eta = u_j - u_i from the splits,
+// num = eta . (2 xi_vec + eta) = r^2 - xi^2 without cancellation, r^2 =
+// xi^2 + num, and s = (r - xi) / xi = num / (xi (r + xi)).
+__device__ __forceinline__ void lean_geometry(const MixedStencil& t, const MixedU& uj,
+                                              const RowSplit& ri, MixedBond2& b)
+{
+    const float2 exy = f2(t.x, t.y);
+    const float2 nxy = __fadd2_rn(__fadd2_rn(f2(uj.hi.x, uj.hi.y), ri.nuh_xy),
+                                  __fadd2_rn(f2(uj.lo.x, uj.lo.y), ri.nul_xy));
+    const float nz = (uj.hi.z + ri.nuh_z) + (uj.lo.z + ri.nul_z);
+    b.rxy = __fadd2_rn(exy, nxy);
+    b.rz = t.z + nz;
+    const float2 pq = __fmul2_rn(nxy, __ffma2_rn(f2(2.f, 2.f), exy, nxy));
+    const float num = fmaf(nz, fmaf(2.f, t.z, nz), pq.x + pq.y);
+    const float r2 = t.xi2 + num;
+    b.rinv = rsqrtf(r2);
+    const float r = r2 * b.rinv;
+    b.s = __fdividef(num, fmaf(r, t.xi, t.xi2));
+}
+
+template <bool FRACTURE>
+__device__ __forceinline__ void stencil_bond(const MixedStencil& t,
+                                             const MixedU* __restrict__ u2_i, const RowSplit& ri,
+                                             bool on, uint32_t bit, const MixedModel& md,
+                                             const ParticleView& p, int64_t i, uint32_t& clr,
+                                             float2& cxy, float& cz)
+{
+    const MixedU uj = u2_i[t.delta];
+    MixedBond2 bd;
+    lean_geometry(t, uj, ri, bd);
+    if (FRACTURE && on && bd.s >= md.s_lo) {
+        if (!ri.nofail && uj.lo.w == 0.f &&
+            (bd.s > md.s_hi || critical_exact64(p.x, p.u, p.npad, i, i + t.delta, md.bbc))) {
+            clr |= bit;
+            on = false;
+        }
+    }
+    const float kf = (!FRACTURE || on) ? uj.hi.w * bd.s * bd.rinv : 0.f;
+    cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
+    cz = fmaf(kf, bd.rz, cz);
+}
+
+// Stencil rows, lean form: bond slot k of row i is entry k of wt (the whole
+// table, or the compacted table of a warp whose rows share one subset). The
+// pair forces of each 8-bond chunk are summed in FP32 and each chunk sum is
+// added to the FP64 row force f; newly broken bits of a 32-bond word are
+// cleared with one store.
+template <bool FRACTURE>
+__device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const EllView& nl,
+                                                   const MixedU* __restrict__ u2_i,
+                                                   const MixedStencil* wt, int cnt,
+                                                   const MixedModel& md, int64_t i,
+                                                   const RowSplit& ri, double (&f)[3])
+{
+    const int64_t np = p.npad;
+    for (int base = 0; base < cnt; base += 32) {
+        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+        uint32_t clr = 0;
+        const int lim = min(32, cnt - base);
+        int b = 0;
+        for (; b + 8 <= lim; b += 8) {
+            const uint32_t w8 = word >> b;
+            float2 cxy = f2(0.f, 0.f);
+            float cz = 0.f;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                stencil_bond<FRACTURE>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u, 1u << (b + u),
+                                       md, p, i, clr, cxy, cz);
+            f[0] += (double)cxy.x;
+            f[1] += (double)cxy.y;
+            f[2] += (double)cz;
+        }
+        if (b < lim) {
+            float2 cxy = f2(0.f, 0.f);
+            float cz = 0.f;
+            for (; b < lim; ++b)
+                stencil_bond<FRACTURE>(wt[base + b], u2_i, ri, (word >> b) & 1u, 1u << b, md, p,
+                                       i, clr, cxy, cz);
+            f[0] += (double)cxy.x;
+            f[1] += (double)cxy.y;
+            f[2] += (double)cz;
+        }
+        if (FRACTURE && clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+    }
+}
+
 template <bool FRACTURE, int MINB, bool PIPE, int FULL = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
     k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep)
 {
-    __shared__ MixedStencil tab[kMixedGeneric];
+    // Dynamic shared memory: the table, then (FULL == 3) one compacted table
+    // of ntab entries per warp of the block.
+    extern __shared__ MixedStencil smem[];
+    MixedStencil* tab = smem;
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // The warp's chunk of 32 rows. Lean form: the block's warps are wstride
+    // chunks apart (one lattice row apart when wstride is the row pitch / 32),
+    // so neighbour lines one warp loads into L1 are reused by the next.
+    int64_t warp;
+    if (FULL == 3 && md.wstride > 1) {
+        const int64_t g = blockIdx.x / md.wstride, c = blockIdx.x % md.wstride;
+        warp = ((kBlock / 32) * g + (threadIdx.x >> 5)) * md.wstride + c;
+    } else {
+        warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    }
+    const int kind = (FULL != 3 || warp < md.nchunks) ? mv.warp_kind[warp] : 0;
+    const MixedStencil* wt = tab;
+    int wcnt = md.ntab;
+    if (FULL == 3 && kind == 3) {
+        // Rows sharing one subset: entry k of the subset goes to slot
+        // (present entries before k) of the warp's compacted table.
+        const int lane = threadIdx.x & 31;
+        const int nmask = (md.ntab + 31) / 32;
+        MixedStencil* mine = smem + md.ntab * (1 + (threadIdx.x >> 5));
+        const uint32_t* wm = mv.warp_pmask + warp * nmask;
+        int before = 0;
+        for (int w = 0; w < nmask; ++w) {
+            const uint32_t pm = wm[w];
+            if ((pm >> lane) & 1u)
+                mine[before + __popc(pm & ((1u << lane) - 1u))] = tab[32 * w + lane];
+            before += __popc(pm);
+        }
+        __syncwarp();
+        wt = mine;
+        wcnt = before;
+    }
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
@@ -485,7 +635,13 @@ __global__ void __launch_bounds__(kBlock, MINB)
     const uint8_t* __restrict__ code = mv.code + i;
     const MixedU* __restrict__ U2 = mv.u2;
     float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-    const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    if (FULL == 3 && kind >= 2) {
+        const RowSplit ri{f2(-uhi.x, -uhi.y), f2(-uli.x, -uli.y), -uhi.z, -uli.z, nofail_i};
+        double f[3] = {0.0, 0.0, 0.0};
+        mixed_stencil_rows<FRACTURE>(p, nl, U2 + i, wt, wcnt, md, i, ri, f);
+        step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
+        return;
+    }
     if (kind == 2 && FULL == 2) {
         float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
         float sz = 0.f, cz = 0.f;
@@ -897,18 +1053,34 @@ __global__ void __launch_bounds__(kBlock, 4)
 // (64 registers), 1 -> 4 blocks with the full-stencil loop software
 // pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
 // rows in unrolled 8-bond chunks with branch-free bond bits, 4 -> 3 with the
-// x / y lanes in paired FP32 instructions (default). Full plate on B200, ms
-// per launch for 3 / 4: 4.15 / 4.12 (4 compiled for 3 or 2 blocks per SM:
-// 5.05; 4 with the neighbour gathers as cp.async copies into shared memory
-// three bonds ahead: 8.28; a shared-memory tile of the lattice with its
-// halo: 5.86).
-// Full plate on B200, ms per launch for 0 / 1 / 2: 4.70 / 4.64 / 4.92.
+// x / y lanes in paired FP32 instructions, 5 -> lean form (default): FP32
+// chunk sums added to FP64 row totals instead of Kahan sums, a break-test
+// branch only for intact bonds near s0, warps whose rows share one stencil
+// subset walking a compacted table, and block warps one lattice row apart;
+// 6 / 7 -> 5 compiled for 5 / 6 blocks per SM.
+// Full plate on B200, ms per launch: 0 / 1 / 2: 4.70 / 4.64 / 4.92; 3 / 4:
+// 4.15 / 4.12 (separate time-step stages); fused steps: 4 4.36, 5 with
+// consecutive block warps 4.19, 5 3.67, 6 4.36 and 7 7.96 (both spill). Also
+// measured and rejected: 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
+// neighbour gathers as cp.async copies into shared memory three bonds ahead
+// 8.28; a shared-memory tile of the lattice with its halo 5.86.
 int mixed_variant()
 {
     static int v = [] {
         const char* e = getenv("CPD_MIXED_VARIANT");
-        int x = e ? atoi(e) : 4;
-        return (x < 0 || x > 4) ? 4 : x;
+        int x = e ? atoi(e) : 5;
+        return (x < 0 || x > 7) ? 5 : x;
+    }();
+    return v;
+}
+
+// Lean form: block warps one lattice row apart (CPD_MIXED_ROW_TILES=0: the
+// warps of a block are consecutive row chunks).
+bool mixed_row_tiles()
+{
+    static bool v = [] {
+        const char* e = getenv("CPD_MIXED_ROW_TILES");
+        return !(e && atoi(e) == 0);
     }();
     return v;
 }
@@ -926,7 +1098,8 @@ int mixed_variant()
 
 void free_mixed(MixedState& m, cudaStream_t st)
 {
-    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.ab};
+    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
+                    m.ab};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
@@ -976,6 +1149,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
             const int nx = 2 * half[0] + 1, ny = 2 * half[1] + 1, nz = 2 * half[2] + 1;
             std::vector<int16_t> lut((size_t)nx * ny * nz, -1);
             std::vector<MixedStencil> tab;
+            int pitch_entry = -1;
             for (int c = -half[2]; c <= half[2]; ++c)
                 for (int b = -half[1]; b <= half[1]; ++b)
                     for (int a = -half[0]; a <= half[0]; ++a) {
@@ -995,7 +1169,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                         e.z = (float)vz;
                         e.xi = (float)len;
                         e.xiinv = (float)(1.0 / len);
+                        e.xi2 = (float)(len * len);
                         e.delta = 0;
+                        e.pad = 0;
+                        if (a == 0 && b == 1 && c == 0) pitch_entry = (int)tab.size();
                         tab.push_back(e);
                     }
             if (lattice && !tab.empty()) {
@@ -1027,12 +1204,16 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 CPD_TRY(dev_free(d_lut, st));
                 CPD_TRY(dev_free(d_delta, st));
                 m.ntab = (int)tab.size();
+                m.row_pitch = pitch_entry >= 0 ? tab[pitch_entry].delta : 0;
                 for (int d = 0; d < 3; ++d) m.h[d] = h[d];
                 const int nmask = (m.ntab + 31) / 32;
                 CPD_TRY(dev_alloc(&m.pmask, sizeof(uint32_t) * nmask * np, st));
                 m.bytes += sizeof(uint32_t) * nmask * np;
+                CPD_TRY(dev_alloc(&m.warp_pmask, sizeof(uint32_t) * nmask * nwarps, st));
+                m.bytes += sizeof(uint32_t) * nmask * nwarps;
                 k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), m.code, m.ntab,
-                                                                 m.pmask, m.warp_kind);
+                                                                 m.pmask, m.warp_kind,
+                                                                 m.warp_pmask);
                 launches++;
                 if (lps) {
                     // The LPS kernels take stencil rows only: every warp of rows
@@ -1094,7 +1275,7 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const int g = blocks_for(rows);
     const int key = (md.fracture ? 4 : 0) + (md.influence == 1 ? 2 : 0) + (with_m ? 1 : 0);
@@ -1116,7 +1297,7 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const int g = blocks_for(rows);
     switch ((md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0)) {
@@ -1134,25 +1315,47 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     if (md.pd == CPD_PD_LPS) return launch_lps_force_mixed(p, nl, md, m, ep, st);
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask};
+    MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     MixedModel mm;
     mm.c = (float)md.c;
     mm.s0 = (float)md.s0;
     mm.guard = (float)(1e-4 * md.s0);
     mm.bbc = md.bond_break_coeff;
+    mm.s_lo = mm.s0 - mm.guard;
+    mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
-    const int g = blocks_for(rows);
-    switch ((md.fracture ? 0 : 10) + mixed_variant()) {
-    case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
-    default: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, 0, st>>>(p, nl, mv, mm, ep); break;
+    mm.nchunks = (rows + 31) / 32;
+    mm.wstride = 1;
+    int g = blocks_for(rows);
+    const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
+    // The lean forms hold a compacted table per warp; past 48 KB of shared
+    // memory per block (ntab > 170) the paired form runs instead.
+    int var = mixed_variant();
+    const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
+    if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
+    if (var >= 5 && m.row_pitch >= 64 && mixed_row_tiles()) {
+        mm.wstride = (int)((m.row_pitch + 16) / 32);
+        const int64_t per = (int64_t)(kBlock / 32) * mm.wstride;
+        g = (int)(((mm.nchunks + per - 1) / per) * mm.wstride);
+    }
+    const size_t sb = var >= 5 ? lean_bytes : tab_bytes;
+    switch ((md.fracture ? 0 : 10) + var) {
+    case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 5: k_pmb_force_mixed<true, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 6: k_pmb_force_mixed<true, 5, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 7: k_pmb_force_mixed<true, 6, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 14: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 15: k_pmb_force_mixed<false, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    case 16: k_pmb_force_mixed<false, 5, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    default: k_pmb_force_mixed<false, 6, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     }
     return 1;
 }
