@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+
 #include <string>
 #include <vector>
 
@@ -67,7 +69,54 @@ struct EllView {
     const int32_t* idx;
     uint32_t* mu;  // nullptr for lists without bond state
     int32_t max_n;
+    // Rows per block of a bond kernel (tile_chunk): warps take chunks of 32
+    // rows; with stride > 1 the warps of a block take chunks stride apart.
+    int32_t stride = 1;
+    int64_t pitch = 0;  // index delta to the next lattice line (0: unknown)
 };
+
+// Row chunk of the calling warp. stride 1: consecutive chunks per block.
+// stride S > 1: block b holds chunks (W g + w) S + c for its warps w < W,
+// with g = b / S and c = b % S, so that on an x-fastest lattice (S = pitch /
+// 32) the block's warps hold neighbouring lattice lines and the neighbour
+// lines one warp brings into L1 serve the next. Both map launched warps one
+// to one onto row chunks (tile_view sizes the grid).
+__device__ __forceinline__ int64_t tile_chunk(const EllView& nl)
+{
+    if (nl.stride > 1) {
+        const int64_t g = blockIdx.x / nl.stride, c = blockIdx.x % nl.stride;
+        return ((int64_t)(blockDim.x >> 5) * g + (threadIdx.x >> 5)) * nl.stride + c;
+    }
+    return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+__device__ __forceinline__ int64_t tile_row(const EllView& nl, int64_t first)
+{
+    return first + 32 * tile_chunk(nl) + (threadIdx.x & 31);
+}
+
+// Tiled view of a list for `rows` rows and its grid (blocks of `block`
+// threads). CPD_ROW_TILES=0 keeps consecutive chunks.
+inline bool row_tiles_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("CPD_ROW_TILES");
+        return !(e && std::atoi(e) == 0);
+    }();
+    return on;
+}
+inline EllView tile_view(EllView v, int64_t rows, int block, int* grid)
+{
+    const int64_t chunks = (rows + 31) / 32, wpb = block / 32;
+    v.stride = 1;
+    if (v.pitch >= 64 && row_tiles_enabled()) {
+        v.stride = (int32_t)((v.pitch + 16) / 32);
+        const int64_t per = wpb * v.stride;
+        *grid = (int)(((chunks + per - 1) / per) * v.stride);
+    } else {
+        *grid = (int)((chunks + wpb - 1) / wpb);
+    }
+    return v;
+}
 
 // Everything a particle kernel needs, passed by value.
 struct ParticleView {
@@ -98,7 +147,8 @@ struct NeighborList {
     int32_t* count = nullptr;
     int32_t* idx = nullptr;
     uint32_t* mu = nullptr;
-    EllView view() const { return EllView{count, idx, mu, max_n}; }
+    int64_t pitch = 0;  // index delta to the next lattice line of a middle row (0: none)
+    EllView view() const { return EllView{count, idx, mu, max_n, 1, pitch}; }
 };
 
 struct BoundaryCondition {
@@ -203,7 +253,6 @@ struct MixedState {
     uint32_t* pmask = nullptr;
     uint32_t* warp_pmask = nullptr;
     int ntab = 0;
-    int64_t row_pitch = 0;  // index delta of the (0, 1, 0) lattice offset (0: none)
     double h[3] = {0, 0, 0};
     size_t bytes = 0;     // device bytes held
     float2* ab = nullptr; // LPS: per-particle FP32 (theta_coeff theta / m, s_coeff / m)

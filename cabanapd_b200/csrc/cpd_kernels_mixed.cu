@@ -283,8 +283,6 @@ struct MixedModel {
     float s_lo, s_hi;  // s0 - guard, s0 + guard
     double bbc;
     int ntab;
-    int wstride;      // lean form: warps of a block are wstride row chunks apart
-    int64_t nchunks;  // row chunks of 32 rows
 };
 
 // Kahan-compensated accumulation of one FP32 term.
@@ -594,17 +592,9 @@ __global__ void __launch_bounds__(kBlock, MINB)
     MixedStencil* tab = smem;
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    // The warp's chunk of 32 rows. Lean form: the block's warps are wstride
-    // chunks apart (one lattice row apart when wstride is the row pitch / 32),
-    // so neighbour lines one warp loads into L1 are reused by the next.
-    int64_t warp;
-    if (FULL == 3 && md.wstride > 1) {
-        const int64_t g = blockIdx.x / md.wstride, c = blockIdx.x % md.wstride;
-        warp = ((kBlock / 32) * g + (threadIdx.x >> 5)) * md.wstride + c;
-    } else {
-        warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    }
-    const int kind = (FULL != 3 || warp < md.nchunks) ? mv.warp_kind[warp] : 0;
+    // The warp's chunk of 32 rows (lean form: tiled, see tile_chunk).
+    const int64_t warp = tile_chunk(nl);
+    const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
     const MixedStencil* wt = tab;
     int wcnt = md.ntab;
     if (FULL == 3 && kind == 3) {
@@ -1056,12 +1046,12 @@ __global__ void __launch_bounds__(kBlock, 4)
 // x / y lanes in paired FP32 instructions, 5 -> lean form (default): FP32
 // chunk sums added to FP64 row totals instead of Kahan sums, a break-test
 // branch only for intact bonds near s0, warps whose rows share one stencil
-// subset walking a compacted table, and block warps one lattice row apart;
-// 6 / 7 -> 5 compiled for 5 / 6 blocks per SM.
+// subset walking a compacted table, and block warps one lattice row apart.
 // Full plate on B200, ms per launch: 0 / 1 / 2: 4.70 / 4.64 / 4.92; 3 / 4:
 // 4.15 / 4.12 (separate time-step stages); fused steps: 4 4.36, 5 with
-// consecutive block warps 4.19, 5 3.67, 6 4.36 and 7 7.96 (both spill). Also
-// measured and rejected: 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
+// consecutive block warps 4.19, 5 3.67. Also measured and rejected: 5
+// compiled for 5 or 6 blocks per SM (48 / 40 registers, spilling) 4.36 /
+// 7.96; 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
 // neighbour gathers as cp.async copies into shared memory three bonds ahead
 // 8.28; a shared-memory tile of the lattice with its halo 5.86.
 int mixed_variant()
@@ -1069,18 +1059,7 @@ int mixed_variant()
     static int v = [] {
         const char* e = getenv("CPD_MIXED_VARIANT");
         int x = e ? atoi(e) : 5;
-        return (x < 0 || x > 7) ? 5 : x;
-    }();
-    return v;
-}
-
-// Lean form: block warps one lattice row apart (CPD_MIXED_ROW_TILES=0: the
-// warps of a block are consecutive row chunks).
-bool mixed_row_tiles()
-{
-    static bool v = [] {
-        const char* e = getenv("CPD_MIXED_ROW_TILES");
-        return !(e && atoi(e) == 0);
+        return (x < 0 || x > 5) ? 5 : x;
     }();
     return v;
 }
@@ -1149,7 +1128,6 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
             const int nx = 2 * half[0] + 1, ny = 2 * half[1] + 1, nz = 2 * half[2] + 1;
             std::vector<int16_t> lut((size_t)nx * ny * nz, -1);
             std::vector<MixedStencil> tab;
-            int pitch_entry = -1;
             for (int c = -half[2]; c <= half[2]; ++c)
                 for (int b = -half[1]; b <= half[1]; ++b)
                     for (int a = -half[0]; a <= half[0]; ++a) {
@@ -1172,7 +1150,6 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                         e.xi2 = (float)(len * len);
                         e.delta = 0;
                         e.pad = 0;
-                        if (a == 0 && b == 1 && c == 0) pitch_entry = (int)tab.size();
                         tab.push_back(e);
                     }
             if (lattice && !tab.empty()) {
@@ -1204,7 +1181,6 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 CPD_TRY(dev_free(d_lut, st));
                 CPD_TRY(dev_free(d_delta, st));
                 m.ntab = (int)tab.size();
-                m.row_pitch = pitch_entry >= 0 ? tab[pitch_entry].delta : 0;
                 for (int d = 0; d < 3; ++d) m.h[d] = h[d];
                 const int nmask = (m.ntab + 31) / 32;
                 CPD_TRY(dev_alloc(&m.pmask, sizeof(uint32_t) * nmask * np, st));
@@ -1309,10 +1285,10 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     return 1;
 }
 
-int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
 {
-    if (md.pd == CPD_PD_LPS) return launch_lps_force_mixed(p, nl, md, m, ep, st);
+    if (md.pd == CPD_PD_LPS) return launch_lps_force_mixed(p, list, md, m, ep, st);
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
     MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
@@ -1324,8 +1300,6 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     mm.s_lo = mm.s0 - mm.guard;
     mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
-    mm.nchunks = (rows + 31) / 32;
-    mm.wstride = 1;
     int g = blocks_for(rows);
     const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
     // The lean forms hold a compacted table per warp; past 48 KB of shared
@@ -1333,11 +1307,8 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     int var = mixed_variant();
     const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
     if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
-    if (var >= 5 && m.row_pitch >= 64 && mixed_row_tiles()) {
-        mm.wstride = (int)((m.row_pitch + 16) / 32);
-        const int64_t per = (int64_t)(kBlock / 32) * mm.wstride;
-        g = (int)(((mm.nchunks + per - 1) / per) * mm.wstride);
-    }
+    EllView nl = list;
+    if (var >= 5) nl = tile_view(list, rows, kBlock, &g);
     const size_t sb = var >= 5 ? lean_bytes : tab_bytes;
     switch ((md.fracture ? 0 : 10) + var) {
     case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
@@ -1346,16 +1317,12 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model&
     case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 5: k_pmb_force_mixed<true, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 6: k_pmb_force_mixed<true, 5, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 7: k_pmb_force_mixed<true, 6, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     case 14: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 15: k_pmb_force_mixed<false, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 16: k_pmb_force_mixed<false, 5, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    default: k_pmb_force_mixed<false, 6, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
+    default: k_pmb_force_mixed<false, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
     }
     return 1;
 }

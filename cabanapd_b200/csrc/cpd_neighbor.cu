@@ -296,6 +296,30 @@ void free_neighbor_list(NeighborList& nl, cudaStream_t st)
     nl = NeighborList{};
 }
 
+// Index delta from a row to its nearest neighbour straight along +y (same x
+// and z within tol): the line pitch of an x-fastest lattice, used only to
+// group bond-kernel warps (tile_view).
+__global__ void k_row_pitch(const double* __restrict__ pos, int64_t npad, int64_t row,
+                            const int32_t* __restrict__ count, const int32_t* __restrict__ idx,
+                            double tol, long long* out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int cnt = count[row];
+    double best = INFINITY;
+    long long d = 0;
+    for (int k = 0; k < cnt; ++k) {
+        const int64_t j = idx[(int64_t)k * npad + row];
+        const double dx = pos[j] - pos[row];
+        const double dy = pos[npad + j] - pos[npad + row];
+        const double dz = pos[2 * npad + j] - pos[2 * npad + row];
+        if (fabs(dx) <= tol && fabs(dz) <= tol && dy > tol && dy < best) {
+            best = dy;
+            d = (long long)(j - row);
+        }
+    }
+    *out = d < 0 ? -d : d;
+}
+
 int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t npad,
                         int64_t begin, double cutoff, const int32_t* user_id,
                         bool with_mu, NeighborList& out, cudaStream_t st,
@@ -423,6 +447,21 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     if (with_mu && out.nwords > 0) {
         k_init_mu<<<blocks_for(npad), kBlock, 0, st>>>(out.count, npad, out.nwords, out.mu);
         launches++;
+    }
+    // Lists on reference positions (PD bonds): the lattice line pitch at a
+    // middle row.
+    out.pitch = 0;
+    if (!disp && n > begin && max_n > 0) {
+        long long* d_pitch = nullptr;
+        CPD_TRY(dev_alloc(&d_pitch, sizeof(long long), st));
+        k_row_pitch<<<1, 32, 0, st>>>(pos, npad, begin + (n - begin) / 2, out.count, out.idx,
+                                      1e-6 * cutoff, d_pitch);
+        launches++;
+        long long pitch = 0;
+        CPD_TRY(cudaMemcpyAsync(&pitch, d_pitch, sizeof(pitch), cudaMemcpyDeviceToHost, st));
+        CPD_TRY(cudaStreamSynchronize(st));
+        CPD_TRY(dev_free(d_pitch, st));
+        out.pitch = pitch;
     }
     CPD_TRY(cudaGetLastError());
     CPD_TRY(dev_free(tmp, st));
