@@ -256,6 +256,10 @@ struct MixedState {
     double h[3] = {0, 0, 0};
     size_t bytes = 0;     // device bytes held
     float2* ab = nullptr; // LPS: per-particle FP32 (theta_coeff theta / m, s_coeff / m)
+    // PMB split form: warps of kinds 2 / 3 (lean kernel) and the others.
+    int32_t* lean_list = nullptr;
+    int32_t* rest_list = nullptr;
+    int64_t nlean = 0, nrest = 0;
     int lps_ok = 0;       // LPS: every row is a stencil row (the mixed LPS kernels apply)
 };
 // lps: set up the LPS mixed kernels too (lps_ok, ab).

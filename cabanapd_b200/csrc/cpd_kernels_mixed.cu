@@ -491,11 +491,6 @@ struct RowSplit {
     bool nofail;
 };
 
-// One bond of a stencil row in the lean form: adds the pair force to
-// (cxy, cz). The break test branches only for an intact bond whose FP32
-// stretch reaches s0 - guard: between s0 - guard and s0 + guard the
-// reference's FP64 expression decides, above it the bond breaks (unless an
-// end is no-fail); a bond that breaks sets its bit in clr.
 // Bond geometry of the lean form: eta = u_j - u_i from the splits,
 // num = eta . (2 xi_vec + eta) = r^2 - xi^2 without cancellation, r^2 =
 // xi^2 + num, and s = (r - xi) / xi = num / (xi (r + xi)).
@@ -516,22 +511,34 @@ __device__ __forceinline__ void lean_geometry(const MixedStencil& t, const Mixed
     b.s = __fdividef(num, fmaf(r, t.xi, t.xi2));
 }
 
-template <bool FRACTURE>
+// One bond of a stencil row in the lean form: adds the pair force to
+// (cxy, cz). Only an intact bond whose FP32 stretch reaches s0 - guard (and
+// whose ends may fail) leaves the fast path: above s0 + guard it breaks (bit
+// set in clr); inside the band it is deferred (bit set in pend) to the exact
+// FP64 test after the word, and contributes no force here.
+template <bool FRACTURE, bool LDG>
 __device__ __forceinline__ void stencil_bond(const MixedStencil& t,
                                              const MixedU* __restrict__ u2_i, const RowSplit& ri,
                                              bool on, uint32_t bit, const MixedModel& md,
-                                             const ParticleView& p, int64_t i, uint32_t& clr,
-                                             float2& cxy, float& cz)
+                                             uint32_t& clr, uint32_t& pend, float2& cxy, float& cz)
 {
-    const MixedU uj = u2_i[t.delta];
+    MixedU uj;
+    if (LDG) {
+        // The split is read-only while the kernel runs (the next one goes
+        // to the other buffer): non-coherent global loads.
+        uj.hi = __ldg(&u2_i[t.delta].hi);
+        uj.lo = __ldg(&u2_i[t.delta].lo);
+    } else {
+        uj = u2_i[t.delta];
+    }
     MixedBond2 bd;
     lean_geometry(t, uj, ri, bd);
-    if (FRACTURE && on && bd.s >= md.s_lo) {
-        if (!ri.nofail && uj.lo.w == 0.f &&
-            (bd.s > md.s_hi || critical_exact64(p.x, p.u, p.npad, i, i + t.delta, md.bbc))) {
+    if (FRACTURE && on && bd.s >= md.s_lo && !ri.nofail && uj.lo.w == 0.f) {
+        if (bd.s > md.s_hi)
             clr |= bit;
-            on = false;
-        }
+        else
+            pend |= bit;
+        on = false;
     }
     const float kf = (!FRACTURE || on) ? uj.hi.w * bd.s * bd.rinv : 0.f;
     cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
@@ -540,10 +547,11 @@ __device__ __forceinline__ void stencil_bond(const MixedStencil& t,
 
 // Stencil rows, lean form: bond slot k of row i is entry k of wt (the whole
 // table, or the compacted table of a warp whose rows share one subset). The
-// pair forces of each 8-bond chunk are summed in FP32 and each chunk sum is
-// added to the FP64 row force f; newly broken bits of a 32-bond word are
-// cleared with one store.
-template <bool FRACTURE>
+// pair forces of each chunk of UNROLL bonds are summed in FP32 and each
+// chunk sum is added to the FP64 row force f. After each 32-bond word the
+// deferred bonds take the reference's FP64 break test; those that hold add
+// their pair force to f. Newly broken bits are cleared with one store.
+template <bool FRACTURE, bool LDG, int UNROLL>
 __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const EllView& nl,
                                                    const MixedU* __restrict__ u2_i,
                                                    const MixedStencil* wt, int cnt,
@@ -553,17 +561,17 @@ __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const 
     const int64_t np = p.npad;
     for (int base = 0; base < cnt; base += 32) {
         const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
-        uint32_t clr = 0;
+        uint32_t clr = 0, pend = 0;
         const int lim = min(32, cnt - base);
         int b = 0;
-        for (; b + 8 <= lim; b += 8) {
+        for (; b + UNROLL <= lim; b += UNROLL) {
             const uint32_t w8 = word >> b;
             float2 cxy = f2(0.f, 0.f);
             float cz = 0.f;
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-                stencil_bond<FRACTURE>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u, 1u << (b + u),
-                                       md, p, i, clr, cxy, cz);
+            for (int u = 0; u < UNROLL; ++u)
+                stencil_bond<FRACTURE, LDG>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u,
+                                            1u << (b + u), md, clr, pend, cxy, cz);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
@@ -572,32 +580,61 @@ __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const 
             float2 cxy = f2(0.f, 0.f);
             float cz = 0.f;
             for (; b < lim; ++b)
-                stencil_bond<FRACTURE>(wt[base + b], u2_i, ri, (word >> b) & 1u, 1u << b, md, p,
-                                       i, clr, cxy, cz);
+                stencil_bond<FRACTURE, LDG>(wt[base + b], u2_i, ri, (word >> b) & 1u, 1u << b, md,
+                                            clr, pend, cxy, cz);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
         }
-        if (FRACTURE && clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+        if (FRACTURE) {
+            while (pend) {
+                const int k = __ffs(pend) - 1;
+                pend &= pend - 1;
+                const MixedStencil t = wt[base + k];
+                if (critical_exact64(p.x, p.u, np, i, i + t.delta, md.bbc)) {
+                    clr |= 1u << k;
+                } else {
+                    const MixedU uj = u2_i[t.delta];
+                    MixedBond2 bd;
+                    lean_geometry(t, uj, ri, bd);
+                    const float kf = uj.hi.w * bd.s * bd.rinv;
+                    f[0] += (double)(kf * bd.rxy.x);
+                    f[1] += (double)(kf * bd.rxy.y);
+                    f[2] += (double)(kf * bd.rz);
+                }
+            }
+            if (clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+        }
     }
 }
 
 template <bool FRACTURE, int MINB, bool PIPE, int FULL = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
-    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep)
+    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
+                      const int32_t* __restrict__ wlist, int64_t wcount)
 {
-    // Dynamic shared memory: the table, then (FULL == 3) one compacted table
-    // of ntab entries per warp of the block.
+    // FULL >= 3: lean form (4: with non-coherent gathers, 5: 4 in 4-bond
+    // chunks). Dynamic shared memory: the table, then (lean) one compacted table
+    // of ntab entries per warp of the block. With a warp list (split form),
+    // the warps listed.
     extern __shared__ MixedStencil smem[];
     MixedStencil* tab = smem;
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    // The warp's chunk of 32 rows (lean form: tiled, see tile_chunk).
-    const int64_t warp = tile_chunk(nl);
+    // The warp's chunk of 32 rows: from the warp list when one is given,
+    // else tiled (tile_chunk).
+    int64_t warp;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        warp = wlist[slot];
+    } else {
+        warp = tile_chunk(nl);
+    }
     const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
     const MixedStencil* wt = tab;
     int wcnt = md.ntab;
-    if (FULL == 3 && kind == 3) {
+    if (FULL >= 3 && kind == 3) {
         // Rows sharing one subset: entry k of the subset goes to slot
         // (present entries before k) of the warp's compacted table.
         const int lane = threadIdx.x & 31;
@@ -625,10 +662,11 @@ __global__ void __launch_bounds__(kBlock, MINB)
     const uint8_t* __restrict__ code = mv.code + i;
     const MixedU* __restrict__ U2 = mv.u2;
     float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-    if (FULL == 3 && kind >= 2) {
+    if (FULL >= 3 && kind >= 2) {
         const RowSplit ri{f2(-uhi.x, -uhi.y), f2(-uli.x, -uli.y), -uhi.z, -uli.z, nofail_i};
         double f[3] = {0.0, 0.0, 0.0};
-        mixed_stencil_rows<FRACTURE>(p, nl, U2 + i, wt, wcnt, md, i, ri, f);
+        mixed_stencil_rows<FRACTURE, (FULL >= 4), (FULL == 5 ? 4 : 8)>(p, nl, U2 + i, wt, wcnt,
+                                                                        md, i, ri, f);
         step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
         return;
     }
@@ -827,6 +865,66 @@ __global__ void __launch_bounds__(kBlock, MINB)
                         (double)sz - (double)cz);
 }
 
+// Prologue of the lean kernels: stages the stencil table in shared memory
+// and takes the calling warp's row chunk from the warp list; a warp whose
+// rows share one stencil subset (kind 3) also stages its compacted table
+// (entry k of the subset at slot "present entries before k"). Returns false
+// for warps past the end of the list.
+__device__ __forceinline__ bool lean_prologue(const MixedView& mv, int ntab,
+                                              const int32_t* __restrict__ wlist, int64_t wcount,
+                                              MixedStencil* smem, int64_t& warp,
+                                              const MixedStencil*& wt, int& wcnt)
+{
+    for (int t = threadIdx.x; t < ntab; t += blockDim.x) smem[t] = mv.table[t];
+    __syncthreads();
+    const int64_t slot = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= wcount) return false;
+    warp = wlist[slot];
+    wt = smem;
+    wcnt = ntab;
+    if (mv.warp_kind[warp] == 3) {
+        const int lane = threadIdx.x & 31;
+        const int nmask = (ntab + 31) / 32;
+        MixedStencil* mine = smem + ntab * (1 + (threadIdx.x >> 5));
+        const uint32_t* wm = mv.warp_pmask + warp * nmask;
+        int before = 0;
+        for (int w = 0; w < nmask; ++w) {
+            const uint32_t pm = wm[w];
+            if ((pm >> lane) & 1u)
+                mine[before + __popc(pm & ((1u << lane) - 1u))] = smem[32 * w + lane];
+            before += __popc(pm);
+        }
+        __syncwarp();
+        wt = mine;
+        wcnt = before;
+    }
+    return true;
+}
+
+// The lean form alone, over a list of warps whose rows are all full stencil
+// rows (kind 2) or share one stencil subset (kind 3); the other warps run
+// k_pmb_force_mixed over their own list. Without the other paths the kernel
+// needs fewer registers.
+template <bool FRACTURE, int MINB, int UNROLL = 8>
+__global__ void __launch_bounds__(kBlock, MINB)
+    k_pmb_force_lean(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
+                     const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    extern __shared__ MixedStencil smem[];
+    int64_t warp;
+    const MixedStencil* wt;
+    int wcnt;
+    if (!lean_prologue(mv, md.ntab, wlist, wcount, smem, warp, wt, wcnt)) return;
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
+    if (i >= p.n) return;
+    const MixedU ui = mv.u2[i];
+    const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z,
+                      FRACTURE ? (ui.lo.w != 0.f) : false};
+    double f[3] = {0.0, 0.0, 0.0};
+    mixed_stencil_rows<FRACTURE, false, UNROLL>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri, f);
+    step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
+}
+
 // ---------------------------------------------------------------------------
 // LPS, mixed precision (force/CabanaPD_LPS.hpp:287-447 with the model of
 // force_models/CabanaPD_LPS.hpp:85-134). Stencil rows only: jobs with an
@@ -839,6 +937,7 @@ __global__ void __launch_bounds__(kBlock, MINB)
 // reference) with the FP64 re-test inside the guard band.
 struct MixedLps {
     float s0, guard;
+    float s_lo, s_hi;  // s0 - guard, s0 + guard
     double bbc;
     double theta_coeff, s_coeff;
     int ntab;
@@ -861,12 +960,20 @@ __device__ __forceinline__ float lps_oxi(const MixedStencil& t)
 template <bool FRACTURE, int INFL, bool WITH_M>
 __global__ void __launch_bounds__(kBlock, 4)
     k_lps_mtheta_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
-                       float2* __restrict__ ab)
+                       float2* __restrict__ ab, const int32_t* __restrict__ wlist,
+                       int64_t wcount)
 {
     __shared__ MixedStencil tab[kMixedGeneric];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // Rows: the listed warps' chunks when a warp list is given.
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        warp = wlist[slot];
+    }
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
@@ -874,7 +981,7 @@ __global__ void __launch_bounds__(kBlock, 4)
     const float2 nuhi_xy = f2(-uhi.x, -uhi.y), nuli_xy = f2(-uli.x, -uli.y);
     const float nuhi_z = -uhi.z, nuli_z = -uli.z;
     const MixedU* __restrict__ u2_i = mv.u2 + i;
-    const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    const int kind = mv.warp_kind[warp];
     float ms = 0.f, mc = 0.f, ts = 0.f, tc = 0.f;
     if (kind == 2) {
         for (int base = 0; base < md.ntab; base += 32) {
@@ -947,12 +1054,20 @@ __device__ __forceinline__ bool lps_critical(float s, bool nofail_i, const Mixed
 template <bool FRACTURE, int INFL>
 __global__ void __launch_bounds__(kBlock, 4)
     k_lps_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
-                      const float2* __restrict__ ab, StepEpilogue ep)
+                      const float2* __restrict__ ab, StepEpilogue ep,
+                      const int32_t* __restrict__ wlist, int64_t wcount)
 {
     __shared__ MixedStencil tab[kMixedGeneric];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // Rows: the listed warps' chunks when a warp list is given.
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        warp = wlist[slot];
+    }
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
@@ -963,7 +1078,7 @@ __global__ void __launch_bounds__(kBlock, 4)
     const float2 abi = ab[i];
     const MixedU* __restrict__ u2_i = mv.u2 + i;
     const float2* __restrict__ ab_i = ab + i;
-    const int kind = mv.warp_kind[((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+    const int kind = mv.warp_kind[warp];
     float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
     float sz = 0.f, cz = 0.f;
     if (kind == 2) {
@@ -1039,27 +1154,213 @@ __global__ void __launch_bounds__(kBlock, 4)
                         (double)sz - (double)cz);
 }
 
+// LPS lean forms, over the warps of kinds 2 and 3 (warp list; the other
+// warps run k_lps_mtheta_mixed / k_lps_force_mixed over theirs): as the PMB
+// lean form, FP32 sums per chunk of 8 bonds added to FP64 row totals, and
+// bonds near s0 deferred to the exact test after each 32-bond word.
+template <int INFL, bool WITH_M>
+__device__ __forceinline__ void lps_theta_bond(const MixedStencil& t,
+                                               const MixedU* __restrict__ u2_i,
+                                               const RowSplit& ri, bool on, float& cm, float& ct)
+{
+    const MixedU uj = u2_i[t.delta];
+    MixedBond2 bd;
+    lean_geometry(t, uj, ri, bd);
+    const float wv = on ? (INFL == 1 ? t.xi : t.xi2) * uj.hi.w : 0.f;
+    if (WITH_M) cm += wv;
+    ct = fmaf(wv, bd.s, ct);
+}
+
+constexpr int kThetaUnroll = 4;  // 8 spills at 64 registers
+
+template <bool FRACTURE, int INFL, bool WITH_M>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_mtheta_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                      float2* __restrict__ ab, const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    extern __shared__ MixedStencil smem[];
+    int64_t warp;
+    const MixedStencil* wt;
+    int wcnt;
+    if (!lean_prologue(mv, md.ntab, wlist, wcount, smem, warp, wt, wcnt)) return;
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const MixedU ui = mv.u2[i];
+    const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z, false};
+    const MixedU* __restrict__ u2_i = mv.u2 + i;
+    double msum = 0.0, tsum = 0.0;
+    for (int base = 0; base < wcnt; base += 32) {
+        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+        const int lim = min(32, wcnt - base);
+        int b = 0;
+        for (; b + kThetaUnroll <= lim; b += kThetaUnroll) {
+            const uint32_t w8 = word >> b;
+            float cm = 0.f, ct = 0.f;
+#pragma unroll
+            for (int u = 0; u < kThetaUnroll; ++u)
+                lps_theta_bond<INFL, WITH_M>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u, cm, ct);
+            msum += (double)cm;
+            tsum += (double)ct;
+        }
+        if (b < lim) {
+            float cm = 0.f, ct = 0.f;
+            for (; b < lim; ++b)
+                lps_theta_bond<INFL, WITH_M>(wt[base + b], u2_i, ri, (word >> b) & 1u, cm, ct);
+            msum += (double)cm;
+            tsum += (double)ct;
+        }
+    }
+    const double m = WITH_M ? msum : p.m[i];
+    const double th = (!FRACTURE || m > 0) ? 3.0 * tsum / m : 0.0;
+    if (WITH_M) p.m[i] = m;
+    p.theta[i] = th;
+    const double a = md.theta_coeff * th / m, b = md.s_coeff / m;
+    p.lps_a[i] = a;
+    p.lps_b[i] = b;
+    ab[i] = make_float2((float)a, (float)b);
+}
+
+// One LPS bond of the lean force (the break rule of lps_critical: only the
+// row's no-fail flag counts).
+template <bool FRACTURE, int INFL>
+__device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
+                                               const MixedU* __restrict__ u2_i,
+                                               const float2* __restrict__ ab_i, float2 abi,
+                                               const RowSplit& ri, bool on, uint32_t bit,
+                                               const MixedLps& md, uint32_t& clr, uint32_t& pend,
+                                               float2& cxy, float& cz)
+{
+    const MixedU uj = u2_i[t.delta];
+    const float2 abj = ab_i[t.delta];
+    MixedBond2 bd;
+    lean_geometry(t, uj, ri, bd);
+    if (FRACTURE && on && bd.s >= md.s_lo && !ri.nofail) {
+        if (bd.s > md.s_hi)
+            clr |= bit;
+        else
+            pend |= bit;
+        on = false;
+    }
+    const float kf = (!FRACTURE || on)
+                         ? (abi.x + abj.x + bd.s * (abi.y + abj.y)) * lps_oxi<INFL>(t) * uj.hi.w *
+                               bd.rinv
+                         : 0.f;
+    cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
+    cz = fmaf(kf, bd.rz, cz);
+}
+
+template <bool FRACTURE, int INFL>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_force_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                     const float2* __restrict__ ab, StepEpilogue ep,
+                     const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    extern __shared__ MixedStencil smem[];
+    int64_t warp;
+    const MixedStencil* wt;
+    int wcnt;
+    if (!lean_prologue(mv, md.ntab, wlist, wcount, smem, warp, wt, wcnt)) return;
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const MixedU ui = mv.u2[i];
+    const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z,
+                      FRACTURE ? (ui.lo.w != 0.f) : false};
+    const MixedU* __restrict__ u2_i = mv.u2 + i;
+    const float2* __restrict__ ab_i = ab + i;
+    const float2 abi = ab[i];
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int base = 0; base < wcnt; base += 32) {
+        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+        uint32_t clr = 0, pend = 0;
+        const int lim = min(32, wcnt - base);
+        int b = 0;
+        for (; b + 8 <= lim; b += 8) {
+            const uint32_t w8 = word >> b;
+            float2 cxy = f2(0.f, 0.f);
+            float cz = 0.f;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                lps_force_bond<FRACTURE, INFL>(wt[base + b + u], u2_i, ab_i, abi, ri,
+                                               (w8 >> u) & 1u, 1u << (b + u), md, clr, pend, cxy,
+                                               cz);
+            f[0] += (double)cxy.x;
+            f[1] += (double)cxy.y;
+            f[2] += (double)cz;
+        }
+        if (b < lim) {
+            float2 cxy = f2(0.f, 0.f);
+            float cz = 0.f;
+            for (; b < lim; ++b)
+                lps_force_bond<FRACTURE, INFL>(wt[base + b], u2_i, ab_i, abi, ri, (word >> b) & 1u,
+                                               1u << b, md, clr, pend, cxy, cz);
+            f[0] += (double)cxy.x;
+            f[1] += (double)cxy.y;
+            f[2] += (double)cz;
+        }
+        if (FRACTURE) {
+            while (pend) {
+                const int k = __ffs(pend) - 1;
+                pend &= pend - 1;
+                const MixedStencil t = wt[base + k];
+                if (critical_exact64(p.x, p.u, np, i, i + t.delta, md.bbc)) {
+                    clr |= 1u << k;
+                } else {
+                    float2 cxy = f2(0.f, 0.f);
+                    float cz = 0.f;
+                    uint32_t none = 0;
+                    lps_force_bond<false, INFL>(t, u2_i, ab_i, abi, ri, true, 0u, md, none, none,
+                                                cxy, cz);
+                    f[0] += (double)cxy.x;
+                    f[1] += (double)cxy.y;
+                    f[2] += (double)cz;
+                }
+            }
+            if (clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+        }
+    }
+    step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
+}
+
+// LPS mixed split form (CPD_LPS_MIXED_SPLIT=0: one kernel over all warps).
+bool lps_mixed_split()
+{
+    static const bool v = [] {
+        const char* e = getenv("CPD_LPS_MIXED_SPLIT");
+        return !(e && atoi(e) == 0);
+    }();
+    return v;
+}
+
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
 // (64 registers), 1 -> 4 blocks with the full-stencil loop software
 // pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
 // rows in unrolled 8-bond chunks with branch-free bond bits, 4 -> 3 with the
-// x / y lanes in paired FP32 instructions, 5 -> lean form (default): FP32
-// chunk sums added to FP64 row totals instead of Kahan sums, a break-test
-// branch only for intact bonds near s0, warps whose rows share one stencil
-// subset walking a compacted table, and block warps one lattice row apart.
-// Full plate on B200, ms per launch: 0 / 1 / 2: 4.70 / 4.64 / 4.92; 3 / 4:
-// 4.15 / 4.12 (separate time-step stages); fused steps: 4 4.36, 5 with
-// consecutive block warps 4.19, 5 3.67. Also measured and rejected: 5
-// compiled for 5 or 6 blocks per SM (48 / 40 registers, spilling) 4.36 /
-// 7.96; 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
+// x / y lanes in paired FP32 instructions, 5 -> lean form: FP32 chunk sums
+// added to FP64 row totals instead of Kahan sums, bonds near s0 deferred to
+// an exact test after each 32-bond word, warps whose rows share one stencil
+// subset walking a compacted table, and block warps one lattice row apart;
+// 6 / 7 / 8 -> 5 with non-coherent gathers / 4-bond chunks / 3 blocks per SM;
+// 9 -> split form (default): k_pmb_force_lean over the warps of kinds 2 and 3
+// (warp list in tile order), then 4 over the other warps; 10 / 11 / 12 -> 9
+// with the lean kernel at 5 blocks and 4-bond chunks / 5 blocks and 2-bond
+// chunks / 6 blocks and 2-bond chunks.
+// Full plate on B200, ms per bond-kernel launch (per step for 9-12): 0 / 1 /
+// 2: 4.70 / 4.64 / 4.92; 3 / 4: 4.15 / 4.12 (separate time-step stages);
+// fused steps: 4 4.36; 5 3.28 (3.67 with the exact test inside the bond
+// loop, 4.19 also with consecutive block warps); 6 / 7 / 8 3.91 / 3.90 /
+// 4.64 (before the deferred test); 9 3.07; 10 / 11 / 12 3.84 / 3.50 / 3.77.
+// Also measured and rejected: 5 compiled for 5 or 6 blocks per SM (spilling)
+// 4.36 / 7.96; 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
 // neighbour gathers as cp.async copies into shared memory three bonds ahead
 // 8.28; a shared-memory tile of the lattice with its halo 5.86.
 int mixed_variant()
 {
     static int v = [] {
         const char* e = getenv("CPD_MIXED_VARIANT");
-        int x = e ? atoi(e) : 5;
-        return (x < 0 || x > 5) ? 5 : x;
+        int x = e ? atoi(e) : 9;
+        return (x < 0 || x > 12) ? 9 : x;
     }();
     return v;
 }
@@ -1078,7 +1379,7 @@ int mixed_variant()
 void free_mixed(MixedState& m, cudaStream_t st)
 {
     void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
-                    m.ab};
+                    m.ab, m.lean_list, m.rest_list};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
@@ -1191,20 +1492,49 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                                                                  m.pmask, m.warp_kind,
                                                                  m.warp_pmask);
                 launches++;
+                const int64_t nw = (rows + 31) / 32;
+                std::vector<uint8_t> kinds(nw);
+                CPD_TRY(cudaMemcpyAsync(kinds.data(), m.warp_kind, nw, cudaMemcpyDeviceToHost,
+                                        st));
+                CPD_TRY(cudaStreamSynchronize(st));
                 if (lps) {
                     // The LPS kernels take stencil rows only: every warp of rows
-                    // must be kind 1 or 2.
-                    const int64_t nw = (rows + 31) / 32;
-                    std::vector<uint8_t> kinds(nw);
-                    CPD_TRY(cudaMemcpyAsync(kinds.data(), m.warp_kind, nw, cudaMemcpyDeviceToHost,
-                                            st));
-                    CPD_TRY(cudaStreamSynchronize(st));
+                    // must be a stencil kind (1, 2 or 3).
                     m.lps_ok = std::all_of(kinds.begin(), kinds.end(),
                                            [](uint8_t k) { return k != 0; }) ? 1 : 0;
                     if (m.lps_ok) {
                         CPD_TRY(dev_alloc(&m.ab, sizeof(float2) * np, st));
                         m.bytes += sizeof(float2) * np;
                     }
+                }
+                {
+                    // Warp lists of the split forms, each in the tile order of
+                    // tile_chunk: warps of kinds 2 and 3, and the rest.
+                    int g = 0;
+                    const EllView tv = tile_view(pd.view(), rows, kBlock, &g);
+                    const int64_t S = tv.stride, W = kBlock / 32;
+                    std::vector<int32_t> lean, rest;
+                    lean.reserve(nw);
+                    for (int64_t b = 0; b < g; ++b)
+                        for (int64_t w = 0; w < W; ++w) {
+                            const int64_t q = S > 1 ? (W * (b / S) + w) * S + b % S : W * b + w;
+                            if (q >= nw) continue;
+                            (kinds[q] >= 2 ? lean : rest).push_back((int32_t)q);
+                        }
+                    m.nlean = (int64_t)lean.size();
+                    m.nrest = (int64_t)rest.size();
+                    if (m.nlean) {
+                        CPD_TRY(dev_alloc(&m.lean_list, sizeof(int32_t) * m.nlean, st));
+                        CPD_TRY(cudaMemcpyAsync(m.lean_list, lean.data(), sizeof(int32_t) * m.nlean,
+                                                cudaMemcpyHostToDevice, st));
+                    }
+                    if (m.nrest) {
+                        CPD_TRY(dev_alloc(&m.rest_list, sizeof(int32_t) * m.nrest, st));
+                        CPD_TRY(cudaMemcpyAsync(m.rest_list, rest.data(), sizeof(int32_t) * m.nrest,
+                                                cudaMemcpyHostToDevice, st));
+                    }
+                    CPD_TRY(cudaStreamSynchronize(st));
+                    m.bytes += sizeof(int32_t) * (size_t)(m.nlean + m.nrest);
                 }
             }
         }
@@ -1239,6 +1569,8 @@ MixedLps to_mixed_lps(const Model& md, const MixedState& m)
     MixedLps l;
     l.s0 = (float)md.s0;
     l.guard = (float)(1e-4 * md.s0);
+    l.s_lo = l.s0 - l.guard;
+    l.s_hi = l.s0 + l.guard;
     l.bbc = md.bond_break_coeff;
     l.theta_coeff = md.theta_coeff;
     l.s_coeff = md.s_coeff;
@@ -1253,19 +1585,46 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
     if (rows <= 0) return 0;
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
-    const int g = blocks_for(rows);
+    const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024;
     const int key = (md.fracture ? 4 : 0) + (md.influence == 1 ? 2 : 0) + (with_m ? 1 : 0);
-    switch (key) {
-    case 0: k_lps_mtheta_mixed<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 1: k_lps_mtheta_mixed<false, 0, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 2: k_lps_mtheta_mixed<false, 1, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 3: k_lps_mtheta_mixed<false, 1, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 4: k_lps_mtheta_mixed<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 5: k_lps_mtheta_mixed<true, 0, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    case 6: k_lps_mtheta_mixed<true, 1, false><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
-    default: k_lps_mtheta_mixed<true, 1, true><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab); break;
+    int n = 0;
+    if (split) {
+        const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
+#define CPD_MT_LEAN(F, I, W)                                                                \
+    k_lps_mtheta_lean<F, I, W><<<gl, kBlock, lean_bytes, st>>>(p, nl, mv, l, m.ab, m.lean_list, \
+                                                               m.nlean)
+        switch (key) {
+        case 0: CPD_MT_LEAN(false, 0, false); break;
+        case 1: CPD_MT_LEAN(false, 0, true); break;
+        case 2: CPD_MT_LEAN(false, 1, false); break;
+        case 3: CPD_MT_LEAN(false, 1, true); break;
+        case 4: CPD_MT_LEAN(true, 0, false); break;
+        case 5: CPD_MT_LEAN(true, 0, true); break;
+        case 6: CPD_MT_LEAN(true, 1, false); break;
+        default: CPD_MT_LEAN(true, 1, true); break;
+        }
+#undef CPD_MT_LEAN
+        ++n;
+        if (m.nrest == 0) return n;
     }
-    return 1;
+    const int32_t* list = split ? m.rest_list : nullptr;
+    const int64_t count = split ? m.nrest : 0;
+    const int g = split ? (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32)) : blocks_for(rows);
+#define CPD_MT(F, I, W) \
+    k_lps_mtheta_mixed<F, I, W><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, list, count)
+    switch (key) {
+    case 0: CPD_MT(false, 0, false); break;
+    case 1: CPD_MT(false, 0, true); break;
+    case 2: CPD_MT(false, 1, false); break;
+    case 3: CPD_MT(false, 1, true); break;
+    case 4: CPD_MT(true, 0, false); break;
+    case 5: CPD_MT(true, 0, true); break;
+    case 6: CPD_MT(true, 1, false); break;
+    default: CPD_MT(true, 1, true); break;
+    }
+#undef CPD_MT
+    return n + 1;
 }
 
 int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
@@ -1275,15 +1634,104 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     if (rows <= 0) return 0;
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
-    const int g = blocks_for(rows);
-    switch ((md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0)) {
-    case 0: k_lps_force_mixed<false, 0><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
-    case 1: k_lps_force_mixed<false, 1><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
-    case 2: k_lps_force_mixed<true, 0><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
-    default: k_lps_force_mixed<true, 1><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep); break;
+    const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024;
+    const int key = (md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0);
+    int n = 0;
+    if (split) {
+        const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
+#define CPD_F_LEAN(F, I)                                                                     \
+    k_lps_force_lean<F, I><<<gl, kBlock, lean_bytes, st>>>(p, nl, mv, l, m.ab, ep, m.lean_list, \
+                                                           m.nlean)
+        switch (key) {
+        case 0: CPD_F_LEAN(false, 0); break;
+        case 1: CPD_F_LEAN(false, 1); break;
+        case 2: CPD_F_LEAN(true, 0); break;
+        default: CPD_F_LEAN(true, 1); break;
+        }
+#undef CPD_F_LEAN
+        ++n;
+        if (m.nrest == 0) return n;
+    }
+    const int32_t* list = split ? m.rest_list : nullptr;
+    const int64_t count = split ? m.nrest : 0;
+    const int g = split ? (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32)) : blocks_for(rows);
+#define CPD_F(F, I) k_lps_force_mixed<F, I><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, ep, list, count)
+    switch (key) {
+    case 0: CPD_F(false, 0); break;
+    case 1: CPD_F(false, 1); break;
+    case 2: CPD_F(true, 0); break;
+    default: CPD_F(true, 1); break;
+    }
+#undef CPD_F
+    return n + 1;
+}
+
+namespace {
+
+// Launches one mixed PMB bond-kernel form (mixed_variant); returns the number
+// of kernels launched.
+template <bool FRACTURE>
+int launch_mixed_form_t(const ParticleView& p, const EllView& list, const MixedView& mv,
+                        const MixedModel& mm, const MixedState& m, const StepEpilogue& ep,
+                        int64_t rows, cudaStream_t st)
+{
+    int g = blocks_for(rows);
+    const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
+    // The lean forms hold a compacted table per warp; past 48 KB of shared
+    // memory per block (ntab > 170) the paired form runs instead.
+    int var = mixed_variant();
+    const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
+    if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
+    if (var >= 9 && !m.lean_list) var = 5;
+    if (var >= 9) {
+        // Split form: lean warps, then the rest.
+        int n = 0;
+        if (m.nlean > 0) {
+            const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
+            switch (var) {
+            case 9: k_pmb_force_lean<FRACTURE, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
+            case 10: k_pmb_force_lean<FRACTURE, 5, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
+            case 11: k_pmb_force_lean<FRACTURE, 5, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
+            default: k_pmb_force_lean<FRACTURE, 6, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
+            }
+            ++n;
+        }
+        if (m.nrest > 0) {
+            const int gr = (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32));
+            k_pmb_force_mixed<FRACTURE, 4, false, 2><<<gr, kBlock, tab_bytes, st>>>(
+                p, list, mv, mm, ep, m.rest_list, m.nrest);
+            ++n;
+        }
+        return n;
+    }
+    EllView nl = list;
+    if (var >= 5) nl = tile_view(list, rows, kBlock, &g);
+    const size_t sb = var >= 5 ? lean_bytes : tab_bytes;
+    const int32_t* nolist = nullptr;
+    switch (var) {
+    case 0: k_pmb_force_mixed<FRACTURE, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 1: k_pmb_force_mixed<FRACTURE, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 2: k_pmb_force_mixed<FRACTURE, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 3: k_pmb_force_mixed<FRACTURE, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 4: k_pmb_force_mixed<FRACTURE, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 6: k_pmb_force_mixed<FRACTURE, 4, false, 4><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 7: k_pmb_force_mixed<FRACTURE, 4, false, 5><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    case 8: k_pmb_force_mixed<FRACTURE, 3, false, 4><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
+    default: k_pmb_force_mixed<FRACTURE, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
     }
     return 1;
 }
+
+int launch_mixed_form(bool fracture, const ParticleView& p, const EllView& list,
+                      const MixedView& mv, const MixedModel& mm, const MixedState& m,
+                      const StepEpilogue& ep, int64_t rows, cudaStream_t st)
+{
+    return fracture ? launch_mixed_form_t<true>(p, list, mv, mm, m, ep, rows, st)
+                    : launch_mixed_form_t<false>(p, list, mv, mm, m, ep, rows, st);
+}
+
+}  // namespace
 
 int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
@@ -1300,31 +1748,7 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Mode
     mm.s_lo = mm.s0 - mm.guard;
     mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
-    int g = blocks_for(rows);
-    const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
-    // The lean forms hold a compacted table per warp; past 48 KB of shared
-    // memory per block (ntab > 170) the paired form runs instead.
-    int var = mixed_variant();
-    const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
-    if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
-    EllView nl = list;
-    if (var >= 5) nl = tile_view(list, rows, kBlock, &g);
-    const size_t sb = var >= 5 ? lean_bytes : tab_bytes;
-    switch ((md.fracture ? 0 : 10) + var) {
-    case 0: k_pmb_force_mixed<true, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 1: k_pmb_force_mixed<true, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 2: k_pmb_force_mixed<true, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 3: k_pmb_force_mixed<true, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 4: k_pmb_force_mixed<true, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 5: k_pmb_force_mixed<true, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 10: k_pmb_force_mixed<false, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 11: k_pmb_force_mixed<false, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 12: k_pmb_force_mixed<false, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 13: k_pmb_force_mixed<false, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    case 14: k_pmb_force_mixed<false, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    default: k_pmb_force_mixed<false, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep); break;
-    }
-    return 1;
+    return launch_mixed_form(md.fracture != 0, p, list, mv, mm, m, ep, rows, st);
 }
 
 }  // namespace cpd
