@@ -275,9 +275,11 @@ def run_reference(args, world, rank):
 
 # ---------------------------------------------------------------------------
 PRECISION = {"exact": 0, "fp64": 1, "mixed": 2}
-KERNEL = {"fp64": "k_pmb_force_fast<fracture>", "mixed": "k_pmb_force_mixed<fracture>",
+KERNEL = {"fp64": "k_pmb_force_fast<fracture>",
+          "mixed": "k_pmb_force_lean<fracture> + k_pmb_force_mixed<fracture> (one bond stage: "
+                   "lean warps, then the rest)",
           "exact": "k_pd_force<PMB, fracture> (bit-exact)"}
-PROFILE = {"fp64": "pmb_force_plate.txt", "mixed": "pmb_force_mixed_plate.txt",
+PROFILE = {"fp64": "pmb_force_plate.txt", "mixed": "pmb_force_lean_plate.txt",
            "exact": "pmb_force_exact_plate.txt"}
 
 
@@ -345,7 +347,8 @@ def measure_other(name, device, stream, steps, warmup):
     if name == "lps":
         prob = P.lps_random_notches(num_cells=LPS_CELLS, steps=steps)
         precs = ["mixed", "fp64"]
-        kernel = {"mixed": "k_lps_mtheta_mixed + k_lps_force_mixed<fracture> (fused step)",
+        kernel = {"mixed": "k_lps_mtheta_lean + k_lps_force_lean<fracture> over lean warps, "
+                           "k_lps_mtheta_mixed + k_lps_force_mixed over the rest (fused step)",
                   "fp64": "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"}
         wl = {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)}
     else:
