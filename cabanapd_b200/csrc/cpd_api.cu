@@ -130,6 +130,8 @@ struct cpd_system {
     int32_t* perm = nullptr;  // internal -> caller index; nullptr = identity
     std::vector<int32_t> h_inv;  // caller -> internal
     double* staging = nullptr;   // [3 n] transfer buffer
+    double* stress = nullptr;    // [9][npad] per-particle stress (cpd_compute_stress)
+    double* stress_staging = nullptr;  // [9 n] its transfer buffer
     double* red = nullptr;       // reduction partials
     int red_cap = 0;
     double* red_out = nullptr;   // small result slots
@@ -156,6 +158,7 @@ struct cpd_system {
     MixedU* u2_alt = nullptr;
     bool neighbors_built = false;
     bool initialized = false;
+    bool stress_ready = false;  // cpd_compute_stress ran since the particles were set
     double max_disp = 0.0;
     int64_t steps_since_rebuild = 0;
     int64_t rebuilds = 0;
@@ -226,7 +229,7 @@ void free_particles(cpd_system* s)
     double** arrays[] = {&s->x,     &s->u,     &s->v,     &s->f,     &s->vol,
                          &s->rho,   &s->m,     &s->theta, &s->lps_a, &s->lps_b,
                          &s->W,     &s->phi,   &s->radius, &s->u_neigh, &s->staging,
-                         &s->red,   &s->red_out};
+                         &s->red,   &s->red_out, &s->stress, &s->stress_staging};
     for (double** a : arrays)
         if (*a) {
             dev_free(*a, s->stream);
@@ -234,6 +237,7 @@ void free_particles(cpd_system* s)
         }
     if (s->nofail) dev_free(s->nofail, s->stream);
     s->nofail = nullptr;
+    s->stress_ready = false;
     if (s->perm) dev_free(s->perm, s->stream);
     s->perm = nullptr;
     for (auto& bc : s->bcs) {
@@ -1136,6 +1140,24 @@ cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
     return CPD_OK;
 }
 
+// CabanaPD_Force.hpp:222-235 computeStress: the stress of the current state
+// (bond bits and, for LPS, the m / theta of the last force update), zeroed
+// first. Allocates its arrays on the first call.
+cpd_status cpd_compute_stress(cpd_system* s)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (!s->stress) {
+        CPD_CUDA(dev_alloc(&s->stress, sizeof(double) * 9 * s->npad, s->stream));
+        CPD_CUDA(dev_alloc(&s->stress_staging, sizeof(double) * 9 * std::max<int64_t>(s->n, 1),
+                           s->stream));
+    }
+    CPD_CUDA(cudaMemsetAsync(s->stress, 0, sizeof(double) * 9 * s->npad, s->stream));
+    if (has_pd(s)) CPD_LAUNCHED(launch_pd_stress(view(s), pd_view(s), s->md, s->stress, s->stream));
+    s->stress_ready = true;
+    return CPD_OK;
+}
+
 // CabanaPD_Solver.hpp:229-279 init(bc): weighted volume once without
 // fracture, updateForce (no contact force unless the contact model is the
 // force model), energy, force BCs at t = 0.
@@ -1219,8 +1241,16 @@ cpd_status cpd_download(cpd_system* s, int32_t field, double* out)
     if (!out) return set_error(CPD_ERR_INVALID_ARGUMENT, "null output");
     CPD_CUDA(cudaSetDevice(s->device));
     const double* src = nullptr;
+    double* staging = s->staging;
     int comps = 1;
     switch (field) {
+    case CPD_FIELD_STRESS:
+        if (!s->stress_ready)
+            return set_error(CPD_ERR_STATE, "stress: call cpd_compute_stress first");
+        src = s->stress;
+        staging = s->stress_staging;
+        comps = 9;
+        break;
     case CPD_FIELD_X: src = s->x; comps = 3; break;
     case CPD_FIELD_U: src = s->u; comps = 3; break;
     case CPD_FIELD_V: src = s->v; comps = 3; break;
@@ -1234,9 +1264,9 @@ cpd_status cpd_download(cpd_system* s, int32_t field, double* out)
     case CPD_FIELD_RADIUS: src = s->radius; break;
     default: return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown field");
     }
-    s->launches += launch_soa_to_aos(src, s->staging, s->n, s->npad, comps, s->perm, s->stream);
+    s->launches += launch_soa_to_aos(src, staging, s->n, s->npad, comps, s->perm, s->stream);
     CPD_CUDA(cudaGetLastError());
-    CPD_CUDA(cudaMemcpyAsync(out, s->staging, sizeof(double) * comps * s->n,
+    CPD_CUDA(cudaMemcpyAsync(out, staging, sizeof(double) * comps * s->n,
                              cudaMemcpyDeviceToHost, s->stream));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     return CPD_OK;
@@ -1262,6 +1292,11 @@ cpd_status cpd_device_field(cpd_system* s, int32_t field, void** ptr, int64_t* s
     case CPD_FIELD_W: p = s->W; break;
     case CPD_FIELD_PHI: p = s->phi; break;
     case CPD_FIELD_RADIUS: p = s->radius; break;
+    case CPD_FIELD_STRESS:
+        if (!s->stress)
+            return set_error(CPD_ERR_STATE, "stress: call cpd_compute_stress first");
+        p = s->stress;
+        break;
     default: return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown field");
     }
     *ptr = p;
@@ -1327,6 +1362,7 @@ cpd_status cpd_device_bytes(const cpd_system* s, uint64_t* bytes)
     }
     for (const auto& bc : s->bcs) b += (uint64_t)bc.count * (bc.values ? 12 : 4);
     if (s->u_alt) b += 24 * np;
+    if (s->stress) b += 72 * np + 72 * std::max<uint64_t>(n, 1);
     if (s->u2_alt) b += sizeof(MixedU) * np;
     if (s->bc_bits) b += 4 * ((np + 31) / 32) + 29 * (uint64_t)s->nbc;
     b += s->pd.bytes + s->contact.bytes + s->mixed.bytes;

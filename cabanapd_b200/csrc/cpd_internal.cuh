@@ -190,6 +190,8 @@ int launch_force_bc(const ParticleView& p, const BoundaryCondition& bc,
 int launch_prenotch(const ParticleView& p, const EllView& nl, const double* v1,
                     const double* v2, const double* p0, double margin,
                     cudaStream_t st);
+int launch_pd_stress(const ParticleView& p, const EllView& nl, const Model& md, double* sigma,
+                     cudaStream_t st);
 int launch_sum_partials(const double* partials, int nblocks, int ncols,
                         double* out, cudaStream_t st);
 int launch_max_partials(const double* partials, int nblocks, double* out,

@@ -330,6 +330,83 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// Per-particle stress: force/CabanaPD_PMB.hpp:157-202 (NoFracture), :341-401
+// (Fracture), :492-537 (LinearPMB); force/CabanaPD_LPS.hpp:221-267
+// (NoFracture), :506-572 (Fracture: intact bonds only). Half the pair force
+// times the reference bond vector, sigma(i, a, b) = sum_k f_a xi_b over the
+// row in row order (the caller zeroes sigma first, CabanaPD_Force.hpp:
+// 229-231). Component-major: sigma[(3 a + b) npad + i]. LPS uses the factors
+// a = theta_coeff theta / m and b = s_coeff / m of the last force update,
+// exact subexpressions of the reference's coefficient.
+template <int MODEL, int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock)
+    k_pd_stress(ParticleView p, EllView nl, ModelDev md, double* __restrict__ sigma)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+    constexpr bool lps = MODEL == M_LPS;
+    constexpr bool linear = MODEL == M_LINEAR_PMB;
+    double a_i = 0.0, b_i = 0.0;
+    if (lps) {
+        a_i = p.lps_a[i];
+        b_i = p.lps_b[i];
+    }
+    const int cnt = nl.count[i];
+    double S[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    uint32_t word = 0;
+    for (int k = 0; k < cnt; ++k) {
+        if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+        const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+        const double vol_j = __ldg(p.vol + j);
+        double fx, fy, fz, xx, xy, xz;
+        if (linear) {
+            double xi, ls;
+            bond_linearized(p.x, p.u, np, j, xi0, xi1, xi2, ui0, ui1, ui2, xi, ls, xx, xy,
+                            xz);
+            const double coeff = 0.5 * (md.c * ls * vol_j);
+            fx = coeff * xx / xi;
+            fy = coeff * xy / xi;
+            fz = coeff * xz / xi;
+        } else {
+            const double mu = FRACTURE ? (double)((word >> (k & 31)) & 1u) : 1.0;
+            if (FRACTURE && lps && !(mu > 0.0)) continue;
+            double xi, r, s, rx, ry, rz;
+            bond_geometry(p.x, p.u, np, j, xi0, xi1, xi2, ui0, ui1, ui2, xi, r, s, rx, ry,
+                          rz, xx, xy, xz);
+            double coeff;
+            if (lps) {
+                const double a_j = __ldg(p.lps_a + j), b_j = __ldg(p.lps_b + j);
+                coeff = (a_i + a_j + s * (b_i + b_j)) * influence<INFL>(xi) * xi * vol_j;
+                coeff *= 0.5;
+            } else {
+                coeff = 0.5 * (md.c * s * vol_j);
+            }
+            if (FRACTURE) {
+                fx = mu * coeff * rx / r;
+                fy = mu * coeff * ry / r;
+                fz = mu * coeff * rz / r;
+            } else {
+                fx = coeff * rx / r;
+                fy = coeff * ry / r;
+                fz = coeff * rz / r;
+            }
+        }
+        S[0] += fx * xx;
+        S[4] += fy * xy;
+        S[8] += fz * xz;
+        S[1] += fx * xy;
+        S[3] += fy * xx;
+        S[2] += fx * xz;
+        S[6] += fz * xx;
+        S[5] += fy * xz;
+        S[7] += fz * xy;
+    }
+    for (int c = 0; c < 9; ++c) sigma[(int64_t)c * np + i] = S[c];
+}
+
 // Single-block fixed-order sum of [nblocks][ncols] partials.
 __global__ void __launch_bounds__(kBlock)
     k_sum_partials(const double* partials, int nblocks, int ncols, double* out)
@@ -722,6 +799,17 @@ int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
 {
     const ModelDev d = to_dev(md);
     CPD_PD_DISPATCH(k_pd_energy, nblocks, p, nl, d, partials);
+    return 1;
+}
+
+int launch_pd_stress(const ParticleView& p, const EllView& nl, const Model& md, double* sigma,
+                     cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    const int g = blocks_for(rows);
+    const ModelDev d = to_dev(md);
+    CPD_PD_DISPATCH(k_pd_stress, g, p, nl, d, sigma);
     return 1;
 }
 

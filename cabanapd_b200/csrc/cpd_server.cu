@@ -242,6 +242,11 @@ struct cpd_server {
                                            bc.idx.data(), bc.values.data()) != CPD_OK)
                 return lib_error("cpd_add_boundary_condition");
         if (cpd_init(j->sys) != CPD_OK) return lib_error("cpd_init");
+        // A kept stress is computed at the end; computing it once here (as
+        // the reference does at init) allocates its arrays before the job's
+        // device bytes are measured.
+        if ((j->keep >> CPD_FIELD_STRESS) & 1u)
+            if (cpd_compute_stress(j->sys) != CPD_OK) return lib_error("cpd_compute_stress");
         int32_t max_n = 0;
         cpd_neighbor_stats(j->sys, &max_n, &j->bonds);
         j->contact = s.params.contact_model != CPD_CONTACT_NONE;
@@ -286,10 +291,14 @@ struct cpd_server {
         double W = 0, D = 0;
         if (cpd_compute_energy(j->sys, &W, &D) != CPD_OK)
             err = std::string("cpd_compute_energy: ") + cpd_last_error();
+        if (err.empty() && ((j->keep >> CPD_FIELD_STRESS) & 1u) &&
+            cpd_compute_stress(j->sys) != CPD_OK)
+            err = std::string("cpd_compute_stress: ") + cpd_last_error();
         std::map<int32_t, std::vector<double>> results;
-        for (int32_t f = 0; f <= CPD_FIELD_RADIUS && err.empty(); f++) {
+        for (int32_t f = 0; f <= CPD_FIELD_STRESS && err.empty(); f++) {
             if (!(j->keep & (1u << f))) continue;
-            std::vector<double> buf((vector_field(f) ? 3 : 1) * (size_t)j->n);
+            const size_t comps = f == CPD_FIELD_STRESS ? 9 : (vector_field(f) ? 3 : 1);
+            std::vector<double> buf(comps * (size_t)j->n);
             if (cpd_download(j->sys, f, buf.data()) != CPD_OK)
                 err = std::string("cpd_download: ") + cpd_last_error();
             results[f].swap(buf);
@@ -563,7 +572,7 @@ cpd_status cpd_job_add_boundary_condition(cpd_job* j, int32_t kind, int32_t comp
 cpd_status cpd_job_keep_fields(cpd_job* j, uint32_t mask)
 {
     if (!j) return fail(CPD_ERR_INVALID_ARGUMENT, "null job");
-    if (mask >> (CPD_FIELD_RADIUS + 1)) return fail(CPD_ERR_INVALID_ARGUMENT, "unknown field bit");
+    if (mask >> (CPD_FIELD_STRESS + 1)) return fail(CPD_ERR_INVALID_ARGUMENT, "unknown field bit");
     j->keep = mask;
     return CPD_OK;
 }

@@ -13,8 +13,16 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libcabanapd_b200.so")
 
 FIELDS = {"x": 0, "u": 1, "v": 2, "f": 3, "vol": 4, "rho": 5, "m": 6,
-          "theta": 7, "W": 8, "phi": 9, "radius": 10}
+          "theta": 7, "W": 8, "phi": 9, "radius": 10, "stress": 11}
 VECTOR_FIELDS = {"x", "u", "v", "f"}
+
+
+def _field_shape(field, n):
+    if field in VECTOR_FIELDS:
+        return (n, 3)
+    if field == "stress":
+        return (n, 3, 3)
+    return (n,)
 FP64_EXACT = 0
 FP64 = 1
 MIXED = 2
@@ -126,6 +134,7 @@ SIGNATURES = {
     "cpd_compute_dilatation": (_I32, [_P]),
     "cpd_compute_force": (_I32, [_P]),
     "cpd_compute_energy": (_I32, [_P, _DP, _DP]),
+    "cpd_compute_stress": (_I32, [_P]),
     "cpd_compute_energy_noalloc": (_I32, [_P, _P, _P, _P]),
     "cpd_init": (_I32, [_P]),
     "cpd_step": (_I32, [_P, _I32]),
@@ -285,6 +294,10 @@ class System:
         self._check(self._lib.cpd_compute_energy(self._h, ctypes.byref(w), ctypes.byref(d)))
         return w.value, d.value
 
+    def compute_stress(self):
+        """Per-particle stress of the current state (get("stress") -> [n, 3, 3])."""
+        self._check(self._lib.cpd_compute_stress(self._h))
+
     def init(self):
         self._check(self._lib.cpd_init(self._h))
 
@@ -305,7 +318,7 @@ class System:
         self._check(self._lib.cpd_step_stage(self._h, int(stage)))
 
     def get(self, field, out=None):
-        shape = (self.n, 3) if field in VECTOR_FIELDS else (self.n,)
+        shape = _field_shape(field, self.n)
         if out is None:
             out = np.zeros(shape)
         self._check(self._lib.cpd_download(self._h, FIELDS[field], out.ctypes.data))
@@ -455,7 +468,7 @@ class Server:
 
     def get(self, job_id, field):
         n = self._n[job_id]
-        out = np.empty((n, 3) if field in VECTOR_FIELDS else (n,), dtype=np.float64)
+        out = np.empty(_field_shape(field, n), dtype=np.float64)
         self._check(self._lib.cpd_server_download(self._h, int(job_id), FIELDS[field],
                                                   out.ctypes.data))
         return out

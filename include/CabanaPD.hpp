@@ -193,6 +193,8 @@ struct Slice {
         return host[d * hstride + i];
 #endif
     }
+    // Tensor fields (stress): component (a, b) is column 3 a + b.
+    CPD_HD T& operator()(int64_t i, int a, int b) const { return (*this)(i, 3 * a + b); }
     std::size_t size() const { return static_cast<std::size_t>(n); }
 };
 
@@ -206,10 +208,14 @@ struct ParticleData {
     std::array<int, 3> nc{};
     std::vector<double> x, u, v, f, vol, rho, W, phi;
     std::vector<int> nofail;
+    // EnergyStressOutput particles: the stress mirror, [9][n] (component
+    // 3 a + b), refreshed with the others.
+    bool with_stress = false;
+    std::vector<double> stress;
     cpd_system* sys = nullptr;
     int64_t dstride = 0;
     double *d_x = nullptr, *d_u = nullptr, *d_v = nullptr, *d_f = nullptr, *d_vol = nullptr,
-           *d_rho = nullptr, *d_W = nullptr, *d_phi = nullptr;
+           *d_rho = nullptr, *d_W = nullptr, *d_phi = nullptr, *d_stress = nullptr;
 
     ParticleData() = default;
     ParticleData(const ParticleData&) = delete;
@@ -238,6 +244,7 @@ struct ParticleData {
         W.resize(m, 0.0);
         phi.resize(m, 0.0);
         nofail.resize(m, 0);
+        if (with_stress) stress.assign(9 * m, 0.0);
         n = m;
     }
     std::vector<double> interleaved(const std::vector<double>& soa) const
@@ -264,6 +271,25 @@ struct ParticleData {
         download3(CPD_FIELD_F, f, tmp);
         cpdCheck(cpd_download(sys, CPD_FIELD_W, W.data()));
         cpdCheck(cpd_download(sys, CPD_FIELD_PHI, phi.data()));
+        if (with_stress && d_stress) {
+            tmp.resize(9 * n);
+            cpdCheck(cpd_download(sys, CPD_FIELD_STRESS, tmp.data()));
+            for (int64_t i = 0; i < n; i++)
+                for (int c = 0; c < 9; c++) stress[c * n + i] = tmp[9 * i + c];
+        }
+    }
+    // CabanaPD_Force.hpp:222-235 computeStress, for EnergyStressOutput
+    // particles (Solver.hpp:243, 486: at init and output steps).
+    void compute_stress()
+    {
+        if (!with_stress || !sys) return;
+        cpdCheck(cpd_compute_stress(sys));
+        if (!d_stress) {
+            void* ptr = nullptr;
+            int64_t stride = 0;
+            cpdCheck(cpd_device_field(sys, CPD_FIELD_STRESS, &ptr, &stride));
+            d_stress = static_cast<double*>(ptr);
+        }
     }
 };
 
@@ -285,7 +311,10 @@ class Particles {
     Kokkos::Array<double, 3> local_mesh_lo{}, local_mesh_hi{};
     Kokkos::Array<double, 3> ghost_mesh_lo{}, ghost_mesh_hi{};
 
-    Particles(MemorySpace, ModelTag, Rest...) : d_(std::make_shared<detail::ParticleData>()) {}
+    Particles(MemorySpace, ModelTag, Rest...) : d_(std::make_shared<detail::ParticleData>())
+    {
+        d_->with_stress = (std::is_same<Rest, EnergyStressOutput>::value || ... || false);
+    }
 
     void domain(std::array<double, 3> low, std::array<double, 3> high, std::array<int, 3> num_cells,
                 int /*halo_width*/)
@@ -349,6 +378,14 @@ class Particles {
     Slice<double> sliceDensity() const { return slice(d_->rho, d_->d_rho); }
     Slice<double> sliceStrainEnergy() const { return slice(d_->W, d_->d_W); }
     Slice<double> sliceDamage() const { return slice(d_->phi, d_->d_phi); }
+    // Particles built with EnergyStressOutput: stress(i, a, b), computed at
+    // init and output steps.
+    Slice<double> sliceStress() const
+    {
+        if (!d_->with_stress)
+            throw std::runtime_error("sliceStress: particles were not built with EnergyStressOutput");
+        return slice(d_->stress, d_->d_stress);
+    }
     // Host-only: the no-fail flags are uploaded with the particles.
     Slice<int> sliceNoFail() const
     {
@@ -961,6 +998,7 @@ class Solver {
     {
         const auto& d = particles.data();
         cpdCheck(cpd_system_create(&params_, &d->sys));
+        d->d_stress = nullptr;
         const int64_t n = d->n;
         const std::vector<double> xi = d->interleaved(d->x);
         const std::vector<int32_t> nofail(d->nofail.begin(), d->nofail.end());
@@ -1010,6 +1048,10 @@ class Solver {
         cpdCheck(cpd_init(d->sys));
         initialized_ = true;
         if (stage_ && stage_->force_update) stage_->apply(0.0);
+        if (d->with_stress) {
+            d->compute_stress();
+            d->refresh_mirrors();
+        }
         cpdCheck(cpd_synchronize(d->sys));
         init_time_ += seconds_since(t0);
     }
@@ -1035,10 +1077,9 @@ class Solver {
             cpdCheck(cpd_step_stage(d->sys, CPD_STAGE_FINAL_HALF));
             if (step % output_frequency == 0) {
                 cpdCheck(cpd_compute_energy(d->sys, &last_W_, &last_D_));
-                if constexpr (sizeof...(Out) > 0) {
-                    d->refresh_mirrors();
-                    (outputs.update(time), ...);
-                }
+                d->compute_stress();
+                if (sizeof...(Out) > 0 || d->with_stress) d->refresh_mirrors();
+                if constexpr (sizeof...(Out) > 0) (outputs.update(time), ...);
                 const double elapsed = seconds_since(t_start);
                 std::ofstream out(output_file_, std::ofstream::app);
                 out << step << "/" << num_steps << " " << std::scientific << std::setprecision(2)

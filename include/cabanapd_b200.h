@@ -31,6 +31,10 @@
  *                            computeDilatation / computeForceFull /
  *                            computeEnergyFull and the free functions
  *                            computeForce / computeEnergy (CabanaPD_Force.hpp:176-219)
+ *   cpd_compute_stress       computeStress + Force<...>::computeStressFull
+ *                            (CabanaPD_Force.hpp:222-235; force/CabanaPD_PMB.hpp:
+ *                            157-202, 341-401, 492-537; force/CabanaPD_LPS.hpp:
+ *                            221-267, 506-572)
  *   cpd_init                 Solver::init(bc[, prenotch]) (CabanaPD_Solver.hpp:229-297)
  *   cpd_step                 Solver::runStep(step, bc) x num_steps
  *                            (CabanaPD_Solver.hpp:332-375)
@@ -113,7 +117,9 @@ enum {
 };
 
 /* Fields for cpd_download / cpd_device_field. Vector fields are returned as
- * [n][3] (x, y, z interleaved, the reference's slice layout). */
+ * [n][3] (x, y, z interleaved, the reference's slice layout); the stress as
+ * [n][3][3] (sliceStress() layout), on the device component-major
+ * [9][stride] with component 3 a + b. */
 enum {
     CPD_FIELD_X = 0,      /* reference position */
     CPD_FIELD_U = 1,      /* displacement */
@@ -125,7 +131,8 @@ enum {
     CPD_FIELD_THETA = 7,  /* LPS dilatation */
     CPD_FIELD_W = 8,      /* strain energy density */
     CPD_FIELD_PHI = 9,    /* damage */
-    CPD_FIELD_RADIUS = 10 /* contact radius (per-particle model) */
+    CPD_FIELD_RADIUS = 10, /* contact radius (per-particle model) */
+    CPD_FIELD_STRESS = 11  /* per-particle stress (after cpd_compute_stress) */
 };
 
 typedef struct cpd_params {
@@ -207,6 +214,15 @@ cpd_status cpd_compute_force(cpd_system* sys);
 /* W_i, damage phi_i and the totals sum(W_i vol_i), sum(phi_i). */
 cpd_status cpd_compute_energy(cpd_system* sys, double* total_strain_energy,
                               double* total_damage);
+/* Per-particle stress sigma_i = sum over row i of (1/2) f_pair (x) xi (the
+ * reference's computeStressFull: half the pair force times the reference bond
+ * vector; LPS with fracture over intact bonds only), of the current state:
+ * bond bits and, for LPS, the m / theta of the last force update. The
+ * reference computes it at init and output steps of particles built with
+ * EnergyStressOutput (Solver.hpp:243, 486). Frozen particles get zero.
+ * Allocates 72 B per particle on the first call. Queued on the stream;
+ * cpd_download(CPD_FIELD_STRESS) waits. */
+cpd_status cpd_compute_stress(cpd_system* sys);
 /* No counterpart in the reference. The same energy and damage computation
  * for callers that may not allocate device memory after set-up (a job
  * server that reserved each job's memory at admission, or a framework that

@@ -74,6 +74,7 @@ struct orc_system {
     Model model;
     int64_t n = 0, frozen = 0;
     std::vector<double> x, u, v, f, vol, rho, m, theta, W, phi, radius, u_neigh;
+    std::vector<double> stress;  // [n][3][3]
     std::vector<int32_t> nofail;
     NList pd_list;
     std::vector<int32_t> mu;  // [n][pd_list.max_n], 1 = intact
@@ -456,6 +457,70 @@ void pd_energy(orc_system& s, double& total_W, double& total_D)
     total_D = D;
 }
 
+// force/CabanaPD_PMB.hpp:157-202 (NoFracture), :341-401 (Fracture),
+// :492-537 (LinearPMB); force/CabanaPD_LPS.hpp:221-267 (NoFracture),
+// :506-572 (Fracture: intact bonds only). Half the pair force times the
+// reference bond vector, stress(i, a, b) += f_a xi_b, accumulated over the
+// row in row order after the tensor is zeroed (CabanaPD_Force.hpp:222-235).
+void pd_stress(orc_system& s)
+{
+    const Model& md = s.model;
+    const NList& nl = s.pd_list;
+    const double* x = s.x.data();
+    const double* u = s.u.data();
+    const bool linear = md.pd == ORC_PD_LINEAR_PMB;
+    const bool lps = md.pd == ORC_PD_LPS;
+    std::fill(s.stress.begin(), s.stress.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = s.frozen; i < s.n; i++) {
+        double* S = &s.stress[9 * (size_t)i];
+        for (int32_t nn = 0; nn < nl.count[i]; nn++) {
+            const int64_t j = nl.idx[(size_t)i * nl.max_n + nn];
+            double fx, fy, fz, xx, xy, xz;
+            if (linear) {
+                double xi, ls;
+                get_linearized_distance(x, u, i, j, xi, ls, xx, xy, xz);
+                const double coeff = 0.5 * (md.c * ls * s.vol[j]);
+                fx = coeff * xx / xi;
+                fy = coeff * xy / xi;
+                fz = coeff * xz / xi;
+            } else {
+                double xi, r, st, rx, ry, rz;
+                get_distance(x, u, i, j, xi, r, st, rx, ry, rz, xx, xy, xz);
+                const int32_t mu = md.fracture ? s.mu[(size_t)i * nl.max_n + nn] : 1;
+                if (md.fracture && lps && !(mu > 0)) continue;
+                double coeff;
+                if (lps) {
+                    coeff = lps_force_coeff(md, st, xi, s.vol[j], s.m[i], s.m[j], s.theta[i],
+                                            s.theta[j]);
+                    coeff *= 0.5;
+                } else {
+                    coeff = 0.5 * (md.c * st * s.vol[j]);
+                }
+                if (md.fracture) {
+                    const double muij = mu;
+                    fx = muij * coeff * rx / r;
+                    fy = muij * coeff * ry / r;
+                    fz = muij * coeff * rz / r;
+                } else {
+                    fx = coeff * rx / r;
+                    fy = coeff * ry / r;
+                    fz = coeff * rz / r;
+                }
+            }
+            S[0] += fx * xx;
+            S[4] += fy * xy;
+            S[8] += fz * xz;
+            S[1] += fx * xy;
+            S[3] += fy * xx;
+            S[2] += fx * xz;
+            S[6] += fz * xx;
+            S[5] += fy * xz;
+            S[7] += fz * xy;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Hertzian contact: force/CabanaPD_Contact.hpp:119-168 with the model of
 // force_models/CabanaPD_Hertzian.hpp:58-87. With per_particle_radius the
@@ -815,6 +880,7 @@ int orc_set_particles(orc_system* s, int64_t n, int64_t n_frozen,
     s->theta.assign(n, 0.0);
     s->W.assign(n, 0.0);
     s->phi.assign(n, 0.0);
+    s->stress.assign(9 * (size_t)n, 0.0);
     s->ready = false;
     return 0;
 }
@@ -938,6 +1004,12 @@ int orc_compute_energy(orc_system* s, double* total_W, double* total_D)
     return 0;
 }
 
+int orc_compute_stress(orc_system* s)
+{
+    if (has_pd(*s)) pd_stress(*s);
+    return 0;
+}
+
 // CabanaPD_Solver.hpp:229-279 init(bc): weighted volume once without
 // fracture, updateForce, energy, then the force BCs at t = 0.
 int orc_init(orc_system* s)
@@ -990,6 +1062,7 @@ int orc_get(const orc_system* s, int32_t field, double* out)
     case ORC_FIELD_W: src = &s->W; break;
     case ORC_FIELD_PHI: src = &s->phi; break;
     case ORC_FIELD_RADIUS: src = &s->radius; break;
+    case ORC_FIELD_STRESS: src = &s->stress; break;
     default: return fail("orc_get: unknown field");
     }
     std::memcpy(out, src->data(), src->size() * sizeof(double));

@@ -58,7 +58,8 @@ enum {
     ORC_FIELD_THETA = 7,
     ORC_FIELD_W = 8,
     ORC_FIELD_PHI = 9,
-    ORC_FIELD_RADIUS = 10
+    ORC_FIELD_RADIUS = 10,
+    ORC_FIELD_STRESS = 11  /* [n][3][3] per-particle stress */
 };
 
 typedef struct orc_params {
@@ -105,6 +106,8 @@ int orc_compute_weighted_volume(orc_system* s);
 int orc_compute_dilatation(orc_system* s);
 int orc_compute_force(orc_system* s);
 int orc_compute_energy(orc_system* s, double* total_W, double* total_D);
+/* CabanaPD_Force.hpp:222-235 computeStress: zeroes and fills the stress. */
+int orc_compute_stress(orc_system* s);
 
 /* Solver-level: init (Solver::init with force BCs) and num_steps runSteps. */
 int orc_init(orc_system* s);

@@ -18,7 +18,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 
 FIELDS = {"x": 0, "u": 1, "v": 2, "f": 3, "vol": 4, "rho": 5, "m": 6,
-          "theta": 7, "W": 8, "phi": 9, "radius": 10}
+          "theta": 7, "W": 8, "phi": 9, "radius": 10, "stress": 11}
 VECTOR_FIELDS = {"x", "u", "v", "f"}
 
 
@@ -74,7 +74,7 @@ def load():
     lib.orc_add_bc.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64,
                                ctypes.c_void_p, dp]
     for name in ("orc_compute_weighted_volume", "orc_compute_dilatation",
-                 "orc_compute_force", "orc_init"):
+                 "orc_compute_force", "orc_compute_stress", "orc_init"):
         getattr(lib, name).argtypes = [P]
     lib.orc_compute_energy.argtypes = [P, dp, dp]
     lib.orc_run.argtypes = [P, ctypes.c_int32]
@@ -208,9 +208,14 @@ class OracleSystem:
     def run(self, num_steps):
         self._check(self._lib.orc_run(self._h, int(num_steps)))
 
+    def compute_stress(self):
+        self._check(self._lib.orc_compute_stress(self._h))
+
     def get(self, field):
         if field in VECTOR_FIELDS:
             out = np.zeros((self.n, 3))
+        elif field == "stress":
+            out = np.zeros((self.n, 3, 3))
         else:
             out = np.zeros(self.n)
         self._check(self._lib.orc_get(self._h, FIELDS[field], _dptr(out)))

@@ -30,7 +30,8 @@ def run_case(make_system, case, kind, coeff):
     sysm.compute_dilatation()
     sysm.compute_force()
     Phi, _ = sysm.compute_energy()
-    out = {k: sysm.get(k) for k in ("x", "f", "W", "vol", "theta")}
+    sysm.compute_stress()  # tstForce.hpp:948
+    out = {k: sysm.get(k) for k in ("x", "f", "W", "vol", "theta", "stress")}
     out["Phi"] = Phi
     out["constants"] = sysm.model_constants()
     out["max_neighbors"] = sysm.neighbor_stats()[0]
@@ -48,6 +49,7 @@ def check_case(res, case, kind, coeff, max_checked=None):
     else:
         ref = R.LPSRef(c["theta_coeff"], c["s_coeff"], infl)
     x, f, W, vol, theta = res["x"], res["f"], res["W"], res["vol"], res["theta"]
+    sigma = res["stress"]
     lo, hi = -1.0 + horizon * bw, 1.0 - horizon * bw
     interior = np.all((x > lo) & (x < hi), axis=1)
     idx = np.nonzero(interior)[0]
@@ -70,6 +72,16 @@ def check_case(res, case, kind, coeff, max_checked=None):
                     failures.append(("W_analytic", p, W[p], aW))
             elif abs(W[p] - aW) > band * W[p]:
                 failures.append(("W_analytic", p, W[p], aW))
+            # tstForce.hpp:744-750: diagonal equal to the reference sum, the
+            # other components (xy, xz, yz, yx, zx, zy) <= 1e-13.
+            ref_sigma = R.ref_stress(ref, kind, horizon, m, coeff)
+            sp = sigma[p]
+            for d in range(3):
+                if not R.float_eq(sp[d, d], ref_sigma[d]):
+                    failures.append(("stress_diag", p, d, sp[d, d], ref_sigma[d]))
+            offdiag = [sp[0, 1], sp[0, 2], sp[1, 2], sp[1, 0], sp[2, 0], sp[2, 1]]
+            if not all(v <= 1e-13 for v in offdiag):
+                failures.append(("stress_offdiag", p, offdiag))
         else:
             if not R.float_eq(f[p, 0], ref_f):
                 failures.append(("fx", p, f[p, 0], ref_f))

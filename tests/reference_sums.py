@@ -133,6 +133,32 @@ def ref_fx(model, kind, horizon, m, u11, x):
     return total
 
 
+def ref_stress(model, kind, horizon, m, s0):
+    """tstForce.hpp:91-133 (PMB) and :345-392 (LPS) computeReferenceStress:
+    the diagonal (xx, yy, zz) at a point with a full neighbourhood under the
+    linear field; the quadratic case is not computed (:394-399: zeros)."""
+    if kind != "linear":
+        return [0.0, 0.0, 0.0]
+    offs, dx = _offsets(horizon, m)
+    vol = dx * dx * dx
+    sigma = [0.0, 0.0, 0.0]
+    if isinstance(model, PMBRef):
+        f_mag = model.force_coeff(s0, vol)
+    else:
+        wv = ref_weighted_volume(model, horizon, m, vol)
+        th = ref_dilatation_linear(model, horizon, m, s0, vol, wv)
+    for xi_x, xi_y, xi_z, xi in offs:
+        if not isinstance(model, PMBRef):
+            f_mag = model.force_coeff(s0, xi, vol, wv, wv, th, th)
+        f_x = f_mag * xi_x / xi
+        f_y = f_mag * xi_y / xi
+        f_z = f_mag * xi_z / xi
+        sigma[0] += 0.5 * f_x * xi_x
+        sigma[1] += 0.5 * f_y * xi_y
+        sigma[2] += 0.5 * f_z * xi_z
+    return sigma
+
+
 def float_eq(a, b, ulps=4):
     """GTest EXPECT_FLOAT_EQ: equal as floats within 4 ULPs."""
     fa, fb = np.float32(a), np.float32(b)

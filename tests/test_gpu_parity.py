@@ -39,6 +39,13 @@ def _assert_same(g, o, fields=("u", "v", "f")):
         assert np.array_equal(a, b), (fld, np.max(np.abs(a - b)))
 
 
+def _stress_pair(g, o):
+    """Per-particle stress of the current states (computeStress)."""
+    g.compute_stress()
+    o.compute_stress()
+    return g.get("stress"), o.get("stress")
+
+
 def _rel(a, b):
     return abs(a - b) / max(abs(b), 1e-300)
 
@@ -55,7 +62,7 @@ def test_force_cases_match_reference_and_oracle(cuda, oracle, case, kind, coeff)
     res_g, _ = force_checks.run_case(lambda p: cuda.System(p), case, kind, coeff)
     force_checks.check_case(res_g, case, kind, coeff, max_checked=40)
     res_o, _ = force_checks.run_case(lambda p: oracle.OracleSystem(p), case, kind, coeff)
-    for fld in ("f", "W", "theta"):
+    for fld in ("f", "W", "theta", "stress"):
         assert np.array_equal(res_g[fld], res_o[fld]), fld
     assert _rel(res_g["Phi"], res_o["Phi"]) <= 1e-12
     assert res_g["constants"] == res_o["constants"]
@@ -118,6 +125,8 @@ def test_plate_impact_fracture_bit_exact(cuda, oracle, ordering):
         wo, do = o.compute_energy()
         assert np.array_equal(g.get("phi"), o.get("phi"))
         assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+        sg, so = _stress_pair(g, o)
+        assert np.array_equal(sg, so)
     assert (o.neighbors()[2] == 0).sum() > (mu0 == 0).sum()  # bonds broke
 
 
@@ -136,6 +145,8 @@ def test_lps_random_notches_bit_exact(cuda, oracle):
     wo, do = o.compute_energy()
     assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
     assert np.array_equal(g.get("W"), o.get("W"))
+    sg, so = _stress_pair(g, o)
+    assert np.array_equal(sg, so)  # LPS with fracture: intact bonds only
 
 
 @pytest.mark.parametrize("model", [P.PD_LINEAR_PMB, P.PD_LINEAR_LPS, P.PD_LPS])
@@ -146,6 +157,8 @@ def test_elastic_models_bit_exact(cuda, oracle, model):
     g.run(30)
     o.run(30)
     _assert_same(g, o, ("u", "v", "f", "theta", "m"))
+    sg, so = _stress_pair(g, o)
+    assert np.array_equal(sg, so)
 
 
 def test_kalthoff_winkler_regression_on_gpu(cuda, golden):
@@ -247,6 +260,8 @@ def test_errors_are_reported(cuda):
         s.prenotch([[1, 0, 0]], [[0, 1, 0]], [[0, 0, 0]])  # no fracture model
     with pytest.raises(cuda.CpdError):
         s.add_bc(P.BC_FORCE_VALUE, [10 ** 6], [0.0])
+    with pytest.raises(cuda.CpdError):
+        s.get("stress")  # cpd_compute_stress not called
 
 
 # ---------------------------------------------------------------------------
@@ -313,6 +328,8 @@ def test_fast_plate_impact(cuda, oracle, ordering):
         wg, dg = g.compute_energy()
         wo, do = o.compute_energy()
         assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+        # The exact stress kernel on states within 1e-12 of each other.
+        assert _nrel(*_stress_pair(g, o)) <= 1e-10
 
 
 def test_fast_lps_random_notches(cuda, oracle):
@@ -365,6 +382,7 @@ def test_mixed_plate_impact(cuda, oracle, ordering):
         wg, dg = g.compute_energy()
         wo, do = o.compute_energy()
         assert _rel(wg, wo) <= 1e-6 and _rel(dg, do) <= 1e-12
+        assert _nrel(*_stress_pair(g, o)) <= 1e-5
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
@@ -393,6 +411,7 @@ def test_mixed_lps_random_notches(cuda, oracle):
         dg = g.compute_energy()[1]
         do = o.compute_energy()[1]
         assert _rel(dg, do) <= 1e-12
+        assert _nrel(*_stress_pair(g, o)) <= 1e-5
     assert (o.neighbors()[2] == 0).sum() > 0
 
 

@@ -39,7 +39,7 @@ def _gxx():
 
 
 @pytest.mark.parametrize("name", ["kalthoff_winkler", "elastic_wave", "random_cracks",
-                                  "hertz_spheres"])
+                                  "hertz_spheres", "stress_cube"])
 def test_examples_compile_as_host_cpp(name):
     """The front end is plain C++17 outside nvcc (KOKKOS_LAMBDA = [=])."""
     r = subprocess.run([_gxx(), "-std=c++17", "-fsyntax-only", "-Wall", "-I", INCLUDE,
@@ -125,7 +125,7 @@ def test_cpp_inputs_match_python_inputs(inputs_probe, tmp_path, deck):
 # GPU
 
 
-def _run_example(name, deck, workdir, precision="exact"):
+def _run_example(name, deck, workdir, precision="exact", args=()):
     exe = os.path.join(BUILD, name)
     if not os.path.exists(exe):
         raise RuntimeError(f"{exe} is missing: build the examples (make -C examples)")
@@ -133,7 +133,7 @@ def _run_example(name, deck, workdir, precision="exact"):
     with open(path, "w") as fh:
         json.dump(deck, fh)
     env = dict(os.environ, CABANAPD_B200_PRECISION=precision)
-    r = subprocess.run([exe, path], cwd=workdir, env=env, capture_output=True, text=True,
+    r = subprocess.run([exe, path, *args], cwd=workdir, env=env, capture_output=True, text=True,
                        timeout=900)
     assert r.returncode == 0, r.stdout + r.stderr
     return r.stdout
@@ -261,3 +261,50 @@ def test_hertz_program_restitution(lib, golden, tmp_path):
     s = lib.System(prob["params"])
     P.setup(s, prob)
     assert hertz_restitution(s, prob) == pytest.approx(e, rel=1e-14, abs=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["pmb", "lps"])
+def test_stress_cube_program(lib, tmp_path, case):
+    """EnergyStressOutput particles through the CabanaPD API (stress_cube.cpp):
+    the stress the solver computes at init meets the reference's stress
+    checks (unit_test/tstForce.hpp:744-750: diagonal FLOAT_EQ the single-point
+    sum, other components <= 1e-13) at interior particles, and equals bit for
+    bit the stress of the same problem driven through the Python binding."""
+    import force_checks
+    import reference_sums as R
+    model_id, dx, bw, _, infl, _ = force_checks.CASES[case]
+    nc = int(2.0 / dx)
+    s0 = 0.1
+    deck = {"low_corner": {"value": [-1.0, -1.0, -1.0]},
+            "high_corner": {"value": [1.0, 1.0, 1.0]},
+            "num_cells": {"value": [nc, nc, nc]}, "horizon": {"value": dx * 3},
+            "density": {"value": 1.0}, "bulk_modulus": {"value": 1.0},
+            "shear_modulus": {"value": 0.5}, "stretch": {"value": s0},
+            "timestep": {"value": 1e-3}, "final_time": {"value": 4.5e-3},
+            "output_frequency": {"value": 2}}
+    _run_example("stress_cube", deck, str(tmp_path), "exact", args=(case,))
+    init = np.loadtxt(tmp_path / "stress_init.txt")
+    final = np.loadtxt(tmp_path / "stress_final.txt")
+    assert np.all(np.isfinite(final)) and final.shape == init.shape
+    x, sigma = init[:, :3], init[:, 3:].reshape(-1, 3, 3)
+
+    prob = P.unit_cube(model_id, dx, s0, "linear", K=1.0, G=0.5, influence_type=infl)
+    s = lib.System(dict(prob["params"], precision=0))
+    P.setup(s, prob)
+    s.compute_stress()
+    assert np.array_equal(x, s.get("x"))
+    assert np.array_equal(sigma, s.get("stress"))
+
+    c = s.model_constants()
+    ref = R.PMBRef(c["c"]) if case == "pmb" else R.LPSRef(c["theta_coeff"], c["s_coeff"], infl)
+    horizon = dx * 3
+    ref_sigma = R.ref_stress(ref, "linear", horizon, 3, s0)
+    lo, hi = -1.0 + horizon * bw, 1.0 - horizon * bw
+    interior = np.nonzero(np.all((x > lo) & (x < hi), axis=1))[0]
+    assert interior.size > 0
+    for p in interior:
+        for d in range(3):
+            assert R.float_eq(sigma[p, d, d], ref_sigma[d]), (p, d, sigma[p, d, d], ref_sigma[d])
+        off = sigma[p][~np.eye(3, dtype=bool)]
+        assert np.all(off <= 1e-13), (p, off)
