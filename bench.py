@@ -13,9 +13,10 @@ headline `value`; the plain FP64 path runs the same steps from the same
 start and is reported beside it (`plain_fp64`, `mixed_vs_plain`), with the
 per-field error of mixed vs FP64 (`mixed_error_vs_fp64`).
 
-`other_workloads` (N = 1): short full-size runs of the LPS fracture box
-(8.0 M particles; mixed beside plain FP64 with the error between them) and
-the Hertzian DEM packing (4.0 M spheres).
+`other_workloads` (N = 1): short runs of the 1.2 M-particle variant of the
+plate, the LPS fracture box (8.0 M particles), the Hertzian DEM packing
+(4.0 M spheres) and the 41^3 PMB elastic wave, each mixed beside plain FP64
+with the error between them.
 
 `serving` (N = 1): a served stream of independent PMB/LPS jobs through the
 job server (continuous batching, mixed precision): capacity from a
@@ -52,6 +53,8 @@ from cabanapd_b200 import problems as P  # noqa: E402
 
 PLATE_CELLS = (800, 400, 36)
 LPS_CELLS = (1000, 400, 20)   # LPS random-notch box, dx = 1e-4: 8.0 M particles
+PLATE_1P2M_CELLS = (376, 188, 17)  # the ~1.2 M-particle variant of the plate
+WAVE_CELLS = 41               # PMB elastic wave, 41^3 particles
 DEM_DIMS = (200, 200, 100)    # Hertz packing: 4.0 M spheres
 CPU_SLAB_X = 50  # bounded CPU sample: the first 50 x-columns of the plate
 
@@ -337,25 +340,41 @@ def _time_system(s, stream, device, steps, warmup):
     return ev0.elapsed_time(ev1), k_ms / max(k_n, 1)
 
 
-def measure_other(name, device, stream, steps, warmup):
-    """A short full-size measurement of another hot-path workload: the LPS
-    fracture box (8.0 M particles), mixed precision beside plain FP64 from
-    the same start with the error of mixed vs FP64, or the Hertzian DEM
-    packing (4.0 M spheres, contact list rebuilt every 10 steps inside the
-    timed steps; Hertz runs in FP64)."""
-    import cabanapd_b200
+def other_workload(name, steps):
+    """(problem, precisions, kernel names, description) of another hot-path
+    workload measured beside the headline plate."""
+    mixed_pmb = ("k_pmb_force_lean<fracture> + k_pmb_force_mixed<fracture> "
+                 "(split bond stage, fused step)")
     if name == "lps":
-        prob = P.lps_random_notches(num_cells=LPS_CELLS, steps=steps)
-        precs = ["mixed", "fp64"]
-        kernel = {"mixed": "k_lps_mtheta_lean + k_lps_force_lean<fracture> over lean warps, "
-                           "k_lps_mtheta_mixed + k_lps_force_mixed over the rest (fused step)",
-                  "fp64": "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"}
-        wl = {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)}
-    else:
-        prob = P.dem_packing(lattice_dims=DEM_DIMS, steps=steps)
-        precs = ["exact"]
-        kernel = {"exact": "k_hertz_force<per-particle radius>"}
-        wl = {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10}
+        return (P.lps_random_notches(num_cells=LPS_CELLS, steps=steps), ["mixed", "fp64"],
+                {"mixed": "k_lps_mtheta_lean + k_lps_force_lean<fracture> over lean warps, "
+                          "k_lps_mtheta_mixed + k_lps_force_mixed over the rest (fused step)",
+                 "fp64": "k_lps_m_theta_1pass + k_lps_force_pf<fracture> (fused step)"},
+                {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)})
+    if name == "plate_1p2m":
+        return (P.plate_impact(num_cells=PLATE_1P2M_CELLS, steps=steps), ["mixed", "fp64"],
+                {"mixed": mixed_pmb, "fp64": "k_pmb_force_fast<fracture> (fused step)"},
+                {"workload": "pmb_fracture_notched_plate_impact_1p2m",
+                 "plate_cells": list(PLATE_1P2M_CELLS)})
+    if name == "wave":
+        return (P.elastic_wave_pmb(n=WAVE_CELLS, steps=steps), ["mixed", "fp64"],
+                {"mixed": mixed_pmb.replace("fracture", "elastic"),
+                 "fp64": "k_pmb_force_fast<elastic> (fused step)"},
+                {"workload": "pmb_elastic_wave", "cells": [WAVE_CELLS] * 3})
+    return (P.dem_packing(lattice_dims=DEM_DIMS, steps=steps), ["mixed", "fp64"],
+            {"mixed": "k_hertz_force_mixed<per-particle radius> (FP64 overlap, FP32 force law)",
+             "fp64": "k_hertz_force<per-particle radius>"},
+            {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10})
+
+
+def measure_other(name, device, stream, steps, warmup):
+    """A short measurement of another hot-path workload: the LPS fracture
+    box (8.0 M particles), the 1.2 M-particle variant of the notched plate or
+    the 41^3 PMB elastic wave, or the Hertzian DEM packing (4.0 M spheres,
+    contact list rebuilt every 10 steps inside the timed steps), each mixed
+    beside plain FP64 from the same start with the error of mixed vs FP64."""
+    import cabanapd_b200
+    prob, precs, kernel, wl = other_workload(name, steps)
     res, systems = {}, {}
     for prec in precs:
         s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
@@ -364,12 +383,13 @@ def measure_other(name, device, stream, steps, warmup):
         _, bonds0 = s.neighbor_stats()
         ms, k_avg = _time_system(s, stream, device, steps, warmup)
         _, bonds1 = s.neighbor_stats()
-        bonds = bonds0 if name == "lps" else 0.5 * (bonds0 + bonds1)
+        bonds = 0.5 * (bonds0 + bonds1) if name == "dem" else bonds0
         res[prec] = dict(precision=prec, ms_per_step=ms / steps,
                          value=bonds * steps / (ms / 1e3), kernel=kernel[prec],
                          kernel_ms_avg=k_avg)
         if name == "dem":
             res[prec]["contact_rebuilds"] = s.contact_rebuilds()
+            res[prec]["contacts"] = bonds
         systems[prec] = s
     head = precs[0]
     out = dict(wl, particles=systems[head].n, bonds=bonds, steps=steps, warmup=warmup,
@@ -377,16 +397,21 @@ def measure_other(name, device, stream, steps, warmup):
     if "fp64" in res and head != "fp64":
         a, b = systems[head], systems["fp64"]
         err = {}
-        for fld in ("u", "v", "f", "theta"):
+        fields = ("u", "v", "f", "theta") if name == "lps" else ("u", "v", "f")
+        for fld in fields:
             x, y = a.get(fld), b.get(fld)
             err[fld] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
-        err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
+        if prob["params"].get("fracture"):
+            err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
         out["plain_fp64"] = res["fp64"]
         out["mixed_vs_plain"] = res["fp64"]["ms_per_step"] / res[head]["ms_per_step"]
         out["mixed_error_vs_fp64"] = err
     for s in systems.values():
         s.close()
     return out
+
+
+OTHER_STEPS = {"lps": 20, "plate_1p2m": 100, "wave": 100, "dem": 50}
 
 
 def run_gpu(args, world, rank, local, pg):
@@ -465,8 +490,8 @@ def run_gpu(args, world, rank, local, pg):
         line["mixed_vs_plain"] = value / plain["value"]
         line["mixed_error_vs_fp64"] = err
     if world == 1 and not args.skip_others:
-        line["other_workloads"] = [measure_other("lps", device, stream, 20, 3),
-                                   measure_other("dem", device, stream, 50, 3)]
+        line["other_workloads"] = [measure_other(w, device, stream, OTHER_STEPS[w], 3)
+                                   for w in ("plate_1p2m", "lps", "dem", "wave")]
     if world == 1 and not args.skip_serve:
         line["serving"] = run_serving(args, device)
     if world == 1 and not args.skip_cpu:
@@ -658,7 +683,7 @@ def main():
     ap.add_argument("--skip-serve", action="store_true", help="omit the served-stream leg")
     ap.add_argument("--skip-others", action="store_true",
                     help="omit the LPS-box and DEM-packing measurements")
-    ap.add_argument("--only-other", choices=["lps", "dem"], default=None,
+    ap.add_argument("--only-other", choices=["lps", "dem", "plate_1p2m", "wave"], default=None,
                     help="measure only that workload (for profiling) and print it")
     ap.add_argument("--serve-jobs", type=int, default=96,
                     help="served stream: number of jobs (512 for the full stream)")
@@ -673,13 +698,17 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    global PLATE_CELLS, LPS_CELLS, DEM_DIMS
+    global PLATE_CELLS, LPS_CELLS, DEM_DIMS, PLATE_1P2M_CELLS, WAVE_CELLS
     if args.cells:
         cells = tuple(int(c) for c in args.cells.split(","))
         if args.only_other == "lps":
             LPS_CELLS = cells
         elif args.only_other == "dem":
             DEM_DIMS = cells
+        elif args.only_other == "plate_1p2m":
+            PLATE_1P2M_CELLS = cells
+        elif args.only_other == "wave":
+            WAVE_CELLS = cells[0]
         else:
             PLATE_CELLS = cells
     world, rank, local, pg = (int(os.environ.get("WORLD_SIZE", "1")),

@@ -467,7 +467,10 @@ cpd_status contact_force(cpd_system* s, bool reset)
     const ParticleView p = view(s);
     cudaEvent_t e0 = nullptr;
     if (!has_pd(s)) CPD_OK_OR_RETURN(timed_begin(s, e0));
-    CPD_LAUNCHED(launch_hertz_force(p, s->contact.view(), s->md, reset, s->stream));
+    if (s->params.precision == CPD_MIXED)
+        CPD_LAUNCHED(launch_hertz_force_mixed(p, s->contact.view(), s->md, reset, s->stream));
+    else
+        CPD_LAUNCHED(launch_hertz_force(p, s->contact.view(), s->md, reset, s->stream));
     return timed_end(s, e0);
 }
 

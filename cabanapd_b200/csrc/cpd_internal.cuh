@@ -185,6 +185,9 @@ int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Mode
                             bool with_m, cudaStream_t st);
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
                        const Model& md, bool reset, cudaStream_t st);
+// Mixed precision (cpd_kernels_mixed.cu): FP64 overlap, FP32 force law.
+int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                             bool reset, cudaStream_t st);
 int launch_force_bc(const ParticleView& p, const BoundaryCondition& bc,
                     cudaStream_t st);
 int launch_prenotch(const ParticleView& p, const EllView& nl, const double* v1,

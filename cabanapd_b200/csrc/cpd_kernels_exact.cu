@@ -469,27 +469,30 @@ __global__ void __launch_bounds__(kBlock, 3)
         double xi, r, s, rx, ry, rz, xx, xy, xz;
         bond_geometry(p.x, p.u, np, j, xi0, xi1, xi2, ui0, ui1, ui2, xi, r, s, rx,
                       ry, rz, xx, xy, xz);
+        const double R_j = PER_PARTICLE ? p.radius[j] : 0.0;
+        const double sum_r = PER_PARTICLE ? R_i + R_j : 2.0 * md.radius;
+        const double delta_n = r - sum_r;
+        // Without overlap the pair adds a zero: skip it (the sum is unchanged;
+        // at most a zero sum keeps the sign the reference's + 0.0 would
+        // clear).
+        if (!(delta_n < 0.0)) continue;
         const double nx = rx / r, ny = ry / r, nz = rz / r;
         const double vx = p.v[j] - vi0;
         const double vy = p.v[np + j] - vi1;
         const double vz = p.v[2 * np + j] - vi2;
         const double vn = vx * nx + vy * ny + vz * nz;
-        double sum_r, Rs, coeff_h_n, ms;
+        double Rs, coeff_h_n, ms;
         if (PER_PARTICLE) {
-            const double R_j = p.radius[j];
-            sum_r = R_i + R_j;
             Rs = R_i * (R_j / (R_i + R_j));
             coeff_h_n = 4.0 / 3.0 * md.Es * sqrt(Rs);
             const double mi = rho_i * vol_i;
             const double mj = p.rho[j] * p.vol[j];
             ms = mi * (mj / (mi + mj));
         } else {
-            sum_r = 2.0 * md.radius;
             Rs = md.Rs;
             coeff_h_n = md.coeff_h_n;
             ms = (rho_i * vol_i) / 2.0;
         }
-        const double delta_n = r - sum_r;
         double coeff = 0.0;
         if (delta_n < 0.0) {
             const double h = -coeff_h_n * pow(fabs(delta_n), 3.0 / 2.0);

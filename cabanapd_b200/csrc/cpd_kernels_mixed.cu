@@ -1323,6 +1323,21 @@ __global__ void __launch_bounds__(kBlock, 4)
     step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
 }
 
+// The split forms (lean kernel, then the rest) pay only on large systems:
+// below about a million rows the second launch's serial tail costs more than
+// the lean kernel saves (B200: 69 K-row PMB wave 0.045 ms single vs 0.070 ms
+// split, 125 K-row LPS box 0.123 vs 0.191 ms; 1.2 M-row plate 0.397 vs
+// 0.376 ms).
+// CPD_SPLIT_MIN_ROWS overrides the threshold (0: split forms at every size).
+int64_t split_min_rows()
+{
+    static const int64_t v = [] {
+        const char* e = getenv("CPD_SPLIT_MIN_ROWS");
+        return e ? (int64_t)atoll(e) : (int64_t)(1 << 20);
+    }();
+    return v;
+}
+
 // LPS mixed split form (CPD_LPS_MIXED_SPLIT=0: one kernel over all warps).
 bool lps_mixed_split()
 {
@@ -1331,6 +1346,77 @@ bool lps_mixed_split()
         return !(e && atoi(e) == 0);
     }();
     return v;
+}
+
+// ---------------------------------------------------------------------------
+// Hertzian contact, mixed precision (force/CabanaPD_Contact.hpp:119-168 with
+// force_models/CabanaPD_Hertzian.hpp:23-88 and per-pair radii). The overlap
+// needs FP64: it is ~1e-7 of the centre distance, below FP32 resolution of
+// the positions. So the deformed pair vector r = (x_j - x_i) + (u_j - u_i),
+// |r| and the overlap delta = |r| - (R_i + R_j) stay FP64 (in the reference's
+// operation order); the force law in the overlap (|delta|^(3/2), the contact
+// stiffness, the damping sqrt(S_n m*) v_n and the normal projection) runs in
+// FP32, and the row force is summed in FP64. Pairs without overlap add no
+// force (the reference adds a zero).
+struct HertzMixed {
+    float Es43, Es2, coeff_h_d;  // 4/3 E*, 2 E*, the damping coefficient
+    float Rs, coeff_h_n;         // single-radius model
+    double sum_r;                // single-radius model: 2 R
+};
+
+template <bool PER_PARTICLE>
+__global__ void __launch_bounds__(kBlock, 3)
+    k_hertz_force_mixed(ParticleView p, EllView nl, HertzMixed md, bool reset)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+    const double vi0 = p.v[i], vi1 = p.v[np + i], vi2 = p.v[2 * np + i];
+    const double R_i = PER_PARTICLE ? p.radius[i] : 0.0;
+    const float inv_vol_i = (float)(1.0 / p.vol[i]);
+    const float m_i = (float)(p.rho[i] * p.vol[i]);
+    double fx = reset ? 0.0 : p.f[i];
+    double fy = reset ? 0.0 : p.f[np + i];
+    double fz = reset ? 0.0 : p.f[2 * np + i];
+    const int cnt = nl.count[i];
+    for (int k = 0; k < cnt; ++k) {
+        const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+        const double rx = (__ldg(p.x + j) - xi0) + (__ldg(p.u + j) - ui0);
+        const double ry = (__ldg(p.x + np + j) - xi1) + (__ldg(p.u + np + j) - ui1);
+        const double rz = (__ldg(p.x + 2 * np + j) - xi2) + (__ldg(p.u + 2 * np + j) - ui2);
+        const double r = sqrt(rx * rx + ry * ry + rz * rz);
+        const double R_j = PER_PARTICLE ? __ldg(p.radius + j) : 0.0;
+        const double delta = r - (PER_PARTICLE ? R_i + R_j : md.sum_r);
+        if (!(delta < 0.0)) continue;
+        const float ad = (float)(-delta);
+        const float rinv = (float)(1.0 / r);
+        const float nx = (float)rx * rinv, ny = (float)ry * rinv, nz = (float)rz * rinv;
+        const float vn = (float)(__ldg(p.v + j) - vi0) * nx + (float)(__ldg(p.v + np + j) - vi1) * ny +
+                         (float)(__ldg(p.v + 2 * np + j) - vi2) * nz;
+        float Rs, coeff_h_n, ms;
+        if (PER_PARTICLE) {
+            const float ri = (float)R_i, rj = (float)R_j;
+            Rs = ri * (rj / (ri + rj));
+            coeff_h_n = md.Es43 * sqrtf(Rs);
+            const float m_j = (float)(__ldg(p.rho + j) * __ldg(p.vol + j));
+            ms = m_i * (m_j / (m_i + m_j));
+        } else {
+            Rs = md.Rs;
+            coeff_h_n = md.coeff_h_n;
+            ms = 0.5f * m_i;
+        }
+        const float h = -coeff_h_n * ad * sqrtf(ad);
+        const float Sn = md.Es2 * sqrtf(Rs * ad);
+        const float coeff = (h - md.coeff_h_d * sqrtf(Sn * ms) * vn) * inv_vol_i;
+        fx += (double)(coeff * nx);
+        fy += (double)(coeff * ny);
+        fz += (double)(coeff * nz);
+    }
+    p.f[i] = fx;
+    p.f[np + i] = fy;
+    p.f[2 * np + i] = fz;
 }
 
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
@@ -1586,7 +1672,8 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024;
+    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024 &&
+                       rows >= split_min_rows();
     const int key = (md.fracture ? 4 : 0) + (md.influence == 1 ? 2 : 0) + (with_m ? 1 : 0);
     int n = 0;
     if (split) {
@@ -1635,7 +1722,8 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024;
+    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024 &&
+                       rows >= split_min_rows();
     const int key = (md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0);
     int n = 0;
     if (split) {
@@ -1683,7 +1771,7 @@ int launch_mixed_form_t(const ParticleView& p, const EllView& list, const MixedV
     int var = mixed_variant();
     const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
     if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
-    if (var >= 9 && !m.lean_list) var = 5;
+    if (var >= 9 && (!m.lean_list || rows < split_min_rows())) var = 5;
     if (var >= 9) {
         // Split form: lean warps, then the rest.
         int n = 0;
@@ -1749,6 +1837,25 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Mode
     mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
     return launch_mixed_form(md.fracture != 0, p, list, mv, mm, m, ep, rows, st);
+}
+
+int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                             bool reset, cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    HertzMixed h;
+    h.Es43 = (float)(4.0 / 3.0 * md.Es);
+    h.Es2 = (float)(2.0 * md.Es);
+    h.coeff_h_d = (float)md.coeff_h_d;
+    h.Rs = (float)md.Rs;
+    h.coeff_h_n = (float)md.coeff_h_n;
+    h.sum_r = 2.0 * md.radius;
+    if (md.per_particle_radius)
+        k_hertz_force_mixed<true><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
+    else
+        k_hertz_force_mixed<false><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
+    return 1;
 }
 
 }  // namespace cpd

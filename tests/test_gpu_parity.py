@@ -187,19 +187,27 @@ def test_hertz_regression_on_gpu(cuda, oracle, golden):
     assert s.contact_rebuilds() == o.contact_rebuilds()
 
 
-def test_dem_packing_parity(cuda, oracle):
+# DEM packings: the config 3 layout (non-overlapping, free flight over the
+# test's steps) and a compressed one (spacing 2.1 mm < 2 R_max: overlapping
+# pairs from the start, so the Hertz force law is exercised).
+DEM_CASES = {"free": dict(spacing=2.5e-3, dt=2e-6), "compressed": dict(spacing=2.1e-3, dt=1e-7)}
+
+
+@pytest.mark.parametrize("case", ["free", "compressed"])
+def test_dem_packing_parity(cuda, oracle, case):
     """Config 3 layout at reduced size: polydisperse Hertz, rebuild every 10
     steps; contact sets identical at each rebuild, fields within 1e-12."""
-    prob = P.dem_packing(lattice_dims=(16, 16, 8), steps=100, dt=2e-6)
+    prob = P.dem_packing(lattice_dims=(16, 16, 8), steps=100, **DEM_CASES[case])
     g, o = _pair(cuda, oracle, prob)
     for _ in range(4):
         g.run(25)
         o.run(25)
         assert g.contact_rebuilds() == o.contact_rebuilds()
         assert np.array_equal(g.neighbors()[1], o.neighbors()[1])
-        for fld in ("u", "v"):
+        for fld in ("u", "v", "f"):
             a, b = g.get(fld), o.get(fld)
             assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), fld
+    assert (np.count_nonzero(o.get("f")) > 0) == (case == "compressed")
 
 
 def test_linear_lps_fracture_is_lps(cuda, oracle):
@@ -435,3 +443,39 @@ def test_mixed_lps_irregular_rows_keep_fp64(cuda, oracle):
     o.run(40)
     assert _nrel(g.get("u"), o.get("u")) <= 1e-12
     assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+
+
+def test_mixed_dem_packing(cuda, oracle):
+    """Config 3 on the mixed Hertz kernel (FP64 overlap, FP32 force law):
+    contact sets identical at each rebuild; displacement within 1e-6 and
+    velocity and force within 1e-5 of the FP64 oracle, norm-wise."""
+    prob = P.dem_packing(lattice_dims=(16, 16, 8), steps=100, **DEM_CASES["compressed"])
+    g, o = _pair_mixed(cuda, oracle, prob)
+    for _ in range(4):
+        g.run(25)
+        o.run(25)
+        assert g.contact_rebuilds() == o.contact_rebuilds()
+        assert np.array_equal(g.neighbors()[1], o.neighbors()[1])
+        assert _nrel(g.get("u"), o.get("u")) <= 1e-6
+        assert _nrel(g.get("v"), o.get("v")) <= 1e-5
+        assert _nrel(g.get("f"), o.get("f")) <= 1e-5
+    assert np.count_nonzero(o.get("f")) > 0
+
+
+def test_split_forms_on_small_systems():
+    """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
+    of full-stencil and shared-subset warps, the general kernels over the
+    rest) run on systems of 2^20 rows and more; a child process forces them
+    onto the small mixed test systems (CPD_SPLIT_MIN_ROWS=0) and runs the
+    mixed parity tests there with the same bars."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ, CPD_SPLIT_MIN_ROWS="0")
+    sel = "test_mixed_plate_impact or test_mixed_lps_random_notches or test_mixed_elastic_wave"
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
+                        os.path.join(here, "test_gpu_parity.py"), "-k", sel],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert "4 passed" in r.stdout, r.stdout[-500:]
