@@ -1437,7 +1437,10 @@ __global__ void __launch_bounds__(kBlock, 3)
 // fused steps: 4 4.36; 5 3.28 (3.67 with the exact test inside the bond
 // loop, 4.19 also with consecutive block warps); 6 / 7 / 8 3.91 / 3.90 /
 // 4.64 (before the deferred test); 9 3.07; 10 / 11 / 12 3.84 / 3.50 / 3.77.
-// Also measured and rejected: 5 compiled for 5 or 6 blocks per SM (spilling)
+// Also measured and rejected: a kernel for the kind-1 warps that walks the
+// union of its rows' subsets (3.06 per step: no faster, as the boundary
+// lanes idle on the entries they lack; and with plain FP32 chunk sums less
+// accurate on boundary rows); 5 compiled for 5 or 6 blocks per SM (spilling)
 // 4.36 / 7.96; 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
 // neighbour gathers as cp.async copies into shared memory three bonds ahead
 // 8.28; a shared-memory tile of the lattice with its halo 5.86.
