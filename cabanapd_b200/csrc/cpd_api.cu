@@ -12,6 +12,7 @@
 #include <numeric>
 #include <string>
 #include <utility>
+#include <unordered_map>
 #include <vector>
 
 #include "cpd_internal.cuh"
@@ -523,7 +524,10 @@ cpd_status build_bc_program(cpd_system* s)
         double add[3] = {0.0, 0.0, 0.0};
     };
     std::vector<std::pair<int32_t, Row>> rows;
-    std::vector<int32_t> where(s->n, -1);
+    size_t listed = 0;
+    for (const auto& bc : s->hbcs) listed += bc.idx.size();
+    std::unordered_map<int32_t, int32_t> where;  // row -> its entry in rows
+    where.reserve(listed);
     bool ok = true;
     for (const auto& bc : s->hbcs) {
         for (size_t b = 0; b < bc.idx.size() && ok; ++b) {
@@ -532,11 +536,9 @@ cpd_status build_bc_program(cpd_system* s)
                 ok = false;
                 break;
             }
-            if (where[q] < 0) {
-                where[q] = (int32_t)rows.size();
-                rows.push_back({q, Row{}});
-            }
-            Row& r = rows[where[q]].second;
+            const auto ins = where.emplace(q, (int32_t)rows.size());
+            if (ins.second) rows.push_back({q, Row{}});
+            Row& r = rows[ins.first->second].second;
             for (int d = 0; d < 3; ++d) {
                 const bool touched = bc.kind != CPD_BC_FORCE_ADD || d == bc.component;
                 if (!touched) continue;
@@ -848,6 +850,7 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
         return set_error(CPD_ERR_INVALID_ARGUMENT, "per-particle radius model needs radius");
     CPD_CUDA(cudaSetDevice(s->device));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
+    PhaseTrace tr("upload");
     free_particles(s);
     s->n = n;
     s->frozen = n_frozen;
@@ -869,44 +872,44 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
     CPD_CUDA(dev_alloc(&s->staging, sizeof(double) * 3 * n, s->stream));
     CPD_CUDA(dev_alloc(&s->red_out, sizeof(double) * 8, s->stream));
     CPD_CUDA(cudaMemsetAsync(s->red_out, 0, sizeof(double) * 8, s->stream));
+    tr.mark("alloc", s->stream);
 
-    // Internal order.
-    std::vector<int32_t> order;
+    // Internal order: the caller's (no permutation) or Morton (perm[k] =
+    // caller index of internal particle k, h_inv its inverse).
+    s->h_inv.clear();
     if (s->params.ordering == CPD_ORDER_MORTON) {
         double cell = has_pd(s) ? s->md.horizon : 2.0 * s->md.radius + s->md.radius_extend;
-        order = morton_order(x, n, n_frozen, cell);
+        const std::vector<int32_t> order = morton_order(x, n, n_frozen, cell);
         CPD_CUDA(dev_alloc(&s->perm, sizeof(int32_t) * n, s->stream));
         CPD_CUDA(cudaMemcpyAsync(s->perm, order.data(), sizeof(int32_t) * n,
                                  cudaMemcpyHostToDevice, s->stream));
-    } else {
-        order.resize(n);
-        std::iota(order.begin(), order.end(), 0);
+        s->h_inv.assign(n, 0);
+        for (int64_t k = 0; k < n; k++) s->h_inv[order[k]] = (int32_t)k;
+        CPD_CUDA(cudaStreamSynchronize(s->stream));
     }
-    s->h_inv.assign(n, 0);
-    for (int64_t k = 0; k < n; k++) s->h_inv[order[k]] = (int32_t)k;
+    tr.mark("order", s->stream);
 
+    // Each upload goes through the staging buffer, so one waits for the
+    // previous conversion kernel (stream order).
     CPD_OK_OR_RETURN(upload_vector(s, x, s->x));
     CPD_OK_OR_RETURN(upload_scalar(s, vol, s->vol));
-    std::vector<double> tmp;
-    if (rho) {
+    if (rho)
         CPD_OK_OR_RETURN(upload_scalar(s, rho, s->rho));
-    } else {
-        tmp.assign(n, 1.0);
-        CPD_OK_OR_RETURN(upload_scalar(s, tmp.data(), s->rho));
-        CPD_CUDA(cudaStreamSynchronize(s->stream));
-    }
-    if (radius) {
+    else
+        s->launches += launch_fill_value(s->rho, n, 1.0, s->stream);
+    if (radius)
         CPD_OK_OR_RETURN(upload_scalar(s, radius, s->radius));
-    } else {
-        tmp.assign(n, s->md.radius);
-        CPD_OK_OR_RETURN(upload_scalar(s, tmp.data(), s->radius));
-        CPD_CUDA(cudaStreamSynchronize(s->stream));
+    else
+        s->launches += launch_fill_value(s->radius, n, s->md.radius, s->stream);
+    if (nofail) {
+        CPD_CUDA(cudaMemcpyAsync(s->staging, nofail, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                                 s->stream));
+        s->launches += launch_nofail_to_u8(reinterpret_cast<const int32_t*>(s->staging),
+                                           s->nofail, n, s->perm, s->stream);
     }
-    std::vector<uint8_t> nf(n, 0);
-    if (nofail)
-        for (int64_t k = 0; k < n; k++) nf[k] = nofail[order[k]] != 0;
-    CPD_CUDA(cudaMemcpyAsync(s->nofail, nf.data(), n, cudaMemcpyHostToDevice, s->stream));
+    CPD_CUDA(cudaGetLastError());
     CPD_CUDA(cudaStreamSynchronize(s->stream));
+    tr.mark("fields", s->stream);
     return CPD_OK;
 }
 
@@ -927,6 +930,7 @@ cpd_status cpd_build_neighbors(cpd_system* s)
     CPD_OK_OR_RETURN(check_ready(s, false));
     CPD_CUDA(cudaSetDevice(s->device));
     std::string err;
+    PhaseTrace tr("neighbors");
     if (has_pd(s)) {
         // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
         int l = build_neighbor_list(s->x, nullptr, s->n, s->npad, s->frozen,
@@ -934,6 +938,7 @@ cpd_status cpd_build_neighbors(cpd_system* s)
                                     s->pd, s->stream, err);
         if (l < 0) return set_error(CPD_ERR_CUDA, "neighbour build: " + err);
         s->launches += l;
+        tr.mark("list", s->stream);
         if (wants_mixed(s)) {
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
                               s->stream, err);
@@ -1044,7 +1049,7 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
     for (int64_t b = 0; b < count; b++) {
         if (indices[b] < 0 || indices[b] >= s->n)
             return set_error(CPD_ERR_INVALID_ARGUMENT, "boundary index out of range");
-        idx[b] = s->h_inv[indices[b]];
+        idx[b] = s->h_inv.empty() ? (int32_t)indices[b] : s->h_inv[indices[b]];
     }
     if (count > 0) {
         CPD_CUDA(dev_alloc(&bc.idx, sizeof(int32_t) * count, s->stream));
@@ -1122,6 +1127,22 @@ cpd_status cpd_compute_force(cpd_system* s)
     return CPD_OK;
 }
 
+// The energy kernel of the system's arithmetic path: the stencil form on the
+// mixed path, the fast FP64 form on the FP64 path (PMB, LPS), the exact form
+// otherwise. Writes W and phi through p and [nb][2] block partials.
+static int launch_energy(const cpd_system* s, const ParticleView& p, double* partials, int nb)
+{
+    if (use_mixed(s) && s->mixed.u2) {
+        const int l = launch_energy_mixed(p, pd_view(s), s->md, s->mixed, partials, nb, s->stream);
+        if (l >= 0) return l;
+    }
+    if (s->params.precision != CPD_FP64_EXACT) {
+        const int l = launch_pd_energy_fast(p, pd_view(s), s->md, partials, nb, s->stream);
+        if (l >= 0) return l;
+    }
+    return launch_pd_energy(p, pd_view(s), s->md, partials, nb, s->stream);
+}
+
 cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
@@ -1130,7 +1151,7 @@ cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
     if (has_pd(s)) {
         const int nb = energy_blocks(s->n - s->frozen);
         CPD_OK_OR_RETURN(ensure_reduction(s, nb));
-        CPD_LAUNCHED(launch_pd_energy(view(s), pd_view(s), s->md, s->red, nb, s->stream));
+        CPD_LAUNCHED(launch_energy(s, view(s), s->red, nb));
         CPD_LAUNCHED(launch_sum_partials(s->red, nb, 2, s->red_out + 2, s->stream));
         CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
                                  cudaMemcpyDeviceToHost, s->stream));
@@ -1177,9 +1198,12 @@ cpd_status cpd_init(cpd_system* s)
     } else if (has_contact(s)) {
         CPD_OK_OR_RETURN(contact_force(s, true));
     }
+    PhaseTrace tr("init");
     if (has_pd(s)) CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
+    tr.mark("energy", s->stream);
     CPD_OK_OR_RETURN(apply_force_bcs(s));
     CPD_OK_OR_RETURN(prepare_fused(s));
+    tr.mark("bcs+fused", s->stream);
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     s->initialized = true;
     return CPD_OK;
@@ -1444,7 +1468,7 @@ extern "C" cpd_status cpd_compute_energy_noalloc(cpd_system* s, double* W_out,
     p.phi = phi_out;
     // Every partial slot the sum reads is written by this launch first, so
     // nothing left in the scratch by an earlier call reaches the result.
-    CPD_LAUNCHED(launch_pd_energy(p, pd_view(s), s->md, scratch, nb, s->stream));
+    CPD_LAUNCHED(launch_energy(s, p, scratch, nb));
     CPD_LAUNCHED(launch_sum_partials(scratch, nb, 2, totals_out, s->stream));
     return CPD_OK;
 }

@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 
 #include <string>
@@ -93,6 +95,32 @@ __device__ __forceinline__ int64_t tile_row(const EllView& nl, int64_t first)
 {
     return first + 32 * tile_chunk(nl) + (threadIdx.x & 31);
 }
+
+// Host-side trace of set-up phases (CPD_TRACE=1): each mark waits for the
+// stream and prints the wall time since the previous mark to stderr.
+// Without the variable a mark does nothing.
+inline bool trace_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("CPD_TRACE");
+        return e && std::atoi(e) != 0;
+    }();
+    return on;
+}
+struct PhaseTrace {
+    const char* scope;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    explicit PhaseTrace(const char* s) : scope(s) {}
+    void mark(const char* phase, cudaStream_t st)
+    {
+        if (!trace_enabled()) return;
+        cudaStreamSynchronize(st);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[cpd trace] %s/%s %.3f ms\n", scope, phase,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
 
 // Tiled view of a list for `rows` rows and its grid (blocks of `block`
 // threads). CPD_ROW_TILES=0 keeps consecutive chunks.
@@ -181,6 +209,10 @@ int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
 bool fast_supported(const Model& md);
 int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
                          const StepEpilogue& ep, cudaStream_t st);
+// Energy / damage of the FP64 and mixed paths (PMB, LPS): -1 for other
+// models (the exact kernel serves those).
+int launch_pd_energy_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                          double* partials, int nblocks, cudaStream_t st);
 int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Model& md,
                             bool with_m, cudaStream_t st);
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
@@ -277,6 +309,9 @@ void free_mixed(MixedState& m, cudaStream_t st);
 int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st);
 int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, double* u_out,
                             MixedU* u2_out, cudaStream_t st);
+// Energy / damage on the mixed path (-1 when the mixed data does not apply).
+int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                        const MixedState& m, double* partials, int nblocks, cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 
@@ -293,6 +328,9 @@ void free_neighbor_list(NeighborList& nl, cudaStream_t st);
 // Layout kernels.
 int launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t npad,
                       int comps, const int32_t* perm, cudaStream_t st);
+int launch_fill_value(double* a, int64_t n, double v, cudaStream_t st);
+int launch_nofail_to_u8(const int32_t* src, uint8_t* dst, int64_t n, const int32_t* perm,
+                        cudaStream_t st);
 int launch_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t npad,
                       int comps, const int32_t* perm, cudaStream_t st);
 int launch_ell_to_rows(const NeighborList& nl, int64_t n, int64_t npad,

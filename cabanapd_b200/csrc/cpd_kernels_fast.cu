@@ -465,6 +465,92 @@ int lps_variant()
     return v;
 }
 
+// Strain energy density and damage at output steps (force/CabanaPD_PMB.hpp:
+// 127-155, 289-339; force/CabanaPD_LPS.hpp:183-219, 449-504), for the FP64
+// and mixed paths: the per-bond terms and row-order sums of k_pd_energy with
+// the bond lengths of bond_fast (correctly rounded square roots from rsqrt
+// plus one correction), so W_i agrees with the exact kernel to ~1e-16
+// relative per term; broken bonds skip the geometry (their term is zero) but
+// count in the damage, which is bit-identical. Block partials of
+// (sum W_i vol_i, sum phi_i) in the exact kernel's layout and tree order.
+template <bool LPS, int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock)
+    k_pd_energy_fast(ParticleView p, EllView nl, FastModel md, double* partials)
+{
+    __shared__ double s_phi[kBlock];
+    __shared__ double s_dmg[kBlock];
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double Phi_i = 0.0, dmg_i = 0.0;
+    if (i < p.n) {
+        const int64_t np = p.npad;
+        const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
+        const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+        const int cnt = nl.count[i];
+        const double vol_i = p.vol[i];
+        double m_i = 0.0, th_i = 0.0;
+        if (LPS) {
+            m_i = p.m[i];
+            th_i = p.theta[i];
+        }
+        double num_bonds = (double)cnt;
+        if (FRACTURE && LPS) {
+            num_bonds = 0.0;
+            for (int k = 0; k < cnt; ++k) {
+                const uint32_t word = nl.mu[(int64_t)(k >> 5) * np + i];
+                num_bonds += (double)((word >> (k & 31)) & 1u);
+            }
+        }
+        double Wi = 0.0, phi_sum = 0.0, vol_H = 0.0;
+        uint32_t word = 0;
+        for (int k = 0; k < cnt; ++k) {
+            if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+            const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+            const double vol_j = __ldg(p.vol + j);
+            const bool intact = !FRACTURE || ((word >> (k & 31)) & 1u);
+            double w = 0.0;
+            if (intact) {
+                Bond b;
+                bond_fast(p.x, p.u, np, j, xi0, xi1, xi2, ui0, ui1, ui2, b);
+                if (LPS) {
+                    const double infl = INFL == 1 ? 1.0 / b.xi : 1.0;
+                    w = 1.0 / num_bonds * 0.5 * md.theta_coeff / 3.0 * (th_i * th_i) +
+                        0.5 * (md.s_coeff / m_i) * infl * b.s * b.s * b.xi * b.xi * vol_j;
+                } else {
+                    w = 0.25 * md.c * b.s * b.s * b.xi * vol_j;
+                }
+            }
+            if (FRACTURE) {
+                Wi += w;
+                phi_sum += intact ? vol_j : 0.0;
+                vol_H += vol_j;
+            } else {
+                Wi += w;
+                Phi_i += w * vol_i;
+            }
+        }
+        p.W[i] = Wi;
+        if (FRACTURE) {
+            dmg_i = 1 - phi_sum / vol_H;
+            p.phi[i] = dmg_i;
+            Phi_i = Wi * vol_i;
+        }
+    }
+    s_phi[threadIdx.x] = Phi_i;
+    s_dmg[threadIdx.x] = dmg_i;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s_phi[threadIdx.x] += s_phi[threadIdx.x + w];
+            s_dmg[threadIdx.x] += s_dmg[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x + 0] = s_phi[0];
+        partials[2 * blockIdx.x + 1] = s_dmg[0];
+    }
+}
+
 // Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-5):
 // 0 no prefetch, 1 indices 2 bonds ahead, 2 indices 4 ahead, 3 / 4 the same
 // plus neighbour gathers one bond ahead, 5 = 1 compiled for 4 blocks of 256
@@ -571,6 +657,34 @@ int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Mode
         }
     }
 #undef CPD_MT
+    return 1;
+}
+
+int launch_pd_energy_fast(const ParticleView& p, const EllView& nl, const Model& md,
+                          double* partials, int nblocks, cudaStream_t st)
+{
+    const FastModel fm = to_fast(md);
+    const bool infl = md.influence == 1;
+    if (md.pd == CPD_PD_PMB) {
+        if (md.fracture)
+            k_pd_energy_fast<false, 0, true><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+        else
+            k_pd_energy_fast<false, 0, false><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+    } else if (md.pd == CPD_PD_LPS) {
+        if (md.fracture) {
+            if (infl)
+                k_pd_energy_fast<true, 1, true><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+            else
+                k_pd_energy_fast<true, 0, true><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+        } else {
+            if (infl)
+                k_pd_energy_fast<true, 1, false><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+            else
+                k_pd_energy_fast<true, 0, false><<<nblocks, kBlock, 0, st>>>(p, nl, fm, partials);
+        }
+    } else {
+        return -1;
+    }
     return 1;
 }
 

@@ -1419,6 +1419,156 @@ __global__ void __launch_bounds__(kBlock, 3)
     p.f[2 * np + i] = fz;
 }
 
+// ---------------------------------------------------------------------------
+// Strain energy density and damage on the mixed path (force/CabanaPD_PMB.hpp:
+// 127-155, 289-339; force/CabanaPD_LPS.hpp:183-219, 449-504). One kernel over
+// all rows in blocks of 256 consecutive rows (the exact kernel's blocks and
+// partials). Warps of full-stencil or shared-subset rows walk the stencil
+// table with the FP32 bond arithmetic of the force kernels, summing the bond
+// terms in FP32 chunks of 8 into FP64; other warps walk their rows with FP64
+// geometry. The damage sums FP64 volumes in row order, so phi_i is the
+// exact kernel's. LPS: W_i = theta_coeff theta_i^2 / 6 (over the intact
+// bonds' 1 / num_bonds shares) + (s_coeff / 2 m_i) sum omega xi^2 s^2 vol_j.
+struct MixedEnergy {
+    double c, theta_coeff, s_coeff;
+    int ntab;
+};
+
+template <bool LPS, int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_energy_mixed(ParticleView p, EllView nl, MixedView mv, MixedEnergy md, double* partials)
+{
+    extern __shared__ MixedStencil smem[];
+    __shared__ double s_phi[kBlock];
+    __shared__ double s_dmg[kBlock];
+    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) smem[t] = mv.table[t];
+    __syncthreads();
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
+    const MixedStencil* wt = smem;
+    int wcnt = md.ntab;
+    if (kind == 3) {
+        const int lane = threadIdx.x & 31;
+        const int nmask = (md.ntab + 31) / 32;
+        MixedStencil* mine = smem + md.ntab * (1 + (threadIdx.x >> 5));
+        const uint32_t* wm = mv.warp_pmask + warp * nmask;
+        int before = 0;
+        for (int w = 0; w < nmask; ++w) {
+            const uint32_t pm = wm[w];
+            if ((pm >> lane) & 1u)
+                mine[before + __popc(pm & ((1u << lane) - 1u))] = smem[32 * w + lane];
+            before += __popc(pm);
+        }
+        __syncwarp();
+        wt = mine;
+        wcnt = before;
+    }
+    double Phi_i = 0.0, dmg_i = 0.0;
+    if (i < p.n) {
+        const int64_t np = p.npad;
+        const int cnt = nl.count[i];
+        const double vol_i = p.vol[i];
+        double bonds_part = 0.0, phi_sum = 0.0, vol_H = 0.0;
+        int intact_n = 0;
+        if (kind >= 2) {
+            const MixedU ui = mv.u2[i];
+            const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z,
+                              -ui.lo.z, false};
+            const MixedU* __restrict__ u2_i = mv.u2 + i;
+            // One bond: its energy term (zero when broken) into the FP32
+            // chunk, and (fracture) its FP64 volume into the damage sums.
+            auto bond = [&](const MixedStencil& t, bool on, float& chunk) {
+                if (FRACTURE) {
+                    const double vol_j = __ldg(p.vol + i + t.delta);
+                    phi_sum += on ? vol_j : 0.0;
+                    vol_H += vol_j;
+                }
+                intact_n += on ? 1 : 0;
+                const MixedU uj = u2_i[t.delta];
+                MixedBond2 bd;
+                lean_geometry(t, uj, ri, bd);
+                // PMB: the w lane holds c vol_j; LPS: vol_j.
+                const float term = LPS ? (INFL == 1 ? t.xi : t.xi2) * uj.hi.w * bd.s * bd.s
+                                       : 0.25f * uj.hi.w * bd.s * bd.s * t.xi;
+                chunk += on ? term : 0.f;
+            };
+            for (int base = 0; base < wcnt; base += 32) {
+                const uint32_t word =
+                    FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
+                const int lim = min(32, wcnt - base);
+                int b = 0;
+                for (; b + 8 <= lim; b += 8) {
+                    const uint32_t w8 = word >> b;
+                    float chunk = 0.f;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) bond(wt[base + b + u], (w8 >> u) & 1u, chunk);
+                    bonds_part += (double)chunk;
+                }
+                if (b < lim) {
+                    float chunk = 0.f;
+                    for (; b < lim; ++b) bond(wt[base + b], (word >> b) & 1u, chunk);
+                    bonds_part += (double)chunk;
+                }
+            }
+        } else {
+            const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
+            const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+            uint32_t word = 0xffffffffu;
+            for (int k = 0; k < cnt; ++k) {
+                if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
+                const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+                const double vol_j = __ldg(p.vol + j);
+                const bool on = (word >> (k & 31)) & 1u;
+                if (FRACTURE) {
+                    phi_sum += on ? vol_j : 0.0;
+                    vol_H += vol_j;
+                }
+                if (!on) continue;
+                ++intact_n;
+                const double xx = __ldg(p.x + j) - xi0, xy = __ldg(p.x + np + j) - xi1,
+                             xz = __ldg(p.x + 2 * np + j) - xi2;
+                const double rx = xx + (__ldg(p.u + j) - ui0);
+                const double ry = xy + (__ldg(p.u + np + j) - ui1);
+                const double rz = xz + (__ldg(p.u + 2 * np + j) - ui2);
+                const double r = sqrt(rx * rx + ry * ry + rz * rz);
+                const double xi = sqrt(xx * xx + xy * xy + xz * xz);
+                const double sv = (r - xi) / xi;
+                bonds_part += LPS ? (INFL == 1 ? xi : xi * xi) * vol_j * sv * sv
+                                  : 0.25 * md.c * vol_j * sv * sv * xi;
+            }
+        }
+        double Wi;
+        if (LPS) {
+            const double th_i = p.theta[i];
+            Wi = (intact_n > 0 ? 0.5 * md.theta_coeff / 3.0 * (th_i * th_i) : 0.0) +
+                 0.5 * (md.s_coeff / p.m[i]) * bonds_part;
+        } else {
+            Wi = bonds_part;
+        }
+        p.W[i] = Wi;
+        if (FRACTURE) {
+            dmg_i = 1 - phi_sum / vol_H;
+            p.phi[i] = dmg_i;
+        }
+        Phi_i = Wi * vol_i;
+    }
+    s_phi[threadIdx.x] = Phi_i;
+    s_dmg[threadIdx.x] = dmg_i;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s_phi[threadIdx.x] += s_phi[threadIdx.x + w];
+            s_dmg[threadIdx.x] += s_dmg[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x + 0] = s_phi[0];
+        partials[2 * blockIdx.x + 1] = s_dmg[0];
+    }
+}
+
 // Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
 // (64 registers), 1 -> 4 blocks with the full-stencil loop software
 // pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
@@ -1478,6 +1628,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                   MixedState& m, cudaStream_t st, std::string& err)
 {
     int launches = 0;
+    PhaseTrace tr("mixed");
     free_mixed(m, st);
     const int64_t np = p.npad;
     CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
@@ -1493,6 +1644,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
     CPD_TRY(cudaMemsetAsync(m.code, kMixedGeneric, (size_t)std::max(pd.max_n, 1) * np, st));
     k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, m.xh, m.xl);
     launches++;
+    tr.mark("alloc+split", st);
     m.ntab = 0;
     const int64_t rows = p.n - p.frozen;
     if (rows > 0 && pd.max_n > 0) {
@@ -1556,9 +1708,12 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                     L.half[d] = half[d];
                 }
                 L.lut = d_lut;
+                tr.mark("spacing+table", st);
                 k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
+                tr.mark("code", st);
                 k_verify_delta<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code);
                 launches += 2;
+                tr.mark("verify", st);
                 std::vector<unsigned int> delta(kMixedGeneric);
                 CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
                                         cudaMemcpyDeviceToHost, st));
@@ -1581,6 +1736,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                                                                  m.pmask, m.warp_kind,
                                                                  m.warp_pmask);
                 launches++;
+                tr.mark("masks", st);
                 const int64_t nw = (rows + 31) / 32;
                 std::vector<uint8_t> kinds(nw);
                 CPD_TRY(cudaMemcpyAsync(kinds.data(), m.warp_kind, nw, cudaMemcpyDeviceToHost,
@@ -1629,6 +1785,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
         }
     }
     CPD_TRY(cudaGetLastError());
+    tr.mark("lists", st);
     return launches;
 }
 
@@ -1858,6 +2015,29 @@ int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Mod
         k_hertz_force_mixed<true><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
     else
         k_hertz_force_mixed<false><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
+    return 1;
+}
+
+int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& md,
+                        const MixedState& m, double* partials, int nblocks, cudaStream_t st)
+{
+    const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    if (m.ntab == 0 || sb > 48 * 1024 || !m.warp_kind) return -1;
+    if (!(md.pd == CPD_PD_PMB || (md.pd == CPD_PD_LPS && m.lps_ok))) return -1;
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
+    const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
+    const int key = (md.pd == CPD_PD_LPS ? 4 : 0) + (md.influence == 1 ? 2 : 0) +
+                    (md.fracture ? 1 : 0);
+    switch (key) {
+    case 0: k_energy_mixed<false, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 1: k_energy_mixed<false, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 2: k_energy_mixed<false, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 3: k_energy_mixed<false, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 4: k_energy_mixed<true, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 5: k_energy_mixed<true, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    case 6: k_energy_mixed<true, 1, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    default: k_energy_mixed<true, 1, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    }
     return 1;
 }
 

@@ -242,6 +242,20 @@ __global__ void k_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t 
     for (int d = 0; d < comps; d++) soa[d * npad + k] = aos[src * comps + d];
 }
 
+__global__ void k_fill_value(double* a, int64_t n, double v)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) a[k] = v;
+}
+
+// Caller-order int32 no-fail flags -> internal-order bytes.
+__global__ void k_nofail_to_u8(const int32_t* src, uint8_t* dst, int64_t n, const int32_t* perm)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    dst[k] = src[perm ? perm[k] : k] != 0;
+}
+
 __global__ void k_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t npad,
                              int comps, const int32_t* perm)
 {
@@ -326,6 +340,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
                         std::string& err)
 {
     int launches = 0;
+    PhaseTrace tr("list");
     const double* pos = x;
     double* y = nullptr;
     if (disp) {
@@ -391,6 +406,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     k_cell_fill<<<blocks_for(n), kBlock, 0, st>>>(cellid, n, cell_start, cell_count, order);
     launches++;
 
+    tr.mark("cells", st);
     // Row counts.
     if (!out.count) CPD_TRY(dev_alloc(&out.count, sizeof(int32_t) * npad, st));
     const double rsqr = cutoff * cutoff;
@@ -419,6 +435,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
         max_n = std::max(max_n, bmax[b]);
         total += bsum[b];
     }
+    tr.mark("count", st);
     // (Re)allocate the padded list when it grows.
     const int32_t cap = std::max(max_n, 1);
     if (!out.idx || cap > out.cap) {
@@ -438,6 +455,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     out.max_n = max_n;
     out.total = total;
     out.nwords = (max_n + 31) / 32;
+    tr.mark("alloc", st);
     if (n > begin) {
         k_fill<<<blocks_for(n - begin), kBlock, 0, st>>>(pos, n, npad, begin, g, cell_start,
                                                         order, rsqr, out.count, user_id,
@@ -448,6 +466,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
         k_init_mu<<<blocks_for(npad), kBlock, 0, st>>>(out.count, npad, out.nwords, out.mu);
         launches++;
     }
+    tr.mark("fill", st);
     // Lists on reference positions (PD bonds): the lattice line pitch at a
     // middle row.
     out.pitch = 0;
@@ -478,6 +497,21 @@ int launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t npad, i
 {
     if (n <= 0) return 0;
     k_aos_to_soa<<<blocks_for(n), kBlock, 0, st>>>(aos, soa, n, npad, comps, perm);
+    return 1;
+}
+
+int launch_fill_value(double* a, int64_t n, double v, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_fill_value<<<blocks_for(n), kBlock, 0, st>>>(a, n, v);
+    return 1;
+}
+
+int launch_nofail_to_u8(const int32_t* src, uint8_t* dst, int64_t n, const int32_t* perm,
+                        cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    k_nofail_to_u8<<<blocks_for(n), kBlock, 0, st>>>(src, dst, n, perm);
     return 1;
 }
 
