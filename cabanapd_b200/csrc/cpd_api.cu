@@ -1129,18 +1129,28 @@ cpd_status cpd_compute_force(cpd_system* s)
 
 // The energy kernel of the system's arithmetic path: the stencil form on the
 // mixed path, the fast FP64 form on the FP64 path (PMB, LPS), the exact form
-// otherwise. Writes W and phi through p and [nb][2] block partials.
-static int launch_energy(const cpd_system* s, const ParticleView& p, double* partials, int nb)
+// otherwise. Writes W and phi through p and block partials [rows][2] into a
+// buffer of capacity rows (at least energy_blocks(rows), nb); returns the
+// partial rows written (nb, or up to nb + 1 for the mixed split form).
+static int launch_energy(cpd_system* s, const ParticleView& p, double* partials, int nb,
+                         int capacity)
 {
     if (use_mixed(s) && s->mixed.u2) {
-        const int l = launch_energy_mixed(p, pd_view(s), s->md, s->mixed, partials, nb, s->stream);
-        if (l >= 0) return l;
+        int l = 0;
+        const int rows = launch_energy_mixed(p, pd_view(s), s->md, s->mixed, partials, nb,
+                                             capacity, &l, s->stream);
+        s->launches += l;
+        if (rows >= 0) return rows;
     }
     if (s->params.precision != CPD_FP64_EXACT) {
         const int l = launch_pd_energy_fast(p, pd_view(s), s->md, partials, nb, s->stream);
-        if (l >= 0) return l;
+        if (l >= 0) {
+            s->launches += l;
+            return nb;
+        }
     }
-    return launch_pd_energy(p, pd_view(s), s->md, partials, nb, s->stream);
+    s->launches += launch_pd_energy(p, pd_view(s), s->md, partials, nb, s->stream);
+    return nb;
 }
 
 cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
@@ -1150,9 +1160,10 @@ cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
     double Wt = 0.0, Dt = 0.0;
     if (has_pd(s)) {
         const int nb = energy_blocks(s->n - s->frozen);
-        CPD_OK_OR_RETURN(ensure_reduction(s, nb));
-        CPD_LAUNCHED(launch_energy(s, view(s), s->red, nb));
-        CPD_LAUNCHED(launch_sum_partials(s->red, nb, 2, s->red_out + 2, s->stream));
+        CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
+        const int rows = launch_energy(s, view(s), s->red, nb, nb + 1);
+        CPD_CUDA(cudaGetLastError());
+        CPD_LAUNCHED(launch_sum_partials(s->red, rows, 2, s->red_out + 2, s->stream));
         CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
                                  cudaMemcpyDeviceToHost, s->stream));
         CPD_CUDA(cudaStreamSynchronize(s->stream));
@@ -1468,7 +1479,8 @@ extern "C" cpd_status cpd_compute_energy_noalloc(cpd_system* s, double* W_out,
     p.phi = phi_out;
     // Every partial slot the sum reads is written by this launch first, so
     // nothing left in the scratch by an earlier call reaches the result.
-    CPD_LAUNCHED(launch_energy(s, p, scratch, nb));
-    CPD_LAUNCHED(launch_sum_partials(scratch, nb, 2, totals_out, s->stream));
+    const int prows = launch_energy(s, p, scratch, nb, kNoAllocMaxBlocks);
+    CPD_CUDA(cudaGetLastError());
+    CPD_LAUNCHED(launch_sum_partials(scratch, prows, 2, totals_out, s->stream));
     return CPD_OK;
 }

@@ -309,9 +309,12 @@ void free_mixed(MixedState& m, cudaStream_t st);
 int launch_split_u(const ParticleView& p, const Model& md, MixedState& m, cudaStream_t st);
 int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, double* u_out,
                             MixedU* u2_out, cudaStream_t st);
-// Energy / damage on the mixed path (-1 when the mixed data does not apply).
+// Energy / damage on the mixed path into [.][2] block partials: returns the
+// number of partial rows written (nblocks, or more when the split form fits
+// in capacity rows), -1 when the mixed data does not apply.
 int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                        const MixedState& m, double* partials, int nblocks, cudaStream_t st);
+                        const MixedState& m, double* partials, int nblocks, int capacity,
+                        int* launches, cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 

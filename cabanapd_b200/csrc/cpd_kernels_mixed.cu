@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(kBlock)
 
 struct LatticeLut {
     double h[3];
+    double hinv[3];  // 1 / h
     int32_t half[3];  // offsets -half..half per axis
     const int16_t* lut;  // [(2 half_x + 1)(2 half_y + 1)(2 half_z + 1)] -> code or -1
 };
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(kBlock)
             bool ok = true;
             for (int d = 0; d < 3; ++d) {
                 const double dd = p.x[d * np + j] - p.x[d * np + i];
-                const double a = rint(dd / L.h[d]);
+                const double a = rint(dd * L.hinv[d]);
                 if (fabs(dd - a * L.h[d]) > 1e-6 * L.h[d] || fabs(a) > L.half[d]) ok = false;
                 o[d] = (int)a;
             }
@@ -163,29 +164,15 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// Per row: first the delta check of every coded bond (a bond whose code's
+// index delta is not its own j - i becomes generic), then the presence bits
+// of the stencil entries the row holds (its codes are a strictly increasing
+// subset of the table); per warp: 2 if every row is the whole table, 3 if
+// every row is the same table subset (the subset is recorded for the warp),
+// 1 if every row is a table subset, else 0.
 __global__ void __launch_bounds__(kBlock)
-    k_verify_delta(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code)
-{
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    const int64_t np = p.npad;
-    const int cnt = nl.count[i];
-    for (int k = 0; k < cnt; ++k) {
-        const int64_t o = (int64_t)k * np + i;
-        const int c = code[o];
-        if (c == kMixedGeneric) continue;
-        const int64_t j = nl.idx[o];
-        if ((long long)delta[c] - (1LL << 31) != (long long)(j - i)) code[o] = (uint8_t)kMixedGeneric;
-    }
-}
-
-// Per row: presence bits of the stencil entries it holds (its codes are a
-// strictly increasing subset of the table); per warp: 2 if every row is the
-// whole table, 3 if every row is the same table subset (the subset is
-// recorded for the warp), 1 if every row is a table subset, else 0.
-__global__ void __launch_bounds__(kBlock)
-    k_row_masks(ParticleView p, EllView nl, const uint8_t* code, int ntab, uint32_t* pmask,
-                uint8_t* kind, uint32_t* warp_pmask)
+    k_row_masks(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code, int ntab,
+                uint32_t* pmask, uint8_t* kind, uint32_t* warp_pmask)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int nmask = (ntab + 31) / 32;
@@ -199,10 +186,17 @@ __global__ void __launch_bounds__(kBlock)
         full = cnt == ntab;
         int prev = -1;
         for (int k = 0; k < cnt; ++k) {
-            const int c = code[(int64_t)k * np + i];
+            const int64_t o = (int64_t)k * np + i;
+            int c = code[o];
+            if (c != kMixedGeneric &&
+                (long long)delta[c] - (1LL << 31) != (long long)(nl.idx[o] - i)) {
+                c = kMixedGeneric;
+                code[o] = (uint8_t)c;
+            }
+            if (!subset) continue;
             if (c >= ntab || c <= prev) {
                 subset = false;
-                break;
+                continue;
             }
             if (c != k) full = false;
             m[c >> 5] |= 1u << (c & 31);
@@ -1436,16 +1430,26 @@ struct MixedEnergy {
 
 template <bool LPS, int INFL, bool FRACTURE>
 __global__ void __launch_bounds__(kBlock, 4)
-    k_energy_mixed(ParticleView p, EllView nl, MixedView mv, MixedEnergy md, double* partials)
+    k_energy_mixed(ParticleView p, EllView nl, MixedView mv, MixedEnergy md, double* partials,
+                   const int32_t* __restrict__ wlist, int64_t wcount)
 {
     extern __shared__ MixedStencil smem[];
     __shared__ double s_phi[kBlock];
     __shared__ double s_dmg[kBlock];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) smem[t] = mv.table[t];
     __syncthreads();
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
+    // Rows: the listed warps' chunks when a warp list is given (a slot past
+    // its end holds no row), else consecutive rows.
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    bool listed = true;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        listed = slot < wcount;
+        warp = listed ? wlist[slot] : 0;
+    }
+    const int64_t i = listed ? p.frozen + 32 * warp + (threadIdx.x & 31) : p.n;
+    const int kind =
+        (listed && warp < ((p.n - p.frozen + 31) >> 5)) ? mv.warp_kind[warp] : 0;
     const MixedStencil* wt = smem;
     int wcnt = md.ntab;
     if (kind == 3) {
@@ -1705,15 +1709,14 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 LatticeLut L;
                 for (int d = 0; d < 3; ++d) {
                     L.h[d] = h[d];
+                    L.hinv[d] = 1.0 / h[d];
                     L.half[d] = half[d];
                 }
                 L.lut = d_lut;
                 tr.mark("spacing+table", st);
                 k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
                 tr.mark("code", st);
-                k_verify_delta<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code);
-                launches += 2;
-                tr.mark("verify", st);
+                launches++;
                 std::vector<unsigned int> delta(kMixedGeneric);
                 CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
                                         cudaMemcpyDeviceToHost, st));
@@ -1724,7 +1727,6 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                                         cudaMemcpyHostToDevice, st));
                 CPD_TRY(cudaStreamSynchronize(st));
                 CPD_TRY(dev_free(d_lut, st));
-                CPD_TRY(dev_free(d_delta, st));
                 m.ntab = (int)tab.size();
                 for (int d = 0; d < 3; ++d) m.h[d] = h[d];
                 const int nmask = (m.ntab + 31) / 32;
@@ -1732,10 +1734,11 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 m.bytes += sizeof(uint32_t) * nmask * np;
                 CPD_TRY(dev_alloc(&m.warp_pmask, sizeof(uint32_t) * nmask * nwarps, st));
                 m.bytes += sizeof(uint32_t) * nmask * nwarps;
-                k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), m.code, m.ntab,
-                                                                 m.pmask, m.warp_kind,
+                k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code,
+                                                                 m.ntab, m.pmask, m.warp_kind,
                                                                  m.warp_pmask);
                 launches++;
+                CPD_TRY(dev_free(d_delta, st));
                 tr.mark("masks", st);
                 const int64_t nw = (rows + 31) / 32;
                 std::vector<uint8_t> kinds(nw);
@@ -2019,8 +2022,10 @@ int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Mod
 }
 
 int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                        const MixedState& m, double* partials, int nblocks, cudaStream_t st)
+                        const MixedState& m, double* partials, int nblocks, int capacity,
+                        int* launches, cudaStream_t st)
 {
+    *launches = 0;
     const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
     if (m.ntab == 0 || sb > 48 * 1024 || !m.warp_kind) return -1;
     if (!(md.pd == CPD_PD_PMB || (md.pd == CPD_PD_LPS && m.lps_ok))) return -1;
@@ -2028,17 +2033,30 @@ int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& m
     const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
     const int key = (md.pd == CPD_PD_LPS ? 4 : 0) + (md.influence == 1 ? 2 : 0) +
                     (md.fracture ? 1 : 0);
-    switch (key) {
-    case 0: k_energy_mixed<false, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 1: k_energy_mixed<false, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 2: k_energy_mixed<false, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 3: k_energy_mixed<false, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 4: k_energy_mixed<true, 0, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 5: k_energy_mixed<true, 0, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    case 6: k_energy_mixed<true, 1, false><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
-    default: k_energy_mixed<true, 1, true><<<nblocks, kBlock, sb, st>>>(p, nl, mv, e, partials); break;
+    // Large systems: the lean warps in their tile order, then the others,
+    // when the partials buffer holds both launches' blocks.
+    const int64_t wpb = kBlock / 32;
+    const int gl = (int)((m.nlean + wpb - 1) / wpb), gr = (int)((m.nrest + wpb - 1) / wpb);
+    const bool split = m.lean_list && p.n - p.frozen >= split_min_rows() && gl + gr <= capacity;
+    auto launch = [&](int grid, double* part, const int32_t* list, int64_t count) {
+        switch (key) {
+        case 0: case 2: k_energy_mixed<false, 0, false><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        case 1: case 3: k_energy_mixed<false, 0, true><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        case 4: k_energy_mixed<true, 0, false><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        case 5: k_energy_mixed<true, 0, true><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        case 6: k_energy_mixed<true, 1, false><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        default: k_energy_mixed<true, 1, true><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, count); break;
+        }
+    };
+    if (!split) {
+        launch(nblocks, partials, nullptr, 0);
+        *launches = 1;
+        return nblocks;
     }
-    return 1;
+    launch(gl, partials, m.lean_list, m.nlean);
+    if (gr > 0) launch(gr, partials + 2 * gl, m.rest_list, m.nrest);
+    *launches = gr > 0 ? 2 : 1;
+    return gl + gr;
 }
 
 }  // namespace cpd
