@@ -33,6 +33,7 @@ struct Grid {
     double lo[3];
     double cell;
     int32_t nc[3];
+    int32_t R;  // visit radius in cells: every pair within the cutoff is at most R cells apart
 };
 
 __global__ void k_positions(const double* x, const double* disp, double* y, int64_t n,
@@ -98,8 +99,12 @@ __global__ void k_cell_fill(const int32_t* cell, int64_t n, const int32_t* cell_
     order[cell_start[c] + slot] = (int32_t)i;
 }
 
-// Walks the 27 cells around particle i and calls emit(j) for every j != i
-// within the cutoff.
+// Calls emit(j) for every j != i within the cutoff: walks the (2R + 1)^2
+// lines of cells around particle i in increasing (z, y); the cells of one
+// line are consecutive cell ids, so their particles are one contiguous run
+// of the cell-sorted order. With cells about cutoff / 3 wide, a lattice
+// holds about one particle per cell and an x-fastest lattice row is emitted
+// in nearly ascending index order (the row sort then moves little).
 template <typename Emit>
 __device__ __forceinline__ void visit_neighbors(const double* __restrict__ pos, int64_t npad,
                                                 const Grid& g, const int32_t* __restrict__ cell_start,
@@ -109,25 +114,23 @@ __device__ __forceinline__ void visit_neighbors(const double* __restrict__ pos, 
     const double px = pos[i], py = pos[npad + i], pz = pos[2 * npad + i];
     int32_t c[3];
     cell_coords(g, px, py, pz, c);
-    for (int dz = -1; dz <= 1; dz++) {
+    const int32_t cx0 = max(c[0] - g.R, 0), cx1 = min(c[0] + g.R, g.nc[0] - 1);
+    for (int dz = -g.R; dz <= g.R; dz++) {
         const int32_t cz = c[2] + dz;
         if (cz < 0 || cz >= g.nc[2]) continue;
-        for (int dy = -1; dy <= 1; dy++) {
+        for (int dy = -g.R; dy <= g.R; dy++) {
             const int32_t cy = c[1] + dy;
             if (cy < 0 || cy >= g.nc[1]) continue;
-            for (int dx = -1; dx <= 1; dx++) {
-                const int32_t cx = c[0] + dx;
-                if (cx < 0 || cx >= g.nc[0]) continue;
-                const int32_t id = cx + g.nc[0] * (cy + g.nc[1] * cz);
-                for (int32_t q = cell_start[id]; q < cell_start[id + 1]; q++) {
-                    const int64_t j = order[q];
-                    if (j == i) continue;
-                    const double ddx = pos[j] - px;
-                    const double ddy = pos[npad + j] - py;
-                    const double ddz = pos[2 * npad + j] - pz;
-                    const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                    if (d2 <= rsqr) emit(j);
-                }
+            const int64_t line = (int64_t)g.nc[0] * (cy + (int64_t)g.nc[1] * cz);
+            const int32_t q1 = cell_start[line + cx1 + 1];
+            for (int32_t q = cell_start[line + cx0]; q < q1; q++) {
+                const int64_t j = order[q];
+                if (j == i) continue;
+                const double ddx = pos[j] - px;
+                const double ddy = pos[npad + j] - py;
+                const double ddz = pos[2 * npad + j] - pz;
+                const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                if (d2 <= rsqr) emit(j);
             }
         }
     }
@@ -370,10 +373,12 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
             lo[d] = std::min(lo[d], part[6 * b + d]);
             hi[d] = std::max(hi[d], part[6 * b + 3 + d]);
         }
-    // Cells at least one cutoff wide (27-cell stencil complete), grown when a
-    // tiny cutoff would give far more cells than particles.
+    // Cells a little over a third of the cutoff wide (visit radius 3), grown
+    // by doubling while the grid would hold far more cells than particles
+    // (visit radius 2, then 1). The 1e-9 margin keeps cutoff / cell below the
+    // radius, so pairs within the cutoff are at most R cells apart.
     Grid g;
-    double cell = cutoff;
+    double cell = cutoff / 3.0 * (1.0 + 1e-9);
     for (;;) {
         for (int d = 0; d < 3; d++) {
             double span = (hi[d] - lo[d]) / cell;
@@ -384,6 +389,7 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     }
     for (int d = 0; d < 3; d++) g.lo[d] = lo[d];
     g.cell = cell;
+    g.R = std::max(1, (int32_t)std::ceil(cutoff / cell - 1e-9));
     const int64_t ncell = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
 
     int32_t *cellid = nullptr, *cell_count = nullptr, *cell_start = nullptr, *order = nullptr;
