@@ -649,6 +649,18 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps)
     double* unxt = start_alt ? s->u : s->u_alt;
     MixedU* u2cur = mixed ? (start_alt ? s->u2_alt : s->mixed.u2) : nullptr;
     MixedU* u2nxt = mixed ? (start_alt ? s->mixed.u2 : s->u2_alt) : nullptr;
+    // Frozen rows are never integrated, so the kernels write only rows from
+    // frozen on: the second buffer takes the frozen rows' displacement (and
+    // its FP32 split) from the system's arrays, where every call starts.
+    if (s->frozen > 0) {
+        const size_t bytes = sizeof(double) * (size_t)s->frozen;
+        for (int d = 0; d < 3; ++d)
+            CPD_CUDA(cudaMemcpyAsync(s->u_alt + (size_t)d * s->npad, s->u + (size_t)d * s->npad,
+                                     bytes, cudaMemcpyDeviceToDevice, s->stream));
+        if (mixed)
+            CPD_CUDA(cudaMemcpyAsync(s->u2_alt, s->mixed.u2, sizeof(MixedU) * (size_t)s->frozen,
+                                     cudaMemcpyDeviceToDevice, s->stream));
+    }
     const ParticleView p = view(s);
     if (mixed)
         CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, ucur, u2cur, s->stream));

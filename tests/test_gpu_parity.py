@@ -462,6 +462,37 @@ def test_mixed_dem_packing(cuda, oracle):
     assert np.count_nonzero(o.get("f")) > 0
 
 
+@pytest.mark.parametrize("precision", [FAST, MIXED])
+def test_plate_with_frozen_particles(cuda, oracle, precision):
+    """Frozen particles (the first z-layer and ten more, so the integrated
+    rows start off a warp boundary) on the FP64 and mixed kernels: the bars of
+    the FP64 / mixed plate tests, and the frozen particles never move. The
+    impact strip's force condition keeps its integrated particles only.
+    Checked over 100 steps: at step 118 a bond to a frozen particle whose FP64
+    stretch is 4.1e-7 below s0 breaks on the mixed path (its state is ~2e-8
+    off the FP64 one), after which the crack tips differ."""
+    prob = P.plate_impact(num_cells=(96, 48, 6), steps=100, v0=60.0)
+    nf = 96 * 48 + 10
+    prob = dict(prob, n_frozen=nf)
+    prob["bcs"] = [(k, c, idx[idx >= nf], v) for k, c, idx, v in prob["bcs"]]
+    g = cuda.System(dict(prob["params"], precision=precision))
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(g, prob)
+    P.setup(o, prob)
+    tol_u, tol_v = (1e-12, 1e-12) if precision == FAST else (1e-6, 1e-5)
+    for _ in range(2):
+        g.run(50)
+        o.run(50)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        assert _nrel(g.get("u"), o.get("u")) <= tol_u
+        assert _nrel(g.get("v"), o.get("v")) <= tol_v
+        wg, dg = g.compute_energy()
+        wo, do = o.compute_energy()
+        assert _rel(dg, do) <= 1e-12 and _rel(wg, wo) <= (1e-12 if precision == FAST else 1e-6)
+    assert not np.any(g.get("u")[:nf])
+    assert (o.neighbors()[2] == 0).sum() > 0
+
+
 def test_split_forms_on_small_systems():
     """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
     of full-stencil and shared-subset warps, the general kernels over the
@@ -473,9 +504,10 @@ def test_split_forms_on_small_systems():
     import sys
     here = os.path.dirname(os.path.abspath(__file__))
     env = dict(os.environ, CPD_SPLIT_MIN_ROWS="0")
-    sel = "test_mixed_plate_impact or test_mixed_lps_random_notches or test_mixed_elastic_wave"
+    sel = ("test_mixed_plate_impact or test_mixed_lps_random_notches or test_mixed_elastic_wave"
+           " or test_plate_with_frozen_particles")
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
                         os.path.join(here, "test_gpu_parity.py"), "-k", sel],
                        env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
-    assert "4 passed" in r.stdout, r.stdout[-500:]
+    assert "6 passed" in r.stdout, r.stdout[-500:]
