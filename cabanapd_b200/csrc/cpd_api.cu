@@ -468,7 +468,9 @@ cpd_status contact_force(cpd_system* s, bool reset)
     const ParticleView p = view(s);
     cudaEvent_t e0 = nullptr;
     if (!has_pd(s)) CPD_OK_OR_RETURN(timed_begin(s, e0));
-    if (s->params.precision == CPD_MIXED)
+    if (s->md.contact == CPD_CONTACT_NORMAL_REPULSION)
+        CPD_LAUNCHED(launch_repulsion_force(p, s->contact.view(), s->md, reset, s->stream));
+    else if (s->params.precision == CPD_MIXED)
         CPD_LAUNCHED(launch_hertz_force_mixed(p, s->contact.view(), s->md, reset, s->stream));
     else
         CPD_LAUNCHED(launch_hertz_force(p, s->contact.view(), s->md, reset, s->stream));
@@ -716,7 +718,8 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
     const cpd_params& P = *params;
     if (P.pd_model < CPD_PD_NONE || P.pd_model > CPD_PD_LINEAR_LPS)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown pd_model");
-    if (P.contact_model != CPD_CONTACT_NONE && P.contact_model != CPD_CONTACT_HERTZ)
+    if (P.contact_model != CPD_CONTACT_NONE && P.contact_model != CPD_CONTACT_HERTZ &&
+        P.contact_model != CPD_CONTACT_NORMAL_REPULSION)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "unknown contact_model");
     if (P.pd_model == CPD_PD_NONE && P.contact_model == CPD_CONTACT_NONE)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "need a PD model or a contact model");
@@ -725,8 +728,10 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         return set_error(CPD_ERR_UNSUPPORTED, "LinearPMB has no fracture variant");
     if (P.pd_model != CPD_PD_NONE && !(P.horizon > 0))
         return set_error(CPD_ERR_INVALID_ARGUMENT, "horizon must be > 0");
-    if (P.contact_model == CPD_CONTACT_HERTZ && !(P.contact_radius > 0))
+    if (P.contact_model != CPD_CONTACT_NONE && !(P.contact_radius > 0))
         return set_error(CPD_ERR_INVALID_ARGUMENT, "contact_radius must be > 0");
+    if (P.contact_model == CPD_CONTACT_NORMAL_REPULSION && !(P.contact_horizon > 0))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "contact_horizon must be > 0");
     if (P.precision != CPD_FP64_EXACT && P.precision != CPD_FP64 && P.precision != CPD_MIXED)
         return set_error(CPD_ERR_UNSUPPORTED, "unknown precision mode");
     if (P.ordering != CPD_ORDER_INPUT && P.ordering != CPD_ORDER_MORTON)
@@ -789,6 +794,14 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
         md.coeff_h_n = 4.0 / 3.0 * md.Es * std::sqrt(md.Rs);
         md.coeff_h_d = -2.0 * std::sqrt(5.0 / 6.0) * md.beta;
         md.per_particle_radius = P.per_particle_radius ? 1 : 0;
+    }
+    if (md.contact == CPD_CONTACT_NORMAL_REPULSION) {
+        // force_models/CabanaPD_Contact.hpp:70-79 (c as the PMB model's)
+        md.radius = P.contact_radius;
+        md.radius_extend = P.radius_extend;
+        md.contact_horizon = P.contact_horizon;
+        const double h = md.contact_horizon;
+        md.c_contact = 18.0 * P.contact_K / (kPi * h * h * h * h);
     }
     e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {

@@ -63,6 +63,8 @@ struct Model {
     double s0 = 0, bond_break_coeff = 0;
     double radius = 0, radius_extend = 0, nu = 0, E = 0, e = 0;
     double Rs = 0, Es = 0, beta = 0, coeff_h_n = 0, coeff_h_d = 0;
+    // Normal repulsion: its own delta and stiffness constant c.
+    double contact_horizon = 0, c_contact = 0;
 };
 
 // Device view of one neighbour list.
@@ -220,6 +222,9 @@ int launch_hertz_force(const ParticleView& p, const EllView& nl,
 // Mixed precision (cpd_kernels_mixed.cu): FP64 overlap, FP32 force law.
 int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                              bool reset, cudaStream_t st);
+// Normal repulsion over the contact list (exact FP64).
+int launch_repulsion_force(const ParticleView& p, const EllView& nl, const Model& md,
+                           bool reset, cudaStream_t st);
 int launch_force_bc(const ParticleView& p, const BoundaryCondition& bc,
                     cudaStream_t st);
 int launch_prenotch(const ParticleView& p, const EllView& nl, const double* v1,

@@ -515,6 +515,49 @@ __global__ void __launch_bounds__(kBlock, 3)
 }
 
 // ---------------------------------------------------------------------------
+// Normal repulsion: force/CabanaPD_Contact.hpp:52-92 with
+// NormalRepulsionModel::forceCoeff (force_models/CabanaPD_Contact.hpp:82-88).
+// A pair whose current distance r is below the contact radius adds
+// ((15 c) sc) vol_j r_d / r per component, sc = (r - radius) / delta_c; the
+// coefficient is negative, so the pair pushes i away from j. Pairs farther
+// apart add a zero and are skipped (only the sign of a zero sum can differ).
+// The reference distance and stretch of getDistance are not used here.
+__global__ void __launch_bounds__(kBlock)
+    k_repulsion_force(ParticleView p, EllView nl, double radius, double c15,
+                      double delta, bool reset)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
+    const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+    double fx = reset ? 0.0 : p.f[i];
+    double fy = reset ? 0.0 : p.f[np + i];
+    double fz = reset ? 0.0 : p.f[2 * np + i];
+    const int cnt = nl.count[i];
+    for (int k = 0; k < cnt; ++k) {
+        const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+        const double xx = __ldg(p.x + j) - xi0;
+        const double eu = __ldg(p.u + j) - ui0;
+        const double xy = __ldg(p.x + np + j) - xi1;
+        const double ev = __ldg(p.u + np + j) - ui1;
+        const double xz = __ldg(p.x + 2 * np + j) - xi2;
+        const double ew = __ldg(p.u + 2 * np + j) - ui2;
+        const double rx = xx + eu, ry = xy + ev, rz = xz + ew;
+        const double r = sqrt(rx * rx + ry * ry + rz * rz);
+        if (!(r < radius)) continue;
+        const double sc = (r - radius) / delta;
+        const double coeff = c15 * sc * p.vol[j];
+        fx += coeff * rx / r;
+        fy += coeff * ry / r;
+        fz += coeff * rz / r;
+    }
+    p.f[i] = fx;
+    p.f[np + i] = fy;
+    p.f[2 * np + i] = fz;
+}
+
+// ---------------------------------------------------------------------------
 // Velocity Verlet: CabanaPD_Integrate.hpp:89-116 (NoContact), :151-193
 // (Contact: also the largest displacement since the last list build).
 template <bool TRACK>
@@ -840,6 +883,16 @@ int launch_hertz_force(const ParticleView& p, const EllView& nl,
         k_hertz_force<true><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, d, reset);
     else
         k_hertz_force<false><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, d, reset);
+    return 1;
+}
+
+int launch_repulsion_force(const ParticleView& p, const EllView& nl, const Model& md,
+                           bool reset, cudaStream_t st)
+{
+    const int64_t rows = p.n - p.frozen;
+    if (rows <= 0) return 0;
+    k_repulsion_force<<<blocks_for(rows), kBlock, 0, st>>>(
+        p, nl, md.radius, 15.0 * md.c_contact, md.contact_horizon, reset);
     return 1;
 }
 

@@ -21,7 +21,7 @@ from .inputs import PI, critical_timestep
 
 # Model / BC numbering shared with the C ABI (include/cabanapd_b200.h).
 PD_NONE, PD_PMB, PD_LPS, PD_LINEAR_PMB, PD_LINEAR_LPS = 0, 1, 2, 3, 4
-CONTACT_NONE, CONTACT_HERTZ = 0, 1
+CONTACT_NONE, CONTACT_HERTZ, CONTACT_NORMAL_REPULSION = 0, 1, 2
 BC_FORCE_VALUE, BC_FORCE_UPDATE, BC_FORCE_ADD = 0, 1, 2
 
 
@@ -353,6 +353,74 @@ def kalthoff_winkler_regression():
     return _problem("kalthoff_winkler", params, x, vol,
                     rho=np.full(x.shape[0], rho0), v0=v, notches=(v1, v2, p0),
                     bcs=bcs, num_steps=steps, output_frequency=50, dx=h)
+
+
+def random_in_cells(low, high, num_cells, rng):
+    """One particle per cell at a uniform random point of the cell (x index
+    fastest), the placement Cabana::InitRandom makes; the reference's own
+    random stream is not reproduced. Returns (x [n,3], vol [n], dx [3])."""
+    low = [float(v) for v in low]
+    high = [float(v) for v in high]
+    nc = [int(v) for v in num_cells]
+    h = [(high[d] - low[d]) / nc[d] for d in range(3)]
+    lo_nodes = [low[d] + np.arange(nc[d], dtype=np.float64) * h[d] for d in range(3)]
+    hi_nodes = [low[d] + (np.arange(nc[d], dtype=np.float64) + 1.0) * h[d] for d in range(3)]
+    zz, yy, xx = np.meshgrid(lo_nodes[2], lo_nodes[1], lo_nodes[0], indexing="ij")
+    lo = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    zz, yy, xx = np.meshgrid(hi_nodes[2], hi_nodes[1], hi_nodes[0], indexing="ij")
+    hi = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1)
+    t = rng.random(lo.shape)
+    x = lo + t * (hi - lo)
+    return np.ascontiguousarray(x), np.full(x.shape[0], h[0] * h[1] * h[2]), h
+
+
+def fragmenting_cylinder(num_cells=(200, 200, 300), size=(0.2, 0.2, 0.3), height=0.1,
+                         outer=0.025, inner=0.02, steps=None, seed=20261204, contact=True,
+                         x=None):
+    """examples/mechanics/fragmenting_cylinder.cpp with its input deck
+    (examples/mechanics/inputs/fragmenting_cylinder.json): a hollow steel
+    cylinder, PMB with fracture (K = 130 GPa, rho = 7800, critical stretch
+    0.02, horizon 0.00417462 + 1e-10 m, G0 = 9 K delta sc^2 / 5), thrown
+    outward by v_r = 200 - 50 z'^2 and v_z = 100 z' m/s, z' = (z - z_min) /
+    (H / 2) - 1. With ``contact`` the fragments repel through normal
+    repulsion (the PD delta and K, radius 0.9 dx / 2, search extension
+    0.01 dx). Particles sit at a seeded random point of their cell and are
+    kept inside the shell (``x`` overrides the placement with given
+    positions, before the shell filter). dt = 1.7e-7 s; the deck's final
+    time 2.4e-4 s gives 1411 steps."""
+    low = [-0.5 * s for s in size]
+    high = [0.5 * s for s in size]
+    if x is None:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        x, vol, h = random_in_cells(low, high, num_cells, rng)
+    else:
+        h = [(high[d] - low[d]) / num_cells[d] for d in range(3)]
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        vol = np.full(x.shape[0], h[0] * h[1] * h[2])
+    center = [0.5 * (low[d] + high[d]) for d in range(3)]
+    rsq = (x[:, 0] - center[0]) ** 2 + (x[:, 1] - center[1]) ** 2
+    keep = ~((rsq < inner * inner) | (rsq > outer * outer) |
+             (x[:, 2] > center[2] + 0.5 * height) | (x[:, 2] < center[2] - 0.5 * height))
+    x = np.ascontiguousarray(x[keep])
+    vol = vol[keep]
+    rho0, K, sc = 7800.0, 130e9, 0.02
+    horizon = 0.00417462 + 1e-10
+    G0 = 9 * K * horizon * (sc * sc) / 5
+    z_min = center[2] - 0.5 * height
+    zf = ((x[:, 2] - z_min) / (0.5 * height)) - 1
+    vr = 200.0 - 50.0 * zf * zf
+    ang = np.arctan2(x[:, 1], x[:, 0])
+    v = np.stack([vr * np.cos(ang), vr * np.sin(ang), 100.0 * zf], axis=1)
+    dt = 1.7e-7
+    if steps is None:
+        steps = int(2.4e-4 / dt)
+    params = dict(pd_model=PD_PMB, fracture=1, horizon=horizon, K=K, G0=G0, dt=dt)
+    if contact:
+        params.update(contact_model=CONTACT_NORMAL_REPULSION, contact_horizon=horizon,
+                      contact_K=K, contact_radius=0.9 * h[0] / 2.0,
+                      radius_extend=0.01 * h[0], rebuild_every=0)
+    return _problem("fragmenting_cylinder", params, x, vol, rho=np.full(x.shape[0], rho0),
+                    v0=np.ascontiguousarray(v), num_steps=steps, output_frequency=50, dx=h)
 
 
 def unit_cube(model, dx, s0, kind, K=1.0, G=0.5, G0=None, influence_type=None):

@@ -52,6 +52,8 @@ class CpdParams(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("ordering", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("contact_horizon", ctypes.c_double),
+        ("contact_K", ctypes.c_double),
     ]
 
 

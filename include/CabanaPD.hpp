@@ -175,6 +175,31 @@ struct HertzianModel {
     }
 };
 
+// Normal repulsion contact (src/force_models/CabanaPD_Contact.hpp:54-89):
+// (delta, contact radius, search-radius extension, K). Pairs closer than the
+// contact radius repel with 15 c (r - radius) / delta vol_j, c as PMB's.
+struct NormalRepulsionModel {
+    using model_tag = NormalRepulsionModel;
+    using model_type = NormalRepulsionModel;
+    using fracture_type = NoFracture;
+    static constexpr bool is_contact = true;
+    double delta = 0.0, radius = 0.0, radius_extend = 0.0, K = 0.0, c = 0.0;
+    NormalRepulsionModel() = default;
+    NormalRepulsionModel(double delta_, double radius_, double extend, double K_)
+        : delta(delta_), radius(radius_), radius_extend(extend), K(K_),
+          c(18.0 * K_ / (pi * delta_ * delta_ * delta_ * delta_)) {}
+    double cutoff() const { return 2.0 * radius + radius_extend; }
+    double extend() const { return radius_extend; }
+    void fill(cpd_params& p) const
+    {
+        p.contact_model = CPD_CONTACT_NORMAL_REPULSION;
+        p.contact_radius = radius;
+        p.radius_extend = radius_extend;
+        p.contact_horizon = delta;
+        p.contact_K = K;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Slices: operator()(i[, d]) reads the device array in device code and the
 // host mirror in host code. Vector fields are component-major on both sides.

@@ -15,7 +15,8 @@
  *   cpd_system_create        ForceModel(...) constructors
  *                            (force_models/CabanaPD_PMB.hpp:165-231,
  *                             force_models/CabanaPD_LPS.hpp:151-253,
- *                             force_models/CabanaPD_Hertzian.hpp:40-56),
+ *                             force_models/CabanaPD_Hertzian.hpp:40-56,
+ *                             force_models/CabanaPD_Contact.hpp:70-79),
  *                            VelocityVerlet(dt) (CabanaPD_Integrate.hpp:80-86)
  *   cpd_upload_particles     Particles::create + Particles::update
  *                            (CabanaPD_Particles.hpp:242-307, 429-443)
@@ -55,7 +56,7 @@
 extern "C" {
 #endif
 
-#define CPD_ABI_VERSION 1
+#define CPD_ABI_VERSION 2
 
 typedef struct cpd_system cpd_system;
 typedef int32_t cpd_status;
@@ -83,8 +84,14 @@ enum {
     CPD_PD_LINEAR_LPS = 4
 };
 
-/* Contact models (force_models/CabanaPD_Hertzian.hpp). */
-enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1 };
+/* Contact models. HERTZ: force_models/CabanaPD_Hertzian.hpp.
+ * NORMAL_REPULSION: force_models/CabanaPD_Contact.hpp:54-89 with
+ * force/CabanaPD_Contact.hpp:42-104, the short-range repulsion that keeps
+ * fragments of a PD body apart: a pair whose current distance r is below
+ * contact_radius adds 15 c (r - contact_radius) / contact_horizon vol_j along
+ * the pair, with c = 18 contact_K / (pi contact_horizon^4). Both search their
+ * pairs on current positions within 2 contact_radius + radius_extend. */
+enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1, CPD_CONTACT_NORMAL_REPULSION = 2 };
 
 /* Kernel arithmetic. EXACT evaluates every per-bond expression with IEEE
  * double operations in the reference's operand order (no FMA contraction),
@@ -94,12 +101,15 @@ enum { CPD_CONTACT_NONE = 0, CPD_CONTACT_HERTZ = 1 };
  * four divisions, FMA allowed; forces agree with EXACT to ~1e-13 relative
  * (norm-wise) and the broken-bond decision is re-evaluated exactly inside a
  * 1e-12 guard band, so broken-bond sets are identical. PMB and LPS use it;
- * the linearized models and Hertz contact always run EXACT.
- * MIXED (PMB without contact): FP32 bond arithmetic with FP32 bond reference
- * vectors precomputed in FP64, Kahan-compensated per-particle force sums,
- * FP64 integration and reductions, and an FP64 re-test of every bond whose
- * stretch is within 1e-4 s0 of s0, so broken-bond sets match FP64; other
- * models run the FP64 kernels under MIXED. */
+ * the linearized models, Hertz contact (outside MIXED) and normal repulsion
+ * always run EXACT.
+ * MIXED (PMB and LPS without contact): FP32 bond arithmetic with bond
+ * reference vectors precomputed in FP64 (lattice stencil tables where rows
+ * share one), FP32 sums of 8-bond chunks added into FP64 row totals, FP64
+ * integration and reductions, and an exact FP64 re-test of every bond whose
+ * stretch is within 1e-4 s0 of s0, so broken-bond sets match FP64. Hertz
+ * contact evaluates its force law in FP32 on FP64 overlaps. The PD kernels
+ * of a system with contact, and the other models, run FP64 under MIXED. */
 enum { CPD_FP64_EXACT = 0, CPD_FP64 = 1, CPD_MIXED = 2 };
 
 /* Internal particle order: INPUT keeps the caller's order; MORTON sorts by
@@ -144,7 +154,8 @@ typedef struct cpd_params {
     double horizon;              /* PD force horizon delta */
     double K, G, G0;             /* bulk modulus, shear modulus, fracture energy */
     double contact_radius;       /* Hertz particle radius (largest radius when
-                                    per_particle_radius = 1) */
+                                    per_particle_radius = 1); normal
+                                    repulsion: the contact radius */
     double radius_extend;        /* contact search-radius extension (skin) */
     double nu, E, restitution;   /* Hertz material */
     double dt;                   /* time step */
@@ -156,6 +167,10 @@ typedef struct cpd_params {
     int32_t precision;           /* CPD_FP64_EXACT, CPD_FP64 or CPD_MIXED */
     int32_t ordering;            /* CPD_ORDER_* */
     int32_t device;              /* CUDA device ordinal */
+    double contact_horizon;      /* normal repulsion: the delta of its
+                                    stiffness (NormalRepulsionModel delta) */
+    double contact_K;            /* normal repulsion: the bulk modulus of its
+                                    stiffness (NormalRepulsionModel K) */
 } cpd_params;
 
 int32_t cpd_abi_version(void);

@@ -76,6 +76,7 @@ inline void finalize() {}
 inline void fence() {}
 
 using std::abs;
+using std::atan2;
 using std::cos;
 using std::exp;
 using std::log;

@@ -49,6 +49,8 @@ struct Model {
     double radius = 0, radius_extend = 0, nu = 0, E = 0, e = 0;
     double Rs = 0, Es = 0, beta = 0, coeff_h_n = 0, coeff_h_d = 0;
     int per_particle_radius = 0;
+    // force_models/CabanaPD_Contact.hpp:70-79 (normal repulsion)
+    double contact_horizon = 0, c_contact = 0;
 };
 
 // Full neighbour list: rows for i in [begin, n), padded to max_n columns,
@@ -589,6 +591,48 @@ void hertz_force(orc_system& s, bool reset)
     }
 }
 
+// Normal repulsion: force/CabanaPD_Contact.hpp:52-92 computeForceFull with
+// NormalRepulsionModel::forceCoeff (force_models/CabanaPD_Contact.hpp:82-88).
+void repulsion_force(orc_system& s, bool reset)
+{
+    const Model& md = s.model;
+    const NList& nl = s.contact_list;
+    const double* x = s.x.data();
+    const double* u = s.u.data();
+    if (reset) std::fill(s.f.begin(), s.f.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = s.frozen; i < s.n; i++) {
+        double fx = s.f[3 * i + 0], fy = s.f[3 * i + 1], fz = s.f[3 * i + 2];
+        for (int32_t nn = 0; nn < nl.count[i]; nn++) {
+            int64_t j = nl.idx[(size_t)i * nl.max_n + nn];
+            double fcx = 0.0, fcy = 0.0, fcz = 0.0;
+            double xi, r, st, rx, ry, rz, xx, xy, xz;
+            get_distance(x, u, i, j, xi, r, st, rx, ry, rz, xx, xy, xz);
+            if (r < md.radius) {
+                const double sc = (r - md.radius) / md.contact_horizon;
+                const double coeff = 15.0 * md.c_contact * sc * s.vol[j];
+                fcx = coeff * rx / r;
+                fcy = coeff * ry / r;
+                fcz = coeff * rz / r;
+            }
+            fx += fcx;
+            fy += fcy;
+            fz += fcz;
+        }
+        s.f[3 * i + 0] = fx;
+        s.f[3 * i + 1] = fy;
+        s.f[3 * i + 2] = fz;
+    }
+}
+
+void contact_force(orc_system& s, bool reset)
+{
+    if (s.model.contact == ORC_CONTACT_NORMAL_REPULSION)
+        repulsion_force(s, reset);
+    else
+        hertz_force(s, reset);
+}
+
 void build_contact_list(orc_system& s, double cutoff)
 {
     // CabanaPD_Particles.hpp:534-553 current positions y = x + u.
@@ -686,7 +730,7 @@ void update_force(orc_system& s)
     }
     if (s.model.contact != ORC_CONTACT_NONE) {
         contact_update(s);
-        hertz_force(s, !has_pd(s));
+        contact_force(s, !has_pd(s));
     }
 }
 
@@ -833,6 +877,15 @@ orc_system* orc_create(const orc_params* p)
         md.coeff_h_n = 4.0 / 3.0 * md.Es * std::sqrt(md.Rs);
         md.coeff_h_d = -2.0 * std::sqrt(5.0 / 6.0) * md.beta;
         md.per_particle_radius = p->per_particle_radius;
+    }
+    if (md.contact == ORC_CONTACT_NORMAL_REPULSION) {
+        // force_models/CabanaPD_Contact.hpp:70-79: c as the PMB model's, from
+        // the contact model's own delta and K.
+        md.radius = p->contact_radius;
+        md.radius_extend = p->radius_extend;
+        md.contact_horizon = p->contact_horizon;
+        const double h = md.contact_horizon;
+        md.c_contact = 18.0 * p->contact_K / (kPi * h * h * h * h);
     }
     s->dt = p->dt;
     s->rebuild_every = p->rebuild_every;
@@ -992,7 +1045,7 @@ int orc_compute_dilatation(orc_system* s)
 int orc_compute_force(orc_system* s)
 {
     if (has_pd(*s)) pd_force(*s);
-    if (s->model.contact != ORC_CONTACT_NONE) hertz_force(*s, !has_pd(*s));
+    if (s->model.contact != ORC_CONTACT_NONE) contact_force(*s, !has_pd(*s));
     return 0;
 }
 int orc_compute_energy(orc_system* s, double* total_W, double* total_D)
@@ -1026,7 +1079,7 @@ int orc_init(orc_system* s)
     // Solver::init calls updateForce only: with a PD model the contact force
     // first appears in runStep (Solver.hpp:361-363); a DEM-only solver's
     // force model is the contact model (reset = true, list just built).
-    if (!has_pd(*s) && s->model.contact != ORC_CONTACT_NONE) hertz_force(*s, true);
+    if (!has_pd(*s) && s->model.contact != ORC_CONTACT_NONE) contact_force(*s, true);
     double W, D;
     if (has_pd(*s)) pd_energy(*s, W, D);
     apply_force_bcs(*s);

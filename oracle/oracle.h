@@ -8,7 +8,8 @@
  *
  * It restates, in plain C++17 + OpenMP, the reference's algorithms for:
  * particle kernels of PMB / LPS / LinearPMB / LinearLPS peridynamics (with
- * and without critical-stretch fracture), Hertzian contact, velocity Verlet,
+ * and without critical-stretch fracture), Hertzian contact, normal
+ * repulsion contact, velocity Verlet,
  * pre-notch bond cutting, force boundary conditions and the Solver's
  * init/runStep orchestration. Each function in oracle.cpp cites the
  * reference file:line it follows (paths relative to the CabanaPD tree).
@@ -41,7 +42,7 @@ enum {
     ORC_PD_LINEAR_PMB = 3,
     ORC_PD_LINEAR_LPS = 4
 };
-enum { ORC_CONTACT_NONE = 0, ORC_CONTACT_HERTZ = 1 };
+enum { ORC_CONTACT_NONE = 0, ORC_CONTACT_HERTZ = 1, ORC_CONTACT_NORMAL_REPULSION = 2 };
 enum {
     ORC_BC_FORCE_VALUE = 0,   /* f(p, d) = value, d = 0..2 */
     ORC_BC_FORCE_UPDATE = 1,  /* f(p, d) += value, d = 0..2 */
@@ -75,6 +76,8 @@ typedef struct orc_params {
     double dt;
     int32_t rebuild_every;   /* contact list: 0 = displacement trigger */
     int32_t per_particle_radius; /* 1: use radius array (polydisperse) */
+    double contact_horizon;  /* normal repulsion: delta of its stiffness */
+    double contact_K;        /* normal repulsion: bulk modulus of its stiffness */
 } orc_params;
 
 orc_system* orc_create(const orc_params* p);

@@ -40,6 +40,8 @@ class OrcParams(ctypes.Structure):
         ("dt", ctypes.c_double),
         ("rebuild_every", ctypes.c_int32),
         ("per_particle_radius", ctypes.c_int32),
+        ("contact_horizon", ctypes.c_double),
+        ("contact_K", ctypes.c_double),
     ]
 
 

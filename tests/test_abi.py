@@ -31,9 +31,10 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_params_layout():
     from cabanapd_b200 import system
     lib = system.load()
-    assert lib.cpd_abi_version() == 1
-    # cpd_params: 4 int32, 10 double, 5 int32 -> 16 + 80 + 20 (+4 padding)
-    assert ctypes.sizeof(system.CpdParams) == 120
+    assert lib.cpd_abi_version() == 2
+    # cpd_params: 4 int32, 10 double, 5 int32 (+4 padding), 2 double
+    # -> 16 + 80 + 20 + 4 + 16
+    assert ctypes.sizeof(system.CpdParams) == 136
 
 
 def test_no_cpu_fallback_without_gpu():

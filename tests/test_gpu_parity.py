@@ -493,6 +493,51 @@ def test_plate_with_frozen_particles(cuda, oracle, precision):
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
+
+def _cylinder(steps):
+    return P.fragmenting_cylinder(num_cells=(60, 60, 40), size=(0.06, 0.06, 0.04),
+                                  height=0.03, steps=steps)
+
+
+@pytest.mark.parametrize("ordering", [0, 1])
+def test_fragmenting_cylinder_bit_exact(cuda, oracle, ordering):
+    """PMB fracture plus normal-repulsion contact (the fragmenting-cylinder
+    example on a shorter cylinder, 21 k particles): the EXACT path equals the
+    oracle bit for bit in u, v, f and the broken bonds, with the contact list
+    rebuilt on current positions every step."""
+    prob = _cylinder(40)
+    g, o = _pair(cuda, oracle, prob, ordering=ordering)
+    for _ in range(2):
+        g.run(20)
+        o.run(20)
+        assert g.contact_rebuilds() == o.contact_rebuilds()
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        _assert_same(g, o)
+        wg, dg = g.compute_energy()
+        wo, do = o.compute_energy()
+        assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+    assert g.contact_rebuilds() == 40 and dg > 0.0
+
+
+def test_fragmenting_cylinder_fp64_and_mixed(cuda, oracle):
+    """The same problem on the FP64 kernels (the PD bond force in its
+    throughput form beside the exact repulsion kernel): within 1e-10 of the
+    oracle (norm-wise), identical broken-bond sets. MIXED runs the FP64 PD
+    kernels when contact is present, so it equals FP64 bit for bit."""
+    prob = _cylinder(40)
+    g, o = _pair_fast(cuda, oracle, prob)
+    m = cuda.System(dict(prob["params"], precision=MIXED))
+    P.setup(m, prob)
+    for _ in range(2):
+        g.run(20)
+        o.run(20)
+        m.run(20)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        for fld in ("u", "v", "f"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-10, fld
+            assert np.array_equal(m.get(fld), g.get(fld)), fld
+
+
 def test_split_forms_on_small_systems():
     """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
     of full-stencil and shared-subset warps, the general kernels over the

@@ -134,3 +134,78 @@ def test_inputs_semantics(tmp_path):
     assert inp["output_file"] == "cabanaPD.out"
     with pytest.raises(RuntimeError):
         Inputs(dict(deck, m={"value": 2}))
+
+
+def _repulsion_pair(oracle, d, radius=0.45e-3, K=130e9, delta=4.17e-3, vol=1e-9):
+    """Two particles a distance d apart along (1, 2, 2)/3 under normal
+    repulsion alone (the contact-only form of the reference's model)."""
+    e = np.array([1.0, 2.0, 2.0]) / 3.0
+    x = np.array([[0.0, 0.0, 0.0], d * e])
+    params = dict(pd_model=P.PD_NONE, contact_model=P.CONTACT_NORMAL_REPULSION,
+                  contact_radius=radius, radius_extend=1e-5, contact_horizon=delta,
+                  contact_K=K, dt=1e-9, rebuild_every=0)
+    s = oracle.OracleSystem(params)
+    s.set_particles(x, np.full(2, vol), np.full(2, 7800.0), np.zeros(2, np.int32), None)
+    s.build_neighbors()
+    s.init()
+    return s, x
+
+
+def test_normal_repulsion_force_law(oracle):
+    """NormalRepulsionModel (force_models/CabanaPD_Contact.hpp:70-88) in
+    Force<NormalRepulsionModel>::computeForceFull (force/CabanaPD_Contact.hpp:
+    52-92): a pair closer than the contact radius gets ((15 c) sc) vol_j r_d /
+    r with sc = (r - radius) / delta, c = 18 K / (pi delta^4), in that
+    operation order; a pair inside the search radius but not closer than the
+    contact radius gets nothing. The reference's own test of this model
+    (unit_test/tstNormalRepulsion.hpp) only constructs it."""
+    radius, K, delta, vol = 0.45e-3, 130e9, 4.17e-3, 1e-9
+    c = 18.0 * K / (math.pi * delta * delta * delta * delta)
+    for d in (0.2e-3, 0.4e-3):
+        s, x = _repulsion_pair(oracle, d, radius, K, delta, vol)
+        f = s.get("f")
+        for i, j in ((0, 1), (1, 0)):
+            r_vec = [(x[j, k] - x[i, k]) + (0.0 - 0.0) for k in range(3)]
+            r = math.sqrt(r_vec[0] * r_vec[0] + r_vec[1] * r_vec[1] + r_vec[2] * r_vec[2])
+            sc = (r - radius) / delta
+            coeff = 15.0 * c * sc * vol
+            want = [0.0 + coeff * r_vec[k] / r for k in range(3)]
+            assert list(f[i]) == want, (d, i, f[i], want)
+        # Repulsive: particle 0 is pushed away from particle 1.
+        assert np.dot(f[0], x[1] - x[0]) < 0.0
+    s, _ = _repulsion_pair(oracle, 0.5e-3, radius, K, delta, vol)
+    assert s.neighbors()[0].tolist() == [1, 1]  # listed (search radius 0.91 mm) ...
+    assert not np.any(s.get("f"))              # ... but beyond the contact radius
+
+
+def test_pd_with_normal_repulsion_adds_forces(oracle):
+    """Solver with a PD model and a contact model (CabanaPD_Solver.hpp:
+    361-363): the contact force is added to the PD force of the same state
+    (computeForce with reset = false). On a displaced fragmenting-cylinder
+    state the hybrid force equals PD + repulsion within rounding, with the
+    repulsion active. In a run at 200 m/s the contact list is rebuilt every
+    step (largest displacement above the 0.01 dx search extension)."""
+    prob = P.fragmenting_cylinder(num_cells=(40, 40, 20), size=(0.06, 0.06, 0.02),
+                                  height=0.015, steps=12)
+    rng = np.random.Generator(np.random.PCG64(7))
+    u = rng.normal(0.0, 2e-5, size=prob["x"].shape)
+    contact_keys = ("contact_model", "contact_horizon", "contact_K", "contact_radius",
+                    "radius_extend", "rebuild_every")
+    pd_only = {k: val for k, val in prob["params"].items() if k not in contact_keys}
+    rep_only = dict(prob["params"], pd_model=P.PD_NONE, fracture=0)
+    forces = []
+    for params in (prob["params"], pd_only, rep_only):
+        s = oracle.OracleSystem(params)
+        s.set_particles(prob["x"], prob["vol"], prob["rho"], prob["nofail"], None)
+        s.set_state(u, prob["v0"])
+        s.build_neighbors()
+        s.compute_force()
+        forces.append(s.get("f"))
+    f, f_pd, f_rep = forces
+    assert np.any(f_rep) and np.any(f_pd)
+    assert np.linalg.norm(f - (f_pd + f_rep)) <= 1e-13 * np.linalg.norm(f)
+
+    hyb = oracle.OracleSystem(prob["params"])
+    P.setup(hyb, prob)
+    hyb.run(12)
+    assert hyb.contact_rebuilds() == 12  # one per step (set-up's build is not counted)

@@ -39,7 +39,7 @@ def _gxx():
 
 
 @pytest.mark.parametrize("name", ["kalthoff_winkler", "elastic_wave", "random_cracks",
-                                  "hertz_spheres", "stress_cube"])
+                                  "hertz_spheres", "stress_cube", "fragmenting_cylinder"])
 def test_examples_compile_as_host_cpp(name):
     """The front end is plain C++17 outside nvcc (KOKKOS_LAMBDA = [=])."""
     r = subprocess.run([_gxx(), "-std=c++17", "-fsyntax-only", "-Wall", "-I", INCLUDE,
@@ -308,3 +308,52 @@ def test_stress_cube_program(lib, tmp_path, case):
             assert R.float_eq(sigma[p, d, d], ref_sigma[d]), (p, d, sigma[p, d, d], ref_sigma[d])
         off = sigma[p][~np.eye(3, dtype=bool)]
         assert np.all(off <= 1e-13), (p, off)
+
+
+def _cylinder_deck(steps, use_contact=True):
+    """The fragmenting-cylinder deck (examples/mechanics/inputs/
+    fragmenting_cylinder.json) on a shorter cylinder in a smaller box."""
+    dt = 1.7e-7
+    return {
+        "dx": {"value": [0.001, 0.001, 0.001]},
+        "system_size": {"value": [0.06, 0.06, 0.04]},
+        "density": {"value": 7800}, "bulk_modulus": {"value": 130e9},
+        "shear_modulus": {"value": 78e9}, "critical_stretch": {"value": 0.02},
+        "horizon": {"value": 0.00417462}, "use_contact": {"value": use_contact},
+        "contact_horizon_factor": {"value": 0.9},
+        "contact_horizon_extend_factor": {"value": 0.01},
+        "cylinder_outer_radius": {"value": 0.025}, "cylinder_inner_radius": {"value": 0.02},
+        "cylinder_height": {"value": 0.03}, "max_radial_velocity": {"value": 200},
+        "min_radial_velocity": {"value": 50}, "max_vertical_velocity": {"value": 100},
+        "final_time": {"value": (steps + 0.5) * dt}, "timestep": {"value": dt},
+        "timestep_safety_factor": {"value": 0.70}, "output_frequency": {"value": steps},
+        "output_reference": {"value": False},
+    }
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_contact", [True, False])
+def test_fragmenting_cylinder_program(lib, tmp_path, use_contact):
+    """PMB fracture with normal-repulsion contact through the CabanaPD API
+    (Solver(inputs, particles, model, contact)): final totals equal the
+    Python-driven run of the same particles bit for bit and fragmentation
+    has started; with contact the list is rebuilt every step (200 m/s)."""
+    steps = 40
+    deck = _cylinder_deck(steps, use_contact)
+    out = _run_example("fragmenting_cylinder", deck, str(tmp_path), "exact")
+    W, D = _printed(out, "strain energy")
+    n = int(_printed(out, "particles")[0])
+    init = np.loadtxt(tmp_path / "cylinder_initial.txt", ndmin=2)
+    assert init.shape == (n, 6)
+    nc = Inputs(str(tmp_path / "fragmenting_cylinder.json"))["num_cells"]
+    prob = P.fragmenting_cylinder(num_cells=nc, size=(0.06, 0.06, 0.04), height=0.03,
+                                  steps=steps, contact=use_contact, x=init[:, :3])
+    assert prob["x"].shape[0] == n
+    prob["v0"] = np.ascontiguousarray(init[:, 3:])
+    s = lib.System(dict(prob["params"], precision=lib.system.FP64_EXACT))
+    P.setup(s, prob)
+    s.run(steps)
+    assert s.compute_energy() == (W, D)
+    assert D > 0.0
+    if use_contact:
+        assert s.contact_rebuilds() == steps
