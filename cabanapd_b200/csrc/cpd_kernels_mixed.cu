@@ -1165,10 +1165,14 @@ __device__ __forceinline__ void lps_theta_bond(const MixedStencil& t,
     ct = fmaf(wv, bd.s, ct);
 }
 
-constexpr int kThetaUnroll = 4;  // 8 spills at 64 registers
+// 4-bond chunks at 3 blocks of 256 per SM: 72 registers, no spills. On the
+// 8.0 M-particle LPS box (B200, ms per mixed step) this form runs 5.08;
+// at 4 blocks (64 registers, spilling) 5.12, 8-bond chunks at 3 blocks
+// 5.21, 2-bond chunks at 4 / 5 blocks 5.22 / 5.15.
+constexpr int kThetaUnroll = 4;
 
 template <bool FRACTURE, int INFL, bool WITH_M>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, 3)
     k_lps_mtheta_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,
                       float2* __restrict__ ab, const int32_t* __restrict__ wlist, int64_t wcount)
 {
@@ -1244,6 +1248,9 @@ __device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
     cz = fmaf(kf, bd.rz, cz);
 }
 
+// 8-bond chunks at 4 blocks of 256 per SM (60 registers). Measured beside it
+// on the 8.0 M-particle LPS box, no faster: 3 blocks, 4-bond chunks at 4 or
+// 5 blocks.
 template <bool FRACTURE, int INFL>
 __global__ void __launch_bounds__(kBlock, 4)
     k_lps_force_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,

@@ -3,9 +3,10 @@
 // A Kokkos-free restatement of the user-facing template API of CabanaPD
 // (src/CabanaPD.hpp and the headers it includes) for the per-timestep
 // mechanics path: Inputs, ForceModel (PMB, LPS, LinearPMB, LinearLPS with
-// and without fracture), HertzianModel, Particles, Region, Prenotch,
-// createBoundaryCondition, BodyTerm, Solver, createOutputTimeSeries and
-// createDisplacementProfile keep their names, argument meaning and call
+// and without fracture), HertzianModel, NormalRepulsionModel, Particles
+// (with output), Region, Prenotch, createBoundaryCondition, BodyTerm,
+// Solver, createOutputTimeSeries and createDisplacementProfile keep their
+// names, argument meaning and call
 // order, so a program written against CabanaPD builds against this header
 // (nvcc -x cu --extended-lambda -std=c++17) and runs on the B200 kernels.
 //
@@ -41,6 +42,7 @@
 #include <iostream>
 #include <memory>
 #include <random>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -322,6 +324,77 @@ template <class T>
 struct is_init : std::integral_constant<bool, std::is_same<T, Cabana::InitUniform>::value ||
                                                   std::is_same<T, Cabana::InitRandom>::value> {};
 
+// Particle output. The reference writes each output step through Cabana's
+// HDF5 (or SILO) particle writer when Cabana was built with one, else it
+// only logs that no output is enabled (CabanaPD_Particles.hpp:622-652). Here
+// the same fields go to an XDMF file with its heavy data in one raw binary
+// file (readable by ParaView and VisIt), when CABANAPD_B200_PARTICLE_OUTPUT
+// is set to anything but "0".
+inline bool particle_output_enabled()
+{
+    const char* e = std::getenv("CABANAPD_B200_PARTICLE_OUTPUT");
+    return e && *e && std::string(e) != "0";
+}
+
+// One output field: its name (the reference's slice label), components per
+// particle (1, 3 or 9) and its values in [n][components] order.
+struct OutputField {
+    std::string name;
+    int components = 1;
+    std::vector<double> values;
+    std::vector<int32_t> ints;  // used instead of values when not empty
+};
+
+// <prefix>_<step>.xmf and <prefix>_<step>.bin: a polyvertex grid at time
+// `time` with the geometry from `positions` ([n][3]) and one node attribute
+// per field, all stored back to back in the .bin file.
+inline void write_xdmf_particles(const std::string& prefix, int step, double time, int64_t n,
+                                 const OutputField& positions,
+                                 const std::vector<OutputField>& fields)
+{
+    const std::string base = prefix + "_" + std::to_string(step);
+    const std::string bin_name = base + ".bin";
+    std::ofstream bin(bin_name, std::ios::binary | std::ios::trunc);
+    if (!bin) throw std::runtime_error("particle output: cannot write " + bin_name);
+    const uint16_t probe = 1;
+    const char* endian = (*reinterpret_cast<const unsigned char*>(&probe) == 1) ? "Little" : "Big";
+    std::ostringstream xml;
+    int64_t offset = 0;
+    auto data_item = [&](const OutputField& fld) {
+        const bool is_int = !fld.ints.empty();
+        const size_t count = static_cast<size_t>(n) * fld.components;
+        if ((is_int ? fld.ints.size() : fld.values.size()) != count)
+            throw std::runtime_error("particle output: field " + fld.name + " has the wrong size");
+        const size_t bytes = count * (is_int ? sizeof(int32_t) : sizeof(double));
+        bin.write(is_int ? reinterpret_cast<const char*>(fld.ints.data())
+                         : reinterpret_cast<const char*>(fld.values.data()),
+                  static_cast<std::streamsize>(bytes));
+        xml << "        <DataItem Format=\"Binary\" Dimensions=\"" << n;
+        if (fld.components > 1) xml << " " << fld.components;
+        xml << "\" NumberType=\"" << (is_int ? "Int" : "Float") << "\" Precision=\""
+            << (is_int ? 4 : 8) << "\" Endian=\"" << endian << "\" Seek=\"" << offset << "\">"
+            << bin_name.substr(bin_name.find_last_of('/') + 1) << "</DataItem>\n";
+        offset += static_cast<int64_t>(bytes);
+    };
+    xml << "<?xml version=\"1.0\" ?>\n<Xdmf Version=\"3.0\">\n  <Domain>\n"
+        << "    <Grid Name=\"particles\" GridType=\"Uniform\">\n"
+        << "      <Time Value=\"" << std::setprecision(17) << time << "\"/>\n"
+        << "      <Topology TopologyType=\"Polyvertex\" NumberOfElements=\"" << n << "\"/>\n"
+        << "      <Geometry GeometryType=\"XYZ\">\n";
+    data_item(positions);
+    xml << "      </Geometry>\n";
+    for (const OutputField& fld : fields) {
+        const char* kind = fld.components == 1 ? "Scalar" : fld.components == 3 ? "Vector" : "Tensor";
+        xml << "      <Attribute Name=\"" << fld.name << "\" AttributeType=\"" << kind
+            << "\" Center=\"Node\">\n";
+        data_item(fld);
+        xml << "      </Attribute>\n";
+    }
+    xml << "    </Grid>\n  </Domain>\n</Xdmf>\n";
+    if (!bin) throw std::runtime_error("particle output: writing " + bin_name + " failed");
+    std::ofstream(base + ".xmf", std::ios::trunc) << xml.str();
+}
+
 }  // namespace detail
 
 // ---------------------------------------------------------------------------
@@ -431,6 +504,54 @@ class Particles {
     int rank() const { return 0; }
 
     const std::shared_ptr<detail::ParticleData>& data() const { return d_; }
+
+    // Particles::output (CabanaPD_Particles.hpp:622-652 with the field lists
+    // of :785-791, :1192-1199, :1323-1331): positions (reference or current),
+    // forces, displacements, velocities and type, then strain energy and
+    // damage, the LPS weighted volume and dilatation, and the stress of
+    // EnergyStressOutput particles, as particles_<output_step>.xmf / .bin
+    // when CABANAPD_B200_PARTICLE_OUTPUT is set (else a one-time notice, as
+    // the reference logs without an output library). The solver calls it at
+    // init and at output steps with the host mirrors refreshed.
+    void output(int output_step, double output_time, bool use_reference) const
+    {
+        if (!detail::particle_output_enabled()) {
+            static bool told = false;
+            if (!told) std::cout << "No particle output enabled." << std::endl;
+            told = true;
+            return;
+        }
+        const int64_t n = d_->n;
+        auto aos = [&](const std::vector<double>& soa, int comps) {
+            std::vector<double> a(static_cast<size_t>(n) * comps);
+            for (int64_t i = 0; i < n; i++)
+                for (int c = 0; c < comps; c++) a[comps * i + c] = soa[c * n + i];
+            return a;
+        };
+        detail::OutputField pos{use_reference ? "reference_positions" : "current_positions", 3,
+                                aos(d_->x, 3), {}};
+        if (!use_reference)
+            for (int64_t i = 0; i < n; i++)
+                for (int c = 0; c < 3; c++) pos.values[3 * i + c] += d_->u[c * n + i];
+        std::vector<detail::OutputField> fields;
+        fields.push_back({"forces", 3, aos(d_->f, 3), {}});
+        fields.push_back({"displacements", 3, aos(d_->u, 3), {}});
+        fields.push_back({"velocities", 3, aos(d_->v, 3), {}});
+        fields.push_back({"type", 1, {}, std::vector<int32_t>(static_cast<size_t>(n), 0)});
+        fields.push_back({"strain_energy", 1, d_->W, {}});
+        fields.push_back({"damage", 1, d_->phi, {}});
+        constexpr bool lps = std::is_same<ModelTag, LPS>::value ||
+                             std::is_same<ModelTag, LinearLPS>::value;
+        if (lps && d_->sys) {
+            std::vector<double> m(static_cast<size_t>(n)), theta(static_cast<size_t>(n));
+            cpdCheck(cpd_download(d_->sys, CPD_FIELD_M, m.data()));
+            cpdCheck(cpd_download(d_->sys, CPD_FIELD_THETA, theta.data()));
+            fields.push_back({"weighted_volume", 1, std::move(m), {}});
+            fields.push_back({"dilatation", 1, std::move(theta), {}});
+        }
+        if (d_->with_stress) fields.push_back({"stress", 9, aos(d_->stress, 9), {}});
+        detail::write_xdmf_particles("particles", output_step, output_time, n, pos, fields);
+    }
 
   private:
     struct AllCells {
@@ -882,7 +1003,7 @@ class Solver {
 
     void init(bool initial_output = true)
     {
-        (void)initial_output;
+        initial_output_ = initial_output;
         init_stages(static_cast<NoCondition*>(nullptr));
     }
     template <std::size_t N>
@@ -894,13 +1015,13 @@ class Solver {
     template <class BC, class = typename std::enable_if<detail::is_condition<BC>::value>::type>
     void init(BC& bc, bool initial_output = true)
     {
-        (void)initial_output;
+        initial_output_ = initial_output;
         init_stages(&bc);
     }
     template <class BC, std::size_t N>
     void init(BC& bc, const Prenotch<N>& notch, bool initial_output = true)
     {
-        (void)initial_output;
+        initial_output_ = initial_output;
         apply_prenotch(notch);
         init_stages(&bc);
     }
@@ -1008,6 +1129,9 @@ class Solver {
         cpdCheck(cpd_neighbor_stats(d->sys, &max_n, &total));
         output_file_ = inputs_.contains("output_file") ? static_cast<std::string>(inputs_["output_file"])
                                                        : std::string("cabanaPD.out");
+        output_reference_ = inputs_.contains("output_reference")
+                                ? static_cast<bool>(inputs_["output_reference"])
+                                : true;
         std::ofstream out(output_file_, std::ofstream::app);
         const std::time_t now = std::time(nullptr);
         out << "CabanaPD (cabanapd_b200) " << std::ctime(&now) << "\n"
@@ -1073,11 +1197,12 @@ class Solver {
         cpdCheck(cpd_init(d->sys));
         initialized_ = true;
         if (stage_ && stage_->force_update) stage_->apply(0.0);
-        if (d->with_stress) {
-            d->compute_stress();
+        if (d->with_stress) d->compute_stress();
+        if (d->with_stress || (initial_output_ && detail::particle_output_enabled()))
             d->refresh_mirrors();
-        }
         cpdCheck(cpd_synchronize(d->sys));
+        // Solver.hpp:245-246: the initial particle output.
+        if (initial_output_) particles.output(0, 0.0, output_reference_);
         init_time_ += seconds_since(t0);
     }
 
@@ -1103,7 +1228,10 @@ class Solver {
             if (step % output_frequency == 0) {
                 cpdCheck(cpd_compute_energy(d->sys, &last_W_, &last_D_));
                 d->compute_stress();
-                if (sizeof...(Out) > 0 || d->with_stress) d->refresh_mirrors();
+                const bool write = detail::particle_output_enabled();
+                if (sizeof...(Out) > 0 || d->with_stress || write) d->refresh_mirrors();
+                // Solver.hpp:479-494: energy, stress, then the particle output.
+                particles.output(step / output_frequency, time, output_reference_);
                 if constexpr (sizeof...(Out) > 0) (outputs.update(time), ...);
                 const double elapsed = seconds_since(t_start);
                 std::ofstream out(output_file_, std::ofstream::app);
@@ -1154,6 +1282,8 @@ class Solver {
     double last_W_ = 0.0, last_D_ = 0.0;
     bool bc_bound_ = false;
     bool initialized_ = false;
+    bool initial_output_ = true;
+    bool output_reference_ = true;
     std::unique_ptr<detail::UserStage> stage_;
 };
 

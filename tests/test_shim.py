@@ -121,18 +121,87 @@ def test_cpp_inputs_match_python_inputs(inputs_probe, tmp_path, deck):
         assert a == float(b), (got, want)
 
 
+_XDMF_PROBE = r"""
+#include <CabanaPD.hpp>
+int main()
+{
+    using CabanaPD::detail::OutputField;
+    const int64_t n = 5;
+    OutputField pos{"reference_positions", 3, {}, {}};
+    OutputField f{"forces", 3, {}, {}}, w{"damage", 1, {}, {}}, s{"stress", 9, {}, {}};
+    OutputField t{"type", 1, {}, std::vector<int32_t>(n, 0)};
+    for (int64_t i = 0; i < n; i++) {
+        for (int c = 0; c < 3; c++) {
+            pos.values.push_back(i + 0.25 * c);
+            f.values.push_back(-1.5 * i + c);
+        }
+        w.values.push_back(0.125 * i);
+        t.ints[i] = static_cast<int32_t>(i % 2);
+        for (int c = 0; c < 9; c++) s.values.push_back(10.0 * i + c);
+    }
+    CabanaPD::detail::write_xdmf_particles("particles", 3, 2.5e-6, n, pos, {f, t, w, s});
+    return 0;
+}
+"""
+
+
+def read_xdmf_particles(path):
+    """Parse a particle XDMF file: (time, {name: array}) with the geometry
+    under the name of the first DataItem's role, "positions"."""
+    import xml.etree.ElementTree as ET
+    root = ET.parse(path).getroot()
+    grid = root.find("Domain/Grid")
+    time = float(grid.find("Time").get("Value"))
+
+    def load(item):
+        dims = [int(v) for v in item.get("Dimensions").split()]
+        dtype = {("Float", "8"): "<f8", ("Int", "4"): "<i4"}[(item.get("NumberType"),
+                                                               item.get("Precision"))]
+        assert item.get("Endian") == "Little" and item.get("Format") == "Binary"
+        data = np.fromfile(os.path.join(os.path.dirname(path), item.text.strip()), dtype=dtype,
+                           count=int(np.prod(dims)), offset=int(item.get("Seek")))
+        return data.reshape(dims)
+
+    out = {"positions": load(grid.find("Geometry/DataItem"))}
+    for att in grid.findall("Attribute"):
+        out[att.get("Name")] = load(att.find("DataItem"))
+    return time, out
+
+
+def test_xdmf_particle_writer(tmp_path):
+    """The particle output format of the front end: an XDMF polyvertex grid
+    whose heavy data (doubles and int32, [n][components]) sit back to back
+    in one binary file, read back exactly."""
+    src = tmp_path / "probe.cpp"
+    src.write_text(_XDMF_PROBE)
+    exe = tmp_path / "probe"
+    r = subprocess.run([_gxx(), "-std=c++17", "-O1", "-I", INCLUDE, str(src), "-o", str(exe)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    time, fields = read_xdmf_particles(str(tmp_path / "particles_3.xmf"))
+    assert time == 2.5e-6
+    i = np.arange(5.0)
+    assert np.array_equal(fields["positions"], i[:, None] + 0.25 * np.arange(3.0)[None, :])
+    assert np.array_equal(fields["forces"], -1.5 * i[:, None] + np.arange(3.0)[None, :])
+    assert np.array_equal(fields["type"], (np.arange(5) % 2).astype(np.int32))
+    assert np.array_equal(fields["damage"], 0.125 * i)
+    assert np.array_equal(fields["stress"], 10.0 * i[:, None] + np.arange(9.0)[None, :])
+
+
 # ---------------------------------------------------------------------------
 # GPU
 
 
-def _run_example(name, deck, workdir, precision="exact", args=()):
+def _run_example(name, deck, workdir, precision="exact", args=(), env_extra=None):
     exe = os.path.join(BUILD, name)
     if not os.path.exists(exe):
         raise RuntimeError(f"{exe} is missing: build the examples (make -C examples)")
     path = os.path.join(workdir, name + ".json")
     with open(path, "w") as fh:
         json.dump(deck, fh)
-    env = dict(os.environ, CABANAPD_B200_PRECISION=precision)
+    env = dict(os.environ, CABANAPD_B200_PRECISION=precision, **(env_extra or {}))
     r = subprocess.run([exe, path, *args], cwd=workdir, env=env, capture_output=True, text=True,
                        timeout=900)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -357,3 +426,39 @@ def test_fragmenting_cylinder_program(lib, tmp_path, use_contact):
     assert D > 0.0
     if use_contact:
         assert s.contact_rebuilds() == steps
+
+
+@pytest.mark.gpu
+def test_particle_output_files(lib, tmp_path):
+    """Particles::output through the Solver (initial output and each output
+    step) with CABANAPD_B200_PARTICLE_OUTPUT set: the LPS program's last
+    output holds the displacements, velocities, forces, damage, weighted
+    volume and dilatation of the Python-driven run bit for bit, at the
+    reference positions (output_reference defaults to true)."""
+    prob, deck = _random_cracks_deck((200, 80, 4), 60)
+    deck["output_frequency"] = {"value": 30}
+    _run_example("random_cracks", deck, str(tmp_path), "exact",
+                 env_extra={"CABANAPD_B200_PARTICLE_OUTPUT": "1"})
+    names = sorted(p.name for p in tmp_path.glob("particles_*.xmf"))
+    assert names == ["particles_0.xmf", "particles_1.xmf", "particles_2.xmf"]
+    t0, first = read_xdmf_particles(str(tmp_path / "particles_0.xmf"))
+    t2, last = read_xdmf_particles(str(tmp_path / "particles_2.xmf"))
+    dt = prob["params"]["dt"]
+    assert t0 == 0.0 and t2 == 60 * dt
+    s = lib.System(dict(prob["params"], precision=lib.system.FP64_EXACT))
+    P.setup(s, prob)
+    assert np.array_equal(first["positions"], s.get("x"))
+    assert not np.any(first["displacements"])
+    s.run(prob["num_steps"])
+    s.compute_energy()
+    assert np.array_equal(last["positions"], s.get("x"))
+    for name, field in (("displacements", "u"), ("velocities", "v"), ("damage", "phi"),
+                        ("weighted_volume", "m"), ("dilatation", "theta"),
+                        ("strain_energy", "W")):
+        assert np.array_equal(last[name], s.get(field)), name
+    assert np.any(last["damage"] > 0)
+    # The program's traction is a device functor added after the library's
+    # force; the Python run applies it as a force BC, so forces agree to
+    # rounding of that sum only.
+    f = s.get("f")
+    assert np.linalg.norm(last["forces"] - f) <= 1e-14 * np.linalg.norm(f)
