@@ -1335,6 +1335,136 @@ cpd_status cpd_download(cpd_system* s, int32_t field, double* out)
     return CPD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// State snapshots: a header, then the device arrays in internal order.
+namespace {
+
+struct StateHeader {
+    uint64_t magic;
+    int64_t version, n, frozen, npad, pd_model, contact, fracture, ordering;
+    int64_t max_n, nwords, total_bonds, contact_max_n, steps_since_rebuild, rebuilds;
+    double max_disp;
+};
+constexpr uint64_t kStateMagic = 0x4554415453445043ull;  // "CPDSTATE" in little-endian bytes
+constexpr int64_t kStateVersion = 1;
+
+// The device arrays of a snapshot, in file order.
+std::vector<std::pair<void*, size_t>> state_sections(cpd_system* s)
+{
+    const size_t vec = sizeof(double) * 3 * (size_t)s->npad;
+    const size_t sca = sizeof(double) * (size_t)s->npad;
+    std::vector<std::pair<void*, size_t>> out = {
+        {s->u, vec}, {s->v, vec}, {s->f, vec},
+        {s->m, sca}, {s->theta, sca}, {s->lps_a, sca}, {s->lps_b, sca}};
+    if (has_pd(s) && s->pd.mu)
+        out.push_back({s->pd.mu, sizeof(uint32_t) * (size_t)s->pd.nwords * (size_t)s->npad});
+    if (has_contact(s)) out.push_back({s->u_neigh, vec});
+    return out;
+}
+
+StateHeader state_header(const cpd_system* s)
+{
+    StateHeader h{};
+    h.magic = kStateMagic;
+    h.version = kStateVersion;
+    h.n = s->n;
+    h.frozen = s->frozen;
+    h.npad = s->npad;
+    h.pd_model = s->md.pd;
+    h.contact = s->md.contact;
+    h.fracture = s->md.fracture;
+    h.ordering = s->params.ordering;
+    h.max_n = s->pd.max_n;
+    h.nwords = s->pd.nwords;
+    h.total_bonds = s->pd.total;
+    h.contact_max_n = has_contact(s) ? s->contact.max_n : 0;
+    h.steps_since_rebuild = s->steps_since_rebuild;
+    h.rebuilds = s->rebuilds;
+    h.max_disp = s->max_disp;
+    return h;
+}
+
+uint64_t state_bytes(cpd_system* s)
+{
+    uint64_t b = sizeof(StateHeader);
+    for (const auto& sec : state_sections(s)) b += sec.second;
+    return b;
+}
+
+}  // namespace
+
+cpd_status cpd_state_bytes(cpd_system* s, uint64_t* bytes)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!bytes) return set_error(CPD_ERR_INVALID_ARGUMENT, "null output");
+    *bytes = state_bytes(s);
+    return CPD_OK;
+}
+
+cpd_status cpd_save_state(cpd_system* s, void* buf, uint64_t bytes)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "cpd_save_state: call cpd_init first");
+    if (!buf || bytes < state_bytes(s))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_save_state: buffer smaller than cpd_state_bytes");
+    CPD_CUDA(cudaSetDevice(s->device));
+    const StateHeader h = state_header(s);
+    std::memcpy(buf, &h, sizeof(h));
+    char* dst = static_cast<char*>(buf) + sizeof(h);
+    for (const auto& sec : state_sections(s)) {
+        CPD_CUDA(cudaMemcpyAsync(dst, sec.first, sec.second, cudaMemcpyDeviceToHost, s->stream));
+        dst += sec.second;
+    }
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
+cpd_status cpd_load_state(cpd_system* s, const void* buf, uint64_t bytes)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "cpd_load_state: call cpd_init first");
+    if (!buf || bytes < sizeof(StateHeader))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_load_state: no snapshot");
+    StateHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    if (h.magic != kStateMagic || h.version != kStateVersion)
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_load_state: not a state snapshot of this version");
+    const StateHeader mine = state_header(s);
+    if (h.n != mine.n || h.frozen != mine.frozen || h.npad != mine.npad ||
+        h.pd_model != mine.pd_model || h.contact != mine.contact ||
+        h.fracture != mine.fracture || h.ordering != mine.ordering || h.max_n != mine.max_n ||
+        h.nwords != mine.nwords || h.total_bonds != mine.total_bonds)
+        return set_error(CPD_ERR_INVALID_ARGUMENT,
+                         "cpd_load_state: the snapshot is of a system set up differently");
+    if (bytes < state_bytes(s))
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_load_state: truncated snapshot");
+    CPD_CUDA(cudaSetDevice(s->device));
+    const char* src = static_cast<const char*>(buf) + sizeof(h);
+    for (const auto& sec : state_sections(s)) {
+        CPD_CUDA(cudaMemcpyAsync(sec.first, src, sec.second, cudaMemcpyHostToDevice, s->stream));
+        src += sec.second;
+    }
+    // Derived device state: the FP32 split of u, and the contact list, which
+    // was built on x + u_neigh (with the 1e-14 tolerance of the set-up build
+    // when no rebuild had happened yet).
+    if (use_mixed(s) && s->mixed.u2)
+        s->launches += launch_split_u(view(s), s->md, s->mixed, s->stream);
+    if (has_contact(s)) {
+        const double cutoff = 2.0 * s->md.radius + s->md.radius_extend + (h.rebuilds == 0 ? 1e-14 : 0.0);
+        std::string err;
+        const int l = build_neighbor_list(s->x, s->u_neigh, s->n, s->npad, s->frozen, cutoff,
+                                          s->perm, false, s->contact, s->stream, err);
+        if (l < 0) return set_error(CPD_ERR_CUDA, "contact neighbour build: " + err);
+        s->launches += l;
+    }
+    s->steps_since_rebuild = h.steps_since_rebuild;
+    s->rebuilds = h.rebuilds;
+    s->max_disp = h.max_disp;
+    s->stress_ready = false;
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    return CPD_OK;
+}
+
 double cpd_max_displacement(const cpd_system* s) { return s ? s->max_disp : 0.0; }
 int64_t cpd_contact_rebuilds(const cpd_system* s) { return s ? s->rebuilds : 0; }
 

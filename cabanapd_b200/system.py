@@ -118,6 +118,9 @@ _D = ctypes.c_double
 _DP = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "cpd_abi_version": (_I32, []),
+    "cpd_state_bytes": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "cpd_save_state": (_I32, [_P, ctypes.c_void_p, ctypes.c_uint64]),
+    "cpd_load_state": (_I32, [_P, ctypes.c_void_p, ctypes.c_uint64]),
     "cpd_last_error": (ctypes.c_char_p, []),
     "cpd_system_create": (_I32, [ctypes.POINTER(CpdParams), ctypes.POINTER(_P)]),
     "cpd_system_destroy": (_I32, [_P]),
@@ -357,6 +360,19 @@ class System:
 
     def kernel_launches(self):
         return self._lib.cpd_kernel_launches(self._h)
+
+    def save_state(self):
+        """Snapshot of the evolving state (cpd_save_state) as a uint8 array."""
+        nbytes = ctypes.c_uint64()
+        self._check(self._lib.cpd_state_bytes(self._h, ctypes.byref(nbytes)))
+        buf = np.empty(nbytes.value, dtype=np.uint8)
+        self._check(self._lib.cpd_save_state(self._h, buf.ctypes.data, buf.size))
+        return buf
+
+    def load_state(self, buf):
+        """Restore a snapshot taken from a system set up the same way."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        self._check(self._lib.cpd_load_state(self._h, buf.ctypes.data, buf.size))
 
 
 def _params_struct(params, precision=FP64_EXACT, ordering=ORDER_INPUT, device=0):

@@ -255,6 +255,22 @@ cpd_status cpd_compute_stress(cpd_system* sys);
 cpd_status cpd_compute_energy_noalloc(cpd_system* sys, double* W_out, double* phi_out,
                                       double* totals_out);
 
+/* State snapshots, for checkpoint / restart and for evicting a job and
+ * resuming it later. No counterpart in the reference. A snapshot holds the
+ * evolving state: displacement, velocity and force, the broken-bond bits,
+ * the LPS weighted volume, dilatation and their force coefficients, and
+ * the contact list's rebuild state (displacement at the last build, step
+ * and rebuild counters). It restores into a system set up the same way
+ * (same parameters, particles, ordering, pre-notches and boundary
+ * conditions, after cpd_init); the continued run is then bit-identical to
+ * the uninterrupted one. A snapshot of a differently set-up system is
+ * rejected with CPD_ERR_INVALID_ARGUMENT. Strain energy, damage and stress
+ * are outputs, not state: compute them again after a restore. Both calls
+ * wait for the stream. */
+cpd_status cpd_state_bytes(cpd_system* sys, uint64_t* bytes);
+cpd_status cpd_save_state(cpd_system* sys, void* host_buf, uint64_t bytes);
+cpd_status cpd_load_state(cpd_system* sys, const void* host_buf, uint64_t bytes);
+
 cpd_status cpd_init(cpd_system* sys);
 /* num_steps velocity-Verlet steps. Asynchronous: returns once the work is
  * queued on the stream (cpd_synchronize or any download waits for it).
