@@ -56,11 +56,23 @@ void system_opened(int dev)
     g_live_systems[dev]++;
 }
 
+// Device memory the pool keeps mapped once no system is live, so that the
+// next system (a job after a job) does not map its memory again: one eighth
+// of the device, at most 32 GiB, or CPD_POOL_KEEP_BYTES.
+size_t pool_keep_bytes()
+{
+    const char* e = getenv("CPD_POOL_KEEP_BYTES");
+    if (e) return (size_t)strtoull(e, nullptr, 10);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+    return std::min(total_b / 8, (size_t)32 << 30);
+}
+
 // Called after the closing system's frees have completed.
 void system_closed(int dev)
 {
     std::lock_guard<std::mutex> lock(g_pool_mutex);
-    if (--g_live_systems[dev] == 0 && g_pool[dev]) cudaMemPoolTrimTo(g_pool[dev], 0);
+    if (--g_live_systems[dev] == 0 && g_pool[dev]) cudaMemPoolTrimTo(g_pool[dev], pool_keep_bytes());
 }
 
 thread_local std::string g_last_error;

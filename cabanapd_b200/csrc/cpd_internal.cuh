@@ -303,6 +303,9 @@ struct MixedState {
     int32_t* rest_list = nullptr;
     int64_t nlean = 0, nrest = 0;
     int lps_ok = 0;       // LPS: every row is a stencil row (the mixed LPS kernels apply)
+    // All particles of one volume v: vol_sums[k] = v + v + ... (k terms,
+    // summed in order), the FP64 volume sum of any k bonds; else nullptr.
+    double* vol_sums = nullptr;
 };
 // lps: set up the LPS mixed kernels too (lps_ok, ab).
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
