@@ -655,7 +655,9 @@ bool fused_ready(const cpd_system* s)
 // for the last step) the next first half step, alternating displacement
 // buffers. The first half step writes to the buffer that makes the last
 // step end in the system's own arrays.
-cpd_status step_fused(cpd_system* s, int32_t num_steps)
+// energy_last: the last step's lean kernel also writes W and phi of its rows
+// (mixed_force_fuses_energy must hold).
+cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false)
 {
     const bool mixed = use_mixed(s);
     const bool start_alt = ((num_steps - 1) & 1) != 0;
@@ -697,6 +699,7 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps)
         ep.mode = k + 1 < num_steps ? 2 : 1;
         ep.u_next = unxt;
         ep.u2_next = u2nxt;
+        ep.energy_vol_sums = energy_last && k + 1 == num_steps ? s->mixed.vol_sums : nullptr;
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, mk, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
         std::swap(ucur, unxt);
@@ -1279,6 +1282,42 @@ cpd_status cpd_step(cpd_system* s, int32_t num_steps)
         CPD_OK_OR_RETURN(apply_force_bcs(s));
         CPD_LAUNCHED(launch_vv_final(p, s->params.dt, s->stream));
     }
+    return CPD_OK;
+}
+
+cpd_status cpd_step_energy(cpd_system* s, int32_t num_steps, double* total_W, double* total_D)
+{
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step_energy");
+    if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
+    CPD_CUDA(cudaSetDevice(s->device));
+    if (num_steps > 0 && !fused_ready(s)) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CPD_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+        if (cs == cudaStreamCaptureStatusNone) CPD_OK_OR_RETURN(prepare_fused(s));
+    }
+    const ParticleView p = view(s);
+    const bool fuse = num_steps > 0 && fused_ready(s) && use_mixed(s) &&
+                      mixed_force_fuses_energy(p, s->md, s->mixed);
+    if (!fuse) {
+        CPD_OK_OR_RETURN(cpd_step(s, num_steps));
+        return cpd_compute_energy(s, total_W, total_D);
+    }
+    CPD_OK_OR_RETURN(step_fused(s, num_steps, true));
+    const int nb = energy_blocks(s->n - s->frozen);
+    CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
+    int l = 0;
+    const int rows = launch_energy_rest_and_totals(p, pd_view(s), s->md, s->mixed, s->red, nb + 1,
+                                                   &l, s->stream);
+    s->launches += l;
+    if (rows < 0) return set_error(CPD_ERR_CUDA, "energy totals: reduction buffer too small");
+    CPD_CUDA(cudaGetLastError());
+    CPD_LAUNCHED(launch_sum_partials(s->red, rows, 2, s->red_out + 2, s->stream));
+    CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    if (total_W) *total_W = s->h_red[2];
+    if (total_D) *total_D = s->h_red[3];
     return CPD_OK;
 }
 

@@ -283,6 +283,10 @@ struct StepEpilogue {
                                        // bit d: then f_d + add_d, else add_d
     const double* bc_add = nullptr;    // [3][nbc]
     int32_t nbc = 0;
+    // Mixed PMB split form: the lean kernel also writes W_i and phi_i of its
+    // rows (the energy pass of the state it computes the force of), with
+    // the damage sums from this table (MixedState::vol_sums).
+    const double* energy_vol_sums = nullptr;
 };
 
 struct MixedState {
@@ -325,6 +329,16 @@ int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& m
                         int* launches, cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
+// Whether launch_pd_force_mixed with ep.energy_vol_sums set writes W and phi
+// of the lean rows (PMB, fracture, one volume, split form).
+bool mixed_force_fuses_energy(const ParticleView& p, const Model& md, const MixedState& m);
+// Energy pass over the rows the lean kernel does not hold (W, phi of those
+// rows; [.][2] block partials to ignore), then the totals over all rows:
+// sum W_i vol_i and sum phi_i into [.][2] block partials. Returns the
+// number of partial rows of the totals.
+int launch_energy_rest_and_totals(const ParticleView& p, const EllView& nl, const Model& md,
+                                  const MixedState& m, double* partials, int capacity,
+                                  int* launches, cudaStream_t st);
 
 // Neighbour build (cpd_neighbor.cu). Builds rows for [begin, n) from
 // positions pos (+ optional displacement disp) with squared distance

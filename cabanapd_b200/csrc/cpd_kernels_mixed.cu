@@ -518,11 +518,12 @@ __device__ __forceinline__ void lean_geometry(const MixedStencil& t, const Mixed
 // whose ends may fail) leaves the fast path: above s0 + guard it breaks (bit
 // set in clr); inside the band it is deferred (bit set in pend) to the exact
 // FP64 test after the word, and contributes no force here.
-template <bool FRACTURE, bool LDG>
+template <bool FRACTURE, bool LDG, bool ENERGY = false>
 __device__ __forceinline__ void stencil_bond(const MixedStencil& t,
                                              const MixedU* __restrict__ u2_i, const RowSplit& ri,
                                              bool on, uint32_t bit, const MixedModel& md,
-                                             uint32_t& clr, uint32_t& pend, float2& cxy, float& cz)
+                                             uint32_t& clr, uint32_t& pend, float2& cxy, float& cz,
+                                             float& wc)
 {
     MixedU uj;
     if (LDG) {
@@ -545,6 +546,8 @@ __device__ __forceinline__ void stencil_bond(const MixedStencil& t,
     const float kf = (!FRACTURE || on) ? uj.hi.w * bd.s * bd.rinv : 0.f;
     cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
     cz = fmaf(kf, bd.rz, cz);
+    // The energy pass's term of an intact bond (k_energy_mixed, PMB).
+    if (ENERGY) wc += (!FRACTURE || on) ? 0.25f * uj.hi.w * bd.s * bd.s * t.xi : 0.f;
 }
 
 // Stencil rows, lean form: bond slot k of row i is entry k of wt (the whole
@@ -553,12 +556,13 @@ __device__ __forceinline__ void stencil_bond(const MixedStencil& t,
 // chunk sum is added to the FP64 row force f. After each 32-bond word the
 // deferred bonds take the reference's FP64 break test; those that hold add
 // their pair force to f. Newly broken bits are cleared with one store.
-template <bool FRACTURE, bool LDG, int UNROLL>
+template <bool FRACTURE, bool LDG, int UNROLL, bool ENERGY = false>
 __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const EllView& nl,
                                                    const MixedU* __restrict__ u2_i,
                                                    const MixedStencil* wt, int cnt,
                                                    const MixedModel& md, int64_t i,
-                                                   const RowSplit& ri, double (&f)[3])
+                                                   const RowSplit& ri, double (&f)[3],
+                                                   double* wtot = nullptr, int* intact = nullptr)
 {
     const int64_t np = p.npad;
     for (int base = 0; base < cnt; base += 32) {
@@ -569,24 +573,26 @@ __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const 
         for (; b + UNROLL <= lim; b += UNROLL) {
             const uint32_t w8 = word >> b;
             float2 cxy = f2(0.f, 0.f);
-            float cz = 0.f;
+            float cz = 0.f, wc = 0.f;
 #pragma unroll
             for (int u = 0; u < UNROLL; ++u)
-                stencil_bond<FRACTURE, LDG>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u,
-                                            1u << (b + u), md, clr, pend, cxy, cz);
+                stencil_bond<FRACTURE, LDG, ENERGY>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u,
+                                                    1u << (b + u), md, clr, pend, cxy, cz, wc);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
+            if (ENERGY) *wtot += (double)wc;
         }
         if (b < lim) {
             float2 cxy = f2(0.f, 0.f);
-            float cz = 0.f;
+            float cz = 0.f, wc = 0.f;
             for (; b < lim; ++b)
-                stencil_bond<FRACTURE, LDG>(wt[base + b], u2_i, ri, (word >> b) & 1u, 1u << b, md,
-                                            clr, pend, cxy, cz);
+                stencil_bond<FRACTURE, LDG, ENERGY>(wt[base + b], u2_i, ri, (word >> b) & 1u,
+                                                    1u << b, md, clr, pend, cxy, cz, wc);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
+            if (ENERGY) *wtot += (double)wc;
         }
         if (FRACTURE) {
             while (pend) {
@@ -603,9 +609,14 @@ __device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const 
                     f[0] += (double)(kf * bd.rxy.x);
                     f[1] += (double)(kf * bd.rxy.y);
                     f[2] += (double)(kf * bd.rz);
+                    if (ENERGY) *wtot += (double)(0.25f * uj.hi.w * bd.s * bd.s * t.xi);
                 }
             }
             if (clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
+        }
+        if (ENERGY) {
+            const uint32_t valid = lim == 32 ? 0xffffffffu : (1u << lim) - 1u;
+            *intact += __popc(FRACTURE ? (word & ~clr & valid) : valid);
         }
     }
 }
@@ -907,7 +918,10 @@ __device__ __forceinline__ bool lean_prologue(const MixedView& mv, int ntab,
 // rows (kind 2) or share one stencil subset (kind 3); the other warps run
 // k_pmb_force_mixed over their own list. Without the other paths the kernel
 // needs fewer registers.
-template <bool FRACTURE, int MINB, int UNROLL = 8>
+// ENERGY: also the energy pass's W_i and phi_i of the rows (the state whose
+// force this launch computes, with the bonds broken in it), the damage from
+// ep.energy_vol_sums (one particle volume).
+template <bool FRACTURE, int MINB, int UNROLL = 8, bool ENERGY = false>
 __global__ void __launch_bounds__(kBlock, MINB)
     k_pmb_force_lean(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
                      const int32_t* __restrict__ wlist, int64_t wcount)
@@ -923,7 +937,16 @@ __global__ void __launch_bounds__(kBlock, MINB)
     const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z,
                       FRACTURE ? (ui.lo.w != 0.f) : false};
     double f[3] = {0.0, 0.0, 0.0};
-    mixed_stencil_rows<FRACTURE, false, UNROLL>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri, f);
+    if (ENERGY) {
+        double wtot = 0.0;
+        int intact = 0;
+        mixed_stencil_rows<FRACTURE, false, UNROLL, true>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri,
+                                                          f, &wtot, &intact);
+        p.W[i] = wtot;
+        if (FRACTURE) p.phi[i] = 1 - ep.energy_vol_sums[intact] / ep.energy_vol_sums[wcnt];
+    } else {
+        mixed_stencil_rows<FRACTURE, false, UNROLL>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri, f);
+    }
     step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
 }
 
@@ -1982,8 +2005,10 @@ int launch_mixed_form_t(const ParticleView& p, const EllView& list, const MixedV
         int n = 0;
         if (m.nlean > 0) {
             const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
+            if (FRACTURE && ep.energy_vol_sums) var = 13;
             switch (var) {
             case 9: k_pmb_force_lean<FRACTURE, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
+            case 13: k_pmb_force_lean<FRACTURE, 4, 8, true><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
             case 10: k_pmb_force_lean<FRACTURE, 5, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
             case 11: k_pmb_force_lean<FRACTURE, 5, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
             default: k_pmb_force_lean<FRACTURE, 6, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
@@ -2042,6 +2067,58 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Mode
     mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
     return launch_mixed_form(md.fracture != 0, p, list, mv, mm, m, ep, rows, st);
+}
+
+bool mixed_force_fuses_energy(const ParticleView& p, const Model& md, const MixedState& m)
+{
+    const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    return md.pd == CPD_PD_PMB && md.fracture && m.vol_sums && m.lean_list && m.nlean > 0 &&
+           mixed_variant() == 9 && lean_bytes <= 48 * 1024 && p.n - p.frozen >= split_min_rows();
+}
+
+// Sum of W_i vol_i and of phi_i over rows [frozen, n), per block.
+__global__ void __launch_bounds__(kBlock)
+    k_row_totals(ParticleView p, double* partials)
+{
+    __shared__ double s_w[kBlock];
+    __shared__ double s_d[kBlock];
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    s_w[threadIdx.x] = i < p.n ? p.W[i] * p.vol[i] : 0.0;
+    s_d[threadIdx.x] = i < p.n ? p.phi[i] : 0.0;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s_w[threadIdx.x] += s_w[threadIdx.x + w];
+            s_d[threadIdx.x] += s_d[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x + 0] = s_w[0];
+        partials[2 * blockIdx.x + 1] = s_d[0];
+    }
+}
+
+int launch_energy_rest_and_totals(const ParticleView& p, const EllView& nl, const Model& md,
+                                  const MixedState& m, double* partials, int capacity,
+                                  int* launches, cudaStream_t st)
+{
+    *launches = 0;
+    const int64_t rows = p.n - p.frozen;
+    const int nb = blocks_for(rows);
+    const int gr = (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32));
+    if (nb > capacity || gr > capacity) return -1;
+    if (gr > 0) {
+        const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
+        const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
+        const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+        k_energy_mixed<false, 0, true, true, false><<<gr, kBlock, sb, st>>>(
+            p, nl, mv, e, partials, m.rest_list, m.nrest, m.vol_sums);
+        ++*launches;
+    }
+    k_row_totals<<<nb, kBlock, 0, st>>>(p, partials);
+    ++*launches;
+    return nb;
 }
 
 int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,

@@ -119,6 +119,8 @@ _DP = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "cpd_abi_version": (_I32, []),
     "cpd_state_bytes": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "cpd_step_energy": (_I32, [_P, _I32, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double)]),
     "cpd_save_state": (_I32, [_P, ctypes.c_void_p, ctypes.c_uint64]),
     "cpd_load_state": (_I32, [_P, ctypes.c_void_p, ctypes.c_uint64]),
     "cpd_last_error": (ctypes.c_char_p, []),
@@ -309,6 +311,14 @@ class System:
     def step(self, num_steps):
         """Queue num_steps steps (asynchronous)."""
         self._check(self._lib.cpd_step(self._h, int(num_steps)))
+
+    def step_energy(self, num_steps):
+        """num_steps steps, then the (strain energy, damage) totals of the
+        final state (cpd_step_energy: the Solver's output step)."""
+        w, d = _D(), _D()
+        self._check(self._lib.cpd_step_energy(self._h, int(num_steps), ctypes.byref(w),
+                                              ctypes.byref(d)))
+        return w.value, d.value
 
     def run(self, num_steps):
         self.step(num_steps)

@@ -1218,14 +1218,21 @@ class Solver {
         }
         const auto t_start = std::chrono::steady_clock::now();
         for (int step = 1; step <= num_steps; step++) {
+            bool energy_done = false;
             if (!stage_) {
                 // No device functor runs between stages: the steps up to the
                 // next output step go to the library in one call (its fused
-                // step where the model has one; bit-identical to the stages).
+                // step where the model has one; bit-identical to the stages),
+                // with the output step's energy when it ends on one.
                 const int next_out = std::min(num_steps, (step / output_frequency + 1) *
                                                              output_frequency);
                 const int last = step % output_frequency == 0 ? step : next_out;
-                cpdCheck(cpd_step(d->sys, last - step + 1));
+                if (last % output_frequency == 0) {
+                    cpdCheck(cpd_step_energy(d->sys, last - step + 1, &last_W_, &last_D_));
+                    energy_done = true;
+                } else {
+                    cpdCheck(cpd_step(d->sys, last - step + 1));
+                }
                 step = last;
             } else {
                 const double time = step * dt;
@@ -1238,7 +1245,7 @@ class Solver {
             }
             if (step % output_frequency == 0) {
                 const double time = step * dt;
-                cpdCheck(cpd_compute_energy(d->sys, &last_W_, &last_D_));
+                if (!energy_done) cpdCheck(cpd_compute_energy(d->sys, &last_W_, &last_D_));
                 d->compute_stress();
                 const bool write = detail::particle_output_enabled();
                 if (sizeof...(Out) > 0 || d->with_stress || write) d->refresh_mirrors();

@@ -280,6 +280,16 @@ cpd_status cpd_init(cpd_system* sys);
  * boundary-condition operation); results are bit-identical to the separate
  * stages of cpd_step_stage. */
 cpd_status cpd_step(cpd_system* sys, int32_t num_steps);
+/* num_steps steps, then the strain energy and damage totals of the final
+ * state: the Solver's output step (CabanaPD_Solver.hpp:479-494) in one
+ * call, the same as cpd_step followed by cpd_compute_energy (W and phi
+ * fields included; damage bit for bit, strain energy within FP32 rounding
+ * of its bond terms on the MIXED path). On the MIXED PMB fracture fused
+ * step of a one-volume particle set, the last step's bond pass also forms
+ * the energy of its lean rows, so only the other rows take the separate
+ * energy pass. Waits for the stream. */
+cpd_status cpd_step_energy(cpd_system* sys, int32_t num_steps, double* total_strain_energy,
+                           double* total_damage);
 cpd_status cpd_synchronize(cpd_system* sys);
 /* One stage of one time step, for callers that run their own device code
  * between stages (CabanaPD_Solver.hpp:332-375 order): INITIAL_HALF is the

@@ -538,21 +538,51 @@ def test_fragmenting_cylinder_fp64_and_mixed(cuda, oracle):
             assert np.array_equal(m.get(fld), g.get(fld)), fld
 
 
+
+def test_step_energy_equals_step_then_energy(cuda, oracle):
+    """cpd_step_energy (the Solver's output step in one call; on the mixed
+    split form with one particle volume the lean rows' energy comes out of
+    the last step's bond pass) against cpd_step + cpd_compute_energy on the
+    same system: same states bit for bit, damage field and total bit for
+    bit, strain energy within FP32 rounding of its terms; and the oracle's
+    totals."""
+    prob = P.plate_impact(num_cells=(96, 48, 6), steps=120, v0=60.0)
+    a = cuda.System(dict(prob["params"], precision=MIXED))
+    b = cuda.System(dict(prob["params"], precision=MIXED))
+    o = oracle.OracleSystem(prob["params"])
+    for s in (a, b, o):
+        P.setup(s, prob)
+    for _ in range(6):
+        wa, da = a.step_energy(20)
+        b.step(20)
+        wb, db = b.compute_energy()
+        o.run(20)
+        wo, do = o.compute_energy()
+        for fld in ("u", "v", "f", "phi"):
+            assert np.array_equal(a.get(fld), b.get(fld)), fld
+        assert np.array_equal(a.neighbors()[2], b.neighbors()[2])
+        assert _nrel(a.get("W"), b.get("W")) <= 1e-6
+        assert _rel(da, db) <= 1e-14 and _rel(wa, wb) <= 1e-6
+        assert _rel(da, do) <= 1e-12 and _rel(wa, wo) <= 1e-6
+    assert da > 0
+
+
 def test_split_forms_on_small_systems():
     """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
     of full-stencil and shared-subset warps, the general kernels over the
-    rest) run on systems of 2^20 rows and more; a child process forces them
-    onto the small mixed test systems (CPD_SPLIT_MIN_ROWS=0) and runs the
-    mixed parity tests there with the same bars."""
+    rest, and the energy fused into the lean kernel by cpd_step_energy) run
+    on systems of 2^20 rows and more; a child process forces them onto the
+    small mixed test systems (CPD_SPLIT_MIN_ROWS=0) and runs the mixed
+    parity tests there with the same bars."""
     import os
     import subprocess
     import sys
     here = os.path.dirname(os.path.abspath(__file__))
     env = dict(os.environ, CPD_SPLIT_MIN_ROWS="0")
     sel = ("test_mixed_plate_impact or test_mixed_lps_random_notches or test_mixed_elastic_wave"
-           " or test_plate_with_frozen_particles")
+           " or test_plate_with_frozen_particles or test_step_energy_equals_step_then_energy")
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
                         os.path.join(here, "test_gpu_parity.py"), "-k", sel],
                        env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
-    assert "6 passed" in r.stdout, r.stdout[-500:]
+    assert "7 passed" in r.stdout, r.stdout[-500:]
