@@ -411,6 +411,7 @@ def measure_other(name, device, stream, steps, warmup):
     return out
 
 
+E2E_JOBS = 3
 OTHER_STEPS = {"lps": 20, "plate_1p2m": 100, "wave": 100, "dem": 50}
 
 
@@ -459,9 +460,9 @@ def run_gpu(args, world, rank, local, pg):
     systems.clear()
 
     if args.skip_e2e:
-        e2e_value, h2d, d2h = None, None, None
+        e2e_value, h2d, d2h, job_ms = None, None, None, None
     else:
-        e2e_value, h2d, d2h = run_e2e(args, prob, device, stream, pg, total_bonds, head)
+        e2e_value, h2d, d2h, job_ms = run_e2e(args, prob, device, stream, pg, total_bonds, head)
     if rank != 0:
         return
     line = {
@@ -480,7 +481,9 @@ def run_gpu(args, world, rank, local, pg):
         "e2e": ({"value": e2e_value, "unit": "bond-updates/s",
                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                  "job": ("upload + neighbour build + prenotch + init + steps + "
-                         "energy/damage read every 10 steps + download u")}
+                         "energy/damage read every 10 steps + download u"),
+                 "jobs": len(job_ms), "job_ms": job_ms,
+                 "statistic": "median over fresh systems"}
                 if e2e_value is not None else None),
         "gpu_launches": res[head]["launches"],
         "clocks": res[head]["clocks"],
@@ -627,40 +630,45 @@ def run_e2e(args, prob, device, stream, pg, total_bonds, prec):
     hnf = pinned(prob["nofail"].astype(np.int32))
     hv0 = pinned(prob["v0"])
     hu = pinned(np.zeros_like(prob["x"]))
-    torch.cuda.synchronize(device)
-    barrier(pg, device)
-    t0 = time.perf_counter()
-    e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
-    e2.set_stream(stream.cuda_stream)
-    s0 = torch.cuda.Event(enable_timing=True)
-    s1 = torch.cuda.Event(enable_timing=True)
-    s0.record(stream)
-    e2.set_particles(hx, hvol, hrho, hnf)
-    e2.set_state(None, hv0)
-    e2.build_neighbors()
-    e2.prenotch(*prob["notches"])
-    for kind, comp, idx, vals in prob["bcs"]:
-        e2.add_bc(kind, idx, vals, component=comp)
-    e2.init()
-    done = 0
-    reads = 0
-    while done < args.steps:
-        k = min(10, args.steps - done)
-        e2.step_energy(k)  # k steps, then the output step's energy / damage totals
-        done += k
-        reads += 1
-    e2.get("u", out=hu)
-    s1.record(stream)
-    torch.cuda.synchronize(device)
-    wall = time.perf_counter() - t0
-    e2e_ms = max(s0.elapsed_time(s1), 1e3 * wall)
-    e2e_ms = reduce_max(pg, e2e_ms, device)
-    del e2
+    def one_job():
+        torch.cuda.synchronize(device)
+        barrier(pg, device)
+        t0 = time.perf_counter()
+        e2 = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION[prec]))
+        e2.set_stream(stream.cuda_stream)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        e2.set_particles(hx, hvol, hrho, hnf)
+        e2.set_state(None, hv0)
+        e2.build_neighbors()
+        e2.prenotch(*prob["notches"])
+        for kind, comp, idx, vals in prob["bcs"]:
+            e2.add_bc(kind, idx, vals, component=comp)
+        e2.init()
+        done = 0
+        reads = 0
+        while done < args.steps:
+            k = min(10, args.steps - done)
+            e2.step_energy(k)  # k steps, then the output step's energy / damage totals
+            done += k
+            reads += 1
+        e2.get("u", out=hu)
+        s1.record(stream)
+        torch.cuda.synchronize(device)
+        wall = time.perf_counter() - t0
+        ms = reduce_max(pg, max(s0.elapsed_time(s1), 1e3 * wall), device)
+        e2.close()
+        return ms, reads
+
+    # The median of E2E_JOBS jobs, each from a fresh system.
+    jobs = [one_job() for _ in range(E2E_JOBS)]
+    e2e_ms = float(np.median([ms for ms, _ in jobs]))
+    reads = jobs[0][1]
     h2d = (hx.nbytes + hvol.nbytes + hrho.nbytes + hnf.nbytes + hv0.nbytes) / args.steps
     d2h = (hu.nbytes + 16 * reads) / args.steps
     e2e_value = total_bonds * args.steps / (e2e_ms / 1e3)
-
-    return e2e_value, h2d, d2h
+    return e2e_value, h2d, d2h, [ms for ms, _ in jobs]
 
 
 def main():
