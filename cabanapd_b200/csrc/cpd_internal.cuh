@@ -310,6 +310,12 @@ struct MixedState {
     // All particles of one volume v: vol_sums[k] = v + v + ... (k terms,
     // summed in order), the FP64 volume sum of any k bonds; else nullptr.
     double* vol_sums = nullptr;
+    double vol_uniform = 0;
+    // LPS with one particle volume and no frozen particles: per particle the
+    // FP32 split of u with the force factors a, b in the w lanes (written by
+    // the m / theta pass, read by the lean force kernel in place of u2 and
+    // ab), so a neighbour is one 32-byte record.
+    MixedU* u2ab = nullptr;
 };
 // lps: set up the LPS mixed kernels too (lps_ok, ab).
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,

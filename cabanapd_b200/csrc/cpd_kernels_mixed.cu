@@ -966,6 +966,7 @@ struct MixedLps {
     double bbc;
     double theta_coeff, s_coeff;
     int ntab;
+    float vol;  // the particle volume when the packed records are used
 };
 
 // omega xi^2 of a stencil entry (force_models/CabanaPD_LPS.hpp:85-106) and
@@ -986,7 +987,7 @@ template <bool FRACTURE, int INFL, bool WITH_M>
 __global__ void __launch_bounds__(kBlock, 4)
     k_lps_mtheta_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
                        float2* __restrict__ ab, const int32_t* __restrict__ wlist,
-                       int64_t wcount)
+                       int64_t wcount, MixedU* __restrict__ pack)
 {
     __shared__ MixedStencil tab[kMixedGeneric];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
@@ -1065,6 +1066,9 @@ __global__ void __launch_bounds__(kBlock, 4)
     p.lps_a[i] = a;
     p.lps_b[i] = b;
     ab[i] = make_float2((float)a, (float)b);
+    if (pack)
+        pack[i] = MixedU{make_float4(uhi.x, uhi.y, uhi.z, (float)a),
+                         make_float4(uli.x, uli.y, uli.z, (float)b)};
 }
 
 __device__ __forceinline__ bool lps_critical(float s, bool nofail_i, const MixedLps& md,
@@ -1205,7 +1209,8 @@ constexpr int kThetaUnroll = 4;
 template <bool FRACTURE, int INFL, bool WITH_M>
 __global__ void __launch_bounds__(kBlock, 3)
     k_lps_mtheta_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,
-                      float2* __restrict__ ab, const int32_t* __restrict__ wlist, int64_t wcount)
+                      float2* __restrict__ ab, const int32_t* __restrict__ wlist, int64_t wcount,
+                      MixedU* __restrict__ pack)
 {
     extern __shared__ MixedStencil smem[];
     int64_t warp;
@@ -1248,11 +1253,16 @@ __global__ void __launch_bounds__(kBlock, 3)
     p.lps_a[i] = a;
     p.lps_b[i] = b;
     ab[i] = make_float2((float)a, (float)b);
+    if (pack)
+        pack[i] = MixedU{make_float4(ui.hi.x, ui.hi.y, ui.hi.z, (float)a),
+                         make_float4(ui.lo.x, ui.lo.y, ui.lo.z, (float)b)};
 }
 
 // One LPS bond of the lean force (the break rule of lps_critical: only the
 // row's no-fail flag counts).
-template <bool FRACTURE, int INFL>
+// PACK: u2_i points into the packed records (a, b in the w lanes; the
+// volume is md.vol), and ab_i is not read.
+template <bool FRACTURE, int INFL, bool PACK = false>
 __device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
                                                const MixedU* __restrict__ u2_i,
                                                const float2* __restrict__ ab_i, float2 abi,
@@ -1261,7 +1271,8 @@ __device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
                                                float2& cxy, float& cz)
 {
     const MixedU uj = u2_i[t.delta];
-    const float2 abj = ab_i[t.delta];
+    const float2 abj = PACK ? f2(uj.hi.w, uj.lo.w) : ab_i[t.delta];
+    const float vol_j = PACK ? md.vol : uj.hi.w;
     MixedBond2 bd;
     lean_geometry(t, uj, ri, bd);
     if (FRACTURE && on && bd.s >= md.s_lo && !ri.nofail) {
@@ -1272,7 +1283,7 @@ __device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
         on = false;
     }
     const float kf = (!FRACTURE || on)
-                         ? (abi.x + abj.x + bd.s * (abi.y + abj.y)) * lps_oxi<INFL>(t) * uj.hi.w *
+                         ? (abi.x + abj.x + bd.s * (abi.y + abj.y)) * lps_oxi<INFL>(t) * vol_j *
                                bd.rinv
                          : 0.f;
     cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
@@ -1282,11 +1293,14 @@ __device__ __forceinline__ void lps_force_bond(const MixedStencil& t,
 // 8-bond chunks at 4 blocks of 256 per SM (60 registers). Measured beside it
 // on the 8.0 M-particle LPS box, no faster: 3 blocks, 4-bond chunks at 4 or
 // 5 blocks.
-template <bool FRACTURE, int INFL>
+// PACK: the neighbours' records come from pack (the m / theta pass's
+// packed copy), one 32-byte load per bond instead of u2 and ab.
+template <bool FRACTURE, int INFL, bool PACK = false>
 __global__ void __launch_bounds__(kBlock, 4)
     k_lps_force_lean(ParticleView p, EllView nl, MixedView mv, MixedLps md,
                      const float2* __restrict__ ab, StepEpilogue ep,
-                     const int32_t* __restrict__ wlist, int64_t wcount)
+                     const int32_t* __restrict__ wlist, int64_t wcount,
+                     const MixedU* __restrict__ pack)
 {
     extern __shared__ MixedStencil smem[];
     int64_t warp;
@@ -1296,12 +1310,13 @@ __global__ void __launch_bounds__(kBlock, 4)
     const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
     const int64_t np = p.npad;
-    const MixedU ui = mv.u2[i];
+    const MixedU ui = PACK ? pack[i] : mv.u2[i];
+    const bool nofail_i = FRACTURE ? (PACK ? p.nofail[i] != 0 : ui.lo.w != 0.f) : false;
     const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z,
-                      FRACTURE ? (ui.lo.w != 0.f) : false};
-    const MixedU* __restrict__ u2_i = mv.u2 + i;
+                      nofail_i};
+    const MixedU* __restrict__ u2_i = (PACK ? pack : mv.u2) + i;
     const float2* __restrict__ ab_i = ab + i;
-    const float2 abi = ab[i];
+    const float2 abi = PACK ? f2(ui.hi.w, ui.lo.w) : ab[i];
     double f[3] = {0.0, 0.0, 0.0};
     for (int base = 0; base < wcnt; base += 32) {
         const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
@@ -1314,9 +1329,9 @@ __global__ void __launch_bounds__(kBlock, 4)
             float cz = 0.f;
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-                lps_force_bond<FRACTURE, INFL>(wt[base + b + u], u2_i, ab_i, abi, ri,
-                                               (w8 >> u) & 1u, 1u << (b + u), md, clr, pend, cxy,
-                                               cz);
+                lps_force_bond<FRACTURE, INFL, PACK>(wt[base + b + u], u2_i, ab_i, abi, ri,
+                                                     (w8 >> u) & 1u, 1u << (b + u), md, clr, pend,
+                                                     cxy, cz);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
@@ -1325,8 +1340,9 @@ __global__ void __launch_bounds__(kBlock, 4)
             float2 cxy = f2(0.f, 0.f);
             float cz = 0.f;
             for (; b < lim; ++b)
-                lps_force_bond<FRACTURE, INFL>(wt[base + b], u2_i, ab_i, abi, ri, (word >> b) & 1u,
-                                               1u << b, md, clr, pend, cxy, cz);
+                lps_force_bond<FRACTURE, INFL, PACK>(wt[base + b], u2_i, ab_i, abi, ri,
+                                                     (word >> b) & 1u, 1u << b, md, clr, pend,
+                                                     cxy, cz);
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
@@ -1342,8 +1358,8 @@ __global__ void __launch_bounds__(kBlock, 4)
                     float2 cxy = f2(0.f, 0.f);
                     float cz = 0.f;
                     uint32_t none = 0;
-                    lps_force_bond<false, INFL>(t, u2_i, ab_i, abi, ri, true, 0u, md, none, none,
-                                                cxy, cz);
+                    lps_force_bond<false, INFL, PACK>(t, u2_i, ab_i, abi, ri, true, 0u, md, none,
+                                                      none, cxy, cz);
                     f[0] += (double)cxy.x;
                     f[1] += (double)cxy.y;
                     f[2] += (double)cz;
@@ -1673,7 +1689,7 @@ int mixed_variant()
 void free_mixed(MixedState& m, cudaStream_t st)
 {
     void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
-                    m.ab, m.lean_list, m.rest_list, m.vol_sums};
+                    m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
@@ -1725,6 +1741,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
             CPD_TRY(cudaMemcpyAsync(m.vol_sums, sums.data(), sizeof(double) * sums.size(),
                                     cudaMemcpyHostToDevice, st));
             m.bytes += sizeof(double) * sums.size();
+            m.vol_uniform = v0;
         }
         double h[3];
         bool lattice = true;
@@ -1818,6 +1835,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                     if (m.lps_ok) {
                         CPD_TRY(dev_alloc(&m.ab, sizeof(float2) * np, st));
                         m.bytes += sizeof(float2) * np;
+                        if (m.vol_sums && p.frozen == 0) {
+                            CPD_TRY(dev_alloc(&m.u2ab, sizeof(MixedU) * np, st));
+                            m.bytes += sizeof(MixedU) * np;
+                        }
                     }
                 }
                 {
@@ -1889,6 +1910,7 @@ MixedLps to_mixed_lps(const Model& md, const MixedState& m)
     l.theta_coeff = md.theta_coeff;
     l.s_coeff = md.s_coeff;
     l.ntab = m.ntab;
+    l.vol = (float)(mixed_wscale(md) * m.vol_uniform);
     return l;
 }
 
@@ -1908,7 +1930,7 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
         const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
 #define CPD_MT_LEAN(F, I, W)                                                                \
     k_lps_mtheta_lean<F, I, W><<<gl, kBlock, lean_bytes, st>>>(p, nl, mv, l, m.ab, m.lean_list, \
-                                                               m.nlean)
+                                                               m.nlean, m.u2ab)
         switch (key) {
         case 0: CPD_MT_LEAN(false, 0, false); break;
         case 1: CPD_MT_LEAN(false, 0, true); break;
@@ -1927,7 +1949,7 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
     const int64_t count = split ? m.nrest : 0;
     const int g = split ? (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32)) : blocks_for(rows);
 #define CPD_MT(F, I, W) \
-    k_lps_mtheta_mixed<F, I, W><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, list, count)
+    k_lps_mtheta_mixed<F, I, W><<<g, kBlock, 0, st>>>(p, nl, mv, l, m.ab, list, count, m.u2ab)
     switch (key) {
     case 0: CPD_MT(false, 0, false); break;
     case 1: CPD_MT(false, 0, true); break;
@@ -1956,9 +1978,13 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     int n = 0;
     if (split) {
         const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
-#define CPD_F_LEAN(F, I)                                                                     \
-    k_lps_force_lean<F, I><<<gl, kBlock, lean_bytes, st>>>(p, nl, mv, l, m.ab, ep, m.lean_list, \
-                                                           m.nlean)
+#define CPD_F_LEAN(F, I)                                                                   \
+    if (m.u2ab)                                                                            \
+        k_lps_force_lean<F, I, true><<<gl, kBlock, lean_bytes, st>>>(                      \
+            p, nl, mv, l, m.ab, ep, m.lean_list, m.nlean, m.u2ab);                         \
+    else                                                                                   \
+        k_lps_force_lean<F, I, false><<<gl, kBlock, lean_bytes, st>>>(                     \
+            p, nl, mv, l, m.ab, ep, m.lean_list, m.nlean, m.u2ab)
         switch (key) {
         case 0: CPD_F_LEAN(false, 0); break;
         case 1: CPD_F_LEAN(false, 1); break;
