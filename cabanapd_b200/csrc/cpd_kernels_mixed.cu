@@ -1583,20 +1583,46 @@ __global__ void __launch_bounds__(kBlock, 4)
                 vol_H = vol_sums[wcnt];
             }
         } else if (!LEAN) {
+            // Per-bond codes: a bond on a stencil entry takes the FP32 form
+            // of the stencil rows (its term into 4-bond FP32 chunks), any
+            // other bond the FP64 form. With one particle volume the damage
+            // sums come from vol_sums, so no FP64 volume is read per bond.
             const double xi0 = p.x[i], xi1 = p.x[np + i], xi2 = p.x[2 * np + i];
             const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
+            const MixedU ui = mv.u2[i];
+            const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z,
+                              -ui.lo.z, false};
+            const MixedU* __restrict__ u2_i = mv.u2 + i;
+            float chunk = 0.f;
+            int in_chunk = 0;
             uint32_t word = 0xffffffffu;
             for (int k = 0; k < cnt; ++k) {
                 if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
-                const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
-                const double vol_j = __ldg(p.vol + j);
                 const bool on = (word >> (k & 31)) & 1u;
-                if (FRACTURE) {
+                if (FRACTURE && !UNI) {
+                    const double vol_j = __ldg(p.vol + __ldg(nl.idx + (int64_t)k * np + i));
                     phi_sum += on ? vol_j : 0.0;
                     vol_H += vol_j;
                 }
                 if (!on) continue;
                 ++intact_n;
+                const uint8_t code = mv.code[(int64_t)k * np + i];
+                if (code < md.ntab) {
+                    const MixedStencil& t = smem[code];
+                    const MixedU uj = u2_i[t.delta];
+                    MixedBond2 bd;
+                    lean_geometry(t, uj, ri, bd);
+                    chunk += LPS ? (INFL == 1 ? t.xi : t.xi2) * uj.hi.w * bd.s * bd.s
+                                 : 0.25f * uj.hi.w * bd.s * bd.s * t.xi;
+                    if (++in_chunk == 4) {
+                        bonds_part += (double)chunk;
+                        chunk = 0.f;
+                        in_chunk = 0;
+                    }
+                    continue;
+                }
+                const int64_t j = __ldg(nl.idx + (int64_t)k * np + i);
+                const double vol_j = __ldg(p.vol + j);
                 const double xx = __ldg(p.x + j) - xi0, xy = __ldg(p.x + np + j) - xi1,
                              xz = __ldg(p.x + 2 * np + j) - xi2;
                 const double rx = xx + (__ldg(p.u + j) - ui0);
@@ -1607,6 +1633,11 @@ __global__ void __launch_bounds__(kBlock, 4)
                 const double sv = (r - xi) / xi;
                 bonds_part += LPS ? (INFL == 1 ? xi : xi * xi) * vol_j * sv * sv
                                   : 0.25 * md.c * vol_j * sv * sv * xi;
+            }
+            bonds_part += (double)chunk;
+            if (FRACTURE && UNI) {
+                phi_sum = vol_sums[intact_n];
+                vol_H = vol_sums[cnt];
             }
         }
         double Wi;
