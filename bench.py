@@ -94,21 +94,29 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Start sampling every 50 ms and wait (up to 3 s) for the first
+        sample, so that sampling covers the timed region that follows."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.index)],
+                 "-lms", "50", "-i", str(self.index)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        t_end = time.perf_counter() + 3.0
+        while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
+        """Summary of the samples read in [t0, t1 + 0.1 s] (host clock; all
+        samples when no window is given)."""
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -119,7 +127,9 @@ class ClockSampler:
         self.thread.join(timeout=5)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for t, line in self.lines:
+            if t0 is not None and not (t0 <= t <= t1 + 0.1):
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -300,11 +310,13 @@ def timed_steps(sys_, stream, args, device, pg, sampler):
         sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
     ev0.record(stream)
     sys_.step(args.steps)
     ev1.record(stream)
     torch.cuda.synchronize(device)
-    clocks = sampler.stop() if sampler else None
+    t1 = time.perf_counter()
+    clocks = sampler.stop(t0, t1) if sampler else None
     barrier(pg, device)
     k_ms, k_n, k_bytes = sys_.kernel_time()
     sys_.set_kernel_timing(False)
