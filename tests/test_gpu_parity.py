@@ -567,6 +567,39 @@ def test_step_energy_equals_step_then_energy(cuda, oracle):
     assert da > 0
 
 
+
+@pytest.mark.parametrize("model", ["pmb", "lps"])
+def test_mixed_with_unequal_volumes(cuda, oracle, model):
+    """Particle volumes that differ (by up to 1e-3, seeded): the mixed path
+    without its one-volume shortcuts (damage sums by FP64 volume gathers,
+    LPS neighbour factors from their own array), against the oracle with
+    the mixed bars; the output step in one call equals step + energy."""
+    if model == "pmb":
+        prob = P.plate_impact(num_cells=(96, 48, 6), steps=80, v0=60.0)
+    else:
+        prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
+        prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
+    rng = np.random.Generator(np.random.PCG64(11))
+    prob["vol"] = prob["vol"] * (1.0 + 1e-3 * rng.random(prob["vol"].size))
+    g, o = _pair_mixed(cuda, oracle, prob)
+    b = cuda.System(dict(prob["params"], precision=MIXED))
+    P.setup(b, prob)
+    for _ in range(3):
+        wg, dg = g.step_energy(20)
+        b.step(20)
+        wb, db = b.compute_energy()
+        o.run(20)
+        wo, do = o.compute_energy()
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        assert _nrel(g.get("u"), o.get("u")) <= 1e-6
+        for fld in ("v", "f"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-5, fld
+        assert np.array_equal(g.get("phi"), o.get("phi"))
+        assert _rel(dg, do) <= 1e-12 and _rel(wg, wo) <= 1e-6
+        assert (wg, dg) == (wb, db)
+    assert (o.neighbors()[2] == 0).sum() > 0
+
+
 def test_split_forms_on_small_systems():
     """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
     of full-stencil and shared-subset warps, the general kernels over the
@@ -580,9 +613,10 @@ def test_split_forms_on_small_systems():
     here = os.path.dirname(os.path.abspath(__file__))
     env = dict(os.environ, CPD_SPLIT_MIN_ROWS="0")
     sel = ("test_mixed_plate_impact or test_mixed_lps_random_notches or test_mixed_elastic_wave"
-           " or test_plate_with_frozen_particles or test_step_energy_equals_step_then_energy")
+           " or test_plate_with_frozen_particles or test_step_energy_equals_step_then_energy"
+           " or test_mixed_with_unequal_volumes")
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
                         os.path.join(here, "test_gpu_parity.py"), "-k", sel],
                        env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
-    assert "7 passed" in r.stdout, r.stdout[-500:]
+    assert "9 passed" in r.stdout, r.stdout[-500:]
