@@ -39,7 +39,15 @@
  *   cpd_init                 Solver::init(bc[, prenotch]) (CabanaPD_Solver.hpp:229-297)
  *   cpd_step                 Solver::runStep(step, bc) x num_steps
  *                            (CabanaPD_Solver.hpp:332-375)
+ *   cpd_step_energy          runStep x num_steps, then the output step's
+ *                            computeEnergy (CabanaPD_Solver.hpp:479-494)
  *   cpd_download             Particles::slice*() + deep_copy to host
+ *
+ * Entry points without a reference counterpart (each says so where it is
+ * declared): cpd_step_stage, cpd_device_field, cpd_set_stream, the kernel
+ * timing calls, cpd_compute_energy_noalloc, the state snapshots
+ * (cpd_state_bytes / cpd_save_state / cpd_load_state), and the job server
+ * (cpd_job_*, cpd_server_*).
  *
  * Errors: every call returns a cpd_status; cpd_last_error() gives the
  * message of the last failure on the calling thread. The reference throws
