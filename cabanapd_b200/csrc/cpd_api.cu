@@ -1241,16 +1241,39 @@ cpd_status cpd_init(cpd_system* s)
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     CPD_OK_OR_RETURN(refresh_mixed_u(s));
+    // Where the mixed PMB split form applies, the initial force pass also
+    // forms the energy of its lean rows, as an output step does.
+    const bool fuse_energy = has_pd(s) && use_mixed(s) &&
+                             mixed_force_fuses_energy(view(s), s->md, s->mixed);
     if (has_pd(s)) {
         // Weighted volume once here without fracture (Solver.hpp:235-239),
         // inside updateForce with fracture (Solver.hpp:466-470): once either way.
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, true));
-        CPD_OK_OR_RETURN(pd_force(s));
+        if (fuse_energy) {
+            StepEpilogue ep;
+            ep.energy_vol_sums = s->mixed.vol_sums;
+            CPD_OK_OR_RETURN(pd_force_on(s, view(s), s->mixed, ep));
+        } else {
+            CPD_OK_OR_RETURN(pd_force(s));
+        }
     } else if (has_contact(s)) {
         CPD_OK_OR_RETURN(contact_force(s, true));
     }
     PhaseTrace tr("init");
-    if (has_pd(s)) CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
+    // Solver.hpp:240-242: the energy and damage of the initial state (the
+    // fields; the totals are not kept).
+    if (fuse_energy) {
+        const int nb = energy_blocks(s->n - s->frozen);
+        CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
+        int l = 0;
+        const int rows = launch_energy_rest_and_totals(view(s), pd_view(s), s->md, s->mixed,
+                                                       s->red, nb + 1, &l, s->stream);
+        s->launches += l;
+        if (rows < 0) return set_error(CPD_ERR_CUDA, "energy totals: reduction buffer too small");
+        CPD_CUDA(cudaGetLastError());
+    } else if (has_pd(s)) {
+        CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
+    }
     tr.mark("energy", s->stream);
     CPD_OK_OR_RETURN(apply_force_bcs(s));
     CPD_OK_OR_RETURN(prepare_fused(s));

@@ -552,6 +552,12 @@ def test_step_energy_equals_step_then_energy(cuda, oracle):
     o = oracle.OracleSystem(prob["params"])
     for s in (a, b, o):
         P.setup(s, prob)
+    # The initial state's fields from init (the force pass forms the lean
+    # rows' energy) against the energy pass on the same state.
+    w0, phi0 = a.get("W"), a.get("phi")
+    a.compute_energy()
+    assert np.array_equal(phi0, a.get("phi"))
+    assert _nrel(w0, a.get("W")) <= 1e-6
     for _ in range(6):
         wa, da = a.step_energy(20)
         b.step(20)
