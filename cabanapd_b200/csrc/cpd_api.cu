@@ -168,6 +168,7 @@ struct cpd_system {
     int32_t nbc = 0;
     // Second displacement buffers of the fused step.
     double* u_alt = nullptr;
+    double* v_alt = nullptr;  // contact-only fused step: second velocity buffer
     MixedU* u2_alt = nullptr;
     bool neighbors_built = false;
     bool initialized = false;
@@ -262,6 +263,8 @@ void free_particles(cpd_system* s)
     free_bc_program(s);
     if (s->u_alt) dev_free(s->u_alt, s->stream);
     s->u_alt = nullptr;
+    if (s->v_alt) dev_free(s->v_alt, s->stream);
+    s->v_alt = nullptr;
     if (s->u2_alt) dev_free(s->u2_alt, s->stream);
     s->u2_alt = nullptr;
     free_neighbor_list(s->pd, s->stream);
@@ -360,15 +363,18 @@ cpd_status ensure_reduction(cpd_system* s, int blocks)
     return CPD_OK;
 }
 
-cpd_status rebuild_contact(cpd_system* s, double cutoff)
+// disp: the current displacement (the system's u unless a fused step holds
+// it in its second buffer).
+cpd_status rebuild_contact(cpd_system* s, double cutoff, const double* disp = nullptr)
 {
+    if (!disp) disp = s->u;
     std::string err;
-    int l = build_neighbor_list(s->x, s->u, s->n, s->npad, s->frozen, cutoff, s->perm,
+    int l = build_neighbor_list(s->x, disp, s->n, s->npad, s->frozen, cutoff, s->perm,
                                 false, s->contact, s->stream, err);
     if (l < 0) return set_error(CPD_ERR_CUDA, "contact neighbour build: " + err);
     s->launches += l;
     // CabanaPD_Neighbor.hpp:127-130: displacement at the last build.
-    CPD_CUDA(cudaMemcpyAsync(s->u_neigh, s->u, sizeof(double) * 3 * s->npad,
+    CPD_CUDA(cudaMemcpyAsync(s->u_neigh, disp, sizeof(double) * 3 * s->npad,
                              cudaMemcpyDeviceToDevice, s->stream));
     s->rebuilds++;
     s->steps_since_rebuild = 0;
@@ -623,9 +629,17 @@ bool fused_steps_enabled()
     return on;
 }
 
+// Contact alone with a fixed rebuild interval: the host knows when the list
+// is rebuilt, so the steps between rebuilds need no read-back.
+bool contact_fusable(const cpd_system* s)
+{
+    return !has_pd(s) && has_contact(s) && s->params.rebuild_every > 0;
+}
+
 bool fusable_kind(const cpd_system* s)
 {
-    return has_pd(s) && !has_contact(s) && (use_fast(s) || use_mixed(s));
+    return (has_pd(s) && !has_contact(s) && (use_fast(s) || use_mixed(s))) ||
+           contact_fusable(s);
 }
 
 // Builds what the fused step needs (second displacement buffers, the row
@@ -637,6 +651,8 @@ cpd_status prepare_fused(cpd_system* s)
     if (s->bc_prog == 0) CPD_OK_OR_RETURN(build_bc_program(s));
     if (s->bc_prog != 1) return CPD_OK;
     if (!s->u_alt) CPD_CUDA(dev_alloc(&s->u_alt, sizeof(double) * 3 * s->npad, s->stream));
+    if (contact_fusable(s) && !s->v_alt)
+        CPD_CUDA(dev_alloc(&s->v_alt, sizeof(double) * 3 * s->npad, s->stream));
     if (use_mixed(s) && !s->u2_alt)
         CPD_CUDA(dev_alloc(&s->u2_alt, sizeof(MixedU) * s->npad, s->stream));
     CPD_CUDA(cudaStreamSynchronize(s->stream));
@@ -647,7 +663,7 @@ cpd_status prepare_fused(cpd_system* s)
 bool fused_ready(const cpd_system* s)
 {
     return fused_steps_enabled() && fusable_kind(s) && s->bc_prog == 1 && s->u_alt &&
-           (!use_mixed(s) || s->u2_alt);
+           (!use_mixed(s) || s->u2_alt) && (!contact_fusable(s) || s->v_alt);
 }
 
 // num_steps steps as: first half step, then one bond kernel per step whose
@@ -657,8 +673,70 @@ bool fused_ready(const cpd_system* s)
 // step end in the system's own arrays.
 // energy_last: the last step's lean kernel also writes W and phi of its rows
 // (mixed_force_fuses_energy must hold).
+// Contact alone (fixed rebuild interval): first half step, then per step the
+// list rebuild when due (on the current displacement) and one contact kernel
+// whose epilogue applies the boundary conditions, the second half step and
+// the next first half step. Neighbours read velocities (damping) as well as
+// displacements, so both alternate between two buffers; the velocity ends in
+// the system's array (copied back after an odd number of steps).
+cpd_status step_fused_contact(cpd_system* s, int32_t num_steps)
+{
+    const bool start_alt = ((num_steps - 1) & 1) != 0;
+    double* ucur = start_alt ? s->u_alt : s->u;
+    double* unxt = start_alt ? s->u : s->u_alt;
+    double* vcur = s->v;
+    double* vnxt = s->v_alt;
+    const size_t vec = sizeof(double) * 3 * (size_t)s->npad;
+    if (s->frozen > 0) {
+        const size_t bytes = sizeof(double) * (size_t)s->frozen;
+        for (int d = 0; d < 3; ++d) {
+            CPD_CUDA(cudaMemcpyAsync(s->u_alt + (size_t)d * s->npad, s->u + (size_t)d * s->npad,
+                                     bytes, cudaMemcpyDeviceToDevice, s->stream));
+            CPD_CUDA(cudaMemcpyAsync(s->v_alt + (size_t)d * s->npad, s->v + (size_t)d * s->npad,
+                                     bytes, cudaMemcpyDeviceToDevice, s->stream));
+        }
+    }
+    const ParticleView p = view(s);
+    CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, false, nullptr, 0, ucur, s->stream));
+    StepEpilogue ep;
+    ep.dt = s->params.dt;
+    ep.half_dt = 0.5 * s->params.dt;
+    ep.bc_bits = s->bc_bits;
+    ep.bc_row = s->bc_row;
+    ep.bc_keep = s->bc_keep;
+    ep.bc_add = s->bc_add;
+    ep.nbc = s->nbc;
+    for (int32_t k = 0; k < num_steps; ++k) {
+        s->steps_since_rebuild++;
+        // CabanaPD_Neighbor.hpp:107-132, every rebuild_every steps.
+        if (s->steps_since_rebuild >= s->params.rebuild_every)
+            CPD_OK_OR_RETURN(rebuild_contact(s, 2.0 * s->md.radius + s->md.radius_extend, ucur));
+        ParticleView pk = p;
+        pk.u = ucur;
+        pk.v = vcur;
+        ep.mode = k + 1 < num_steps ? 2 : 1;
+        ep.u_next = unxt;
+        ep.v_next = vnxt;
+        cudaEvent_t e0;
+        CPD_OK_OR_RETURN(timed_begin(s, e0));
+        if (s->params.precision == CPD_MIXED)
+            CPD_LAUNCHED(launch_hertz_force_mixed(pk, s->contact.view(), s->md, true, s->stream,
+                                                  &ep));
+        else
+            CPD_LAUNCHED(launch_hertz_force(pk, s->contact.view(), s->md, true, s->stream, &ep));
+        CPD_OK_OR_RETURN(timed_end(s, e0));
+        std::swap(vcur, vnxt);
+        if (k + 1 < num_steps) std::swap(ucur, unxt);
+    }
+    // The last kernel wrote the final velocity into vcur (after the swap).
+    if (vcur != s->v)
+        CPD_CUDA(cudaMemcpyAsync(s->v, vcur, vec, cudaMemcpyDeviceToDevice, s->stream));
+    return CPD_OK;
+}
+
 cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false)
 {
+    if (contact_fusable(s)) return step_fused_contact(s, num_steps);
     const bool mixed = use_mixed(s);
     const bool start_alt = ((num_steps - 1) & 1) != 0;
     double* ucur = start_alt ? s->u_alt : s->u;

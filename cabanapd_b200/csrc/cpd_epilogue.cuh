@@ -5,9 +5,10 @@
 // kernels + two integrator kernels (CabanaPD_Solver.hpp:332-375 order,
 // CabanaPD_Integrate.hpp:89-145 arithmetic).
 //
-// Neighbours of other rows may still be reading this row's displacement, so
-// the next displacement goes to a second buffer (u_next); the caller swaps
-// buffers between steps. Every operation is a separately rounded IEEE
+// Neighbours of other rows may still be reading this row's displacement
+// (and, in contact steps, its velocity), so the next displacement goes to a
+// second buffer (u_next, and v_next when set); the caller swaps buffers
+// between steps. Every operation is a separately rounded IEEE
 // operation in the order of the separate kernels (k_force_bc, k_vv_final,
 // k_vv_initial), so fused and separate steps give identical bits.
 #pragma once
@@ -69,10 +70,11 @@ __device__ __forceinline__ void step_epilogue(const ParticleView& p, const StepE
     const double hm = __ddiv_rn(ep.half_dt, p.rho[i]);
     double v[3];
     for (int d = 0; d < 3; ++d) v[d] = __dadd_rn(p.v[d * np + i], __dmul_rn(hm, f[d]));
+    double* const v_out = ep.v_next ? ep.v_next : p.v;
     if (ep.mode == 1) {
         for (int d = 0; d < 3; ++d) {
             p.f[d * np + i] = f[d];
-            p.v[d * np + i] = v[d];
+            v_out[d * np + i] = v[d];
         }
         return;
     }
@@ -80,7 +82,7 @@ __device__ __forceinline__ void step_epilogue(const ParticleView& p, const StepE
     double u[3];
     for (int d = 0; d < 3; ++d) {
         v[d] = __dadd_rn(v[d], __dmul_rn(hm, f[d]));
-        p.v[d * np + i] = v[d];
+        v_out[d * np + i] = v[d];
         u[d] = __dadd_rn(p.u[d * np + i], __dmul_rn(ep.dt, v[d]));
         ep.u_next[d * np + i] = u[d];
     }

@@ -217,11 +217,13 @@ int launch_pd_energy_fast(const ParticleView& p, const EllView& nl, const Model&
                           double* partials, int nblocks, cudaStream_t st);
 int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Model& md,
                             bool with_m, cudaStream_t st);
+// ep (optional): the contact-only fused step's epilogue instead of storing f.
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
-                       const Model& md, bool reset, cudaStream_t st);
+                       const Model& md, bool reset, cudaStream_t st,
+                       const StepEpilogue* ep = nullptr);
 // Mixed precision (cpd_kernels_mixed.cu): FP64 overlap, FP32 force law.
 int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                             bool reset, cudaStream_t st);
+                             bool reset, cudaStream_t st, const StepEpilogue* ep = nullptr);
 // Normal repulsion over the contact list (exact FP64).
 int launch_repulsion_force(const ParticleView& p, const EllView& nl, const Model& md,
                            bool reset, cudaStream_t st);
@@ -287,6 +289,9 @@ struct StepEpilogue {
     // rows (the energy pass of the state it computes the force of), with
     // the damage sums from this table (MixedState::vol_sums).
     const double* energy_vol_sums = nullptr;
+    // Contact steps: neighbours read this row's velocity during the pass
+    // (Hertz damping), so the new velocity goes to this second buffer.
+    double* v_next = nullptr;
 };
 
 struct MixedState {

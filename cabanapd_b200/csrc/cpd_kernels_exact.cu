@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "cpd_internal.cuh"
+#include "cpd_epilogue.cuh"
 
 namespace cpd {
 namespace {
@@ -448,9 +449,11 @@ __global__ void __launch_bounds__(kBlock)
 // R* = R_i (R_j / (R_i + R_j)), overlap r - (R_i + R_j) and
 // m* = m_i (m_j / (m_i + m_j)), which round to the single-radius values when
 // R_i == R_j.
-template <bool PER_PARTICLE>
+// EPI: a contact-only fused step; the epilogue finishes the row (force BC,
+// half steps, next displacement and velocity into the second buffers).
+template <bool PER_PARTICLE, bool EPI = false>
 __global__ void __launch_bounds__(kBlock, 3)
-    k_hertz_force(ParticleView p, EllView nl, ModelDev md, bool reset)
+    k_hertz_force(ParticleView p, EllView nl, ModelDev md, bool reset, StepEpilogue ep)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -508,6 +511,10 @@ __global__ void __launch_bounds__(kBlock, 3)
         fx += 0.0;
         fy += 0.0;
         fz += 0.0;
+    }
+    if (EPI) {
+        step_epilogue<false>(p, ep, i, fx, fy, fz);
+        return;
     }
     p.f[i] = fx;
     p.f[np + i] = fy;
@@ -874,15 +881,23 @@ int launch_max_partials(const double* partials, int nblocks, double* out,
 }
 
 int launch_hertz_force(const ParticleView& p, const EllView& nl,
-                       const Model& md, bool reset, cudaStream_t st)
+                       const Model& md, bool reset, cudaStream_t st, const StepEpilogue* ep)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
     const ModelDev d = to_dev(md);
-    if (md.per_particle_radius)
-        k_hertz_force<true><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, d, reset);
-    else
-        k_hertz_force<false><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, d, reset);
+    const StepEpilogue e = ep ? *ep : StepEpilogue{};
+    const int g = blocks_for(rows);
+    if (ep) {
+        if (md.per_particle_radius)
+            k_hertz_force<true, true><<<g, kBlock, 0, st>>>(p, nl, d, true, e);
+        else
+            k_hertz_force<false, true><<<g, kBlock, 0, st>>>(p, nl, d, true, e);
+    } else if (md.per_particle_radius) {
+        k_hertz_force<true><<<g, kBlock, 0, st>>>(p, nl, d, reset, e);
+    } else {
+        k_hertz_force<false><<<g, kBlock, 0, st>>>(p, nl, d, reset, e);
+    }
     return 1;
 }
 

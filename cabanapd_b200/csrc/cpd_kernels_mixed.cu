@@ -1412,9 +1412,11 @@ struct HertzMixed {
     double sum_r;                // single-radius model: 2 R
 };
 
-template <bool PER_PARTICLE>
+// EPI: a contact-only fused step; the epilogue finishes the row (force BC,
+// half steps, next displacement and velocity into the second buffers).
+template <bool PER_PARTICLE, bool EPI = false>
 __global__ void __launch_bounds__(kBlock, 3)
-    k_hertz_force_mixed(ParticleView p, EllView nl, HertzMixed md, bool reset)
+    k_hertz_force_mixed(ParticleView p, EllView nl, HertzMixed md, bool reset, StepEpilogue ep)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -1461,6 +1463,10 @@ __global__ void __launch_bounds__(kBlock, 3)
         fx += (double)(coeff * nx);
         fy += (double)(coeff * ny);
         fz += (double)(coeff * nz);
+    }
+    if (EPI) {
+        step_epilogue<false>(p, ep, i, fx, fy, fz);
+        return;
     }
     p.f[i] = fx;
     p.f[np + i] = fy;
@@ -2179,7 +2185,7 @@ int launch_energy_rest_and_totals(const ParticleView& p, const EllView& nl, cons
 }
 
 int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
-                             bool reset, cudaStream_t st)
+                             bool reset, cudaStream_t st, const StepEpilogue* ep)
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
@@ -2190,10 +2196,18 @@ int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Mod
     h.Rs = (float)md.Rs;
     h.coeff_h_n = (float)md.coeff_h_n;
     h.sum_r = 2.0 * md.radius;
-    if (md.per_particle_radius)
-        k_hertz_force_mixed<true><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
-    else
-        k_hertz_force_mixed<false><<<blocks_for(rows), kBlock, 0, st>>>(p, nl, h, reset);
+    const StepEpilogue e = ep ? *ep : StepEpilogue{};
+    const int g = blocks_for(rows);
+    if (ep) {
+        if (md.per_particle_radius)
+            k_hertz_force_mixed<true, true><<<g, kBlock, 0, st>>>(p, nl, h, true, e);
+        else
+            k_hertz_force_mixed<false, true><<<g, kBlock, 0, st>>>(p, nl, h, true, e);
+    } else if (md.per_particle_radius) {
+        k_hertz_force_mixed<true><<<g, kBlock, 0, st>>>(p, nl, h, reset, e);
+    } else {
+        k_hertz_force_mixed<false><<<g, kBlock, 0, st>>>(p, nl, h, reset, e);
+    }
     return 1;
 }
 

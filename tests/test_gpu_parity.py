@@ -226,15 +226,20 @@ def test_linear_lps_fracture_is_lps(cuda, oracle):
 
 
 @pytest.mark.parametrize("precision", [1, 2])
-@pytest.mark.parametrize("problem", ["plate", "lps"])
+@pytest.mark.parametrize("problem", ["plate", "lps", "dem"])
 def test_fused_step_equals_separate_stages(cuda, precision, problem):
     """cpd_step runs one bond kernel per step with the boundary conditions
     and both half steps in its epilogue (alternating displacement buffers);
     the four separate stages of cpd_step_stage give the same bits, for odd and
     even chunk lengths (ForceValue BC on the plate, per-particle ForceAdd
-    traction on the LPS box)."""
+    traction on the LPS box). The compressed DEM packing (contact alone,
+    rebuilt every 10 steps) alternates velocity buffers as well, since the
+    contact damping reads neighbour velocities; its rebuilds fall inside
+    the chunks."""
     if problem == "plate":
         prob = P.plate_impact(num_cells=(96, 48, 6), steps=60, v0=60.0)
+    elif problem == "dem":
+        prob = P.dem_packing(lattice_dims=(16, 16, 8), steps=60, **DEM_CASES["compressed"])
     else:
         prob = P.lps_random_notches(num_cells=(100, 40, 4), steps=60)
         prob["bcs"] = [(k, c, i, v * 25.0) for k, c, i, v in prob["bcs"]]
@@ -247,8 +252,12 @@ def test_fused_step_equals_separate_stages(cuda, precision, problem):
                 b.step_stage(stage)
         for fld in ("u", "v", "f"):
             assert np.array_equal(a.get(fld), b.get(fld)), (chunk, fld)
+        assert np.array_equal(a.neighbors()[1], b.neighbors()[1])
         assert np.array_equal(a.neighbors()[2], b.neighbors()[2])
+        assert a.contact_rebuilds() == b.contact_rebuilds()
     assert a.compute_energy() == b.compute_energy()
+    if problem == "dem":
+        assert a.contact_rebuilds() == 6 and np.any(a.get("f"))
 
 
 def test_errors_are_reported(cuda):
