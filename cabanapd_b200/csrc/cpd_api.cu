@@ -1051,10 +1051,15 @@ cpd_status cpd_build_neighbors(cpd_system* s)
     PhaseTrace tr("neighbors");
     if (has_pd(s)) {
         // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
+        double hmin[3];
+        const bool spacing = wants_mixed(s);
         int l = build_neighbor_list(s->x, nullptr, s->n, s->npad, s->frozen,
                                     s->md.horizon + 1e-14, s->perm, s->md.fracture != 0,
-                                    s->pd, s->stream, err);
+                                    s->pd, s->stream, err, spacing ? hmin : nullptr);
         if (l < 0) return set_error(CPD_ERR_CUDA, "neighbour build: " + err);
+        s->pd.hmin_valid = spacing;
+        if (spacing)
+            for (int d = 0; d < 3; ++d) s->pd.hmin[d] = hmin[d];
         s->launches += l;
         tr.mark("list", s->stream);
         if (wants_mixed(s)) {

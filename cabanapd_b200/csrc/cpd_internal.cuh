@@ -178,6 +178,10 @@ struct NeighborList {
     int32_t* idx = nullptr;
     uint32_t* mu = nullptr;
     int64_t pitch = 0;  // index delta to the next lattice line of a middle row (0: none)
+    // Per axis the smallest nonzero pair separation, from the count pass
+    // when requested (hmin_valid).
+    double hmin[3] = {0, 0, 0};
+    bool hmin_valid = false;
     EllView view() const { return EllView{count, idx, mu, max_n, 1, pitch}; }
 };
 
@@ -358,7 +362,8 @@ struct BuildScratch;
 int build_neighbor_list(const double* pos, const double* disp, int64_t n,
                         int64_t npad, int64_t begin, double cutoff,
                         const int32_t* user_id, bool with_mu,
-                        NeighborList& out, cudaStream_t st, std::string& err);
+                        NeighborList& out, cudaStream_t st, std::string& err,
+                        double* min_spacing = nullptr);
 void free_neighbor_list(NeighborList& nl, cudaStream_t st);
 
 // Layout kernels.

@@ -1762,15 +1762,21 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
         CPD_TRY(dev_alloc(&d_min, 4 * sizeof(unsigned long long), st));
         CPD_TRY(cudaMemsetAsync(d_min, 0x7f, 3 * sizeof(unsigned long long), st));
         CPD_TRY(cudaMemsetAsync(d_min + 3, 0, sizeof(unsigned long long), st));
-        k_min_spacing<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_min);
+        // The neighbour build's count pass may have found the spacing already.
+        if (!pd.hmin_valid) {
+            k_min_spacing<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_min);
+            launches++;
+        }
         k_vol_uniform<<<blocks_for(p.n), kBlock, 0, st>>>(p.vol, p.n, d_min + 3);
-        launches += 2;
+        launches++;
         unsigned long long hmin[4];
         double v0 = 0.0;
         CPD_TRY(cudaMemcpyAsync(hmin, d_min, sizeof(hmin), cudaMemcpyDeviceToHost, st));
         CPD_TRY(cudaMemcpyAsync(&v0, p.vol, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPD_TRY(cudaStreamSynchronize(st));
         CPD_TRY(dev_free(d_min, st));
+        if (pd.hmin_valid)
+            for (int d = 0; d < 3; ++d) std::memcpy(&hmin[d], &pd.hmin[d], sizeof(double));
         if (hmin[3] == 0) {
             // The damage sums of the energy pass then depend only on how
             // many bonds are summed (in order, each adding v).

@@ -15,6 +15,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -136,19 +137,47 @@ __device__ __forceinline__ void visit_neighbors(const double* __restrict__ pos, 
     }
 }
 
+// min_out (optional, 3 slots): per axis the smallest nonzero |x_j - x_i|
+// over the accepted pairs (the bit patterns of non-negative doubles order
+// like the values), the lattice spacing the mixed path's stencil needs.
 __global__ void __launch_bounds__(kBlock)
     k_count(const double* pos, int64_t n, int64_t npad, int64_t begin, Grid g,
-            const int32_t* cell_start, const int32_t* order, double rsqr, int32_t* count)
+            const int32_t* cell_start, const int32_t* order, double rsqr, int32_t* count,
+            unsigned long long* min_out)
 {
+    __shared__ unsigned long long s_min[3][kBlock];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npad) return;
-    if (i < begin || i >= n) {
-        count[i] = 0;
-        return;
+    double m[3] = {INFINITY, INFINITY, INFINITY};
+    if (i < npad) {
+        if (i < begin || i >= n) {
+            count[i] = 0;
+        } else {
+            int32_t cnt = 0;
+            const double xi0 = pos[i], xi1 = pos[npad + i], xi2 = pos[2 * npad + i];
+            visit_neighbors(pos, npad, g, cell_start, order, i, rsqr, [&](int64_t j) {
+                cnt++;
+                if (min_out) {
+                    const double a0 = fabs(pos[j] - xi0), a1 = fabs(pos[npad + j] - xi1),
+                                 a2 = fabs(pos[2 * npad + j] - xi2);
+                    if (a0 > 0.0) m[0] = fmin(m[0], a0);
+                    if (a1 > 0.0) m[1] = fmin(m[1], a1);
+                    if (a2 > 0.0) m[2] = fmin(m[2], a2);
+                }
+            });
+            count[i] = cnt;
+        }
     }
-    int32_t cnt = 0;
-    visit_neighbors(pos, npad, g, cell_start, order, i, rsqr, [&](int64_t) { cnt++; });
-    count[i] = cnt;
+    if (!min_out) return;  // uniform across the grid
+    for (int d = 0; d < 3; ++d) s_min[d][threadIdx.x] = __double_as_longlong(m[d]);
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int d = 0; d < 3; ++d)
+                s_min[d][threadIdx.x] = min(s_min[d][threadIdx.x], s_min[d][threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) atomicMin(min_out + d, s_min[d][0]);
 }
 
 __global__ void k_count_stats(const int32_t* count, int64_t npad, int32_t* block_max,
@@ -340,7 +369,7 @@ __global__ void k_row_pitch(const double* __restrict__ pos, int64_t npad, int64_
 int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t npad,
                         int64_t begin, double cutoff, const int32_t* user_id,
                         bool with_mu, NeighborList& out, cudaStream_t st,
-                        std::string& err)
+                        std::string& err, double* min_spacing)
 {
     int launches = 0;
     PhaseTrace tr("list");
@@ -416,9 +445,17 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     // Row counts.
     if (!out.count) CPD_TRY(dev_alloc(&out.count, sizeof(int32_t) * npad, st));
     const double rsqr = cutoff * cutoff;
+    unsigned long long* d_min = nullptr;
+    if (min_spacing) {
+        CPD_TRY(dev_alloc(&d_min, 3 * sizeof(unsigned long long), st));
+        CPD_TRY(cudaMemsetAsync(d_min, 0x7f, 3 * sizeof(unsigned long long), st));
+    }
     k_count<<<blocks_for(npad), kBlock, 0, st>>>(pos, n, npad, begin, g, cell_start, order,
-                                                 rsqr, out.count);
+                                                 rsqr, out.count, d_min);
     launches++;
+    unsigned long long hmin[3] = {0, 0, 0};
+    if (d_min)
+        CPD_TRY(cudaMemcpyAsync(hmin, d_min, sizeof(hmin), cudaMemcpyDeviceToHost, st));
     const int nbc = blocks_for(npad);
     int32_t* d_bmax = nullptr;
     long long* d_bsum = nullptr;
@@ -435,6 +472,10 @@ int build_neighbor_list(const double* x, const double* disp, int64_t n, int64_t 
     CPD_TRY(cudaStreamSynchronize(st));
     CPD_TRY(dev_free(d_bmax, st));
     CPD_TRY(dev_free(d_bsum, st));
+    if (d_min) {
+        CPD_TRY(dev_free(d_min, st));
+        for (int d = 0; d < 3; ++d) std::memcpy(&min_spacing[d], &hmin[d], sizeof(double));
+    }
     int32_t max_n = 0;
     long long total = 0;
     for (int b = 0; b < nbc; b++) {
