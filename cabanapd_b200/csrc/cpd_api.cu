@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -1654,6 +1655,16 @@ cpd_status cpd_device_field(cpd_system* s, int32_t field, void** ptr, int64_t* s
     return CPD_OK;
 }
 
+cpd_status cpd_bond_bits(cpd_system* s, void** bits, int32_t* words, int64_t* stride)
+{
+    if (!s || !bits) return set_error(CPD_ERR_INVALID_ARGUMENT, "null argument");
+    CPD_OK_OR_RETURN(check_ready(s, true));
+    *bits = s->md.fracture ? s->pd.mu : nullptr;
+    if (words) *words = s->md.fracture ? s->pd.nwords : 0;
+    if (stride) *stride = s->npad;
+    return CPD_OK;
+}
+
 cpd_status cpd_set_kernel_timing(cpd_system* s, int32_t enable)
 {
     if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
@@ -1740,7 +1751,11 @@ constexpr int kNoAllocMaxBlocks = 16384;  // 256-row blocks: 4,194,304 rows
 static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks];
 
 constexpr int kMaxDevices = 64;
-double* g_noalloc_ptr[kMaxDevices] = {};
+// Several host threads (the job server's set-up threads, or a caller's own)
+// may make the first call on a device at the same time, so each entry is an
+// atomic: every thread that finds it empty looks the address up and stores
+// the same value.
+std::atomic<double*> g_noalloc_ptr[kMaxDevices] = {};
 
 // Host code may not use g_noalloc_scratch's name as a device address; the
 // address is fetched once per device, with that device current.
@@ -1748,16 +1763,18 @@ cpd_status noalloc_scratch(int device, double** out)
 {
     if (device < 0 || device >= kMaxDevices)
         return set_error(CPD_ERR_UNSUPPORTED, "device ordinal above the no-allocation table");
-    if (!g_noalloc_ptr[device]) {
+    double* ptr = g_noalloc_ptr[device].load(std::memory_order_acquire);
+    if (!ptr) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
             return set_error(CPD_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation "
                                                        "scratch): ") +
                                                cudaGetErrorString(e));
-        g_noalloc_ptr[device] = static_cast<double*>(p);
+        ptr = static_cast<double*>(p);
+        g_noalloc_ptr[device].store(ptr, std::memory_order_release);
     }
-    *out = g_noalloc_ptr[device];
+    *out = ptr;
     return CPD_OK;
 }
 
@@ -1782,9 +1799,17 @@ extern "C" cpd_status cpd_compute_energy_noalloc(cpd_system* s, double* W_out,
     CPD_OK_OR_RETURN(noalloc_scratch(s->device, &scratch));
     if (!has_pd(s)) {
         // A DEM-only system has no strain energy or damage (cpd_compute_energy
-        // returns zeros as well).
+        // returns zeros as well): every row of both buffers is zero.
+        CPD_CUDA(cudaMemsetAsync(W_out, 0, sizeof(double) * (size_t)s->npad, s->stream));
+        CPD_CUDA(cudaMemsetAsync(phi_out, 0, sizeof(double) * (size_t)s->npad, s->stream));
         CPD_CUDA(cudaMemsetAsync(totals_out, 0, 2 * sizeof(double), s->stream));
         return CPD_OK;
+    }
+    // The energy kernels write rows [frozen, n); frozen rows read 0, as in
+    // cpd_compute_energy.
+    if (s->frozen > 0) {
+        CPD_CUDA(cudaMemsetAsync(W_out, 0, sizeof(double) * (size_t)s->frozen, s->stream));
+        CPD_CUDA(cudaMemsetAsync(phi_out, 0, sizeof(double) * (size_t)s->frozen, s->stream));
     }
     ParticleView p = view(s);
     p.W = W_out;

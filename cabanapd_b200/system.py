@@ -151,6 +151,8 @@ SIGNATURES = {
     "cpd_max_displacement": (_D, [_P]),
     "cpd_contact_rebuilds": (_I64, [_P]),
     "cpd_device_field": (_I32, [_P, _I32, ctypes.POINTER(_P), ctypes.POINTER(_I64)]),
+    "cpd_bond_bits": (_I32, [_P, ctypes.POINTER(_P), ctypes.POINTER(_I32),
+                             ctypes.POINTER(_I64)]),
     "cpd_set_kernel_timing": (_I32, [_P, _I32]),
     "cpd_kernel_time": (_I32, [_P, _DP, ctypes.POINTER(_I64), _DP]),
     "cpd_kernel_launches": (_I64, [_P]),
@@ -350,6 +352,14 @@ class System:
         self._check(self._lib.cpd_device_field(self._h, FIELDS[field], ctypes.byref(ptr),
                                                ctypes.byref(stride)))
         return ptr.value, stride.value
+
+    def bond_bits(self):
+        """(device pointer, words, stride) of the broken-bond bits
+        (cpd_bond_bits): uint32 [words][stride], internal order."""
+        ptr, words, stride = _P(), _I32(), _I64()
+        self._check(self._lib.cpd_bond_bits(self._h, ctypes.byref(ptr), ctypes.byref(words),
+                                            ctypes.byref(stride)))
+        return ptr.value, words.value, stride.value
 
     def set_stream(self, stream_handle):
         self._check(self._lib.cpd_set_stream(self._h, stream_handle))

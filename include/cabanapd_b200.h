@@ -24,6 +24,7 @@
  *   cpd_build_neighbors      Neighbor ctor (CabanaPD_Neighbor.hpp:44-66,
  *                            199-210): full list, cutoff + 1e-14, mu = 1
  *   cpd_neighbor_stats       Neighbor::getStatistics (Neighbor.hpp:80-102)
+ *   cpd_bond_bits            Neighbor::brokenBonds (Neighbor.hpp:219), as bits
  *   cpd_prenotch             Prenotch<N>::create (CabanaPD_Prenotch.hpp:215-263)
  *   cpd_add_boundary_condition  createBoundaryCondition / BodyTerm
  *                            (CabanaPD_Boundary.hpp:34-204, CabanaPD_BodyTerm.hpp:25-69)
@@ -251,7 +252,8 @@ cpd_status cpd_compute_stress(cpd_system* sys);
  * server that reserved each job's memory at admission, or a framework that
  * owns all device memory through its own pool). W_out and phi_out are caller
  * device buffers of at least the system's stride (cpd_device_field) doubles,
- * filled in the internal particle order; totals_out is a caller device
+ * filled in the internal particle order (frozen rows, and every row of a
+ * system without a PD model, are set to 0); totals_out is a caller device
  * buffer of 2 doubles (sum W_i vol_i, sum phi_i). Queued on the system's
  * stream without waiting. Scratch is a fixed 256 KB array inside the library
  * (held on every GPU that loads it until exit), which limits a call to
@@ -324,6 +326,16 @@ int64_t cpd_contact_rebuilds(const cpd_system* sys);
  * ([3][stride] for vectors), for user kernels between steps. */
 cpd_status cpd_device_field(cpd_system* sys, int32_t field, void** ptr,
                             int64_t* stride);
+
+/* Device view of the broken-bond state (Neighbor::brokenBonds,
+ * CabanaPD_Neighbor.hpp:219, which hands out the mu view): one bit per bond,
+ * uint32 bits[words][stride] in the internal particle order, bit b of word w
+ * of row i covering bond slot 32 w + b of that row (1 = intact). Slots follow
+ * the row order of cpd_download_neighbors. Systems built from the same
+ * particles in the same order have the same layout, so their bond states
+ * compare word for word on the device. *bits is NULL for systems without
+ * fracture. Read it between steps; the bond kernels rewrite it. */
+cpd_status cpd_bond_bits(cpd_system* sys, void** bits, int32_t* words, int64_t* stride);
 
 /* Per-kernel device time: when enabled, the bond kernels of every step are
  * bracketed by CUDA events on the system stream.

@@ -987,6 +987,27 @@ int orc_get_neighbors(const orc_system* s, int32_t* counts, int32_t* idx,
     return 0;
 }
 
+// The broken-bond state packed as the product stores it (for comparing
+// large systems without the full neighbour arrays): bits[w][n], bit b of
+// word w of row i = mu of slot 32 w + b (1 = intact).
+int orc_get_bond_bits(const orc_system* s, uint32_t* bits)
+{
+    const NList& nl = s->pd_list;
+    if (s->mu.empty()) return fail("orc_get_bond_bits: no bond state");
+    const int32_t words = (nl.max_n + 31) / 32;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < s->n; i++)
+        for (int32_t w = 0; w < words; w++) {
+            uint32_t v = 0;
+            for (int32_t b = 0; b < 32; b++) {
+                const int32_t k = 32 * w + b;
+                if (k < nl.count[i] && s->mu[(size_t)i * nl.max_n + k] > 0) v |= 1u << b;
+            }
+            bits[(size_t)w * s->n + i] = v;
+        }
+    return 0;
+}
+
 // CabanaPD_Prenotch.hpp:215-263 Prenotch::create: i over [0, local).
 int orc_prenotch(orc_system* s, int32_t k, const double* v1, const double* v2,
                  const double* p0)

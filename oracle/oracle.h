@@ -98,6 +98,9 @@ int orc_neighbor_stats(const orc_system* s, int32_t* max_n, int64_t* total);
 /* counts[n]; idx/mu padded [n][max_n] */
 int orc_get_neighbors(const orc_system* s, int32_t* counts, int32_t* idx,
                       int32_t* mu);
+/* bits[w][n]: bit b of word w of row i = mu of slot 32 w + b (the product's
+ * packing, cpd_bond_bits, without its row padding). */
+int orc_get_bond_bits(const orc_system* s, uint32_t* bits);
 int orc_prenotch(orc_system* s, int32_t k, const double* v1, const double* v2,
                  const double* p0);
 int orc_add_bc(orc_system* s, int32_t kind, int32_t component, int64_t count,

@@ -73,6 +73,7 @@ def load():
     lib.orc_get_neighbors.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p]
     lib.orc_prenotch.argtypes = [P, ctypes.c_int32, dp, dp, dp]
+    lib.orc_get_bond_bits.argtypes = [P, ctypes.c_void_p]
     lib.orc_add_bc.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64,
                                ctypes.c_void_p, dp]
     for name in ("orc_compute_weighted_volume", "orc_compute_dilatation",
@@ -175,6 +176,14 @@ class OracleSystem:
         self._lib.orc_get_neighbors(self._h, counts.ctypes.data, idx.ctypes.data,
                                     mu.ctypes.data)
         return counts, idx[:, :mx], mu[:, :mx]
+
+    def bond_bits(self):
+        """Broken-bond state packed as uint32 [words][n] (the product's
+        cpd_bond_bits layout without its row padding)."""
+        mx, _ = self.neighbor_stats()
+        bits = np.zeros(((mx + 31) // 32, self.n), dtype=np.uint32)
+        self._check(self._lib.orc_get_bond_bits(self._h, bits.ctypes.data))
+        return bits
 
     def prenotch(self, v1, v2, p0):
         v1 = np.ascontiguousarray(v1, dtype=np.float64).reshape(-1, 3)
