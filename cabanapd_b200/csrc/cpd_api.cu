@@ -432,6 +432,19 @@ bool use_mixed(const cpd_system* s)
     return wants_mixed(s) && (s->md.pd == CPD_PD_PMB || s->mixed.lps_ok);
 }
 
+// CPD_FP64 PMB without contact on a lattice: the stencil kernel takes the
+// stencil rows (set up with the neighbour list when wants_stencil64).
+bool wants_stencil64(const cpd_system* s)
+{
+    return s->params.precision == CPD_FP64 && s->md.contact == CPD_CONTACT_NONE &&
+           s->md.pd == CPD_PD_PMB;
+}
+
+bool use_stencil64(const cpd_system* s)
+{
+    return wants_stencil64(s) && stencil64_ready(s->mixed);
+}
+
 // The throughput FP64 kernels serve CPD_FP64, and CPD_MIXED where the mixed
 // kernels do not apply.
 bool use_fast(const cpd_system* s)
@@ -448,9 +461,13 @@ cpd_status pd_force_on(cpd_system* s, const ParticleView& p, const MixedState& m
 {
     cudaEvent_t e0;
     CPD_OK_OR_RETURN(timed_begin(s, e0));
-    if (use_mixed(s))
+    if (use_mixed(s)) {
         CPD_LAUNCHED(launch_pd_force_mixed(p, pd_view(s), s->md, m, ep, s->stream));
-    else if (use_fast(s))
+    } else if (use_stencil64(s)) {
+        // Outside the fused step the gather records follow p.u here.
+        if (ep.mode == 0) CPD_LAUNCHED(launch_pack_u4(p, p.u, 0, p.n, m.u4, s->stream));
+        CPD_LAUNCHED(launch_pd_force_stencil64(p, pd_view(s), s->md, m, ep, s->stream));
+    } else if (use_fast(s))
         CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, ep, s->stream));
     else
         CPD_LAUNCHED(launch_pd_force(p, pd_view(s), s->md, s->stream));
@@ -744,6 +761,9 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false
     double* unxt = start_alt ? s->u : s->u_alt;
     MixedU* u2cur = mixed ? (start_alt ? s->u2_alt : s->mixed.u2) : nullptr;
     MixedU* u2nxt = mixed ? (start_alt ? s->mixed.u2 : s->u2_alt) : nullptr;
+    const bool sten = use_stencil64(s);
+    double4* u4cur = sten ? (start_alt ? s->mixed.u4_alt : s->mixed.u4) : nullptr;
+    double4* u4nxt = sten ? (start_alt ? s->mixed.u4 : s->mixed.u4_alt) : nullptr;
     // Frozen rows are never integrated, so the kernels write only rows from
     // frozen on: the second buffer takes the frozen rows' displacement (and
     // its FP32 split) from the system's arrays, where every call starts.
@@ -761,6 +781,12 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false
         CPD_LAUNCHED(launch_vv_initial_mixed(p, s->md, s->params.dt, ucur, u2cur, s->stream));
     else
         CPD_LAUNCHED(launch_vv_initial(p, s->params.dt, false, nullptr, 0, ucur, s->stream));
+    if (sten) {
+        // Gather records of the first step's displacement, and the frozen
+        // rows of the second buffer (the kernels write rows from frozen on).
+        CPD_LAUNCHED(launch_pack_u4(p, ucur, 0, s->n, u4cur, s->stream));
+        CPD_LAUNCHED(launch_pack_u4(p, s->u, 0, s->frozen, u4nxt, s->stream));
+    }
     StepEpilogue ep;
     ep.dt = s->params.dt;
     ep.half_dt = 0.5 * s->params.dt;
@@ -775,14 +801,17 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false
         pk.u = ucur;
         MixedState mk = s->mixed;
         mk.u2 = u2cur;
+        mk.u4 = u4cur;
         ep.mode = k + 1 < num_steps ? 2 : 1;
         ep.u_next = unxt;
         ep.u2_next = u2nxt;
+        ep.u4_next = u4nxt;
         ep.energy_vol_sums = energy_last && k + 1 == num_steps ? s->mixed.vol_sums : nullptr;
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, mk, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
         std::swap(ucur, unxt);
         std::swap(u2cur, u2nxt);
+        std::swap(u4cur, u4nxt);
     }
     s->steps_since_rebuild += num_steps;
     return CPD_OK;
@@ -1053,7 +1082,7 @@ cpd_status cpd_build_neighbors(cpd_system* s)
     if (has_pd(s)) {
         // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
         double hmin[3];
-        const bool spacing = wants_mixed(s);
+        const bool spacing = wants_mixed(s) || wants_stencil64(s);
         int l = build_neighbor_list(s->x, nullptr, s->n, s->npad, s->frozen,
                                     s->md.horizon + 1e-14, s->perm, s->md.fracture != 0,
                                     s->pd, s->stream, err, spacing ? hmin : nullptr);
@@ -1067,6 +1096,11 @@ cpd_status cpd_build_neighbors(cpd_system* s)
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
                               s->stream, err);
             if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
+            s->launches += l;
+        } else if (wants_stencil64(s)) {
+            l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, false, s->mixed,
+                              s->stream, err, &s->md);
+            if (l < 0) return set_error(CPD_ERR_CUDA, "stencil set-up: " + err);
             s->launches += l;
         }
     }

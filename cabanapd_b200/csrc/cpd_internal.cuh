@@ -213,8 +213,10 @@ int launch_pd_energy(const ParticleView& p, const EllView& nl, const Model& md,
                      double* partials, int nblocks, cudaStream_t st);
 // Throughput-form FP64 kernels (cpd_kernels_fast.cu): PMB and LPS.
 bool fast_supported(const Model& md);
+// wlist: only the listed warps of 32 rows (wcount of them).
 int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
-                         const StepEpilogue& ep, cudaStream_t st);
+                         const StepEpilogue& ep, cudaStream_t st,
+                         const int32_t* wlist = nullptr, int64_t wcount = 0);
 // Energy / damage of the FP64 and mixed paths (PMB, LPS): -1 for other
 // models (the exact kernel serves those).
 int launch_pd_energy_fast(const ParticleView& p, const EllView& nl, const Model& md,
@@ -272,6 +274,51 @@ struct MixedView {
     const uint32_t* pmask;     // [ceil(ntab/32)][npad] stencil entries present per row
     const uint32_t* warp_pmask;  // [warp][ceil(ntab/32)] the common subset of a kind-3 warp
 };
+// Lattice-stencil bond kernels (cpd_kernels_stencil.cu). On a lattice the
+// rows of stencil warps (warp kinds 1-3) hold subsets of one table of bond
+// offsets in table order, so bond slot k of a full row is entry k and its
+// neighbour is i + delta_k. The table rides in the kernel's parameter space:
+// the bond loop is unrolled over the entries, every entry constant is an
+// immediate constant-bank operand, and no index or per-bond code is read.
+constexpr int kStencilMax = 128;  // entries of the unrolled kernels
+constexpr int kStencilPoly = 9;   // coefficients of the FP64 stretch polynomial
+// Half-width of the range of q = (r^2 - xi^2) / xi^2 the stretch polynomial
+// covers; bonds outside it take the exact formula.
+constexpr double kStencilQ = 0.03;
+struct StencilEntry64 {
+    double ex, ey, ez;        // bond reference vector xi (FP64 lattice offset)
+    double tx, ty, tz;        // 2 xi
+    double ixi2;              // 1 / xi^2
+    // Pair force factor F = (c vol / xi) (1 - xi / r) = K num H(num / xi^2)
+    // with K = c vol / xi^3 and the stretch polynomial H (Stencil64::h), so
+    // that the pair force is F r_vec (= c s vol r_vec / r,
+    // force/CabanaPD_PMB.hpp:266-270).
+    double K;
+    int64_t boff;             // (neighbour index - particle index) * 32: record bytes
+    int32_t doff;             // neighbour index - particle index
+    // num lies in the polynomial's range and below the break band when the
+    // high word of |num| is below khi.
+    uint32_t khi;
+};
+struct Stencil64 {
+    int32_t ntab = 0, nwords = 0;
+    int32_t np = 0;        // coefficients of h in use (8 or 9)
+    double bbc = 0;        // bond_break_coeff (the exact re-test)
+    double c = 0;          // micromodulus (the exact formula)
+    // H(q) = sum_k h[k] q^k ~ 1 / (sqrt(1+q) (1 + sqrt(1+q))) on |q| <= kStencilQ,
+    // so that 1 - xi / r = q H(q) with q = (r^2 - xi^2) / xi^2.
+    double h[kStencilPoly];
+    StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
+};
+// Where the stencil kernels find their rows: the warp list (kinds 1-3, tile
+// order), the kinds, and the per-row presence masks over the table.
+struct StencilRows {
+    const uint8_t* warp_kind;
+    const uint32_t* pmask;  // [ceil(ntab / 32)][npad]
+    const int32_t* wlist;
+    int64_t wcount;
+};
+
 // What a throughput bond kernel does after summing row i's force
 // (cpd_epilogue.cuh): mode 0 stores f; mode 1 applies the row's force
 // boundary condition and the second half step (v); mode 2 also applies the
@@ -296,6 +343,8 @@ struct StepEpilogue {
     // Contact steps: neighbours read this row's velocity during the pass
     // (Hertz damping), so the new velocity goes to this second buffer.
     double* v_next = nullptr;
+    // FP64 stencil path: the next displacement's gather records as well.
+    double4* u4_next = nullptr;
 };
 
 struct MixedState {
@@ -325,10 +374,38 @@ struct MixedState {
     // the m / theta pass, read by the lean force kernel in place of u2 and
     // ab), so a neighbour is one 32-byte record.
     MixedU* u2ab = nullptr;
+    // FP64 stencil path (CPD_FP64, PMB): the table in kernel-parameter form
+    // (host memory, built at set-up), and the displacement as 32-byte gather
+    // records (u_x, u_y, u_z, vol) with `guard` zero records on either side,
+    // so i + delta of an absent stencil entry stays inside the allocation.
+    Stencil64* st64 = nullptr;
+    double4* u4 = nullptr;       // record of particle 0
+    double4* u4_base = nullptr;  // allocation
+    double4* u4_alt = nullptr;   // the fused step's second buffer, same form
+    double4* u4_alt_base = nullptr;
+    int64_t guard = 0;
+    int64_t nstencil = 0;        // warps of kinds 1-3 (stencil_list)
+    int32_t* stencil_list = nullptr;
+    int64_t nirregular = 0;      // warps of kind 0 (irregular_list)
+    int32_t* irregular_list = nullptr;
 };
-// lps: set up the LPS mixed kernels too (lps_ok, ab).
+// lps: set up the LPS mixed kernels too (lps_ok, ab). fp64_stencil: set up
+// the stencil data for the FP64 stencil kernel only (no FP32 copies).
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
-                  MixedState& m, cudaStream_t st, std::string& err);
+                  MixedState& m, cudaStream_t st, std::string& err,
+                  const Model* fp64_stencil = nullptr);
+// FP64 stencil path (cpd_kernels_stencil.cu).
+// Builds m.st64 and the gather records (false: the stencil does not apply).
+bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
+                       const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
+                       std::string& err);
+void free_stencil64(MixedState& m, cudaStream_t st);
+bool stencil64_ready(const MixedState& m);
+// Gather records of rows [begin, end) from the displacement u (SoA).
+int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_t end,
+                   double4* u4, cudaStream_t st);
+int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
+                              const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                             const MixedState& m, bool with_m, cudaStream_t st);
 double mixed_wscale(const Model& md);

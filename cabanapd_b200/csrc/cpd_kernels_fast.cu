@@ -142,31 +142,59 @@ __device__ __forceinline__ void gather(const ParticleView& p, int64_t np, int64_
     g.nofail = FRACTURE ? (__ldg(p.nofail + j) != 0) : false;
 }
 
+// Neighbour indices of one ELL row read PF bonds ahead of use (a shift
+// register), so the index load of bond k + PF overlaps the work of bond k.
+template <int PF>
+struct IndexStream {
+    const int32_t* __restrict__ idx;
+    int64_t np;
+    int cnt;
+    int32_t q[PF];
+    __device__ __forceinline__ IndexStream(const int32_t* row, int64_t stride, int count)
+        : idx(row), np(stride), cnt(count)
+    {
+#pragma unroll
+        for (int a = 0; a < PF; ++a) q[a] = a < cnt ? __ldg(idx + (int64_t)a * np) : 0;
+    }
+    // Index of bond k (called for k = 0, 1, ... in order).
+    __device__ __forceinline__ int64_t next(int k)
+    {
+        const int64_t j = q[0];
+#pragma unroll
+        for (int a = 0; a + 1 < PF; ++a) q[a] = q[a + 1];
+        q[PF - 1] = (k + PF < cnt) ? __ldg(idx + (int64_t)(k + PF) * np) : 0;
+        return j;
+    }
+};
+
 // PMB force (force/CabanaPD_PMB.hpp:89-125, :222-287).
 //
 // Latency hiding: each bond's work hangs off its neighbour index, which
-// streams from HBM. The indices of the next PF bonds are loaded PF
-// iterations ahead (a shift register in registers), and with GP the
-// neighbour's position / displacement / volume are gathered one bond ahead,
-// so a warp keeps several independent loads in flight while it computes.
-template <bool FRACTURE, int PF, bool GP, int MINB = 1>
-__global__ void __launch_bounds__(kBlock, MINB)
-    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
+// streams from HBM; the indices of the next two bonds are loaded two
+// iterations ahead (IndexStream), and the kernel is compiled for 4 blocks of
+// 256 threads per SM (64 registers). With a warp list the warps take the
+// listed chunks of 32 rows (the irregular rows beside the stencil kernel),
+// else one thread per row from the first row on.
+template <bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep,
+                     const int32_t* __restrict__ wlist, int64_t wcount)
 {
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t i;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        i = p.frozen + 32 * (int64_t)wlist[slot] + (threadIdx.x & 31);
+    } else {
+        i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    }
     if (i >= p.n) return;
     const int64_t np = p.npad;
     const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
     const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
     const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
     const int cnt = nl.count[i];
-    const int32_t* __restrict__ idx = nl.idx + i;
-    constexpr int Q = PF > 0 ? PF : 1;
-    int32_t q[Q];
-#pragma unroll
-    for (int a = 0; a < Q; ++a) q[a] = (PF > 0 && a < cnt) ? __ldg(idx + (int64_t)a * np) : 0;
-    Gather g_next;
-    if (GP && cnt > 0) gather<FRACTURE>(p, np, PF > 0 ? q[0] : __ldg(idx), g_next);
+    IndexStream<2> js(nl.idx + i, np, cnt);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     uint32_t word = 0;
     bool dirty = false;
@@ -176,24 +204,9 @@ __global__ void __launch_bounds__(kBlock, MINB)
             dirty = false;
             word = nl.mu[(int64_t)(k >> 5) * np + i];
         }
-        int64_t j;
-        if (PF > 0) {
-            j = q[0];
-#pragma unroll
-            for (int a = 0; a + 1 < Q; ++a) q[a] = q[a + 1];
-            q[Q - 1] = (k + Q < cnt) ? __ldg(idx + (int64_t)(k + Q) * np) : 0;
-        } else {
-            j = __ldg(idx + (int64_t)k * np);
-        }
+        const int64_t j = js.next(k);
         Gather g;
-        if (GP) {
-            g = g_next;
-            if (k + 1 < cnt)
-                gather<FRACTURE>(p, np, PF > 0 ? q[0] : __ldg(idx + (int64_t)(k + 1) * np),
-                                 g_next);
-        } else {
-            gather<FRACTURE>(p, np, j, g);
-        }
+        gather<FRACTURE>(p, np, j, g);
         Bond b;
         bond_from(g.x0, g.x1, g.x2, g.u0, g.u1, g.u2, xi0, xi1, xi2v, ui0, ui1, ui2, b);
         bool intact = true;
@@ -219,146 +232,6 @@ __global__ void __launch_bounds__(kBlock, MINB)
     if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
     step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
-
-// LPS weighted volume and dilatation fused (force/CabanaPD_LPS.hpp:89-141,
-// :287-378): m_i first, then theta_i with the just-computed m_i, in one
-// pass over the row (two loops; the second re-reads the row from L1/L2).
-// Stores a = theta_coeff theta / m and b = s_coeff / m for the force loop.
-template <int INFL, bool FRACTURE, bool WITH_M>
-__global__ void __launch_bounds__(kBlock)
-    k_lps_m_theta_fast(ParticleView p, EllView nl, FastModel md)
-{
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    const int64_t np = p.npad;
-    const double* __restrict__ X = p.x;
-    const double* __restrict__ U = p.u;
-    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
-    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
-    const int cnt = nl.count[i];
-    const int32_t* __restrict__ idx = nl.idx + i;
-    double mi;
-    if (WITH_M) {
-        mi = 0.0;
-        uint32_t word = 0;
-        for (int k = 0; k < cnt; ++k) {
-            if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
-            if (FRACTURE && !((word >> (k & 31)) & 1u)) continue;
-            const int64_t j = __ldg(idx + (int64_t)k * np);
-            const double xx = __ldg(X + j) - xi0;
-            const double xy = __ldg(X + np + j) - xi1;
-            const double xz = __ldg(X + 2 * np + j) - xi2v;
-            const double x2 = norm2_ref(xx, xy, xz);
-            const double y = rsqrt(x2);
-            const double xi = sqrt_from_rsqrt(x2, y);
-            // omega xi^2 (force_models/CabanaPD_LPS.hpp:100-106)
-            const double w = INFL == 1 ? xi : xi * xi;
-            mi = fma(w, __ldg(p.vol + j), mi);
-        }
-        p.m[i] = mi;
-    } else {
-        mi = p.m[i];
-    }
-    double th = 0.0;
-    if (!FRACTURE || mi > 0) {
-        uint32_t word = 0;
-        for (int k = 0; k < cnt; ++k) {
-            if (FRACTURE && (k & 31) == 0) word = nl.mu[(int64_t)(k >> 5) * np + i];
-            if (FRACTURE && !((word >> (k & 31)) & 1u)) continue;
-            const int64_t j = __ldg(idx + (int64_t)k * np);
-            Bond b;
-            bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
-            // omega s xi^2 vol_j (force_models/CabanaPD_LPS.hpp:108-116)
-            const double w = INFL == 1 ? b.s * b.xi : b.s * b.xi * b.xi;
-            th = fma(w, __ldg(p.vol + j), th);
-        }
-        th = 3.0 * th / mi;
-    }
-    p.theta[i] = th;
-    p.lps_a[i] = md.theta_coeff * th / mi;
-    p.lps_b[i] = md.s_coeff / mi;
-}
-
-// LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447).
-template <int INFL, bool FRACTURE>
-__global__ void __launch_bounds__(kBlock)
-    k_lps_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
-{
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    const int64_t np = p.npad;
-    const double* __restrict__ X = p.x;
-    const double* __restrict__ U = p.u;
-    const double xi0 = X[i], xi1 = X[np + i], xi2v = X[2 * np + i];
-    const double ui0 = U[i], ui1 = U[np + i], ui2 = U[2 * np + i];
-    const double a_i = p.lps_a[i], b_i = p.lps_b[i];
-    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
-    const int cnt = nl.count[i];
-    const int32_t* __restrict__ idx = nl.idx + i;
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    uint32_t word = 0;
-    bool dirty = false;
-    for (int k = 0; k < cnt; ++k) {
-        if (FRACTURE && (k & 31) == 0) {
-            if (dirty) nl.mu[(int64_t)((k >> 5) - 1) * np + i] = word;
-            dirty = false;
-            word = nl.mu[(int64_t)(k >> 5) * np + i];
-        }
-        const int64_t j = __ldg(idx + (int64_t)k * np);
-        Bond b;
-        bond_fast(X, U, np, j, xi0, xi1, xi2v, ui0, ui1, ui2, b);
-        bool intact = true;
-        if (FRACTURE) {
-            // nofail(i) tested twice by the reference (force/CabanaPD_LPS.hpp:417-418).
-            const uint32_t bit = 1u << (k & 31);
-            if (!nofail_i && critical_fast(b, md.bond_break_coeff)) {
-                if (word & bit) {
-                    word &= ~bit;
-                    dirty = true;
-                }
-                intact = false;
-            } else {
-                intact = (word & bit) != 0;
-            }
-        }
-        if (intact) {
-            const double a_j = __ldg(p.lps_a + j), b_j = __ldg(p.lps_b + j);
-            // (force_models/CabanaPD_LPS.hpp:118-134) omega xi vol_j / r
-            const double oxi = INFL == 1 ? 1.0 : b.xi;
-            const double kf = (a_i + a_j + b.s * (b_i + b_j)) * oxi * __ldg(p.vol + j) * b.rinv;
-            fx = fma(kf, b.rx, fx);
-            fy = fma(kf, b.ry, fy);
-            fz = fma(kf, b.rz, fz);
-        }
-    }
-    if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
-    step_epilogue<false>(p, ep, i, fx, fy, fz);
-}
-
-// Neighbour indices of one ELL row read PF bonds ahead of use (a shift
-// register), so the index load of bond k + PF overlaps the work of bond k.
-template <int PF>
-struct IndexStream {
-    const int32_t* __restrict__ idx;
-    int64_t np;
-    int cnt;
-    int32_t q[PF];
-    __device__ __forceinline__ IndexStream(const int32_t* row, int64_t stride, int count)
-        : idx(row), np(stride), cnt(count)
-    {
-#pragma unroll
-        for (int a = 0; a < PF; ++a) q[a] = a < cnt ? __ldg(idx + (int64_t)a * np) : 0;
-    }
-    // Index of bond k (called for k = 0, 1, ... in order).
-    __device__ __forceinline__ int64_t next(int k)
-    {
-        const int64_t j = q[0];
-#pragma unroll
-        for (int a = 0; a + 1 < PF; ++a) q[a] = q[a + 1];
-        q[PF - 1] = (k + PF < cnt) ? __ldg(idx + (int64_t)(k + PF) * np) : 0;
-        return j;
-    }
-};
 
 // LPS weighted volume and dilatation in ONE pass over the row
 // (force/CabanaPD_LPS.hpp:89-141, :287-378): both sums accumulate per bond,
@@ -453,18 +326,6 @@ __global__ void __launch_bounds__(kBlock, 4)
     step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
-// LPS kernel form, from CPD_LPS_VARIANT: 0 two-pass m / theta and plain
-// loops; 1 (default) one-pass m / theta, index streaming, 4 blocks per SM.
-int lps_variant()
-{
-    static int v = [] {
-        const char* e = getenv("CPD_LPS_VARIANT");
-        const int x = e ? atoi(e) : 1;
-        return (x < 0 || x > 1) ? 1 : x;
-    }();
-    return v;
-}
-
 // Strain energy density and damage at output steps (force/CabanaPD_PMB.hpp:
 // 127-155, 289-339; force/CabanaPD_LPS.hpp:183-219, 449-504), for the FP64
 // and mixed paths: the per-bond terms and row-order sums of k_pd_energy with
@@ -551,21 +412,6 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
-// Kernel variant of the PMB force loop, from CPD_FORCE_VARIANT (0-5):
-// 0 no prefetch, 1 indices 2 bonds ahead, 2 indices 4 ahead, 3 / 4 the same
-// plus neighbour gathers one bond ahead, 5 = 1 compiled for 4 blocks of 256
-// per SM (64 registers). Full plate on B200, ms per launch: 11.3 / 11.3 /
-// 9.0 / 11.9 / 11.8 / 7.3, so 5 is the default.
-int fast_variant()
-{
-    static int v = [] {
-        const char* e = getenv("CPD_FORCE_VARIANT");
-        int x = e ? atoi(e) : 5;
-        return (x < 0 || x > 5) ? 5 : x;
-    }();
-    return v;
-}
-
 FastModel to_fast(const Model& m)
 {
     return FastModel{m.c, m.theta_coeff, m.s_coeff, m.bond_break_coeff};
@@ -579,52 +425,28 @@ bool fast_supported(const Model& md)
 }
 
 int launch_pd_force_fast(const ParticleView& p, const EllView& nl, const Model& md,
-                         const StepEpilogue& ep, cudaStream_t st)
+                         const StepEpilogue& ep, cudaStream_t st, const int32_t* wlist,
+                         int64_t wcount)
 {
     const int64_t rows = p.n - p.frozen;
-    if (rows <= 0) return 0;
-    const int g = blocks_for(rows);
+    if (rows <= 0 || (wlist && wcount <= 0)) return 0;
+    const int g = wlist ? (int)((wcount + kBlock / 32 - 1) / (kBlock / 32)) : blocks_for(rows);
     const FastModel fm = to_fast(md);
     if (md.pd == CPD_PD_PMB) {
-        // Variant: index prefetch distance and neighbour-gather pipelining.
-        switch (md.fracture ? fast_variant() : 100 + fast_variant()) {
-        case 0: k_pmb_force_fast<true, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 1: k_pmb_force_fast<true, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 2: k_pmb_force_fast<true, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 3: k_pmb_force_fast<true, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 4: k_pmb_force_fast<true, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 5: k_pmb_force_fast<true, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 100: k_pmb_force_fast<false, 0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 101: k_pmb_force_fast<false, 2, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 102: k_pmb_force_fast<false, 4, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 103: k_pmb_force_fast<false, 2, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        case 105: k_pmb_force_fast<false, 2, false, 4><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        default: k_pmb_force_fast<false, 4, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep); break;
-        }
-    } else if (lps_variant() == 1) {
-        if (md.influence == 1) {
-            if (md.fracture)
-                k_lps_force_pf<1, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-            else
-                k_lps_force_pf<1, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-        } else {
-            if (md.fracture)
-                k_lps_force_pf<0, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-            else
-                k_lps_force_pf<0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-        }
+        if (md.fracture)
+            k_pmb_force_fast<true><<<g, kBlock, 0, st>>>(p, nl, fm, ep, wlist, wcount);
+        else
+            k_pmb_force_fast<false><<<g, kBlock, 0, st>>>(p, nl, fm, ep, wlist, wcount);
+    } else if (md.influence == 1) {
+        if (md.fracture)
+            k_lps_force_pf<1, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
+        else
+            k_lps_force_pf<1, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
     } else {
-        if (md.influence == 1) {
-            if (md.fracture)
-                k_lps_force_fast<1, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-            else
-                k_lps_force_fast<1, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-        } else {
-            if (md.fracture)
-                k_lps_force_fast<0, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-            else
-                k_lps_force_fast<0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
-        }
+        if (md.fracture)
+            k_lps_force_pf<0, true><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
+        else
+            k_lps_force_pf<0, false><<<g, kBlock, 0, st>>>(p, nl, fm, ep);
     }
     return 1;
 }
@@ -636,13 +458,7 @@ int launch_lps_m_theta_fast(const ParticleView& p, const EllView& nl, const Mode
     if (rows <= 0) return 0;
     const int g = blocks_for(rows);
     const FastModel fm = to_fast(md);
-#define CPD_MT(I, F, W)                                                          \
-    do {                                                                         \
-        if (lps_variant() == 1)                                                  \
-            k_lps_m_theta_1pass<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm);       \
-        else                                                                     \
-            k_lps_m_theta_fast<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm);        \
-    } while (0)
+#define CPD_MT(I, F, W) k_lps_m_theta_1pass<I, F, W><<<g, kBlock, 0, st>>>(p, nl, fm)
     if (md.influence == 1) {
         if (md.fracture) {
             if (with_m) CPD_MT(1, true, true); else CPD_MT(1, true, false);

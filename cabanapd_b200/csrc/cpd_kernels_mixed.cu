@@ -1727,33 +1727,41 @@ int mixed_variant()
 
 void free_mixed(MixedState& m, cudaStream_t st)
 {
+    free_stencil64(m, st);
     void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
-                    m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab};
+                    m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab, m.stencil_list,
+                    m.irregular_list};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
 }
 
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
-                  MixedState& m, cudaStream_t st, std::string& err)
+                  MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil)
 {
     int launches = 0;
     PhaseTrace tr("mixed");
     free_mixed(m, st);
     const int64_t np = p.npad;
-    CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
-    CPD_TRY(dev_alloc(&m.xl, sizeof(float4) * np, st));
-    CPD_TRY(dev_alloc(&m.u2, sizeof(MixedU) * np, st));
+    // The FP64 stencil path needs the table, masks and warp lists only.
+    const bool fp32 = fp64_stencil == nullptr;
+    if (fp32) {
+        CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
+        CPD_TRY(dev_alloc(&m.xl, sizeof(float4) * np, st));
+        CPD_TRY(dev_alloc(&m.u2, sizeof(MixedU) * np, st));
+        m.bytes = (2 * sizeof(float4) + sizeof(MixedU)) * np;
+    }
     CPD_TRY(dev_alloc(&m.table, sizeof(MixedStencil) * kMixedGeneric, st));
     CPD_TRY(dev_alloc(&m.code, (size_t)std::max(pd.max_n, 1) * np, st));
     const int64_t nwarps = (np + 31) / 32 + 8;
     CPD_TRY(dev_alloc(&m.warp_kind, nwarps, st));
-    m.bytes = (2 * sizeof(float4) + sizeof(MixedU)) * np + sizeof(MixedStencil) * kMixedGeneric +
-              (size_t)std::max(pd.max_n, 1) * np + nwarps;
+    m.bytes += sizeof(MixedStencil) * kMixedGeneric + (size_t)std::max(pd.max_n, 1) * np + nwarps;
     CPD_TRY(cudaMemsetAsync(m.warp_kind, 0, nwarps, st));
     CPD_TRY(cudaMemsetAsync(m.code, kMixedGeneric, (size_t)std::max(pd.max_n, 1) * np, st));
-    k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, m.xh, m.xl);
-    launches++;
+    if (fp32) {
+        k_split<<<blocks_for(p.n), kBlock, 0, st>>>(p.x, p.n, np, m.xh, m.xl);
+        launches++;
+    }
     tr.mark("alloc+split", st);
     m.ntab = 0;
     const int64_t rows = p.n - p.frozen;
@@ -1887,33 +1895,50 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                     }
                 }
                 {
-                    // Warp lists of the split forms, each in the tile order of
-                    // tile_chunk: warps of kinds 2 and 3, and the rest.
+                    // Warp lists, each in the tile order of tile_chunk: warps
+                    // of kinds 2 and 3 and the rest (the split mixed forms);
+                    // warps of kinds 1-3 and of kind 0 (the stencil kernels).
                     int g = 0;
                     const EllView tv = tile_view(pd.view(), rows, kBlock, &g);
                     const int64_t S = tv.stride, W = kBlock / 32;
-                    std::vector<int32_t> lean, rest;
+                    std::vector<int32_t> lean, rest, sten, irr;
                     lean.reserve(nw);
+                    sten.reserve(nw);
                     for (int64_t b = 0; b < g; ++b)
                         for (int64_t w = 0; w < W; ++w) {
                             const int64_t q = S > 1 ? (W * (b / S) + w) * S + b % S : W * b + w;
                             if (q >= nw) continue;
                             (kinds[q] >= 2 ? lean : rest).push_back((int32_t)q);
+                            (kinds[q] >= 1 ? sten : irr).push_back((int32_t)q);
                         }
-                    m.nlean = (int64_t)lean.size();
-                    m.nrest = (int64_t)rest.size();
-                    if (m.nlean) {
-                        CPD_TRY(dev_alloc(&m.lean_list, sizeof(int32_t) * m.nlean, st));
-                        CPD_TRY(cudaMemcpyAsync(m.lean_list, lean.data(), sizeof(int32_t) * m.nlean,
-                                                cudaMemcpyHostToDevice, st));
-                    }
-                    if (m.nrest) {
-                        CPD_TRY(dev_alloc(&m.rest_list, sizeof(int32_t) * m.nrest, st));
-                        CPD_TRY(cudaMemcpyAsync(m.rest_list, rest.data(), sizeof(int32_t) * m.nrest,
-                                                cudaMemcpyHostToDevice, st));
+                    auto upload = [&](const std::vector<int32_t>& v, int32_t** dst,
+                                      int64_t* count) -> bool {
+                        *count = (int64_t)v.size();
+                        if (v.empty()) return true;
+                        if (dev_alloc(dst, sizeof(int32_t) * v.size(), st) != cudaSuccess)
+                            return false;
+                        m.bytes += sizeof(int32_t) * v.size();
+                        return cudaMemcpyAsync(*dst, v.data(), sizeof(int32_t) * v.size(),
+                                               cudaMemcpyHostToDevice, st) == cudaSuccess;
+                    };
+                    if (!upload(lean, &m.lean_list, &m.nlean) ||
+                        !upload(rest, &m.rest_list, &m.nrest) ||
+                        !upload(sten, &m.stencil_list, &m.nstencil) ||
+                        !upload(irr, &m.irregular_list, &m.nirregular)) {
+                        err = "warp lists: " + std::string(cudaGetErrorString(cudaGetLastError()));
+                        return -1;
                     }
                     CPD_TRY(cudaStreamSynchronize(st));
-                    m.bytes += sizeof(int32_t) * (size_t)(m.nlean + m.nrest);
+                }
+                if (!fp32) {
+                    if (!prepare_stencil64(p, *fp64_stencil, h, tab.data(), m.ntab, m, st, err) &&
+                        !err.empty())
+                        return -1;
+                    launches += m.u4 ? 1 : 0;
+                    // The FP64 kernels read no bond codes.
+                    CPD_TRY(dev_free(m.code, st));
+                    m.code = nullptr;
+                    m.bytes -= (size_t)std::max(pd.max_n, 1) * np;
                 }
             }
         }
