@@ -288,11 +288,10 @@ def run_reference(args, world, rank):
 
 # ---------------------------------------------------------------------------
 PRECISION = {"exact": 0, "fp64": 1, "mixed": 2}
-KERNEL = {"fp64": "k_pmb_force_fast<fracture>",
-          "mixed": "k_pmb_force_lean<fracture> + k_pmb_force_mixed<fracture> (one bond stage: "
-                   "lean warps, then the rest)",
+KERNEL = {"fp64": "k_pmb_stencil64<fracture> (lattice-stencil FP64 bond stage, fused step)",
+          "mixed": "k_pmb_stencil32<fracture> (lattice-stencil FP32 bond stage, fused step)",
           "exact": "k_pd_force<PMB, fracture> (bit-exact)"}
-PROFILE = {"fp64": "pmb_force_plate.txt", "mixed": "pmb_force_lean_plate.txt",
+PROFILE = {"fp64": "pmb_stencil64_plate.txt", "mixed": "pmb_stencil32_plate.txt",
            "exact": "pmb_force_exact_plate.txt"}
 
 
@@ -355,8 +354,8 @@ def _time_system(s, stream, device, steps, warmup):
 def other_workload(name, steps):
     """(problem, precisions, kernel names, description) of another hot-path
     workload measured beside the headline plate."""
-    mixed_pmb = ("k_pmb_force_lean<fracture> + k_pmb_force_mixed<fracture> "
-                 "(split bond stage, fused step)")
+    mixed_pmb = "k_pmb_stencil32<fracture> (fused step)"
+    fp64_pmb = "k_pmb_stencil64<fracture> (fused step)"
     if name == "lps":
         return (P.lps_random_notches(num_cells=LPS_CELLS, steps=steps), ["mixed", "fp64"],
                 {"mixed": "k_lps_mtheta_lean + k_lps_force_lean<fracture> over lean warps, "
@@ -365,13 +364,13 @@ def other_workload(name, steps):
                 {"workload": "lps_fracture_random_notches", "cells": list(LPS_CELLS)})
     if name == "plate_1p2m":
         return (P.plate_impact(num_cells=PLATE_1P2M_CELLS, steps=steps), ["mixed", "fp64"],
-                {"mixed": mixed_pmb, "fp64": "k_pmb_force_fast<fracture> (fused step)"},
+                {"mixed": mixed_pmb, "fp64": fp64_pmb},
                 {"workload": "pmb_fracture_notched_plate_impact_1p2m",
                  "plate_cells": list(PLATE_1P2M_CELLS)})
     if name == "wave":
         return (P.elastic_wave_pmb(n=WAVE_CELLS, steps=steps), ["mixed", "fp64"],
                 {"mixed": mixed_pmb.replace("fracture", "elastic"),
-                 "fp64": "k_pmb_force_fast<elastic> (fused step)"},
+                 "fp64": fp64_pmb.replace("fracture", "elastic")},
                 {"workload": "pmb_elastic_wave", "cells": [WAVE_CELLS] * 3})
     return (P.dem_packing(lattice_dims=DEM_DIMS, steps=steps), ["mixed", "fp64"],
             {"mixed": "k_hertz_force_mixed<per-particle radius> (FP64 overlap, FP32 force law)",

@@ -171,6 +171,7 @@ struct cpd_system {
     double* u_alt = nullptr;
     double* v_alt = nullptr;  // contact-only fused step: second velocity buffer
     MixedU* u2_alt = nullptr;
+    MixedU* u2_alt_base = nullptr;  // allocation: u2_alt with the split's guard records
     bool neighbors_built = false;
     bool initialized = false;
     bool stress_ready = false;  // cpd_compute_stress ran since the particles were set
@@ -266,8 +267,8 @@ void free_particles(cpd_system* s)
     s->u_alt = nullptr;
     if (s->v_alt) dev_free(s->v_alt, s->stream);
     s->v_alt = nullptr;
-    if (s->u2_alt) dev_free(s->u2_alt, s->stream);
-    s->u2_alt = nullptr;
+    if (s->u2_alt_base) dev_free(s->u2_alt_base, s->stream);
+    s->u2_alt = s->u2_alt_base = nullptr;
     free_neighbor_list(s->pd, s->stream);
     free_neighbor_list(s->contact, s->stream);
     free_mixed(s->mixed, s->stream);
@@ -671,8 +672,12 @@ cpd_status prepare_fused(cpd_system* s)
     if (!s->u_alt) CPD_CUDA(dev_alloc(&s->u_alt, sizeof(double) * 3 * s->npad, s->stream));
     if (contact_fusable(s) && !s->v_alt)
         CPD_CUDA(dev_alloc(&s->v_alt, sizeof(double) * 3 * s->npad, s->stream));
-    if (use_mixed(s) && !s->u2_alt)
-        CPD_CUDA(dev_alloc(&s->u2_alt, sizeof(MixedU) * s->npad, s->stream));
+    if (use_mixed(s) && !s->u2_alt) {
+        const size_t recs = (size_t)(s->npad + 2 * s->mixed.guard);
+        CPD_CUDA(dev_alloc(&s->u2_alt_base, sizeof(MixedU) * recs, s->stream));
+        CPD_CUDA(cudaMemsetAsync(s->u2_alt_base, 0, sizeof(MixedU) * recs, s->stream));
+        s->u2_alt = s->u2_alt_base + s->mixed.guard;
+    }
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     return CPD_OK;
 }
@@ -689,8 +694,6 @@ bool fused_ready(const cpd_system* s)
 // for the last step) the next first half step, alternating displacement
 // buffers. The first half step writes to the buffer that makes the last
 // step end in the system's own arrays.
-// energy_last: the last step's lean kernel also writes W and phi of its rows
-// (mixed_force_fuses_energy must hold).
 // Contact alone (fixed rebuild interval): first half step, then per step the
 // list rebuild when due (on the current displacement) and one contact kernel
 // whose epilogue applies the boundary conditions, the second half step and
@@ -752,7 +755,7 @@ cpd_status step_fused_contact(cpd_system* s, int32_t num_steps)
     return CPD_OK;
 }
 
-cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false)
+cpd_status step_fused(cpd_system* s, int32_t num_steps)
 {
     if (contact_fusable(s)) return step_fused_contact(s, num_steps);
     const bool mixed = use_mixed(s);
@@ -806,7 +809,6 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, bool energy_last = false
         ep.u_next = unxt;
         ep.u2_next = u2nxt;
         ep.u4_next = u4nxt;
-        ep.energy_vol_sums = energy_last && k + 1 == num_steps ? s->mixed.vol_sums : nullptr;
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, mk, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
         std::swap(ucur, unxt);
@@ -1079,6 +1081,10 @@ cpd_status cpd_build_neighbors(cpd_system* s)
     CPD_CUDA(cudaSetDevice(s->device));
     std::string err;
     PhaseTrace tr("neighbors");
+    // The fused step's second split buffer carries the guard of the stencil
+    // set up below: it is allocated again when the step is next prepared.
+    if (s->u2_alt_base) dev_free(s->u2_alt_base, s->stream);
+    s->u2_alt = s->u2_alt_base = nullptr;
     if (has_pd(s)) {
         // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
         double hmin[3];
@@ -1094,7 +1100,8 @@ cpd_status cpd_build_neighbors(cpd_system* s)
         tr.mark("list", s->stream);
         if (wants_mixed(s)) {
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
-                              s->stream, err);
+                              s->stream, err, nullptr,
+                              s->md.pd == CPD_PD_PMB ? &s->md : nullptr);
             if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
             s->launches += l;
         } else if (wants_stencil64(s)) {
@@ -1359,39 +1366,18 @@ cpd_status cpd_init(cpd_system* s)
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     CPD_OK_OR_RETURN(refresh_mixed_u(s));
-    // Where the mixed PMB split form applies, the initial force pass also
-    // forms the energy of its lean rows, as an output step does.
-    const bool fuse_energy = has_pd(s) && use_mixed(s) &&
-                             mixed_force_fuses_energy(view(s), s->md, s->mixed);
     if (has_pd(s)) {
         // Weighted volume once here without fracture (Solver.hpp:235-239),
         // inside updateForce with fracture (Solver.hpp:466-470): once either way.
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, true));
-        if (fuse_energy) {
-            StepEpilogue ep;
-            ep.energy_vol_sums = s->mixed.vol_sums;
-            CPD_OK_OR_RETURN(pd_force_on(s, view(s), s->mixed, ep));
-        } else {
-            CPD_OK_OR_RETURN(pd_force(s));
-        }
+        CPD_OK_OR_RETURN(pd_force(s));
     } else if (has_contact(s)) {
         CPD_OK_OR_RETURN(contact_force(s, true));
     }
     PhaseTrace tr("init");
     // Solver.hpp:240-242: the energy and damage of the initial state (the
     // fields; the totals are not kept).
-    if (fuse_energy) {
-        const int nb = energy_blocks(s->n - s->frozen);
-        CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
-        int l = 0;
-        const int rows = launch_energy_rest_and_totals(view(s), pd_view(s), s->md, s->mixed,
-                                                       s->red, nb + 1, &l, s->stream);
-        s->launches += l;
-        if (rows < 0) return set_error(CPD_ERR_CUDA, "energy totals: reduction buffer too small");
-        CPD_CUDA(cudaGetLastError());
-    } else if (has_pd(s)) {
-        CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
-    }
+    if (has_pd(s)) CPD_OK_OR_RETURN(cpd_compute_energy(s, nullptr, nullptr));
     tr.mark("energy", s->stream);
     CPD_OK_OR_RETURN(apply_force_bcs(s));
     CPD_OK_OR_RETURN(prepare_fused(s));
@@ -1437,29 +1423,8 @@ cpd_status cpd_step_energy(cpd_system* s, int32_t num_steps, double* total_W, do
         CPD_CUDA(cudaStreamIsCapturing(s->stream, &cs));
         if (cs == cudaStreamCaptureStatusNone) CPD_OK_OR_RETURN(prepare_fused(s));
     }
-    const ParticleView p = view(s);
-    const bool fuse = num_steps > 0 && fused_ready(s) && use_mixed(s) &&
-                      mixed_force_fuses_energy(p, s->md, s->mixed);
-    if (!fuse) {
-        CPD_OK_OR_RETURN(cpd_step(s, num_steps));
-        return cpd_compute_energy(s, total_W, total_D);
-    }
-    CPD_OK_OR_RETURN(step_fused(s, num_steps, true));
-    const int nb = energy_blocks(s->n - s->frozen);
-    CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
-    int l = 0;
-    const int rows = launch_energy_rest_and_totals(p, pd_view(s), s->md, s->mixed, s->red, nb + 1,
-                                                   &l, s->stream);
-    s->launches += l;
-    if (rows < 0) return set_error(CPD_ERR_CUDA, "energy totals: reduction buffer too small");
-    CPD_CUDA(cudaGetLastError());
-    CPD_LAUNCHED(launch_sum_partials(s->red, rows, 2, s->red_out + 2, s->stream));
-    CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
-                             cudaMemcpyDeviceToHost, s->stream));
-    CPD_CUDA(cudaStreamSynchronize(s->stream));
-    if (total_W) *total_W = s->h_red[2];
-    if (total_D) *total_D = s->h_red[3];
-    return CPD_OK;
+    CPD_OK_OR_RETURN(cpd_step(s, num_steps));
+    return cpd_compute_energy(s, total_W, total_D);
 }
 
 cpd_status cpd_step_stage(cpd_system* s, int32_t stage)
@@ -1758,7 +1723,7 @@ cpd_status cpd_device_bytes(const cpd_system* s, uint64_t* bytes)
     for (const auto& bc : s->bcs) b += (uint64_t)bc.count * (bc.values ? 12 : 4);
     if (s->u_alt) b += 24 * np;
     if (s->stress) b += 72 * np + 72 * std::max<uint64_t>(n, 1);
-    if (s->u2_alt) b += sizeof(MixedU) * np;
+    if (s->u2_alt) b += sizeof(MixedU) * (np + 2 * (uint64_t)s->mixed.guard);
     if (s->bc_bits) b += 4 * ((np + 31) / 32) + 29 * (uint64_t)s->nbc;
     b += s->pd.bytes + s->contact.bytes + s->mixed.bytes;
     *bytes = b;

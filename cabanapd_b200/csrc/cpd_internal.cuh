@@ -125,20 +125,13 @@ struct PhaseTrace {
 };
 
 // Tiled view of a list for `rows` rows and its grid (blocks of `block`
-// threads). CPD_ROW_TILES=0 keeps consecutive chunks.
-inline bool row_tiles_enabled()
-{
-    static const bool on = [] {
-        const char* e = std::getenv("CPD_ROW_TILES");
-        return !(e && std::atoi(e) == 0);
-    }();
-    return on;
-}
+// threads): with a lattice line pitch of 64 rows or more, a block's warps
+// take chunks one lattice line apart.
 inline EllView tile_view(EllView v, int64_t rows, int block, int* grid)
 {
     const int64_t chunks = (rows + 31) / 32, wpb = block / 32;
     v.stride = 1;
-    if (v.pitch >= 64 && row_tiles_enabled()) {
+    if (v.pitch >= 64) {
         v.stride = (int32_t)((v.pitch + 16) / 32);
         const int64_t per = wpb * v.stride;
         *grid = (int)(((chunks + per - 1) / per) * v.stride);
@@ -285,7 +278,7 @@ constexpr int kStencilPoly = 9;   // coefficients of the FP64 stretch polynomial
 // Half-width of the range of q = (r^2 - xi^2) / xi^2 the stretch polynomial
 // covers; bonds outside it take the exact formula.
 constexpr double kStencilQ = 0.03;
-struct StencilEntry64 {
+struct __align__(16) StencilEntry64 {
     double ex, ey, ez;        // bond reference vector xi (FP64 lattice offset)
     double tx, ty, tz;        // 2 xi
     double ixi2;              // 1 / xi^2
@@ -310,6 +303,26 @@ struct Stencil64 {
     double h[kStencilPoly];
     StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
 };
+// The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
+constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial
+struct __align__(16) StencilEntry32 {
+    float2 exy;               // bond reference vector xi (FP32 of the lattice
+    float ez;                 // offset), x and y paired for the FP32x2 operations
+    float tz;                 // 2 xi (z)
+    float2 txy;               // 2 xi (x, y)
+    float ixi2;               // 1 / xi^2
+    float K;                  // c vol / xi^3 (c / xi^3 with per-particle volumes)
+    int64_t boff;             // (neighbour index - particle index) * 32: record bytes
+    int32_t doff;             // neighbour index - particle index
+    uint32_t khi;             // |num| inside the window: its bits below khi
+};
+struct Stencil32 {
+    int32_t ntab = 0, nwords = 0;
+    double bbc = 0, c = 0;
+    float h[kStencilPoly32];  // H(q) ~ 1 / (sqrt(1+q) (1 + sqrt(1+q))), FP32
+    StencilEntry32 e[kStencilMax];  // past ntab: zero (no force, never deferred)
+};
+
 // Where the stencil kernels find their rows: the warp list (kinds 1-3, tile
 // order), the kinds, and the per-row presence masks over the table.
 struct StencilRows {
@@ -336,10 +349,6 @@ struct StepEpilogue {
                                        // bit d: then f_d + add_d, else add_d
     const double* bc_add = nullptr;    // [3][nbc]
     int32_t nbc = 0;
-    // Mixed PMB split form: the lean kernel also writes W_i and phi_i of its
-    // rows (the energy pass of the state it computes the force of), with
-    // the damage sums from this table (MixedState::vol_sums).
-    const double* energy_vol_sums = nullptr;
     // Contact steps: neighbours read this row's velocity during the pass
     // (Hertz damping), so the new velocity goes to this second buffer.
     double* v_next = nullptr;
@@ -379,6 +388,10 @@ struct MixedState {
     // records (u_x, u_y, u_z, vol) with `guard` zero records on either side,
     // so i + delta of an absent stencil entry stays inside the allocation.
     Stencil64* st64 = nullptr;
+    // Mixed PMB stencil kernel: its table, and the allocation behind u2
+    // (u2 = u2_base + guard; `guard` zero records on either side).
+    Stencil32* st32 = nullptr;
+    MixedU* u2_base = nullptr;
     double4* u4 = nullptr;       // record of particle 0
     double4* u4_base = nullptr;  // allocation
     double4* u4_alt = nullptr;   // the fused step's second buffer, same form
@@ -391,9 +404,10 @@ struct MixedState {
 };
 // lps: set up the LPS mixed kernels too (lps_ok, ab). fp64_stencil: set up
 // the stencil data for the FP64 stencil kernel only (no FP32 copies).
+// md_pmb (mixed PMB): also the table of the mixed stencil kernel.
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err,
-                  const Model* fp64_stencil = nullptr);
+                  const Model* fp64_stencil = nullptr, const Model* md_pmb = nullptr);
 // FP64 stencil path (cpd_kernels_stencil.cu).
 // Builds m.st64 and the gather records (false: the stencil does not apply).
 bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
@@ -401,6 +415,11 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
                        std::string& err);
 void free_stencil64(MixedState& m, cudaStream_t st);
 bool stencil64_ready(const MixedState& m);
+// Mixed PMB: builds m.st32 (false: the stencil kernel does not apply).
+bool prepare_stencil32(const Model& md, const double* h, const MixedStencil* tab, int ntab,
+                       MixedState& m);
+int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
+                              const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 // Gather records of rows [begin, end) from the displacement u (SoA).
 int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_t end,
                    double4* u4, cudaStream_t st);
@@ -421,17 +440,6 @@ int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& m
                         int* launches, cudaStream_t st);
 int launch_pd_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
-// Whether launch_pd_force_mixed with ep.energy_vol_sums set writes W and phi
-// of the lean rows (PMB, fracture, one volume, split form).
-bool mixed_force_fuses_energy(const ParticleView& p, const Model& md, const MixedState& m);
-// Energy pass over the rows the lean kernel does not hold (W, phi of those
-// rows; [.][2] block partials to ignore), then the totals over all rows:
-// sum W_i vol_i and sum phi_i into [.][2] block partials. Returns the
-// number of partial rows of the totals.
-int launch_energy_rest_and_totals(const ParticleView& p, const EllView& nl, const Model& md,
-                                  const MixedState& m, double* partials, int capacity,
-                                  int* launches, cudaStream_t st);
-
 // Neighbour build (cpd_neighbor.cu). Builds rows for [begin, n) from
 // positions pos (+ optional displacement disp) with squared distance
 // <= cutoff^2; rows sorted by ascending user_id of the neighbour.

@@ -381,66 +381,11 @@ __device__ __forceinline__ bool mixed_critical(float s, float nofail_j, bool nof
     return s >= md.s0;
 }
 
-// Full-stencil rows (every table entry present, bond slot k = entry k):
-// the table is walked in chunks of 8 bonds with the bond bits of a chunk
-// tested at constant positions, broken bonds contribute a zero term instead
-// of a branch, and the newly broken bits of a 32-bond word are cleared once.
-template <bool FRACTURE>
-__device__ __forceinline__ void mixed_full_rows(const ParticleView& p, const EllView& nl,
-                                                const MixedU* __restrict__ u2_i,
-                                                const MixedStencil* tab,
-                                                const MixedModel& md, int64_t i,
-                                                const float4& uhi, const float4& uli,
-                                                bool nofail_i, float (&sum)[3], float (&comp)[3])
-{
-    const int64_t np = p.npad;
-    for (int base = 0; base < md.ntab; base += 32) {
-        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
-        uint32_t clr = 0;
-        const int lim = min(32, md.ntab - base);
-        int b = 0;
-        for (; b + 8 <= lim; b += 8) {
-            const uint32_t w8 = word >> b;
-            uint32_t c8 = 0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const MixedStencil t = tab[base + b + u];
-                const MixedU uj = u2_i[t.delta];
-                MixedBond bd;
-                mixed_bond(t.x, t.y, t.z, t.xi, t.xiinv, uj.hi, uj.lo, uhi, uli, bd);
-                float kf = uj.hi.w * bd.s * bd.rinv;
-                if (FRACTURE) {
-                    const bool crit = mixed_critical(bd.s, uj.lo.w, nofail_i, md, p, i,
-                                                     i + t.delta);
-                    c8 |= (uint32_t)crit << u;
-                    kf = (((w8 >> u) & 1u) && !crit) ? kf : 0.f;
-                }
-                kahan_add(sum[0], comp[0], kf * bd.rx);
-                kahan_add(sum[1], comp[1], kf * bd.ry);
-                kahan_add(sum[2], comp[2], kf * bd.rz);
-            }
-            clr |= c8 << b;
-        }
-        for (; b < lim; ++b) {
-            const MixedStencil t = tab[base + b];
-            const MixedU uj = u2_i[t.delta];
-            MixedBond bd;
-            mixed_bond(t.x, t.y, t.z, t.xi, t.xiinv, uj.hi, uj.lo, uhi, uli, bd);
-            float kf = uj.hi.w * bd.s * bd.rinv;
-            if (FRACTURE) {
-                const bool crit = mixed_critical(bd.s, uj.lo.w, nofail_i, md, p, i, i + t.delta);
-                clr |= (uint32_t)crit << b;
-                kf = (((word >> b) & 1u) && !crit) ? kf : 0.f;
-            }
-            kahan_add(sum[0], comp[0], kf * bd.rx);
-            kahan_add(sum[1], comp[1], kf * bd.ry);
-            kahan_add(sum[2], comp[2], kf * bd.rz);
-        }
-        if (FRACTURE && (word & clr)) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
-    }
-}
-
-// mixed_full_rows with the x / y lanes in paired FP32 instructions.
+// Full-stencil rows (every table entry present, bond slot k = entry k),
+// x / y lanes in paired FP32 instructions: the table is walked in chunks of
+// 8 bonds with the bond bits of a chunk tested at constant positions, broken
+// bonds contribute a zero term instead of a branch, and the newly broken
+// bits of a 32-bond word are cleared once.
 template <bool FRACTURE>
 __device__ __forceinline__ void mixed_full_rows2(const ParticleView& p, const EllView& nl,
                                                  const MixedU* __restrict__ u2_i,
@@ -513,129 +458,19 @@ __device__ __forceinline__ void lean_geometry(const MixedStencil& t, const Mixed
     b.s = __fdividef(num, fmaf(r, t.xi, t.xi2));
 }
 
-// One bond of a stencil row in the lean form: adds the pair force to
-// (cxy, cz). Only an intact bond whose FP32 stretch reaches s0 - guard (and
-// whose ends may fail) leaves the fast path: above s0 + guard it breaks (bit
-// set in clr); inside the band it is deferred (bit set in pend) to the exact
-// FP64 test after the word, and contributes no force here.
-template <bool FRACTURE, bool LDG, bool ENERGY = false>
-__device__ __forceinline__ void stencil_bond(const MixedStencil& t,
-                                             const MixedU* __restrict__ u2_i, const RowSplit& ri,
-                                             bool on, uint32_t bit, const MixedModel& md,
-                                             uint32_t& clr, uint32_t& pend, float2& cxy, float& cz,
-                                             float& wc)
-{
-    MixedU uj;
-    if (LDG) {
-        // The split is read-only while the kernel runs (the next one goes
-        // to the other buffer): non-coherent global loads.
-        uj.hi = __ldg(&u2_i[t.delta].hi);
-        uj.lo = __ldg(&u2_i[t.delta].lo);
-    } else {
-        uj = u2_i[t.delta];
-    }
-    MixedBond2 bd;
-    lean_geometry(t, uj, ri, bd);
-    if (FRACTURE && on && bd.s >= md.s_lo && !ri.nofail && uj.lo.w == 0.f) {
-        if (bd.s > md.s_hi)
-            clr |= bit;
-        else
-            pend |= bit;
-        on = false;
-    }
-    const float kf = (!FRACTURE || on) ? uj.hi.w * bd.s * bd.rinv : 0.f;
-    cxy = __ffma2_rn(f2(kf, kf), bd.rxy, cxy);
-    cz = fmaf(kf, bd.rz, cz);
-    // The energy pass's term of an intact bond (k_energy_mixed, PMB).
-    if (ENERGY) wc += (!FRACTURE || on) ? 0.25f * uj.hi.w * bd.s * bd.s * t.xi : 0.f;
-}
-
-// Stencil rows, lean form: bond slot k of row i is entry k of wt (the whole
-// table, or the compacted table of a warp whose rows share one subset). The
-// pair forces of each chunk of UNROLL bonds are summed in FP32 and each
-// chunk sum is added to the FP64 row force f. After each 32-bond word the
-// deferred bonds take the reference's FP64 break test; those that hold add
-// their pair force to f. Newly broken bits are cleared with one store.
-template <bool FRACTURE, bool LDG, int UNROLL, bool ENERGY = false>
-__device__ __forceinline__ void mixed_stencil_rows(const ParticleView& p, const EllView& nl,
-                                                   const MixedU* __restrict__ u2_i,
-                                                   const MixedStencil* wt, int cnt,
-                                                   const MixedModel& md, int64_t i,
-                                                   const RowSplit& ri, double (&f)[3],
-                                                   double* wtot = nullptr, int* intact = nullptr)
-{
-    const int64_t np = p.npad;
-    for (int base = 0; base < cnt; base += 32) {
-        const uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
-        uint32_t clr = 0, pend = 0;
-        const int lim = min(32, cnt - base);
-        int b = 0;
-        for (; b + UNROLL <= lim; b += UNROLL) {
-            const uint32_t w8 = word >> b;
-            float2 cxy = f2(0.f, 0.f);
-            float cz = 0.f, wc = 0.f;
-#pragma unroll
-            for (int u = 0; u < UNROLL; ++u)
-                stencil_bond<FRACTURE, LDG, ENERGY>(wt[base + b + u], u2_i, ri, (w8 >> u) & 1u,
-                                                    1u << (b + u), md, clr, pend, cxy, cz, wc);
-            f[0] += (double)cxy.x;
-            f[1] += (double)cxy.y;
-            f[2] += (double)cz;
-            if (ENERGY) *wtot += (double)wc;
-        }
-        if (b < lim) {
-            float2 cxy = f2(0.f, 0.f);
-            float cz = 0.f, wc = 0.f;
-            for (; b < lim; ++b)
-                stencil_bond<FRACTURE, LDG, ENERGY>(wt[base + b], u2_i, ri, (word >> b) & 1u,
-                                                    1u << b, md, clr, pend, cxy, cz, wc);
-            f[0] += (double)cxy.x;
-            f[1] += (double)cxy.y;
-            f[2] += (double)cz;
-            if (ENERGY) *wtot += (double)wc;
-        }
-        if (FRACTURE) {
-            while (pend) {
-                const int k = __ffs(pend) - 1;
-                pend &= pend - 1;
-                const MixedStencil t = wt[base + k];
-                if (critical_exact64(p.x, p.u, np, i, i + t.delta, md.bbc)) {
-                    clr |= 1u << k;
-                } else {
-                    const MixedU uj = u2_i[t.delta];
-                    MixedBond2 bd;
-                    lean_geometry(t, uj, ri, bd);
-                    const float kf = uj.hi.w * bd.s * bd.rinv;
-                    f[0] += (double)(kf * bd.rxy.x);
-                    f[1] += (double)(kf * bd.rxy.y);
-                    f[2] += (double)(kf * bd.rz);
-                    if (ENERGY) *wtot += (double)(0.25f * uj.hi.w * bd.s * bd.s * t.xi);
-                }
-            }
-            if (clr) nl.mu[(int64_t)(base >> 5) * np + i] = word & ~clr;
-        }
-        if (ENERGY) {
-            const uint32_t valid = lim == 32 ? 0xffffffffu : (1u << lim) - 1u;
-            *intact += __popc(FRACTURE ? (word & ~clr & valid) : valid);
-        }
-    }
-}
-
-template <bool FRACTURE, int MINB, bool PIPE, int FULL = 0>
-__global__ void __launch_bounds__(kBlock, MINB)
+// General mixed PMB kernel: rows that the stencil kernel does not take
+// (irregular rows, tables over its size), one warp per chunk of 32 rows of
+// the warp list, or every chunk in tile order without one. Dynamic shared
+// memory: the stencil table.
+template <bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
     k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
                       const int32_t* __restrict__ wlist, int64_t wcount)
 {
-    // FULL >= 3: lean form (4: with non-coherent gathers, 5: 4 in 4-bond
-    // chunks). Dynamic shared memory: the table, then (lean) one compacted table
-    // of ntab entries per warp of the block. With a warp list (split form),
-    // the warps listed.
     extern __shared__ MixedStencil smem[];
     MixedStencil* tab = smem;
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
     __syncthreads();
-    // The warp's chunk of 32 rows: from the warp list when one is given,
-    // else tiled (tile_chunk).
     int64_t warp;
     if (wlist) {
         const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
@@ -645,26 +480,6 @@ __global__ void __launch_bounds__(kBlock, MINB)
         warp = tile_chunk(nl);
     }
     const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
-    const MixedStencil* wt = tab;
-    int wcnt = md.ntab;
-    if (FULL >= 3 && kind == 3) {
-        // Rows sharing one subset: entry k of the subset goes to slot
-        // (present entries before k) of the warp's compacted table.
-        const int lane = threadIdx.x & 31;
-        const int nmask = (md.ntab + 31) / 32;
-        MixedStencil* mine = smem + md.ntab * (1 + (threadIdx.x >> 5));
-        const uint32_t* wm = mv.warp_pmask + warp * nmask;
-        int before = 0;
-        for (int w = 0; w < nmask; ++w) {
-            const uint32_t pm = wm[w];
-            if ((pm >> lane) & 1u)
-                mine[before + __popc(pm & ((1u << lane) - 1u))] = tab[32 * w + lane];
-            before += __popc(pm);
-        }
-        __syncwarp();
-        wt = mine;
-        wcnt = before;
-    }
     const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
     const int64_t np = p.npad;
@@ -675,81 +490,13 @@ __global__ void __launch_bounds__(kBlock, MINB)
     const uint8_t* __restrict__ code = mv.code + i;
     const MixedU* __restrict__ U2 = mv.u2;
     float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-    if (FULL >= 3 && kind >= 2) {
-        const RowSplit ri{f2(-uhi.x, -uhi.y), f2(-uli.x, -uli.y), -uhi.z, -uli.z, nofail_i};
-        double f[3] = {0.0, 0.0, 0.0};
-        mixed_stencil_rows<FRACTURE, (FULL >= 4), (FULL == 5 ? 4 : 8)>(p, nl, U2 + i, wt, wcnt,
-                                                                        md, i, ri, f);
-        step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
-        return;
-    }
-    if (kind == 2 && FULL == 2) {
+    if (kind == 2) {
         float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
         float sz = 0.f, cz = 0.f;
         mixed_full_rows2<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sxy, cxy, sz,
                                    cz);
         step_epilogue<true>(p, ep, i, (double)sxy.x - (double)cxy.x,
                             (double)sxy.y - (double)cxy.y, (double)sz - (double)cz);
-        return;
-    }
-    if (kind == 2 && FULL == 1) {
-        float sum[3] = {0.f, 0.f, 0.f}, comp[3] = {0.f, 0.f, 0.f};
-        mixed_full_rows<FRACTURE>(p, nl, U2 + i, tab, md, i, uhi, uli, nofail_i, sum, comp);
-        step_epilogue<true>(p, ep, i, (double)sum[0] - (double)comp[0],
-                            (double)sum[1] - (double)comp[1], (double)sum[2] - (double)comp[2]);
-        return;
-    }
-    if (kind == 2 && PIPE) {
-        // Full-stencil warp, software-pipelined: the next entry's table row
-        // and neighbour data are loaded before the current bond is computed.
-        const MixedU* __restrict__ u2_i = U2 + i;
-        MixedStencil tn = tab[0];
-        float4 uhn = u2_i[tn.delta].hi, uln = u2_i[tn.delta].lo;
-        for (int base = 0; base < cnt; base += 32) {
-            uint32_t word = FRACTURE ? nl.mu[(int64_t)(base >> 5) * np + i] : 0xffffffffu;
-            const uint32_t old = word;
-            const int lim = min(32, cnt - base);
-            for (int b = 0; b < lim; ++b) {
-                const int k = base + b;
-                const MixedStencil t = tn;
-                const float4 uhj = uhn, ulj = uln;
-                if (k + 1 < cnt) {
-                    tn = tab[k + 1];
-                    uhn = u2_i[tn.delta].hi;
-                    uln = u2_i[tn.delta].lo;
-                }
-                const float nx = (uhj.x - uhi.x) + (ulj.x - uli.x);
-                const float ny = (uhj.y - uhi.y) + (ulj.y - uli.y);
-                const float nz = (uhj.z - uhi.z) + (ulj.z - uli.z);
-                const float rx = t.x + nx, ry = t.y + ny, rz = t.z + nz;
-                const float r2 = rx * rx + ry * ry + rz * rz;
-                const float rinv = rsqrtf(r2);
-                const float r = r2 * rinv;
-                const float num = nx * (2.f * t.x + nx) + ny * (2.f * t.y + ny) + nz * (2.f * t.z + nz);
-                const float s = __fdividef(num * t.xiinv, r + t.xi);
-                bool intact = true;
-                if (FRACTURE) {
-                    bool crit = false;
-                    if (!nofail_i && ulj.w == 0.f) {
-                        if (fabsf(s - md.s0) <= md.guard)
-                            crit = critical_exact64(p.x, p.u, np, i, i + t.delta, md.bbc);
-                        else
-                            crit = s >= md.s0;
-                    }
-                    if (crit) word &= ~(1u << b);
-                    intact = (word >> b) & 1u;
-                }
-                if (intact) {
-                    const float kf = uhj.w * s * rinv;
-                    kahan_add(sx, cx, kf * rx);
-                    kahan_add(sy, cy, kf * ry);
-                    kahan_add(sz, cz, kf * rz);
-                }
-            }
-            if (FRACTURE && word != old) nl.mu[(int64_t)(base >> 5) * np + i] = word;
-        }
-        step_epilogue<true>(p, ep, i, (double)sx - (double)cx, (double)sy - (double)cy,
-                            (double)sz - (double)cz);
         return;
     }
     if (kind != 0) {
@@ -912,42 +659,6 @@ __device__ __forceinline__ bool lean_prologue(const MixedView& mv, int ntab,
         wcnt = before;
     }
     return true;
-}
-
-// The lean form alone, over a list of warps whose rows are all full stencil
-// rows (kind 2) or share one stencil subset (kind 3); the other warps run
-// k_pmb_force_mixed over their own list. Without the other paths the kernel
-// needs fewer registers.
-// ENERGY: also the energy pass's W_i and phi_i of the rows (the state whose
-// force this launch computes, with the bonds broken in it), the damage from
-// ep.energy_vol_sums (one particle volume).
-template <bool FRACTURE, int MINB, int UNROLL = 8, bool ENERGY = false>
-__global__ void __launch_bounds__(kBlock, MINB)
-    k_pmb_force_lean(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
-                     const int32_t* __restrict__ wlist, int64_t wcount)
-{
-    extern __shared__ MixedStencil smem[];
-    int64_t warp;
-    const MixedStencil* wt;
-    int wcnt;
-    if (!lean_prologue(mv, md.ntab, wlist, wcount, smem, warp, wt, wcnt)) return;
-    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
-    if (i >= p.n) return;
-    const MixedU ui = mv.u2[i];
-    const RowSplit ri{f2(-ui.hi.x, -ui.hi.y), f2(-ui.lo.x, -ui.lo.y), -ui.hi.z, -ui.lo.z,
-                      FRACTURE ? (ui.lo.w != 0.f) : false};
-    double f[3] = {0.0, 0.0, 0.0};
-    if (ENERGY) {
-        double wtot = 0.0;
-        int intact = 0;
-        mixed_stencil_rows<FRACTURE, false, UNROLL, true>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri,
-                                                          f, &wtot, &intact);
-        p.W[i] = wtot;
-        if (FRACTURE) p.phi[i] = 1 - ep.energy_vol_sums[intact] / ep.energy_vol_sums[wcnt];
-    } else {
-        mixed_stencil_rows<FRACTURE, false, UNROLL>(p, nl, mv.u2 + i, wt, wcnt, md, i, ri, f);
-    }
-    step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1386,16 +1097,6 @@ int64_t split_min_rows()
     return v;
 }
 
-// LPS mixed split form (CPD_LPS_MIXED_SPLIT=0: one kernel over all warps).
-bool lps_mixed_split()
-{
-    static const bool v = [] {
-        const char* e = getenv("CPD_LPS_MIXED_SPLIT");
-        return !(e && atoi(e) == 0);
-    }();
-    return v;
-}
-
 // ---------------------------------------------------------------------------
 // Hertzian contact, mixed precision (force/CabanaPD_Contact.hpp:119-168 with
 // force_models/CabanaPD_Hertzian.hpp:23-88 and per-pair radii). The overlap
@@ -1679,41 +1380,6 @@ __global__ void __launch_bounds__(kBlock, 4)
     }
 }
 
-// Mixed-kernel variant, from CPD_MIXED_VARIANT: 0 -> 4 blocks of 256 per SM
-// (64 registers), 1 -> 4 blocks with the full-stencil loop software
-// pipelined, 2 -> pipelined with 3 blocks (more registers), 3 -> full-stencil
-// rows in unrolled 8-bond chunks with branch-free bond bits, 4 -> 3 with the
-// x / y lanes in paired FP32 instructions, 5 -> lean form: FP32 chunk sums
-// added to FP64 row totals instead of Kahan sums, bonds near s0 deferred to
-// an exact test after each 32-bond word, warps whose rows share one stencil
-// subset walking a compacted table, and block warps one lattice row apart;
-// 6 / 7 / 8 -> 5 with non-coherent gathers / 4-bond chunks / 3 blocks per SM;
-// 9 -> split form (default): k_pmb_force_lean over the warps of kinds 2 and 3
-// (warp list in tile order), then 4 over the other warps; 10 / 11 / 12 -> 9
-// with the lean kernel at 5 blocks and 4-bond chunks / 5 blocks and 2-bond
-// chunks / 6 blocks and 2-bond chunks.
-// Full plate on B200, ms per bond-kernel launch (per step for 9-12): 0 / 1 /
-// 2: 4.70 / 4.64 / 4.92; 3 / 4: 4.15 / 4.12 (separate time-step stages);
-// fused steps: 4 4.36; 5 3.28 (3.67 with the exact test inside the bond
-// loop, 4.19 also with consecutive block warps); 6 / 7 / 8 3.91 / 3.90 /
-// 4.64 (before the deferred test); 9 3.07; 10 / 11 / 12 3.84 / 3.50 / 3.77.
-// Also measured and rejected: a kernel for the kind-1 warps that walks the
-// union of its rows' subsets (3.06 per step: no faster, as the boundary
-// lanes idle on the entries they lack; and with plain FP32 chunk sums less
-// accurate on boundary rows); 5 compiled for 5 or 6 blocks per SM (spilling)
-// 4.36 / 7.96; 4 compiled for 3 or 2 blocks per SM 5.05; 4 with the
-// neighbour gathers as cp.async copies into shared memory three bonds ahead
-// 8.28; a shared-memory tile of the lattice with its halo 5.86.
-int mixed_variant()
-{
-    static int v = [] {
-        const char* e = getenv("CPD_MIXED_VARIANT");
-        int x = e ? atoi(e) : 9;
-        return (x < 0 || x > 12) ? 9 : x;
-    }();
-    return v;
-}
-
 #define CPD_TRY(call)                                                     \
     do {                                                                  \
         cudaError_t e_ = (call);                                          \
@@ -1728,7 +1394,9 @@ int mixed_variant()
 void free_mixed(MixedState& m, cudaStream_t st)
 {
     free_stencil64(m, st);
-    void* ptrs[] = {m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
+    delete m.st32;
+    m.st32 = nullptr;
+    void* ptrs[] = {m.xh, m.xl, m.u2_base, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
                     m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab, m.stencil_list,
                     m.irregular_list};
     for (void* q : ptrs)
@@ -1737,7 +1405,8 @@ void free_mixed(MixedState& m, cudaStream_t st)
 }
 
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
-                  MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil)
+                  MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil,
+                  const Model* md_pmb)
 {
     int launches = 0;
     PhaseTrace tr("mixed");
@@ -1748,8 +1417,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
     if (fp32) {
         CPD_TRY(dev_alloc(&m.xh, sizeof(float4) * np, st));
         CPD_TRY(dev_alloc(&m.xl, sizeof(float4) * np, st));
-        CPD_TRY(dev_alloc(&m.u2, sizeof(MixedU) * np, st));
-        m.bytes = (2 * sizeof(float4) + sizeof(MixedU)) * np;
+        m.bytes = 2 * sizeof(float4) * np;
     }
     CPD_TRY(dev_alloc(&m.table, sizeof(MixedStencil) * kMixedGeneric, st));
     CPD_TRY(dev_alloc(&m.code, (size_t)std::max(pd.max_n, 1) * np, st));
@@ -1930,6 +1598,8 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                     }
                     CPD_TRY(cudaStreamSynchronize(st));
                 }
+                if (fp32 && !lps && md_pmb)
+                    prepare_stencil32(*md_pmb, h, tab.data(), m.ntab, m);
                 if (!fp32) {
                     if (!prepare_stencil64(p, *fp64_stencil, h, tab.data(), m.ntab, m, st, err) &&
                         !err.empty())
@@ -1942,6 +1612,16 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 }
             }
         }
+    }
+    if (fp32) {
+        // The split of u, with zero guard records on either side for the
+        // stencil kernel's reads at i + delta of absent entries.
+        if (!m.st32) m.guard = 0;
+        const size_t recs = (size_t)(np + 2 * m.guard);
+        CPD_TRY(dev_alloc(&m.u2_base, sizeof(MixedU) * recs, st));
+        CPD_TRY(cudaMemsetAsync(m.u2_base, 0, sizeof(MixedU) * recs, st));
+        m.u2 = m.u2_base + m.guard;
+        m.bytes += sizeof(MixedU) * recs;
     }
     CPD_TRY(cudaGetLastError());
     tr.mark("lists", st);
@@ -1992,7 +1672,7 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024 &&
+    const bool split = m.lean_list && lean_bytes <= 48 * 1024 &&
                        rows >= split_min_rows();
     const int key = (md.fracture ? 4 : 0) + (md.influence == 1 ? 2 : 0) + (with_m ? 1 : 0);
     int n = 0;
@@ -2042,7 +1722,7 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-    const bool split = lps_mixed_split() && m.lean_list && lean_bytes <= 48 * 1024 &&
+    const bool split = m.lean_list && lean_bytes <= 48 * 1024 &&
                        rows >= split_min_rows();
     const int key = (md.fracture ? 2 : 0) + (md.influence == 1 ? 1 : 0);
     int n = 0;
@@ -2079,74 +1759,6 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
     return n + 1;
 }
 
-namespace {
-
-// Launches one mixed PMB bond-kernel form (mixed_variant); returns the number
-// of kernels launched.
-template <bool FRACTURE>
-int launch_mixed_form_t(const ParticleView& p, const EllView& list, const MixedView& mv,
-                        const MixedModel& mm, const MixedState& m, const StepEpilogue& ep,
-                        int64_t rows, cudaStream_t st)
-{
-    int g = blocks_for(rows);
-    const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
-    // The lean forms hold a compacted table per warp; past 48 KB of shared
-    // memory per block (ntab > 170) the paired form runs instead.
-    int var = mixed_variant();
-    const size_t lean_bytes = (1 + kBlock / 32) * tab_bytes;
-    if (var >= 5 && lean_bytes > 48 * 1024) var = 4;
-    if (var >= 9 && (!m.lean_list || rows < split_min_rows())) var = 5;
-    if (var >= 9) {
-        // Split form: lean warps, then the rest.
-        int n = 0;
-        if (m.nlean > 0) {
-            const int gl = (int)((m.nlean + kBlock / 32 - 1) / (kBlock / 32));
-            if (FRACTURE && ep.energy_vol_sums) var = 13;
-            switch (var) {
-            case 9: k_pmb_force_lean<FRACTURE, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
-            case 13: k_pmb_force_lean<FRACTURE, 4, 8, true><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
-            case 10: k_pmb_force_lean<FRACTURE, 5, 4><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
-            case 11: k_pmb_force_lean<FRACTURE, 5, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
-            default: k_pmb_force_lean<FRACTURE, 6, 2><<<gl, kBlock, lean_bytes, st>>>(p, list, mv, mm, ep, m.lean_list, m.nlean); break;
-            }
-            ++n;
-        }
-        if (m.nrest > 0) {
-            const int gr = (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32));
-            k_pmb_force_mixed<FRACTURE, 4, false, 2><<<gr, kBlock, tab_bytes, st>>>(
-                p, list, mv, mm, ep, m.rest_list, m.nrest);
-            ++n;
-        }
-        return n;
-    }
-    EllView nl = list;
-    if (var >= 5) nl = tile_view(list, rows, kBlock, &g);
-    const size_t sb = var >= 5 ? lean_bytes : tab_bytes;
-    const int32_t* nolist = nullptr;
-    switch (var) {
-    case 0: k_pmb_force_mixed<FRACTURE, 4, false><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 1: k_pmb_force_mixed<FRACTURE, 4, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 2: k_pmb_force_mixed<FRACTURE, 3, true><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 3: k_pmb_force_mixed<FRACTURE, 4, false, 1><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 4: k_pmb_force_mixed<FRACTURE, 4, false, 2><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 6: k_pmb_force_mixed<FRACTURE, 4, false, 4><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 7: k_pmb_force_mixed<FRACTURE, 4, false, 5><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    case 8: k_pmb_force_mixed<FRACTURE, 3, false, 4><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    default: k_pmb_force_mixed<FRACTURE, 4, false, 3><<<g, kBlock, sb, st>>>(p, nl, mv, mm, ep, nolist, 0); break;
-    }
-    return 1;
-}
-
-int launch_mixed_form(bool fracture, const ParticleView& p, const EllView& list,
-                      const MixedView& mv, const MixedModel& mm, const MixedState& m,
-                      const StepEpilogue& ep, int64_t rows, cudaStream_t st)
-{
-    return fracture ? launch_mixed_form_t<true>(p, list, mv, mm, m, ep, rows, st)
-                    : launch_mixed_form_t<false>(p, list, mv, mm, m, ep, rows, st);
-}
-
-}  // namespace
-
 int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Model& md,
                           const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
 {
@@ -2162,59 +1774,31 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Mode
     mm.s_lo = mm.s0 - mm.guard;
     mm.s_hi = mm.s0 + mm.guard;
     mm.ntab = m.ntab;
-    return launch_mixed_form(md.fracture != 0, p, list, mv, mm, m, ep, rows, st);
-}
-
-bool mixed_force_fuses_energy(const ParticleView& p, const Model& md, const MixedState& m)
-{
-    const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-    return md.pd == CPD_PD_PMB && md.fracture && m.vol_sums && m.lean_list && m.nlean > 0 &&
-           mixed_variant() == 9 && lean_bytes <= 48 * 1024 && p.n - p.frozen >= split_min_rows();
-}
-
-// Sum of W_i vol_i and of phi_i over rows [frozen, n), per block.
-__global__ void __launch_bounds__(kBlock)
-    k_row_totals(ParticleView p, double* partials)
-{
-    __shared__ double s_w[kBlock];
-    __shared__ double s_d[kBlock];
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    s_w[threadIdx.x] = i < p.n ? p.W[i] * p.vol[i] : 0.0;
-    s_d[threadIdx.x] = i < p.n ? p.phi[i] : 0.0;
-    __syncthreads();
-    for (int w = kBlock / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            s_w[threadIdx.x] += s_w[threadIdx.x + w];
-            s_d[threadIdx.x] += s_d[threadIdx.x + w];
+    const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
+    if (m.st32) {
+        // Stencil warps on the unrolled table walk, irregular warps on the
+        // general kernel.
+        int n = launch_pd_force_stencil32(p, list, md, m, ep, st);
+        if (m.nirregular > 0) {
+            const int gr = (int)((m.nirregular + kBlock / 32 - 1) / (kBlock / 32));
+            if (md.fracture)
+                k_pmb_force_mixed<true><<<gr, kBlock, tab_bytes, st>>>(
+                    p, list, mv, mm, ep, m.irregular_list, m.nirregular);
+            else
+                k_pmb_force_mixed<false><<<gr, kBlock, tab_bytes, st>>>(
+                    p, list, mv, mm, ep, m.irregular_list, m.nirregular);
+            ++n;
         }
-        __syncthreads();
+        return n;
     }
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x + 0] = s_w[0];
-        partials[2 * blockIdx.x + 1] = s_d[0];
-    }
-}
-
-int launch_energy_rest_and_totals(const ParticleView& p, const EllView& nl, const Model& md,
-                                  const MixedState& m, double* partials, int capacity,
-                                  int* launches, cudaStream_t st)
-{
-    *launches = 0;
-    const int64_t rows = p.n - p.frozen;
-    const int nb = blocks_for(rows);
-    const int gr = (int)((m.nrest + kBlock / 32 - 1) / (kBlock / 32));
-    if (nb > capacity || gr > capacity) return -1;
-    if (gr > 0) {
-        const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
-        const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
-        const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
-        k_energy_mixed<false, 0, true, true, false><<<gr, kBlock, sb, st>>>(
-            p, nl, mv, e, partials, m.rest_list, m.nrest, m.vol_sums);
-        ++*launches;
-    }
-    k_row_totals<<<nb, kBlock, 0, st>>>(p, partials);
-    ++*launches;
-    return nb;
+    // No stencil kernel (a table over its size, or no lattice): the general
+    // kernel over every row.
+    const int g = blocks_for(rows);
+    if (md.fracture)
+        k_pmb_force_mixed<true><<<g, kBlock, tab_bytes, st>>>(p, list, mv, mm, ep, nullptr, 0);
+    else
+        k_pmb_force_mixed<false><<<g, kBlock, tab_bytes, st>>>(p, list, mv, mm, ep, nullptr, 0);
+    return 1;
 }
 
 int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Model& md,

@@ -38,6 +38,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -60,38 +61,48 @@ inline uint32_t hi_word(double v)
     return (uint32_t)(b >> 32);
 }
 
-// h(q) = 1 / (sqrt(1+q) (1 + sqrt(1+q))) interpolated at n Chebyshev nodes
-// of [-Q, Q]; monomial coefficients in q (long double Gaussian elimination
-// on the Vandermonde system in t = q / Q, then scaled by Q^-k).
-void fit_stretch_poly(long double Q, int n, long double* out)
+// h(q) = 1 / (sqrt(1+q) (1 + sqrt(1+q))) as a polynomial of n coefficients
+// on [-Q, Q] (monomial coefficients in q; long double Gaussian elimination on
+// the Vandermonde system in t = q / Q at Chebyshev nodes, then scaled by
+// Q^-k). Unanchored: h interpolated at n nodes. Anchored: the constant term
+// is h(0) = 1/2 exactly and G(q) = (h(q) - 1/2) / q = -(s + 2) / (2 s (1 +
+// s)^2), s = sqrt(1 + q), is interpolated at n - 1 nodes, so the relative
+// error vanishes as q -> 0 instead of leaving a uniform bias of the size of
+// the interpolation error (which the FP32 kernel's 4 coefficients would
+// turn into a systematic stiffness error of ~5e-8).
+void fit_stretch_poly(long double Q, int n, long double* out, bool anchored = false)
 {
+    const int m = anchored ? n - 1 : n;
     long double A[kStencilPoly][kStencilPoly + 1];
-    for (int r = 0; r < n; ++r) {
-        const long double t = cosl(3.141592653589793238462643383279503L * (r + 0.5L) / n);
+    for (int r = 0; r < m; ++r) {
+        const long double t = cosl(3.141592653589793238462643383279503L * (r + 0.5L) / m);
         const long double s = sqrtl(1.0L + t * Q);
         long double pw = 1.0L;
-        for (int c = 0; c < n; ++c) {
+        for (int c = 0; c < m; ++c) {
             A[r][c] = pw;
             pw *= t;
         }
-        A[r][n] = 1.0L / (s * (1.0L + s));
+        A[r][m] = anchored ? -(s + 2.0L) / (2.0L * s * (1.0L + s) * (1.0L + s))
+                           : 1.0L / (s * (1.0L + s));
     }
-    for (int c = 0; c < n; ++c) {
+    for (int c = 0; c < m; ++c) {
         int piv = c;
-        for (int r = c + 1; r < n; ++r)
+        for (int r = c + 1; r < m; ++r)
             if (fabsl(A[r][c]) > fabsl(A[piv][c])) piv = r;
-        for (int k = 0; k <= n; ++k) std::swap(A[c][k], A[piv][k]);
+        for (int k = 0; k <= m; ++k) std::swap(A[c][k], A[piv][k]);
         const long double d = A[c][c];
-        for (int k = 0; k <= n; ++k) A[c][k] /= d;
-        for (int r = 0; r < n; ++r) {
+        for (int k = 0; k <= m; ++k) A[c][k] /= d;
+        for (int r = 0; r < m; ++r) {
             if (r == c) continue;
             const long double f = A[r][c];
-            for (int k = 0; k <= n; ++k) A[r][k] -= f * A[c][k];
+            for (int k = 0; k <= m; ++k) A[r][k] -= f * A[c][k];
         }
     }
+    const int o = anchored ? 1 : 0;
+    if (anchored) out[0] = 0.5L;
     long double qk = 1.0L;
-    for (int k = 0; k < n; ++k) {
-        out[k] = A[k][n] / qk;
+    for (int k = 0; k < m; ++k) {
+        out[k + o] = A[k][m] / qk;
         qk *= Q;
     }
 }
@@ -161,10 +172,86 @@ __device__ __forceinline__ void stencil_bond64(const StencilEntry64& e, const do
     fz = fma(F, e.ez + hz, fz);
 }
 
+// Row i's present and intact table entries as entry-order bits (bit k of
+// ew[w] = entry 32 w + k). Kind-2 rows hold the whole table, so bond slot k
+// is entry k; other stencil rows hold the entries of their presence mask in
+// table order, so their s-th present entry is bond slot s.
+template <bool FRACTURE>
+__device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilRows& sr,
+                                               int ntab, int nwords, int kind, int64_t i,
+                                               int64_t np, uint32_t (&ew)[4])
+{
+    uint32_t pm[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        uint32_t full = 0u;
+        if (w < nwords) {
+            const int rem = ntab - 32 * w;
+            full = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+        }
+        pm[w] = w < nwords ? (kind == 2 ? full : sr.pmask[(int64_t)w * np + i]) : 0u;
+    }
+    if (!FRACTURE) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) ew[w] = pm[w];
+        return;
+    }
+    uint32_t mw[4];
+    int cnt = 0, intact = 0;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        mw[w] = w < nwords ? nl.mu[(int64_t)w * np + i] : 0u;
+        cnt += __popc(pm[w]);
+        intact += __popc(mw[w]);
+    }
+    if (kind == 2) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) ew[w] = mw[w] & pm[w];
+    } else if (intact == cnt) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) ew[w] = pm[w];
+    } else {
+        // Slot order -> entry order: the s-th present entry takes the s-th
+        // bit of the slot-order words.
+        int sw = 0, sb = 0;
+        uint32_t src = mw[0];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint32_t out = 0u, q = pm[w];
+            while (q) {
+                const int b = __ffs(q) - 1;
+                q &= q - 1;
+                out |= (src & 1u) << b;
+                src >>= 1;
+                if (++sb == 32) {
+                    sb = 0;
+                    ++sw;
+                    src = sw == 1 ? mw[1] : (sw == 2 ? mw[2] : mw[3]);
+                }
+            }
+            ew[w] = out;
+        }
+    }
+}
+
+// Marks broken the bond of row i at table entry 32 w + b (its slot: the
+// row's present entries before it).
+__device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilRows& sr,
+                                               int kind, int64_t i, int64_t np, int w, int b)
+{
+    int s = 32 * w + b;
+    if (kind != 2) {
+        s = 0;
+        for (int v = 0; v < w; ++v) s += __popc(sr.pmask[(int64_t)v * np + i]);
+        s += __popc(sr.pmask[(int64_t)w * np + i] & ((1u << b) - 1u));
+    }
+    nl.mu[(int64_t)(s >> 5) * np + i] &= ~(1u << (s & 31));
+}
+
 // One warp per chunk of 32 rows of the stencil warp list; each row walks the
 // whole table (NT >= ntab entries, unrolled), and its own entries that are
-// present and intact are the bits of ew (entry order: bit k of word w =
-// entry 32 w + k). NP: coefficients of the stretch polynomial.
+// present and intact are the bits of ew. NP: coefficients of the stretch
+// polynomial.
 template <bool FRACTURE, bool UNIFORM, int NT, int NP>
 __global__ void __launch_bounds__(kBlock, 4)
     k_pmb_stencil64(ParticleView p, EllView nl, StencilRows sr,
@@ -175,61 +262,11 @@ __global__ void __launch_bounds__(kBlock, 4)
     if (slot >= sr.wcount) return;
     const int64_t warp = sr.wlist[slot];
     const int64_t i = p.frozen + 32 * warp + lane;
-    const bool live = i < p.n;
+    if (i >= p.n) return;
     const int64_t np = p.npad;
     const int kind = sr.warp_kind[warp];
-    uint32_t pm[4], ew[4];
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        uint32_t full = 0u;
-        if (w < st.nwords) {
-            const int rem = st.ntab - 32 * w;
-            full = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
-        }
-        pm[w] = (w < st.nwords && live) ? (kind == 2 ? full : sr.pmask[(int64_t)w * np + i]) : 0u;
-    }
-    if (!live) return;
-    if (FRACTURE) {
-        uint32_t mw[4];
-        int cnt = 0, intact = 0;
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            mw[w] = w < st.nwords ? nl.mu[(int64_t)w * np + i] : 0u;
-            cnt += __popc(pm[w]);
-            intact += __popc(mw[w]);
-        }
-        if (kind == 2) {
-#pragma unroll
-            for (int w = 0; w < 4; ++w) ew[w] = mw[w] & pm[w];
-        } else if (intact == cnt) {
-#pragma unroll
-            for (int w = 0; w < 4; ++w) ew[w] = pm[w];
-        } else {
-            // Slot order -> entry order: the row's s-th present entry holds
-            // slot s; its bit is the s-th bit of the slot-order words.
-            int sw = 0, sb = 0;
-            uint32_t src = mw[0];
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                uint32_t out = 0u, q = pm[w];
-                while (q) {
-                    const int b = __ffs(q) - 1;
-                    q &= q - 1;
-                    out |= (src & 1u) << b;
-                    src >>= 1;
-                    if (++sb == 32) {
-                        sb = 0;
-                        ++sw;
-                        src = sw == 1 ? mw[1] : (sw == 2 ? mw[2] : mw[3]);
-                    }
-                }
-                ew[w] = out;
-            }
-        }
-    } else {
-#pragma unroll
-        for (int w = 0; w < 4; ++w) ew[w] = pm[w];
-    }
+    uint32_t ew[4];
+    row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
     const double4 ui = U4[i];
     const char* __restrict__ rb = reinterpret_cast<const char*>(U4 + i);
     double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -237,7 +274,10 @@ __global__ void __launch_bounds__(kBlock, 4)
     // Fully unrolled, every entry of the table for every row: an absent entry
     // (no bit in ew) reads the record at i + delta_k (a neighbour, or a zero
     // guard record) and adds nothing, which costs less than a branch per
-    // entry. Entries past ntab are zero-filled and add nothing either.
+    // entry. Entries past ntab are zero-filled and add nothing either. (A
+    // loop over chunks of 8 entries with the table in shared memory keeps
+    // the code inside the instruction cache but waits on the shared-memory
+    // loads: 4.75 vs 3.25 ms per step on the full plate.)
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
         const int w = k >> 5;
@@ -258,16 +298,8 @@ __global__ void __launch_bounds__(kBlock, 4)
                 const int b = __ffs(q) - 1;
                 q &= q - 1;
                 const int k = 32 * w + b;
-                if (!exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
-                    continue;
-                // Broken: clear its slot's bit (slot = present entries before k).
-                int s = k;
-                if (kind != 2) {
-                    s = 0;
-                    for (int v = 0; v < w; ++v) s += __popc(sr.pmask[(int64_t)v * np + i]);
-                    s += __popc(sr.pmask[(int64_t)w * np + i] & ((1u << b) - 1u));
-                }
-                nl.mu[(int64_t)(s >> 5) * np + i] &= ~(1u << (s & 31));
+                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
+                    clear_bond_bit(nl, sr, kind, i, np, w, b);
             }
         }
         fx = f[0];
@@ -275,6 +307,169 @@ __global__ void __launch_bounds__(kBlock, 4)
         fz = f[2];
     }
     step_epilogue<false>(p, ep, i, fx, fy, fz);
+}
+
+// Two rows per thread: the warp takes two chunks of the warp list and each
+// lane walks the table for one row of each, so every entry's code and
+// constants serve two rows (half the instruction fetch per bond) and the
+// two rows' chains interleave.
+template <bool FRACTURE>
+__device__ __forceinline__ void finish_pending(const ParticleView& p, const EllView& nl,
+                                               const StencilRows& sr, const Stencil64& st,
+                                               int kind, int64_t i, int64_t np,
+                                               const uint32_t (&pend)[4], double (&f)[3])
+{
+    if (!(pend[0] | pend[1] | pend[2] | pend[3])) return;
+    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        uint32_t q = pend[w];
+        while (q) {
+            const int b = __ffs(q) - 1;
+            q &= q - 1;
+            const int k = 32 * w + b;
+            if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
+                clear_bond_bit(nl, sr, kind, i, np, w, b);
+        }
+    }
+}
+
+template <bool FRACTURE, bool UNIFORM, int NT, int NP>
+__global__ void __launch_bounds__(kBlock, 2)
+    k_pmb_stencil64x2(ParticleView p, EllView nl, StencilRows sr,
+                      const double4* __restrict__ U4, StepEpilogue ep, const Stencil64 st)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t sa = 2 * ((int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5));
+    if (sa >= sr.wcount) return;
+    const bool hasb = sa + 1 < sr.wcount;
+    const int64_t wa = sr.wlist[sa], wb = hasb ? sr.wlist[sa + 1] : wa;
+    const int64_t ia = p.frozen + 32 * wa + lane, ib = p.frozen + 32 * wb + lane;
+    const bool la = ia < p.n, lb = hasb && ib < p.n;
+    if (!la && !lb) return;
+    const int64_t np = p.npad;
+    // A row that does not exist reads a live row's records and adds nothing.
+    const int64_t ra = la ? ia : ib, rbw = lb ? ib : ra;
+    const int ka = sr.warp_kind[wa], kb = sr.warp_kind[wb];
+    uint32_t ewa[4] = {0u, 0u, 0u, 0u}, ewb[4] = {0u, 0u, 0u, 0u};
+    if (la) row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, ka, ia, np, ewa);
+    if (lb) row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kb, ib, np, ewb);
+    const double4 uia = U4[ra], uib = U4[rbw];
+    const char* __restrict__ pa = reinterpret_cast<const char*>(U4 + ra);
+    const char* __restrict__ pb = reinterpret_cast<const char*>(U4 + rbw);
+    double fa[3] = {0.0, 0.0, 0.0}, fb[3] = {0.0, 0.0, 0.0};
+    uint32_t penda[4] = {0u, 0u, 0u, 0u}, pendb[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const int w = k >> 5;
+        const uint32_t bit = 1u << (k & 31);
+        const StencilEntry64& e = st.e[k];
+        const double4 uja = *reinterpret_cast<const double4*>(pa + e.boff);
+        const double4 ujb = *reinterpret_cast<const double4*>(pb + e.boff);
+        stencil_bond64<UNIFORM, NP>(e, st.h, uja, uia, (ewa[w] & bit) != 0u, bit, penda[w],
+                                    fa[0], fa[1], fa[2]);
+        stencil_bond64<UNIFORM, NP>(e, st.h, ujb, uib, (ewb[w] & bit) != 0u, bit, pendb[w],
+                                    fb[0], fb[1], fb[2]);
+    }
+    if (la) {
+        finish_pending<FRACTURE>(p, nl, sr, st, ka, ia, np, penda, fa);
+        step_epilogue<false>(p, ep, ia, fa[0], fa[1], fa[2]);
+    }
+    if (lb) {
+        finish_pending<FRACTURE>(p, nl, sr, st, kb, ib, np, pendb, fb);
+        step_epilogue<false>(p, ep, ib, fb[0], fb[1], fb[2]);
+    }
+}
+
+// Mixed precision (CPD_MIXED, PMB): the same table walk in FP32 on the FP32
+// split of u (MixedU: hi.xyz + lo.xyz, hi.w = c vol, lo.w = no-fail flag).
+// eta = (hi_j - hi_i) + (lo_j - lo_i) keeps ~1e-7 relative accuracy under
+// large rigid motion; num, q and the pair force as in the FP64 kernel, with
+// an FP32 polynomial (kStencilPoly32 coefficients, anchored at h(0) = 1/2:
+// error ~3e-8 relative at the plate's window edge, vanishing with q). Pair
+// forces are summed in FP32 over chunks of 8 entries and each chunk sum is
+// added to the FP64 row force. Bonds within 1e-4 s0 of the
+// break (in q) or outside the polynomial's range take the FP64 exact path.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// x and y in paired FP32 operations (FADD2 / FMUL2 / FFMA2), z alone.
+template <bool UNIFORM>
+__device__ __forceinline__ void stencil_bond32(const StencilEntry32& e, const float* h,
+                                               const MixedU& uj, const float2& nh_xy,
+                                               float nh_z, const float2& nl_xy, float nl_z,
+                                               bool on, uint32_t bit, uint32_t& pend,
+                                               float2& cxy, float& cz)
+{
+    const float2 hxy = __fadd2_rn(__fadd2_rn(f2(uj.hi.x, uj.hi.y), nh_xy),
+                                  __fadd2_rn(f2(uj.lo.x, uj.lo.y), nl_xy));
+    const float hz = (uj.hi.z + nh_z) + (uj.lo.z + nl_z);
+    const float2 pxy = __fmul2_rn(hxy, __fadd2_rn(hxy, e.txy));
+    const float num = fmaf(hz, hz + e.tz, pxy.x + pxy.y);
+    const float q = num * e.ixi2;
+    const float t = fmaf(fmaf(fmaf(h[3], q, h[2]), q, h[1]), q, h[0]);
+    float F = (num * e.K) * t;
+    if (!UNIFORM) F *= uj.hi.w;
+    const bool in = (__float_as_uint(num) & 0x7fffffffu) < e.khi;
+    if (on && !in) pend |= bit;
+    F = (on && in) ? F : 0.f;
+    cxy = __ffma2_rn(f2(F, F), __fadd2_rn(e.exy, hxy), cxy);
+    cz = fmaf(F, e.ez + hz, cz);
+}
+
+template <bool FRACTURE, bool UNIFORM, int NT>
+__global__ void __launch_bounds__(kBlock, 3)
+    k_pmb_stencil32(ParticleView p, EllView nl, StencilRows sr, const MixedU* __restrict__ U2,
+                    StepEpilogue ep, const Stencil32 st)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    if (slot >= sr.wcount) return;
+    const int64_t warp = sr.wlist[slot];
+    const int64_t i = p.frozen + 32 * warp + lane;
+    if (i >= p.n) return;
+    const int64_t np = p.npad;
+    const int kind = sr.warp_kind[warp];
+    uint32_t ew[4];
+    row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
+    const MixedU ui = U2[i];
+    const float2 nh_xy = f2(-ui.hi.x, -ui.hi.y), nl_xy = f2(-ui.lo.x, -ui.lo.y);
+    const float nh_z = -ui.hi.z, nl_z = -ui.lo.z;
+    const char* __restrict__ rb = reinterpret_cast<const char*>(U2 + i);
+    double f[3] = {0.0, 0.0, 0.0};
+    float2 cxy = f2(0.f, 0.f);
+    float cz = 0.f;
+    uint32_t pend[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const int w = k >> 5;
+        const uint32_t bit = 1u << (k & 31);
+        const StencilEntry32& e = st.e[k];
+        const MixedU uj = *reinterpret_cast<const MixedU*>(rb + e.boff);
+        stencil_bond32<UNIFORM>(e, st.h, uj, nh_xy, nh_z, nl_xy, nl_z, (ew[w] & bit) != 0u, bit,
+                                pend[w], cxy, cz);
+        if ((k & 7) == 7 || k == NT - 1) {
+            f[0] += (double)cxy.x;
+            f[1] += (double)cxy.y;
+            f[2] += (double)cz;
+            cxy = f2(0.f, 0.f);
+            cz = 0.f;
+        }
+    }
+    if (pend[0] | pend[1] | pend[2] | pend[3]) {
+        const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint32_t q = pend[w];
+            while (q) {
+                const int b = __ffs(q) - 1;
+                q &= q - 1;
+                const int k = 32 * w + b;
+                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
+                    clear_bond_bit(nl, sr, kind, i, np, w, b);
+            }
+        }
+    }
+    step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
 }
 
 }  // namespace
@@ -336,7 +531,9 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
         const long double xi = sqrtl(x2);
         e.ixi2 = (double)(1.0L / x2);
         e.K = (double)(scale / (xi * x2));
-        e.doff = tab[k].delta;
+        // An entry that no row holds (a thin body) has no index delta: its
+        // bonds are absent everywhere, and it reads the row's own record.
+        e.doff = tab[k].delta == INT32_MAX ? 0 : tab[k].delta;
         e.boff = (int64_t)e.doff * (int64_t)sizeof(double4);
         // |num| below T = qwin xi^2 when the high word of |num| is below
         // T's: every such num is below T (conservative by < 2^-20 of T).
@@ -360,6 +557,82 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
     return true;
 }
 
+bool prepare_stencil32(const Model& md, const double* h, const MixedStencil* tab, int ntab,
+                       MixedState& m)
+{
+    delete m.st32;
+    m.st32 = nullptr;
+    if (md.pd != CPD_PD_PMB || ntab <= 0 || ntab > kStencilMax) return false;
+    Stencil32* S = new Stencil32();
+    S->ntab = ntab;
+    S->nwords = (ntab + 31) / 32;
+    S->bbc = md.bond_break_coeff;
+    S->c = md.c;
+    const bool uniform = m.vol_sums != nullptr;
+    const long double scale = (long double)md.c * (uniform ? (long double)m.vol_uniform : 1.0L);
+    // Window |q| < qwin: the break band of the FP32 kernels (stretch within
+    // 1e-4 s0 of s0) and the polynomial's range.
+    const double s_lo = md.s0 * (1.0 - 1e-4);
+    const double qc_lo = (1.0 + s_lo) * (1.0 + s_lo) - 1.0;
+    const double qwin = md.fracture ? std::min(kStencilQ, qc_lo) : kStencilQ;
+    long double hc[kStencilPoly] = {};
+    fit_stretch_poly(qwin > 1e-6 ? (long double)qwin : 1e-6L, kStencilPoly32, hc, true);
+    for (int k = 0; k < kStencilPoly32; ++k) S->h[k] = (float)hc[k];
+    int64_t G = 0;
+    for (int k = 0; k < ntab; ++k) {
+        StencilEntry32& e = S->e[k];
+        const double a = std::nearbyint((double)tab[k].x / h[0]);
+        const double b = std::nearbyint((double)tab[k].y / h[1]);
+        const double c = std::nearbyint((double)tab[k].z / h[2]);
+        const double vx = a * h[0], vy = b * h[1], vz = c * h[2];
+        e.exy = make_float2((float)vx, (float)vy);
+        e.ez = (float)vz;
+        e.txy = make_float2(2.f * e.exy.x, 2.f * e.exy.y);
+        e.tz = 2.f * e.ez;
+        // Lengths of the FP32 vectors the kernel works with, so that the
+        // force law is consistent with the geometry it sees: constants from
+        // the FP64 lengths would give each bond length class a stiffness
+        // error of ~1e-7 that accumulates over a run (measured: 1.2e-6 vs
+        // 5e-7 in u after 100 steps of the 41^3 elastic wave).
+        const long double fx = e.exy.x, fy = e.exy.y, fz = e.ez;
+        const long double x2 = fx * fx + fy * fy + fz * fz;
+        e.ixi2 = (float)(1.0L / x2);
+        e.K = (float)(scale / (sqrtl(x2) * x2));
+        e.doff = tab[k].delta == INT32_MAX ? 0 : tab[k].delta;  // (as in the FP64 table)
+        e.boff = (int64_t)e.doff * (int64_t)sizeof(MixedU);
+        const float T = (float)(qwin * (double)x2);
+        uint32_t tb;
+        std::memcpy(&tb, &T, sizeof tb);
+        e.khi = qwin > 0.0 ? tb : 0u;
+        G = std::max<int64_t>(G, std::abs((int64_t)e.doff));
+    }
+    m.st32 = S;
+    m.guard = G + 32;
+    return true;
+}
+
+int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
+                              const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
+{
+    if (p.n - p.frozen <= 0 || m.nstencil <= 0) return 0;
+    const StencilRows sr{m.warp_kind, m.pmask, m.stencil_list, m.nstencil};
+    const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
+    const bool uniform = m.vol_sums != nullptr;
+    const Stencil32& S = *m.st32;
+    const bool t122 = S.ntab == 122;
+#define CPD_ST32(F, U, NT) \
+    k_pmb_stencil32<F, U, NT><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2, ep, S)
+    if (!uniform) {
+        if (md.fracture) CPD_ST32(true, false, 128); else CPD_ST32(false, false, 128);
+    } else if (md.fracture) {
+        if (t122) CPD_ST32(true, true, 122); else CPD_ST32(true, true, 128);
+    } else {
+        if (t122) CPD_ST32(false, true, 122); else CPD_ST32(false, true, 128);
+    }
+#undef CPD_ST32
+    return 1;
+}
+
 int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_t end,
                    double4* u4, cudaStream_t st)
 {
@@ -378,8 +651,15 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
         const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
         const bool uniform = m.vol_sums != nullptr;
         const Stencil64& S = *m.st64;
-#define CPD_ST64(F, U, NT, NP) \
-    k_pmb_stencil64<F, U, NT, NP><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S)
+        static const bool x2 = getenv("CPD_EXP_X2") != nullptr;
+        const int g2 = (int)((m.nstencil + kBlock / 16 - 1) / (kBlock / 16));
+#define CPD_ST64(F, U, NT, NP)                                                               \
+    do {                                                                                     \
+        if (x2)                                                                              \
+            k_pmb_stencil64x2<F, U, NT, NP><<<g2, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S);  \
+        else                                                                                 \
+            k_pmb_stencil64<F, U, NT, NP><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S);     \
+    } while (0)
         // Unrolled forms: the 122-entry table of a cubic lattice at a
         // 3.01-spacing horizon, else 128 entries (zero past ntab).
         const bool t122 = S.ntab == 122;

@@ -162,3 +162,14 @@ def test_five_spacing_horizon(cuda, oracle, precision):
     g, o = _run(cuda, oracle, prob, precision, 20)
     assert g.neighbor_stats()[0] > 500
     _check(g, o, precision)
+
+
+@pytest.mark.parametrize("precision", [FAST, MIXED])
+def test_thin_plate_with_stencil_entries_no_row_holds(cuda, oracle, precision):
+    """Two cell layers: the stencil table (built from the horizon) has
+    entries two and three layers apart that no row holds. The stencil
+    kernels walk every entry; those read the row's own record and add
+    nothing (they once carried an unset index delta)."""
+    prob = _plate((40, 20, 2))
+    g, o = _run(cuda, oracle, prob, precision, 30)
+    _check(g, o, precision)

@@ -596,24 +596,21 @@ def test_fragmenting_cylinder_fp64_and_mixed(cuda, oracle):
 
 
 def test_step_energy_equals_step_then_energy(cuda, oracle):
-    """cpd_step_energy (the Solver's output step in one call; on the mixed
-    split form with one particle volume the lean rows' energy comes out of
-    the last step's bond pass) against cpd_step + cpd_compute_energy on the
-    same system: same states bit for bit, damage field and total bit for
-    bit, strain energy within FP32 rounding of its terms; and the oracle's
-    totals."""
+    """cpd_step_energy (the Solver's output step in one call) against
+    cpd_step + cpd_compute_energy on the same system: states, fields and
+    totals bit for bit; and the oracle's totals."""
     prob = P.plate_impact(num_cells=(96, 48, 6), steps=120, v0=60.0)
     a = cuda.System(dict(prob["params"], precision=MIXED))
     b = cuda.System(dict(prob["params"], precision=MIXED))
     o = oracle.OracleSystem(prob["params"])
     for s in (a, b, o):
         P.setup(s, prob)
-    # The initial state's fields from init (the force pass forms the lean
-    # rows' energy) against the energy pass on the same state.
+    # The initial state's fields from init against the energy pass on the
+    # same state.
     w0, phi0 = a.get("W"), a.get("phi")
     a.compute_energy()
     assert np.array_equal(phi0, a.get("phi"))
-    assert _nrel(w0, a.get("W")) <= 1e-6
+    assert np.array_equal(w0, a.get("W"))
     for _ in range(6):
         wa, da = a.step_energy(20)
         b.step(20)
@@ -623,8 +620,8 @@ def test_step_energy_equals_step_then_energy(cuda, oracle):
         for fld in ("u", "v", "f", "phi"):
             assert np.array_equal(a.get(fld), b.get(fld)), fld
         assert np.array_equal(a.neighbors()[2], b.neighbors()[2])
-        assert _nrel(a.get("W"), b.get("W")) <= 1e-6
-        assert _rel(da, db) <= 1e-14 and _rel(wa, wb) <= 1e-6
+        assert np.array_equal(a.get("W"), b.get("W"))
+        assert (wa, da) == (wb, db)
         assert _rel(da, do) <= 1e-12 and _rel(wa, wo) <= 1e-6
     assert da > 0
 
@@ -663,12 +660,12 @@ def test_mixed_with_unequal_volumes(cuda, oracle, model):
 
 
 def test_split_forms_on_small_systems():
-    """The split mixed forms (k_pmb_force_lean / k_lps_*_lean over the lists
-    of full-stencil and shared-subset warps, the general kernels over the
-    rest, and the energy fused into the lean kernel by cpd_step_energy) run
-    on systems of 2^20 rows and more; a child process forces them onto the
-    small mixed test systems (CPD_SPLIT_MIN_ROWS=0) and runs the mixed
-    parity tests there with the same bars."""
+    """The split mixed forms (the LPS lean kernels over the lists of
+    full-stencil and shared-subset warps with the general kernels over the
+    rest, and the mixed energy pass in the same two parts) run on systems of
+    2^20 rows and more; a child process forces them onto the small mixed
+    test systems (CPD_SPLIT_MIN_ROWS=0) and runs the mixed parity tests
+    there with the same bars."""
     import os
     import subprocess
     import sys
