@@ -277,7 +277,9 @@ __global__ void __launch_bounds__(kBlock, 4)
     // entry. Entries past ntab are zero-filled and add nothing either. (A
     // loop over chunks of 8 entries with the table in shared memory keeps
     // the code inside the instruction cache but waits on the shared-memory
-    // loads: 4.75 vs 3.25 ms per step on the full plate.)
+    // loads: 4.75 vs 3.25 ms per step on the full plate; two rows per thread
+    // halves the instruction fetch per bond but needs 128 registers, and
+    // at 2 blocks per SM: 3.76 ms.)
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
         const int w = k >> 5;
@@ -307,78 +309,6 @@ __global__ void __launch_bounds__(kBlock, 4)
         fz = f[2];
     }
     step_epilogue<false>(p, ep, i, fx, fy, fz);
-}
-
-// Two rows per thread: the warp takes two chunks of the warp list and each
-// lane walks the table for one row of each, so every entry's code and
-// constants serve two rows (half the instruction fetch per bond) and the
-// two rows' chains interleave.
-template <bool FRACTURE>
-__device__ __forceinline__ void finish_pending(const ParticleView& p, const EllView& nl,
-                                               const StencilRows& sr, const Stencil64& st,
-                                               int kind, int64_t i, int64_t np,
-                                               const uint32_t (&pend)[4], double (&f)[3])
-{
-    if (!(pend[0] | pend[1] | pend[2] | pend[3])) return;
-    const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        uint32_t q = pend[w];
-        while (q) {
-            const int b = __ffs(q) - 1;
-            q &= q - 1;
-            const int k = 32 * w + b;
-            if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
-                clear_bond_bit(nl, sr, kind, i, np, w, b);
-        }
-    }
-}
-
-template <bool FRACTURE, bool UNIFORM, int NT, int NP>
-__global__ void __launch_bounds__(kBlock, 2)
-    k_pmb_stencil64x2(ParticleView p, EllView nl, StencilRows sr,
-                      const double4* __restrict__ U4, StepEpilogue ep, const Stencil64 st)
-{
-    const int lane = threadIdx.x & 31;
-    const int64_t sa = 2 * ((int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5));
-    if (sa >= sr.wcount) return;
-    const bool hasb = sa + 1 < sr.wcount;
-    const int64_t wa = sr.wlist[sa], wb = hasb ? sr.wlist[sa + 1] : wa;
-    const int64_t ia = p.frozen + 32 * wa + lane, ib = p.frozen + 32 * wb + lane;
-    const bool la = ia < p.n, lb = hasb && ib < p.n;
-    if (!la && !lb) return;
-    const int64_t np = p.npad;
-    // A row that does not exist reads a live row's records and adds nothing.
-    const int64_t ra = la ? ia : ib, rbw = lb ? ib : ra;
-    const int ka = sr.warp_kind[wa], kb = sr.warp_kind[wb];
-    uint32_t ewa[4] = {0u, 0u, 0u, 0u}, ewb[4] = {0u, 0u, 0u, 0u};
-    if (la) row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, ka, ia, np, ewa);
-    if (lb) row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kb, ib, np, ewb);
-    const double4 uia = U4[ra], uib = U4[rbw];
-    const char* __restrict__ pa = reinterpret_cast<const char*>(U4 + ra);
-    const char* __restrict__ pb = reinterpret_cast<const char*>(U4 + rbw);
-    double fa[3] = {0.0, 0.0, 0.0}, fb[3] = {0.0, 0.0, 0.0};
-    uint32_t penda[4] = {0u, 0u, 0u, 0u}, pendb[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-    for (int k = 0; k < NT; ++k) {
-        const int w = k >> 5;
-        const uint32_t bit = 1u << (k & 31);
-        const StencilEntry64& e = st.e[k];
-        const double4 uja = *reinterpret_cast<const double4*>(pa + e.boff);
-        const double4 ujb = *reinterpret_cast<const double4*>(pb + e.boff);
-        stencil_bond64<UNIFORM, NP>(e, st.h, uja, uia, (ewa[w] & bit) != 0u, bit, penda[w],
-                                    fa[0], fa[1], fa[2]);
-        stencil_bond64<UNIFORM, NP>(e, st.h, ujb, uib, (ewb[w] & bit) != 0u, bit, pendb[w],
-                                    fb[0], fb[1], fb[2]);
-    }
-    if (la) {
-        finish_pending<FRACTURE>(p, nl, sr, st, ka, ia, np, penda, fa);
-        step_epilogue<false>(p, ep, ia, fa[0], fa[1], fa[2]);
-    }
-    if (lb) {
-        finish_pending<FRACTURE>(p, nl, sr, st, kb, ib, np, pendb, fb);
-        step_epilogue<false>(p, ep, ib, fb[0], fb[1], fb[2]);
-    }
 }
 
 // Mixed precision (CPD_MIXED, PMB): the same table walk in FP32 on the FP32
@@ -651,15 +581,8 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
         const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
         const bool uniform = m.vol_sums != nullptr;
         const Stencil64& S = *m.st64;
-        static const bool x2 = getenv("CPD_EXP_X2") != nullptr;
-        const int g2 = (int)((m.nstencil + kBlock / 16 - 1) / (kBlock / 16));
-#define CPD_ST64(F, U, NT, NP)                                                               \
-    do {                                                                                     \
-        if (x2)                                                                              \
-            k_pmb_stencil64x2<F, U, NT, NP><<<g2, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S);  \
-        else                                                                                 \
-            k_pmb_stencil64<F, U, NT, NP><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S);     \
-    } while (0)
+#define CPD_ST64(F, U, NT, NP) \
+    k_pmb_stencil64<F, U, NT, NP><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, ep, S)
         // Unrolled forms: the 122-entry table of a cubic lattice at a
         // 3.01-spacing horizon, else 128 entries (zero past ntab).
         const bool t122 = S.ntab == 122;
