@@ -1,8 +1,8 @@
 """Generates tests/golden/reference_expectations.json from the reference's
 own test sources (read as text; the reference cannot be built here).
 
-Run from the repository root in a container that has the reference tree:
-    python tests/golden/make_golden.py /root/reference
+Run from the repository root, naming the CabanaPD source tree:
+    python tests/golden/make_golden.py <path to the CabanaPD tree>
 The tests read only the committed JSON, never the reference tree.
 """
 import json
@@ -58,4 +58,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the CabanaPD tree>")
+    main(sys.argv[1])
