@@ -18,11 +18,13 @@ plate, the LPS fracture box (8.0 M particles), the Hertzian DEM packing
 (4.0 M spheres) and the 41^3 PMB elastic wave, each mixed beside plain FP64
 with the error between them.
 
-`serving` (N = 1): a served stream of independent PMB/LPS jobs through the
-job server (continuous batching, mixed precision): capacity from a
-saturated pass, then Poisson arrivals at 0.8 x capacity with p50/p99 job
-latency, beside the same jobs run one at a time on the plain FP64 path
-(--serve-jobs 512 --serve-n 1e3 2e6 for the full 512-job stream).
+`serving` (N = 1): the served stream of 512 independent PMB/LPS jobs
+(particles log-uniform in [1e3, 2e6], 200-2000 steps) through the job
+server (continuous batching, mixed precision, jobs of at most 32768
+particles advanced in batch groups): capacity from a saturated pass, then
+Poisson arrivals at 0.8 x capacity with p50/p99 job latency, the per-job
+server (batch groups off) on the same saturated stream, and the same jobs
+one at a time on the plain FP64 path under the same arrivals in real time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -347,8 +349,9 @@ def _time_system(s, stream, device, steps, warmup):
     s.step(steps)
     ev1.record(stream)
     torch.cuda.synchronize(device)
-    k_ms, k_n, _ = s.kernel_time()
-    return ev0.elapsed_time(ev1), k_ms / max(k_n, 1)
+    k_ms, k_n, k_bytes = s.kernel_time()
+    s.set_kernel_timing(False)
+    return ev0.elapsed_time(ev1), k_ms / max(k_n, 1), k_bytes
 
 
 def other_workload(name, steps):
@@ -392,12 +395,33 @@ def measure_other(name, device, stream, steps, warmup):
         s.set_stream(stream.cuda_stream)
         P.setup(s, prob)
         _, bonds0 = s.neighbor_stats()
-        ms, k_avg = _time_system(s, stream, device, steps, warmup)
+        ms, k_avg, k_bytes = _time_system(s, stream, device, steps, warmup)
         _, bonds1 = s.neighbor_stats()
         bonds = 0.5 * (bonds0 + bonds1) if name == "dem" else bonds0
         res[prec] = dict(precision=prec, ms_per_step=ms / steps,
                          value=bonds * steps / (ms / 1e3), kernel=kernel[prec],
                          kernel_ms_avg=k_avg)
+        hbm, hbm_kind = peaks()
+        rows = s.n - prob["n_frozen"]
+        if name == "lps":
+            # Both row passes of a step: the force pass's bytes (as the
+            # library counts them) plus the weighted-volume / dilatation
+            # pass (read x, u, vol, count, write m, theta and the two force
+            # factors: 92 B per row; 4 B index + 1/8 B bond bit per bond),
+            # over the whole step's time.
+            step_bytes = k_bytes + 92.0 * rows + 4.125 * bonds0
+            achieved = step_bytes / (ms / steps / 1e3) / 1e9
+            res[prec]["roofline"] = {
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": hbm_kind,
+                "algorithmic_bytes_per_step": step_bytes, "timed": "whole step"}
+        elif name == "dem":
+            achieved = k_bytes / (k_avg / 1e3) / 1e9
+            res[prec]["roofline"] = {
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": hbm_kind,
+                "algorithmic_bytes_per_launch": k_bytes,
+                "timed": "contact kernel with the step epilogue"}
         if name == "dem":
             res[prec]["contact_rebuilds"] = s.contact_rebuilds()
             res[prec]["contacts"] = bonds
@@ -405,15 +429,27 @@ def measure_other(name, device, stream, steps, warmup):
     head = precs[0]
     out = dict(wl, particles=systems[head].n, bonds=bonds, steps=steps, warmup=warmup,
                unit="bond-updates/s", **res[head])
+    if name == "dem" and DEM_FULL_STEPS > warmup + steps:
+        # The packing's mixed-vs-FP64 error over its full run (few pairs
+        # overlap in the first steps, where both Hertz kernels skip them).
+        for s in systems.values():
+            s.step(DEM_FULL_STEPS - warmup - steps)
+            s.synchronize()
+        out_steps = DEM_FULL_STEPS
+    else:
+        out_steps = warmup + steps
     if "fp64" in res and head != "fp64":
         a, b = systems[head], systems["fp64"]
-        err = {}
+        err = {"after_steps": out_steps}
         fields = ("u", "v", "f", "theta") if name == "lps" else ("u", "v", "f")
         for fld in fields:
             x, y = a.get(fld), b.get(fld)
             err[fld] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
         if prob["params"].get("fracture"):
             err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
+        if name == "dem":
+            err["contact_rebuilds"] = [a.contact_rebuilds(), b.contact_rebuilds()]
+            err["contacts"] = [a.neighbor_stats()[1], b.neighbor_stats()[1]]
         out["plain_fp64"] = res["fp64"]
         out["mixed_vs_plain"] = res["fp64"]["ms_per_step"] / res[head]["ms_per_step"]
         out["mixed_error_vs_fp64"] = err
@@ -424,6 +460,7 @@ def measure_other(name, device, stream, steps, warmup):
 
 E2E_JOBS = 3
 OTHER_STEPS = {"lps": 20, "plate_1p2m": 100, "wave": 100, "dem": 50}
+DEM_FULL_STEPS = 5000  # the packing's full run, for its mixed-vs-FP64 error
 
 
 def run_gpu(args, world, rank, local, pg):
@@ -530,25 +567,27 @@ def _latency_summary(lat):
 
 def run_serving(args, device):
     """Served stream: independent PMB/LPS jobs through the job server
-    (mixed precision), beside the same jobs run one at a time on the plain
-    FP64 path. Three passes over the same seeded jobs:
-    1. saturated: all jobs submitted at t = 0; capacity = jobs / makespan;
+    (mixed precision). Passes over the same seeded jobs:
+    1. saturated: all jobs submitted at t = 0 (batch groups on for jobs of
+       at most --serve-batch particles); capacity = jobs / makespan;
     2. served: Poisson arrivals at 0.8 x capacity (seeded), latency =
        finish - arrival for every job;
-    3. one at a time, plain FP64: each job alone (set-up, steps, energy,
-       u read back), timed; its FIFO latencies under the same arrivals
-       follow from those measured service times (a single server that takes
-       jobs in order: start = max(arrival, previous finish))."""
+    3. per-job server, saturated: the same server with batch groups off
+       (every job on its own stream and graph), for comparison;
+    4. one at a time, plain FP64, the same arrivals in real time: each job
+       alone (set-up, steps, energy, u read back) once it has arrived and
+       the previous one is done; latency = finish - arrival."""
     import cabanapd_b200
     n_lo, n_hi = args.serve_n
     jobs = P.served_jobs(count=args.serve_jobs, n_range=(n_lo, n_hi),
                          steps_range=tuple(args.serve_steps), seed=args.serve_seed)
     budget = int(args.serve_budget_gb * 1e9)
 
-    def serve(arrivals):
+    def serve(arrivals, batch_max):
         srv = cabanapd_b200.Server(device=device, max_active=args.serve_active,
                                    steps_per_launch=args.serve_k, hbm_budget_bytes=budget,
-                                   setup_threads=args.serve_setup_threads)
+                                   setup_threads=args.serve_setup_threads,
+                                   batch_max_particles=batch_max)
         ids = []
         t0 = time.perf_counter()
         for prob, at in zip(jobs, arrivals):
@@ -574,36 +613,43 @@ def run_serving(args, device):
                 "jobs_per_s": len(sts) / span, "latency_s": _latency_summary(lat),
                 "queue_wait_s": _latency_summary(wait),
                 "setup_s": dict(_latency_summary(setup), total=sum(setup)),
+                "batched_jobs": sum(1 for j in jobs if batch_max > 0 and j["x"].shape[0] <= batch_max),
                 "peak_resident_bytes": stats["peak_resident_bytes"],
                 "gpu_launches": stats["kernel_launches"]}
 
-    saturated = serve([0.0] * len(jobs))
+    saturated = serve([0.0] * len(jobs), args.serve_batch)
     capacity = saturated["jobs_per_s"]
     rate = 0.8 * capacity
     rng = np.random.Generator(np.random.PCG64(args.serve_seed + 1))
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs))).tolist()
-    served = serve(arrivals)
+    served = serve(arrivals, args.serve_batch)
+    per_job = None if args.serve_quick else serve([0.0] * len(jobs), 0)
 
-    service, bonds_total = [], 0
-    for prob in jobs:
-        t0 = time.perf_counter()
+    # One at a time on the plain FP64 path, the same arrivals in real time.
+    lat, service, bonds_total = [], [], 0
+    t0 = time.perf_counter()
+    for prob, at in zip(jobs, arrivals):
+        idle = at - (time.perf_counter() - t0)
+        if idle > 0:
+            time.sleep(idle)
+        ts = time.perf_counter()
         s = cabanapd_b200.System(dict(prob["params"], device=device, precision=PRECISION["fp64"]))
         P.setup(s, prob)
         s.run(prob["num_steps"])
         s.compute_energy()
         s.get("u")
-        service.append(time.perf_counter() - t0)
+        tf = time.perf_counter()
+        service.append(tf - ts)
+        lat.append(tf - t0 - at)
         bonds_total += s.neighbor_stats()[1] * prob["num_steps"]
         s.close()
-    finish, lat = 0.0, []
-    for at, sv in zip(arrivals, service):
-        finish = max(at, finish) + sv
-        lat.append(finish - at)
-    one_at_a_time = {"service_time_sum_s": sum(service),
-                     "throughput_bond_updates_per_s": bonds_total / sum(service),
+    span = time.perf_counter() - t0
+    one_at_a_time = {"arrivals": "the served pass's Poisson arrivals, in real time",
+                     "makespan_s": span, "service_time_sum_s": sum(service),
+                     "throughput_bond_updates_per_s": bonds_total / span,
                      "latency_s": _latency_summary(lat)}
     kinds = {k: sum(1 for j in jobs if j["kind"] == k) for k in ("wave", "plate", "lps")}
-    return {
+    out = {
         "workload": (f"{len(jobs)} independent jobs: {kinds['wave']} PMB elastic-wave cubes, "
                      f"{kinds['plate']} PMB notched plates, {kinds['lps']} LPS random-notch "
                      f"boxes; particles log-uniform in [{n_lo:.0f}, {n_hi:.0f}], steps "
@@ -612,6 +658,7 @@ def run_serving(args, device):
         "precision": "mixed (FP32 bonds / FP64 state, PMB and LPS)",
         "server": {"max_active": args.serve_active, "steps_per_launch": args.serve_k,
                    "setup_threads": args.serve_setup_threads,
+                   "batch_max_particles": args.serve_batch,
                    "cuda_graphs": True, "hbm_budget_bytes": budget},
         "capacity_jobs_per_s": capacity,
         "saturated": saturated,
@@ -621,6 +668,11 @@ def run_serving(args, device):
         "throughput_vs_one_at_a_time": (served["throughput_bond_updates_per_s"] /
                                         one_at_a_time["throughput_bond_updates_per_s"]),
     }
+    if per_job is not None:
+        out["per_job_server_saturated"] = per_job
+        out["batched_vs_per_job_saturated"] = (saturated["throughput_bond_updates_per_s"] /
+                                               per_job["throughput_bond_updates_per_s"])
+    return out
 
 
 def run_e2e(args, prob, device, stream, pg, total_bonds, prec):
@@ -703,10 +755,13 @@ def main():
                     help="omit the LPS-box and DEM-packing measurements")
     ap.add_argument("--only-other", choices=["lps", "dem", "plate_1p2m", "wave"], default=None,
                     help="measure only that workload (for profiling) and print it")
-    ap.add_argument("--serve-jobs", type=int, default=96,
-                    help="served stream: number of jobs (512 for the full stream)")
-    ap.add_argument("--serve-n", type=float, nargs=2, default=[1e3, 2e5],
-                    help="served stream: particle-count range (1e3 2e6 for the full stream)")
+    ap.add_argument("--serve-jobs", type=int, default=512, help="served stream: number of jobs")
+    ap.add_argument("--serve-n", type=float, nargs=2, default=[1e3, 2e6],
+                    help="served stream: particle-count range")
+    ap.add_argument("--serve-batch", type=int, default=32768,
+                    help="served stream: jobs of at most this many particles run in batch groups")
+    ap.add_argument("--serve-quick", action="store_true",
+                    help="served stream: omit the per-job-server comparison pass")
     ap.add_argument("--serve-steps", type=int, nargs=2, default=[200, 2000])
     ap.add_argument("--serve-seed", type=int, default=20261203)
     ap.add_argument("--serve-active", type=int, default=16)

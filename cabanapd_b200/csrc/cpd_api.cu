@@ -128,6 +128,13 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
         if (s_ != CPD_OK) return s_;                                                \
     } while (0)
 
+#define CPD_NOT_IN_BATCH(sys)                                                       \
+    do {                                                                            \
+        if ((sys) && (sys)->batch)                                                  \
+            return set_error(CPD_ERR_STATE, "the system belongs to a batch "        \
+                                            "(cpd_batch_destroy releases it)");     \
+    } while (0)
+
 struct cpd_system {
     cpd_params params{};
     Model md;
@@ -174,6 +181,9 @@ struct cpd_system {
     MixedU* u2_alt_base = nullptr;  // allocation: u2_alt with the split's guard records
     bool neighbors_built = false;
     bool initialized = false;
+    // The batch that advances this system (cpd_batch_create); while set,
+    // calls that change the system's state are refused.
+    const void* batch = nullptr;
     bool stress_ready = false;  // cpd_compute_stress ran since the particles were set
     double max_disp = 0.0;
     int64_t steps_since_rebuild = 0;
@@ -433,12 +443,13 @@ bool use_mixed(const cpd_system* s)
     return wants_mixed(s) && (s->md.pd == CPD_PD_PMB || s->mixed.lps_ok);
 }
 
-// CPD_FP64 PMB without contact on a lattice: the stencil kernel takes the
-// stencil rows (set up with the neighbour list when wants_stencil64).
+// CPD_FP64 PMB or LPS without contact on a lattice: the stencil kernels take
+// the stencil rows (set up with the neighbour list when wants_stencil64; LPS
+// needs one particle volume and every row a stencil row).
 bool wants_stencil64(const cpd_system* s)
 {
     return s->params.precision == CPD_FP64 && s->md.contact == CPD_CONTACT_NONE &&
-           s->md.pd == CPD_PD_PMB;
+           (s->md.pd == CPD_PD_PMB || s->md.pd == CPD_PD_LPS);
 }
 
 bool use_stencil64(const cpd_system* s)
@@ -486,6 +497,12 @@ cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, const MixedState
         CPD_LAUNCHED(launch_lps_mtheta_mixed(p, pd_view(s), s->md, m, compute_m, s->stream));
         return CPD_OK;
     }
+    if (use_stencil64(s)) {
+        // m.u4 holds p.u (the fused step keeps it so; lps_prepare packs it).
+        CPD_LAUNCHED(launch_lps_mtheta_stencil64(p, pd_view(s), s->md, m, compute_m,
+                                                 s->stream));
+        return CPD_OK;
+    }
     if (use_fast(s)) {
         CPD_LAUNCHED(launch_lps_m_theta_fast(p, pd_view(s), s->md, compute_m, s->stream));
         return CPD_OK;
@@ -497,7 +514,9 @@ cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, const MixedState
 
 cpd_status lps_prepare(cpd_system* s, bool compute_m)
 {
-    return lps_prepare_on(s, view(s), s->mixed, compute_m);
+    const ParticleView p = view(s);
+    if (use_stencil64(s)) CPD_LAUNCHED(launch_pack_u4(p, p.u, 0, p.n, s->mixed.u4, s->stream));
+    return lps_prepare_on(s, p, s->mixed, compute_m);
 }
 
 cpd_status contact_force(cpd_system* s, bool reset)
@@ -830,6 +849,83 @@ cpd_status check_ready(const cpd_system* s, bool need_neighbors)
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Hooks for the batched step (cpd_batch.cu).
+namespace cpd {
+
+cpd_status batch_attach(cpd_system* s, const void* batch, BatchInstance* out, int64_t* bonds)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    if (s->batch) return set_error(CPD_ERR_STATE, "the system already belongs to a batch");
+    if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before batching a system");
+    if (!has_pd(s) || has_contact(s))
+        return set_error(CPD_ERR_INVALID_ARGUMENT,
+                         "a batch takes peridynamic systems without contact");
+    if (s->params.precision == CPD_FP64_EXACT)
+        return set_error(CPD_ERR_INVALID_ARGUMENT,
+                         "a batch runs the CPD_FP64 or CPD_MIXED kernels, not CPD_FP64_EXACT");
+    if (!fused_ready(s))
+        return set_error(CPD_ERR_STATE,
+                         "the system's boundary conditions do not fit the fused step");
+    CPD_CUDA(cudaSetDevice(s->device));
+    BatchInstance b;
+    std::memset(static_cast<void*>(&b), 0, sizeof b);
+    b.p = view(s);
+    b.nl = pd_view(s);
+    b.ep.dt = s->params.dt;
+    b.ep.half_dt = 0.5 * s->params.dt;
+    b.ep.c = mixed_wscale(s->md);
+    b.ep.bc_bits = s->bc_bits;
+    b.ep.bc_row = s->bc_row;
+    b.ep.bc_keep = s->bc_keep;
+    b.ep.bc_add = s->bc_add;
+    b.ep.nbc = s->nbc;
+    b.u_alt = s->u_alt;
+    b.fm = to_fast(s->md);
+    b.wscale = mixed_wscale(s->md);
+    b.pd = s->md.pd;
+    b.fracture = s->md.fracture;
+    b.influence = s->md.influence;
+    const MixedState& m = s->mixed;
+    if (use_mixed(s)) {
+        b.body = kBatchMixed;
+        b.mv = MixedView{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
+        b.u2_alt = s->u2_alt;
+        b.ab = m.ab;
+        b.mm = to_mixed_model(s->md, m);
+        b.ml = to_mixed_lps(s->md, m);
+    } else if (use_fast(s)) {
+        b.body = kBatchFast;
+    } else {
+        return set_error(CPD_ERR_INVALID_ARGUMENT, "no batch kernel for this model");
+    }
+    // Frozen rows are never integrated: the second buffers take them once.
+    if (s->frozen > 0) {
+        const size_t bytes = sizeof(double) * (size_t)s->frozen;
+        for (int d = 0; d < 3; ++d)
+            CPD_CUDA(cudaMemcpyAsync(s->u_alt + (size_t)d * s->npad, s->u + (size_t)d * s->npad,
+                                     bytes, cudaMemcpyDeviceToDevice, s->stream));
+        if (b.body == kBatchMixed)
+            CPD_CUDA(cudaMemcpyAsync(s->u2_alt, m.u2, sizeof(MixedU) * (size_t)s->frozen,
+                                     cudaMemcpyDeviceToDevice, s->stream));
+    }
+    *out = b;
+    *bonds = s->pd.total;
+    s->batch = batch;
+    return CPD_OK;
+}
+
+void batch_detach(cpd_system* s)
+{
+    if (s) s->batch = nullptr;
+}
+
+cudaStream_t system_stream(const cpd_system* s) { return s->stream; }
+int system_device(const cpd_system* s) { return s->device; }
+int64_t system_rows(const cpd_system* s) { return s->n - s->frozen; }
+
+}  // namespace cpd
+
 // ===========================================================================
 extern "C" {
 
@@ -947,6 +1043,7 @@ cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
 
 cpd_status cpd_system_destroy(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     if (!s) return CPD_OK;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
@@ -993,6 +1090,7 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
                                 const double* vol, const double* rho, const int32_t* nofail,
                                 const double* radius)
 {
+    CPD_NOT_IN_BATCH(s);
     if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
     if (n <= 0 || n >= (int64_t)1 << 31 || n_frozen < 0 || n_frozen > n || !x || !vol)
         return set_error(CPD_ERR_INVALID_ARGUMENT, "cpd_upload_particles: bad arguments");
@@ -1065,6 +1163,7 @@ cpd_status cpd_upload_particles(cpd_system* s, int64_t n, int64_t n_frozen, cons
 
 cpd_status cpd_set_state(cpd_system* s, const double* u, const double* v)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, false));
     CPD_CUDA(cudaSetDevice(s->device));
     if (u) CPD_OK_OR_RETURN(upload_vector(s, u, s->u));
@@ -1077,6 +1176,7 @@ cpd_status cpd_set_state(cpd_system* s, const double* u, const double* v)
 
 cpd_status cpd_build_neighbors(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, false));
     CPD_CUDA(cudaSetDevice(s->device));
     std::string err;
@@ -1165,6 +1265,7 @@ cpd_status cpd_download_neighbors(cpd_system* s, int32_t* counts, int32_t* indic
 cpd_status cpd_prenotch(cpd_system* s, int32_t count, const double* v1, const double* v2,
                         const double* p0)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     if (!has_pd(s) || !s->md.fracture)
         return set_error(CPD_ERR_STATE, "Cannot create prenotch in system without fracture.");
@@ -1198,6 +1299,7 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
                                       int64_t count, const int64_t* indices,
                                       const double* values)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, false));
     if (kind < CPD_BC_FORCE_VALUE || kind > CPD_BC_FORCE_ADD || count < 0 || !values ||
         (count > 0 && !indices))
@@ -1241,6 +1343,7 @@ cpd_status cpd_add_boundary_condition(cpd_system* s, int32_t kind, int32_t compo
 
 cpd_status cpd_clear_boundary_conditions(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
     CPD_CUDA(cudaStreamSynchronize(s->stream));
     for (auto& bc : s->bcs) {
@@ -1256,6 +1359,7 @@ cpd_status cpd_clear_boundary_conditions(cpd_system* s)
 
 cpd_status cpd_compute_weighted_volume(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     if (is_lps(s)) CPD_LAUNCHED(launch_lps_weighted_volume(view(s), pd_view(s), s->md, s->stream));
@@ -1265,6 +1369,7 @@ cpd_status cpd_compute_weighted_volume(cpd_system* s)
 
 cpd_status cpd_compute_dilatation(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare(s, false));
@@ -1283,6 +1388,7 @@ cpd_status refresh_mixed_u(cpd_system* s)
 
 cpd_status cpd_compute_force(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     CPD_OK_OR_RETURN(refresh_mixed_u(s));
@@ -1363,6 +1469,7 @@ cpd_status cpd_compute_stress(cpd_system* s)
 // force model), energy, force BCs at t = 0.
 cpd_status cpd_init(cpd_system* s)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
     CPD_OK_OR_RETURN(refresh_mixed_u(s));
@@ -1390,6 +1497,7 @@ cpd_status cpd_init(cpd_system* s)
 // CabanaPD_Solver.hpp:332-375 runStep(step, bc), num_steps times.
 cpd_status cpd_step(cpd_system* s, int32_t num_steps)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step");
     if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
@@ -1414,6 +1522,7 @@ cpd_status cpd_step(cpd_system* s, int32_t num_steps)
 
 cpd_status cpd_step_energy(cpd_system* s, int32_t num_steps, double* total_W, double* total_D)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step_energy");
     if (num_steps < 0) return set_error(CPD_ERR_INVALID_ARGUMENT, "num_steps < 0");
@@ -1429,6 +1538,7 @@ cpd_status cpd_step_energy(cpd_system* s, int32_t num_steps, double* total_W, do
 
 cpd_status cpd_step_stage(cpd_system* s, int32_t stage)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     if (!s->initialized) return set_error(CPD_ERR_STATE, "call cpd_init before cpd_step_stage");
     CPD_CUDA(cudaSetDevice(s->device));
@@ -1578,6 +1688,7 @@ cpd_status cpd_save_state(cpd_system* s, void* buf, uint64_t bytes)
 
 cpd_status cpd_load_state(cpd_system* s, const void* buf, uint64_t bytes)
 {
+    CPD_NOT_IN_BATCH(s);
     CPD_OK_OR_RETURN(check_ready(s, true));
     if (!s->initialized) return set_error(CPD_ERR_STATE, "cpd_load_state: call cpd_init first");
     if (!buf || bytes < sizeof(StateHeader))

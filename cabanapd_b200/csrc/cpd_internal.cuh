@@ -141,6 +141,28 @@ inline EllView tile_view(EllView v, int64_t rows, int block, int* grid)
     return v;
 }
 
+// Model constants of the throughput kernels, as the kernels take them:
+// the FP64 form (cpd_kernels_fast.cu) and the FP32 forms of the mixed PMB
+// and LPS kernels (cpd_kernels_mixed.cu), with the guard band of the FP64
+// re-test around s0.
+struct FastModel {
+    double c, theta_coeff, s_coeff, bond_break_coeff;
+};
+struct MixedModel {
+    float c, s0, guard;
+    float s_lo, s_hi;  // s0 - guard, s0 + guard
+    double bbc;
+    int ntab;
+};
+struct MixedLps {
+    float s0, guard;
+    float s_lo, s_hi;  // s0 - guard, s0 + guard
+    double bbc;
+    double theta_coeff, s_coeff;
+    int ntab;
+    float vol;  // the particle volume when the packed records are used
+};
+
 // Everything a particle kernel needs, passed by value.
 struct ParticleView {
     int64_t n, frozen, npad;
@@ -303,6 +325,31 @@ struct Stencil64 {
     double h[kStencilPoly];
     StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
 };
+// LPS form of the FP64 stencil table (one particle volume v). With q = (r^2 -
+// xi^2) / xi^2 the stretch is s = q S(q), S(q) = 1 / (1 + sqrt(1 + q)), and
+// xi / r = W(q) = 1 / sqrt(1 + q), both as polynomials on the entry window;
+// the weighted-volume weight omega xi^2 v and the force factor omega xi v /
+// xi (times W = xi / r gives omega xi v / r) are entry constants
+// (force_models/CabanaPD_LPS.hpp:85-134).
+struct __align__(16) StencilEntryL64 {
+    double ex, ey, ez;        // bond reference vector xi (FP64 lattice offset)
+    double tx, ty, tz;        // 2 xi
+    double ixi2;              // 1 / xi^2
+    double wv;                // omega xi^2 v (influence 0: xi^2 v; 1: xi v)
+    double fv;                // omega v (influence 0: v; 1: v / xi)
+    int64_t boff;             // (neighbour index - particle index) * 32: record bytes
+    int32_t doff;             // neighbour index - particle index
+    uint32_t kwin;            // |num| inside the polynomials' window: high word below kwin
+    uint32_t kbrk;            // ... and below the break band (force pass)
+    uint32_t pad;
+};
+struct StencilL64 {
+    int32_t ntab = 0, nwords = 0;
+    double bbc = 0, theta_coeff = 0, s_coeff = 0;
+    double hs[kStencilPoly];  // S(q), monomial coefficients (past the degree: 0)
+    double hw[kStencilPoly];  // W(q)
+    StencilEntryL64 e[kStencilMax];  // past ntab: zero (no contribution, never deferred)
+};
 // The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
 constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial
 struct __align__(16) StencilEntry32 {
@@ -388,6 +435,12 @@ struct MixedState {
     // records (u_x, u_y, u_z, vol) with `guard` zero records on either side,
     // so i + delta of an absent stencil entry stays inside the allocation.
     Stencil64* st64 = nullptr;
+    // FP64 LPS stencil path: its table, and per particle (a, b) = (theta_coeff
+    // theta / m, s_coeff / m) as one 16-byte gather record, with the guard
+    // records of u4 on either side.
+    StencilL64* stl64 = nullptr;
+    double2* ab64 = nullptr;       // record of particle 0
+    double2* ab64_base = nullptr;  // allocation
     // Mixed PMB stencil kernel: its table, and the allocation behind u2
     // (u2 = u2_base + guard; `guard` zero records on either side).
     Stencil32* st32 = nullptr;
@@ -425,6 +478,10 @@ int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_
                    double4* u4, cudaStream_t st);
 int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
+// FP64 LPS stencil path: weighted volume (with_m) and dilatation of every
+// row from the gather records m.u4 (which must hold p.u).
+int launch_lps_mtheta_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
+                                const MixedState& m, bool with_m, cudaStream_t st);
 int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                             const MixedState& m, bool with_m, cudaStream_t st);
 double mixed_wscale(const Model& md);
@@ -463,5 +520,84 @@ int launch_ell_to_rows(const NeighborList& nl, int64_t n, int64_t npad,
                        const int32_t* perm, const int32_t* user_id,
                        int32_t* counts, int32_t* indices, int32_t* mu,
                        cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Batched step of many systems (cpd_batch.cu). Each instance is a set-up
+// system; the batch kernels read its device views from a table
+// (BatchInstance, one per instance) and take their rows in tiles of up to
+// kBatchTileWarps chunks of 32 rows of one instance. Per chunk of K steps an
+// instance advances r = min(K, remaining) steps: the first half step into
+// buffer (r - 1) & 1 (0: the system's own arrays, 1: its second buffers), then
+// per step s < r one bond pass whose epilogue writes the other buffer, so
+// that the last step ends in the system's arrays, as cpd_step's fused step.
+constexpr int kBatchTileWarps = 8;
+// Step s of a K-step chunk for an instance with `remaining` steps left:
+// r = min(K, remaining); the step runs when s < r, reads buffer cur =
+// ((r - 1) ^ s) & 1 and writes the other, and its epilogue takes the next
+// first half step (mode 2) but on the last step (mode 1).
+struct BatchStep {
+    int run, cur, mode;
+};
+__host__ __device__ inline BatchStep batch_step(int32_t remaining, int32_t K, int32_t s)
+{
+    const int32_t r = remaining < K ? remaining : K;
+    BatchStep b;
+    b.run = s < r;
+    b.cur = ((r - 1) ^ s) & 1;
+    b.mode = s + 1 < r ? 2 : 1;
+    return b;
+}
+enum BatchBody : int32_t { kBatchFast = 0, kBatchMixed = 1 };
+struct BatchInstance {
+    ParticleView p;      // p.u: buffer 0 (the system's displacement)
+    EllView nl;          // PD list (mu null without fracture)
+    StepEpilogue ep;     // dt, boundary-condition row program, split factor
+    MixedView mv;        // mixed body: mv.u2 = buffer 0's FP32 split
+    double* u_alt;       // buffer 1
+    MixedU* u2_alt;      // buffer 1's split (mixed body)
+    float2* ab;          // mixed LPS: FP32 force factors per particle
+    FastModel fm;
+    MixedModel mm;
+    MixedLps ml;
+    double wscale;       // the mixed split's factor (c for PMB, 1 for LPS)
+    int32_t body;        // BatchBody
+    int32_t pd;          // CPD_PD_PMB or CPD_PD_LPS
+    int32_t fracture, influence;
+};
+struct BatchTile {
+    int32_t inst;        // instance
+    int32_t warp0;       // first chunk of 32 rows (counted from the first movable row)
+    int32_t nwarps;      // chunks in the tile (<= kBatchTileWarps)
+    int32_t lps;         // 1: the instance is an LPS instance
+};
+// One pass of step s of a K-step chunk over the tiles of one body: pass 0
+// the LPS weighted volume / dilatation of LPS tiles, pass 1 the bond force
+// and step epilogue. Persistent blocks: grid blocks take tiles grid apart.
+int launch_batch_fast(const BatchInstance* inst, const int32_t* remaining,
+                      const BatchTile* tiles, int32_t ntiles, int32_t K, int32_t s,
+                      int32_t pass, int grid, cudaStream_t st);
+int launch_batch_mixed(const BatchInstance* inst, const int32_t* remaining,
+                       const BatchTile* tiles, int32_t ntiles, int32_t K, int32_t s,
+                       int32_t pass, int grid, cudaStream_t st);
+// Resident blocks per SM of the batch kernels (occupancy at their launch
+// bounds), for the persistent grid.
+int batch_fast_blocks_per_sm();
+int batch_mixed_blocks_per_sm();
+// System side of a batch (cpd_api.cu): batch_attach validates system s
+// (set up, initialised, PD without contact, CPD_FP64 or CPD_MIXED, fused step
+// prepared), fills its table entry and directed-bond count, and marks it as
+// advanced by `batch` (state-changing calls are then refused until
+// batch_detach).
+cpd_status batch_attach(cpd_system* s, const void* batch, BatchInstance* out, int64_t* bonds);
+void batch_detach(cpd_system* s);
+cudaStream_t system_stream(const cpd_system* s);
+int system_device(const cpd_system* s);
+int64_t system_rows(const cpd_system* s);
+// The stream a batch issues its chunks on (cpd_batch.cu).
+cudaStream_t batch_stream(const cpd_batch* b);
+// Model constant forms of the throughput kernels.
+FastModel to_fast(const Model& m);
+MixedModel to_mixed_model(const Model& md, const MixedState& m);
+MixedLps to_mixed_lps(const Model& md, const MixedState& m);
 
 }  // namespace cpd

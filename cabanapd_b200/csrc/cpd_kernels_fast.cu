@@ -34,10 +34,6 @@ constexpr double kGuard = 1e-12;
 
 inline int blocks_for(int64_t rows) { return (int)((rows + kBlock - 1) / kBlock); }
 
-struct FastModel {
-    double c, theta_coeff, s_coeff, bond_break_coeff;
-};
-
 // The reference's break test for bond vector xi = (xx, xy, xz) and deformed
 // vector r = (rx, ry, rz), with every operation rounded separately.
 __device__ __noinline__ bool critical_exact(double xx, double xy, double xz, double rx,
@@ -175,20 +171,13 @@ struct IndexStream {
 // 256 threads per SM (64 registers). With a warp list the warps take the
 // listed chunks of 32 rows (the irregular rows beside the stencil kernel),
 // else one thread per row from the first row on.
+// Row i's bonds, force boundary condition and step epilogue (the body of
+// k_pmb_force_fast and of the batch kernel's PMB rows).
 template <bool FRACTURE>
-__global__ void __launch_bounds__(kBlock, 4)
-    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep,
-                     const int32_t* __restrict__ wlist, int64_t wcount)
+__device__ __forceinline__ void pmb_fast_row(const ParticleView& p, const EllView& nl,
+                                             const FastModel& md, const StepEpilogue& ep,
+                                             int64_t i)
 {
-    int64_t i;
-    if (wlist) {
-        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-        if (slot >= wcount) return;
-        i = p.frozen + 32 * (int64_t)wlist[slot] + (threadIdx.x & 31);
-    } else {
-        i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    }
-    if (i >= p.n) return;
     const int64_t np = p.npad;
     const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
     const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
@@ -233,17 +222,32 @@ __global__ void __launch_bounds__(kBlock, 4)
     step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
+template <bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_pmb_force_fast(ParticleView p, EllView nl, FastModel md, StepEpilogue ep,
+                     const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    int64_t i;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        i = p.frozen + 32 * (int64_t)wlist[slot] + (threadIdx.x & 31);
+    } else {
+        i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    }
+    if (i >= p.n) return;
+    pmb_fast_row<FRACTURE>(p, nl, md, ep, i);
+}
+
 // LPS weighted volume and dilatation in ONE pass over the row
 // (force/CabanaPD_LPS.hpp:89-141, :287-378): both sums accumulate per bond,
 // theta_i = 3 sum(omega s xi^2 vol_j) / m_i at the end (the reference divides
 // each term by m_i; the factored division differs by rounding only). With
 // WITH_M false, m_i is read (the elastic model computes it once).
 template <int INFL, bool FRACTURE, bool WITH_M>
-__global__ void __launch_bounds__(kBlock, 4)
-    k_lps_m_theta_1pass(ParticleView p, EllView nl, FastModel md)
+__device__ __forceinline__ void lps_m_theta_row(const ParticleView& p, const EllView& nl,
+                                                const FastModel& md, int64_t i)
 {
-    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
     const int64_t np = p.npad;
     const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
     const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
@@ -272,14 +276,22 @@ __global__ void __launch_bounds__(kBlock, 4)
     p.lps_b[i] = md.s_coeff / mi;
 }
 
-// LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447) with the row's
-// indices streamed two bonds ahead, compiled for 4 blocks of 256 per SM.
-template <int INFL, bool FRACTURE>
+template <int INFL, bool FRACTURE, bool WITH_M>
 __global__ void __launch_bounds__(kBlock, 4)
-    k_lps_force_pf(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
+    k_lps_m_theta_1pass(ParticleView p, EllView nl, FastModel md)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
+    lps_m_theta_row<INFL, FRACTURE, WITH_M>(p, nl, md, i);
+}
+
+// LPS force (force/CabanaPD_LPS.hpp:143-181, :380-447) with the row's
+// indices streamed two bonds ahead, compiled for 4 blocks of 256 per SM.
+template <int INFL, bool FRACTURE>
+__device__ __forceinline__ void lps_force_row(const ParticleView& p, const EllView& nl,
+                                              const FastModel& md, const StepEpilogue& ep,
+                                              int64_t i)
+{
     const int64_t np = p.npad;
     const double xi0 = p.x[i], xi1 = p.x[np + i], xi2v = p.x[2 * np + i];
     const double ui0 = p.u[i], ui1 = p.u[np + i], ui2 = p.u[2 * np + i];
@@ -324,6 +336,15 @@ __global__ void __launch_bounds__(kBlock, 4)
     }
     if (FRACTURE && dirty && cnt > 0) nl.mu[(int64_t)((cnt - 1) >> 5) * np + i] = word;
     step_epilogue<false>(p, ep, i, fx, fy, fz);
+}
+
+template <int INFL, bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_force_pf(ParticleView p, EllView nl, FastModel md, StepEpilogue ep)
+{
+    const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    lps_force_row<INFL, FRACTURE>(p, nl, md, ep, i);
 }
 
 // Strain energy density and damage at output steps (force/CabanaPD_PMB.hpp:
@@ -412,12 +433,95 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// Batched step over many systems (cpd_batch.cu): persistent blocks take
+// tiles grid apart; a tile is up to kBatchTileWarps chunks of 32 rows of one
+// instance, whose table entry is staged in shared memory when the block's
+// instance changes. Rows run the bodies of the single-system kernels above
+// (pass 0: LPS weighted volume when fracture, and dilatation; pass 1: bond
+// force and step epilogue) on the instance's current buffer.
+__global__ void __launch_bounds__(kBlock, 3)
+    k_batch_fast(const BatchInstance* __restrict__ insts, const int32_t* __restrict__ remaining,
+                 const BatchTile* __restrict__ tiles, int32_t ntiles, int32_t K, int32_t s,
+                 int32_t pass)
+{
+    static_assert(sizeof(BatchInstance) % 4 == 0 && sizeof(BatchInstance) <= 4 * kBlock,
+                  "instance entry staged by one word per thread");
+    __shared__ __align__(16) uint32_t dbuf[sizeof(BatchInstance) / 4];
+    BatchInstance& d = *reinterpret_cast<BatchInstance*>(dbuf);
+    const int w = threadIdx.x >> 5;
+    int32_t loaded = -1;
+    for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile tl = tiles[t];
+        if (pass == 0 && !tl.lps) continue;
+        const BatchStep bs = batch_step(remaining[tl.inst], K, s);
+        if (!bs.run) continue;
+        if (tl.inst != loaded) {
+            // The instance's entry, with this step's buffers patched in:
+            // p.u the current displacement, ep the epilogue of step s.
+            __syncthreads();
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(insts + tl.inst);
+            if (threadIdx.x < sizeof(BatchInstance) / 4) dbuf[threadIdx.x] = src[threadIdx.x];
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double* const u0 = d.p.u;
+                d.p.u = bs.cur ? d.u_alt : u0;
+                d.ep.u_next = bs.cur ? u0 : d.u_alt;
+                d.ep.mode = bs.mode;
+            }
+            __syncthreads();
+            loaded = tl.inst;
+        }
+        if (w >= tl.nwarps) continue;
+        const int64_t i = d.p.frozen + 32 * (int64_t)(tl.warp0 + w) + (threadIdx.x & 31);
+        if (i >= d.p.n) continue;
+        const bool infl = d.influence == 1;
+        if (pass == 0) {
+            if (d.fracture) {
+                if (infl) lps_m_theta_row<1, true, true>(d.p, d.nl, d.fm, i);
+                else lps_m_theta_row<0, true, true>(d.p, d.nl, d.fm, i);
+            } else {
+                if (infl) lps_m_theta_row<1, false, false>(d.p, d.nl, d.fm, i);
+                else lps_m_theta_row<0, false, false>(d.p, d.nl, d.fm, i);
+            }
+            continue;
+        }
+        if (d.pd == CPD_PD_PMB) {
+            if (d.fracture) pmb_fast_row<true>(d.p, d.nl, d.fm, d.ep, i);
+            else pmb_fast_row<false>(d.p, d.nl, d.fm, d.ep, i);
+        } else if (infl) {
+            if (d.fracture) lps_force_row<1, true>(d.p, d.nl, d.fm, d.ep, i);
+            else lps_force_row<1, false>(d.p, d.nl, d.fm, d.ep, i);
+        } else {
+            if (d.fracture) lps_force_row<0, true>(d.p, d.nl, d.fm, d.ep, i);
+            else lps_force_row<0, false>(d.p, d.nl, d.fm, d.ep, i);
+        }
+    }
+}
+
+}  // namespace
+
 FastModel to_fast(const Model& m)
 {
     return FastModel{m.c, m.theta_coeff, m.s_coeff, m.bond_break_coeff};
 }
 
-}  // namespace
+int launch_batch_fast(const BatchInstance* inst, const int32_t* remaining,
+                      const BatchTile* tiles, int32_t ntiles, int32_t K, int32_t s,
+                      int32_t pass, int grid, cudaStream_t st)
+{
+    if (ntiles <= 0 || grid <= 0) return 0;
+    k_batch_fast<<<grid, kBlock, 0, st>>>(inst, remaining, tiles, ntiles, K, s, pass);
+    return 1;
+}
+
+int batch_fast_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_fast, kBlock, 0) !=
+        cudaSuccess)
+        n = 1;
+    return n > 0 ? n : 1;
+}
 
 bool fast_supported(const Model& md)
 {

@@ -280,13 +280,6 @@ __global__ void __launch_bounds__(kBlock)
     out[i] = split_u(u[0], u[1], u[2], c * p.vol[i], p.nofail[i]);
 }
 
-struct MixedModel {
-    float c, s0, guard;
-    float s_lo, s_hi;  // s0 - guard, s0 + guard
-    double bbc;
-    int ntab;
-};
-
 // Kahan-compensated accumulation of one FP32 term.
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float term)
 {
@@ -458,30 +451,16 @@ __device__ __forceinline__ void lean_geometry(const MixedStencil& t, const Mixed
     b.s = __fdividef(num, fmaf(r, t.xi, t.xi2));
 }
 
-// General mixed PMB kernel: rows that the stencil kernel does not take
-// (irregular rows, tables over its size), one warp per chunk of 32 rows of
-// the warp list, or every chunk in tile order without one. Dynamic shared
-// memory: the stencil table.
+// Row i (of warp chunk `warp`) of the general mixed PMB kernel, with the
+// stencil table staged at tab (the body of k_pmb_force_mixed and of the
+// batch kernel's mixed PMB rows).
 template <bool FRACTURE>
-__global__ void __launch_bounds__(kBlock, 4)
-    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
-                      const int32_t* __restrict__ wlist, int64_t wcount)
+__device__ __forceinline__ void pmb_mixed_row(const ParticleView& p, const EllView& nl,
+                                              const MixedView& mv, const MixedStencil* tab,
+                                              const MixedModel& md, const StepEpilogue& ep,
+                                              int64_t warp, int64_t i)
 {
-    extern __shared__ MixedStencil smem[];
-    MixedStencil* tab = smem;
-    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
-    __syncthreads();
-    int64_t warp;
-    if (wlist) {
-        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-        if (slot >= wcount) return;
-        warp = wlist[slot];
-    } else {
-        warp = tile_chunk(nl);
-    }
     const int kind = warp < ((p.n - p.frozen + 31) >> 5) ? mv.warp_kind[warp] : 0;
-    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
-    if (i >= p.n) return;
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
     const float4 uhi = ui.hi, uli = ui.lo;
@@ -625,6 +604,32 @@ __global__ void __launch_bounds__(kBlock, 4)
                         (double)sz - (double)cz);
 }
 
+// General mixed PMB kernel: rows that the stencil kernel does not take
+// (irregular rows, tables over its size), one warp per chunk of 32 rows of
+// the warp list, or every chunk in tile order without one. Dynamic shared
+// memory: the stencil table.
+template <bool FRACTURE>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_pmb_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedModel md, StepEpilogue ep,
+                      const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    extern __shared__ MixedStencil smem[];
+    MixedStencil* tab = smem;
+    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
+    __syncthreads();
+    int64_t warp;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        warp = wlist[slot];
+    } else {
+        warp = tile_chunk(nl);
+    }
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
+    if (i >= p.n) return;
+    pmb_mixed_row<FRACTURE>(p, nl, mv, tab, md, ep, warp, i);
+}
+
 // Prologue of the lean kernels: stages the stencil table in shared memory
 // and takes the calling warp's row chunk from the warp list; a warp whose
 // rows share one stencil subset (kind 3) also stages its compacted table
@@ -671,14 +676,6 @@ __device__ __forceinline__ bool lean_prologue(const MixedView& mv, int ntab,
 // sums and kept as FP32 pairs for the neighbours' force loop. The break test
 // follows the LPS rule (no-fail of the row only, tested twice by the
 // reference) with the FP64 re-test inside the guard band.
-struct MixedLps {
-    float s0, guard;
-    float s_lo, s_hi;  // s0 - guard, s0 + guard
-    double bbc;
-    double theta_coeff, s_coeff;
-    int ntab;
-    float vol;  // the particle volume when the packed records are used
-};
 
 // omega xi^2 of a stencil entry (force_models/CabanaPD_LPS.hpp:85-106) and
 // the omega xi factor of the force coefficient (:118-134).
@@ -695,23 +692,12 @@ __device__ __forceinline__ float lps_oxi(const MixedStencil& t)
 
 // Weighted volume (when WITH_M) and dilatation of one row, one pass.
 template <bool FRACTURE, int INFL, bool WITH_M>
-__global__ void __launch_bounds__(kBlock, 4)
-    k_lps_mtheta_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
-                       float2* __restrict__ ab, const int32_t* __restrict__ wlist,
-                       int64_t wcount, MixedU* __restrict__ pack)
+__device__ __forceinline__ void lps_mtheta_mixed_row(const ParticleView& p, const EllView& nl,
+                                                     const MixedView& mv,
+                                                     const MixedStencil* tab,
+                                                     const MixedLps& md, float2* ab,
+                                                     MixedU* pack, int64_t warp, int64_t i)
 {
-    __shared__ MixedStencil tab[kMixedGeneric];
-    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
-    __syncthreads();
-    // Rows: the listed warps' chunks when a warp list is given.
-    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (wlist) {
-        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-        if (slot >= wcount) return;
-        warp = wlist[slot];
-    }
-    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
-    if (i >= p.n) return;
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
     const float4 uhi = ui.hi, uli = ui.lo;
@@ -782,20 +768,11 @@ __global__ void __launch_bounds__(kBlock, 4)
                          make_float4(uli.x, uli.y, uli.z, (float)b)};
 }
 
-__device__ __forceinline__ bool lps_critical(float s, bool nofail_i, const MixedLps& md,
-                                             const ParticleView& p, int64_t i, int64_t j)
-{
-    // force/CabanaPD_LPS.hpp:417-418: only the row's no-fail flag counts.
-    if (nofail_i) return false;
-    if (fabsf(s - md.s0) <= md.guard) return critical_exact64(p.x, p.u, p.npad, i, j, md.bbc);
-    return s >= md.s0;
-}
-
-template <bool FRACTURE, int INFL>
+template <bool FRACTURE, int INFL, bool WITH_M>
 __global__ void __launch_bounds__(kBlock, 4)
-    k_lps_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
-                      const float2* __restrict__ ab, StepEpilogue ep,
-                      const int32_t* __restrict__ wlist, int64_t wcount)
+    k_lps_mtheta_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                       float2* __restrict__ ab, const int32_t* __restrict__ wlist,
+                       int64_t wcount, MixedU* __restrict__ pack)
 {
     __shared__ MixedStencil tab[kMixedGeneric];
     for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
@@ -809,6 +786,26 @@ __global__ void __launch_bounds__(kBlock, 4)
     }
     const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
     if (i >= p.n) return;
+    lps_mtheta_mixed_row<FRACTURE, INFL, WITH_M>(p, nl, mv, tab, md, ab, pack, warp, i);
+}
+
+__device__ __forceinline__ bool lps_critical(float s, bool nofail_i, const MixedLps& md,
+                                             const ParticleView& p, int64_t i, int64_t j)
+{
+    // force/CabanaPD_LPS.hpp:417-418: only the row's no-fail flag counts.
+    if (nofail_i) return false;
+    if (fabsf(s - md.s0) <= md.guard) return critical_exact64(p.x, p.u, p.npad, i, j, md.bbc);
+    return s >= md.s0;
+}
+
+template <bool FRACTURE, int INFL>
+__device__ __forceinline__ void lps_force_mixed_row(const ParticleView& p, const EllView& nl,
+                                                    const MixedView& mv,
+                                                    const MixedStencil* tab,
+                                                    const MixedLps& md, const float2* ab,
+                                                    const StepEpilogue& ep, int64_t warp,
+                                                    int64_t i)
+{
     const int64_t np = p.npad;
     const MixedU ui = mv.u2[i];
     const float4 uhi = ui.hi, uli = ui.lo;
@@ -892,6 +889,27 @@ __global__ void __launch_bounds__(kBlock, 4)
     }
     step_epilogue<true>(p, ep, i, (double)sxy.x - (double)cxy.x, (double)sxy.y - (double)cxy.y,
                         (double)sz - (double)cz);
+}
+
+template <bool FRACTURE, int INFL>
+__global__ void __launch_bounds__(kBlock, 4)
+    k_lps_force_mixed(ParticleView p, EllView nl, MixedView mv, MixedLps md,
+                      const float2* __restrict__ ab, StepEpilogue ep,
+                      const int32_t* __restrict__ wlist, int64_t wcount)
+{
+    __shared__ MixedStencil tab[kMixedGeneric];
+    for (int t = threadIdx.x; t < md.ntab; t += blockDim.x) tab[t] = mv.table[t];
+    __syncthreads();
+    // Rows: the listed warps' chunks when a warp list is given.
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wlist) {
+        const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+        if (slot >= wcount) return;
+        warp = wlist[slot];
+    }
+    const int64_t i = p.frozen + 32 * warp + (threadIdx.x & 31);
+    if (i >= p.n) return;
+    lps_force_mixed_row<FRACTURE, INFL>(p, nl, mv, tab, md, ab, ep, warp, i);
 }
 
 // LPS lean forms, over the warps of kinds 2 and 3 (warp list; the other
@@ -1380,6 +1398,89 @@ __global__ void __launch_bounds__(kBlock, 4)
     }
 }
 
+// Batched step over many systems (cpd_batch.cu), mixed bodies: as
+// k_batch_fast, and the instance's stencil table is staged in shared memory
+// with its table entry. Pass 0: LPS weighted volume (fracture) and
+// dilatation; pass 1: bond force and step epilogue.
+__global__ void __launch_bounds__(kBlock, 3)
+    k_batch_mixed(const BatchInstance* __restrict__ insts, const int32_t* __restrict__ remaining,
+                  const BatchTile* __restrict__ tiles, int32_t ntiles, int32_t K, int32_t s,
+                  int32_t pass)
+{
+    static_assert(sizeof(BatchInstance) % 4 == 0 && sizeof(BatchInstance) <= 4 * kBlock,
+                  "instance entry staged by one word per thread");
+    __shared__ __align__(16) uint32_t dbuf[sizeof(BatchInstance) / 4];
+    __shared__ MixedStencil tab[kMixedGeneric];
+    BatchInstance& d = *reinterpret_cast<BatchInstance*>(dbuf);
+    const int w = threadIdx.x >> 5;
+    int32_t loaded = -1;
+    for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile tl = tiles[t];
+        if (pass == 0 && !tl.lps) continue;
+        const BatchStep bs = batch_step(remaining[tl.inst], K, s);
+        if (!bs.run) continue;
+        if (tl.inst != loaded) {
+            __syncthreads();
+            const BatchInstance* src = insts + tl.inst;
+            if (threadIdx.x < sizeof(BatchInstance) / 4)
+                dbuf[threadIdx.x] = reinterpret_cast<const uint32_t*>(src)[threadIdx.x];
+            const int ntab = src->pd == CPD_PD_PMB ? src->mm.ntab : src->ml.ntab;
+            const MixedStencil* table = src->mv.table;
+            for (int k = threadIdx.x; k < ntab; k += blockDim.x) tab[k] = table[k];
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                // This step's buffers (as k_batch_fast), and the split's.
+                double* const u0 = d.p.u;
+                MixedU* const s0 = const_cast<MixedU*>(d.mv.u2);
+                d.p.u = bs.cur ? d.u_alt : u0;
+                d.mv.u2 = bs.cur ? d.u2_alt : s0;
+                d.ep.u_next = bs.cur ? u0 : d.u_alt;
+                d.ep.u2_next = bs.cur ? s0 : d.u2_alt;
+                d.ep.mode = bs.mode;
+            }
+            __syncthreads();
+            loaded = tl.inst;
+        }
+        if (w >= tl.nwarps) continue;
+        const int64_t warp = tl.warp0 + w;
+        const int64_t i = d.p.frozen + 32 * warp + (threadIdx.x & 31);
+        if (i >= d.p.n) continue;
+        const bool infl = d.influence == 1;
+        if (pass == 0) {
+            if (d.fracture) {
+                if (infl)
+                    lps_mtheta_mixed_row<true, 1, true>(d.p, d.nl, d.mv, tab, d.ml, d.ab,
+                                                        nullptr, warp, i);
+                else
+                    lps_mtheta_mixed_row<true, 0, true>(d.p, d.nl, d.mv, tab, d.ml, d.ab,
+                                                        nullptr, warp, i);
+            } else {
+                if (infl)
+                    lps_mtheta_mixed_row<false, 1, false>(d.p, d.nl, d.mv, tab, d.ml, d.ab,
+                                                          nullptr, warp, i);
+                else
+                    lps_mtheta_mixed_row<false, 0, false>(d.p, d.nl, d.mv, tab, d.ml, d.ab,
+                                                          nullptr, warp, i);
+            }
+            continue;
+        }
+        if (d.pd == CPD_PD_PMB) {
+            if (d.fracture) pmb_mixed_row<true>(d.p, d.nl, d.mv, tab, d.mm, d.ep, warp, i);
+            else pmb_mixed_row<false>(d.p, d.nl, d.mv, tab, d.mm, d.ep, warp, i);
+        } else if (infl) {
+            if (d.fracture)
+                lps_force_mixed_row<true, 1>(d.p, d.nl, d.mv, tab, d.ml, d.ab, d.ep, warp, i);
+            else
+                lps_force_mixed_row<false, 1>(d.p, d.nl, d.mv, tab, d.ml, d.ab, d.ep, warp, i);
+        } else {
+            if (d.fracture)
+                lps_force_mixed_row<true, 0>(d.p, d.nl, d.mv, tab, d.ml, d.ab, d.ep, warp, i);
+            else
+                lps_force_mixed_row<false, 0>(d.p, d.nl, d.mv, tab, d.ml, d.ab, d.ep, warp, i);
+        }
+    }
+}
+
 #define CPD_TRY(call)                                                     \
     do {                                                                  \
         cudaError_t e_ = (call);                                          \
@@ -1438,8 +1539,13 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
         CPD_TRY(dev_alloc(&d_min, 4 * sizeof(unsigned long long), st));
         CPD_TRY(cudaMemsetAsync(d_min, 0x7f, 3 * sizeof(unsigned long long), st));
         CPD_TRY(cudaMemsetAsync(d_min + 3, 0, sizeof(unsigned long long), st));
-        // The neighbour build's count pass may have found the spacing already.
-        if (!pd.hmin_valid) {
+        // The neighbour build's count pass may have found the spacing already
+        // (over the pairs it visited, which are the list's pairs). With
+        // CPD_CHECK_SPACING=1 the list is walked anyway and the two must agree
+        // bit for bit: a debug check that the list holds exactly those pairs.
+        const char* chk = getenv("CPD_CHECK_SPACING");
+        const bool check = pd.hmin_valid && chk && chk[0] == '1';
+        if (!pd.hmin_valid || check) {
             k_min_spacing<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_min);
             launches++;
         }
@@ -1451,6 +1557,15 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
         CPD_TRY(cudaMemcpyAsync(&v0, p.vol, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPD_TRY(cudaStreamSynchronize(st));
         CPD_TRY(dev_free(d_min, st));
+        if (check) {
+            for (int d = 0; d < 3; ++d) {
+                if (std::memcmp(&hmin[d], &pd.hmin[d], sizeof(double)) != 0) {
+                    err = "lattice spacing of the count pass differs from the list's on axis " +
+                          std::to_string(d);
+                    return -1;
+                }
+            }
+        }
         if (pd.hmin_valid)
             for (int d = 0; d < 3; ++d) std::memcpy(&hmin[d], &pd.hmin[d], sizeof(double));
         if (hmin[3] == 0) {
@@ -1649,6 +1764,37 @@ int launch_vv_initial_mixed(const ParticleView& p, const Model& md, double dt, d
     return 1;
 }
 
+MixedModel to_mixed_model(const Model& md, const MixedState& m)
+{
+    MixedModel mm;
+    mm.c = (float)md.c;
+    mm.s0 = (float)md.s0;
+    mm.guard = (float)(1e-4 * md.s0);
+    mm.bbc = md.bond_break_coeff;
+    mm.s_lo = mm.s0 - mm.guard;
+    mm.s_hi = mm.s0 + mm.guard;
+    mm.ntab = m.ntab;
+    return mm;
+}
+
+int launch_batch_mixed(const BatchInstance* inst, const int32_t* remaining,
+                       const BatchTile* tiles, int32_t ntiles, int32_t K, int32_t s,
+                       int32_t pass, int grid, cudaStream_t st)
+{
+    if (ntiles <= 0 || grid <= 0) return 0;
+    k_batch_mixed<<<grid, kBlock, 0, st>>>(inst, remaining, tiles, ntiles, K, s, pass);
+    return 1;
+}
+
+int batch_mixed_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_mixed, kBlock, 0) !=
+        cudaSuccess)
+        n = 1;
+    return n > 0 ? n : 1;
+}
+
 MixedLps to_mixed_lps(const Model& md, const MixedState& m)
 {
     MixedLps l;
@@ -1766,14 +1912,7 @@ int launch_pd_force_mixed(const ParticleView& p, const EllView& list, const Mode
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
     MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
-    MixedModel mm;
-    mm.c = (float)md.c;
-    mm.s0 = (float)md.s0;
-    mm.guard = (float)(1e-4 * md.s0);
-    mm.bbc = md.bond_break_coeff;
-    mm.s_lo = mm.s0 - mm.guard;
-    mm.s_hi = mm.s0 + mm.guard;
-    mm.ntab = m.ntab;
+    const MixedModel mm = to_mixed_model(md, m);
     const size_t tab_bytes = sizeof(MixedStencil) * m.ntab;
     if (m.st32) {
         // Stencil warps on the unrolled table walk, irregular warps on the

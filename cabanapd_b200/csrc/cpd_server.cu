@@ -94,6 +94,7 @@ struct Job {
     std::atomic<double> t_start{-1.0};
     double W = 0, D = 0;
     bool contact = false;
+    bool batched = false;  // advanced in a batch group (small PD job)
     cpd_system* sys = nullptr;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -104,6 +105,22 @@ struct Job {
     std::deque<Chunk> inflight;
     std::vector<cudaEvent_t> spare;
     std::map<int32_t, std::vector<double>> results;
+};
+
+// A batch group: small jobs advanced together by one cpd_batch (one
+// persistent-block launch per step for all of them). Chunks complete in
+// order; each records how many steps every job took in it.
+struct GroupChunk {
+    cudaEvent_t ev = nullptr;
+    std::vector<int32_t> steps;
+};
+struct Group {
+    cpd_batch* batch = nullptr;
+    std::vector<Job*> jobs;
+    std::vector<int32_t> left;       // steps not yet launched, per job
+    std::vector<char> done;          // finished and handed back
+    std::deque<GroupChunk> inflight;
+    std::vector<cudaEvent_t> spare;
 };
 
 bool vector_field(int32_t f)
@@ -161,6 +178,7 @@ struct cpd_server {
     std::map<int64_t, std::unique_ptr<Job>> jobs;
     std::deque<Job*> queue;     // submitted, not admitted
     std::vector<Job*> admitted; // set up, not yet picked by the launcher
+    std::vector<Job*> pending_batch;  // set up small jobs for the next batch group
     std::vector<Job*> retire;   // all steps done, not yet finalised
     int64_t resident = 0;
     uint64_t resident_bytes = 0, peak_bytes = 0;
@@ -210,6 +228,17 @@ struct cpd_server {
         return prio_greatest + (int32_t)std::lround(t * (prio_least - prio_greatest));
     }
 
+    // Small peridynamic jobs without contact, in the throughput precisions,
+    // go to batch groups (cfg.batch_max_particles > 0).
+    bool batchable(const cpd_job& s) const
+    {
+        const int32_t pd = s.params.pd_model;
+        return cfg.batch_max_particles > 0 && s.n <= cfg.batch_max_particles &&
+               s.steps > 0 && (pd == CPD_PD_PMB || pd == CPD_PD_LPS) &&
+               s.params.contact_model == CPD_CONTACT_NONE &&
+               (s.params.precision == CPD_FP64 || s.params.precision == CPD_MIXED);
+    }
+
     // Builds the job's system. Returns an empty string on success.
     std::string setup(Job* j)
     {
@@ -250,10 +279,12 @@ struct cpd_server {
         int32_t max_n = 0;
         cpd_neighbor_stats(j->sys, &max_n, &j->bonds);
         j->contact = s.params.contact_model != CPD_CONTACT_NONE;
+        j->batched = batchable(s);
         // Contact systems decide neighbour rebuilds on the host between
-        // steps, so only the PD-only step is captured.
+        // steps, so only the PD-only step is captured; batched jobs run in
+        // their group's graphs.
         const int32_t k = std::min(cfg.steps_per_launch, j->steps);
-        if (cfg.use_graphs && !j->contact && k > 0) {
+        if (cfg.use_graphs && !j->contact && !j->batched && k > 0) {
             const int64_t before = cpd_kernel_launches(j->sys);
             cudaGraph_t g = nullptr;
             bool ok = cudaStreamBeginCapture(j->stream, cudaStreamCaptureModeThreadLocal) ==
@@ -386,7 +417,10 @@ struct cpd_server {
                 peak_bytes = std::max(peak_bytes, resident_bytes);
                 j->state = CPD_JOB_RUNNING;
                 j->t_ready = now();
-                admitted.push_back(j);
+                if (j->batched)
+                    pending_batch.push_back(j);
+                else
+                    admitted.push_back(j);
                 cv_launcher.notify_one();
                 // Retire finished jobs before setting up the next one.
                 if (!retire.empty()) break;
@@ -425,24 +459,167 @@ struct cpd_server {
         return true;
     }
 
+    // ---- batch groups (launcher thread) -----------------------------------
+    // A group of the pending small jobs; a job the batch refuses (e.g. its
+    // boundary conditions do not fit the fused step) runs on its own.
+    void form_group(const std::vector<Job*>& jobs, std::vector<Group*>& groups,
+                    std::vector<Job*>& running)
+    {
+        std::vector<cpd_system*> sys;
+        std::vector<int32_t> steps;
+        for (Job* j : jobs) {
+            sys.push_back(j->sys);
+            steps.push_back(j->steps);
+        }
+        cpd_batch* b = nullptr;
+        if (cpd_batch_create(sys.data(), (int32_t)sys.size(), steps.data(), &b) != CPD_OK) {
+            if (jobs.size() > 1) {
+                for (Job* j : jobs) form_group({j}, groups, running);
+            } else {
+                jobs[0]->batched = false;
+                running.push_back(jobs[0]);
+            }
+            return;
+        }
+        auto g = std::make_unique<Group>();
+        g->batch = b;
+        g->jobs = jobs;
+        g->left = steps;
+        g->done.assign(jobs.size(), 0);
+        for (int e = 0; e < kInflight; e++) {
+            cudaEvent_t ev = nullptr;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess)
+                g->spare.push_back(ev);
+        }
+        groups.push_back(g.release());
+    }
+
+    // Completed chunks (finished jobs are handed back by the batch and go to
+    // `finished`) and new chunks, up to kInflight. False on a device or
+    // launch error.
+    bool service_group(Group* g, bool& progressed, std::vector<Job*>& finished, std::string& err)
+    {
+        while (!g->inflight.empty()) {
+            const cudaError_t q = cudaEventQuery(g->inflight.front().ev);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) {
+                err = std::string("device error: ") + cudaGetErrorString(q);
+                return false;
+            }
+            const GroupChunk& c = g->inflight.front();
+            for (size_t k = 0; k < g->jobs.size(); ++k) {
+                Job* j = g->jobs[k];
+                j->steps_done += c.steps[k];
+                if (!g->done[k] && j->steps_done == j->steps) {
+                    if (cpd_batch_release(g->batch, (int32_t)k) != CPD_OK) {
+                        err = std::string("cpd_batch_release: ") + cpd_last_error();
+                        return false;
+                    }
+                    g->done[k] = 1;
+                    finished.push_back(j);
+                }
+            }
+            g->spare.push_back(c.ev);
+            g->inflight.pop_front();
+            progressed = true;
+        }
+        const bool more = std::any_of(g->left.begin(), g->left.end(), [](int32_t v) { return v > 0; });
+        if (more && (int)g->inflight.size() < kInflight && !g->spare.empty()) {
+            const int32_t K = cfg.steps_per_launch;
+            if (cpd_batch_step(g->batch, K) != CPD_OK) {
+                err = std::string("cpd_batch_step: ") + cpd_last_error();
+                return false;
+            }
+            GroupChunk c;
+            c.ev = g->spare.back();
+            g->spare.pop_back();
+            c.steps.resize(g->jobs.size());
+            for (size_t k = 0; k < g->jobs.size(); ++k) {
+                c.steps[k] = std::min(K, g->left[k]);
+                g->left[k] -= c.steps[k];
+                Job* j = g->jobs[k];
+                j->steps_launched += c.steps[k];
+                if (c.steps[k] > 0 && j->t_start < 0) j->t_start = now();
+            }
+            if (cudaEventRecord(c.ev, cpd::batch_stream(g->batch)) != cudaSuccess) {
+                g->spare.push_back(c.ev);
+                err = "cudaEventRecord failed";
+                return false;
+            }
+            g->inflight.push_back(std::move(c));
+            progressed = true;
+        }
+        return true;
+    }
+
+    // Destroys a group whose jobs all finished, or (failed) fails the rest.
+    void close_group(Group* g, const std::string& err)
+    {
+        const int64_t n = cpd_batch_launches(g->batch);
+        cpd_batch_destroy(g->batch);
+        for (auto& c : g->inflight) cudaEventDestroy(c.ev);
+        for (cudaEvent_t e : g->spare) cudaEventDestroy(e);
+        std::vector<Job*> failed;
+        for (size_t k = 0; k < g->jobs.size(); ++k)
+            if (!g->done[k]) failed.push_back(g->jobs[k]);
+        for (Job* j : failed) {
+            if (j->stream) cudaStreamSynchronize(j->stream);
+            release_device(j);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        launches += n;
+        for (Job* j : failed) {
+            resident--;
+            resident_bytes -= std::max(j->bytes, j->est_bytes);
+            finish_failed(j, err.empty() ? std::string("batch group failed") : err);
+        }
+        delete g;
+    }
+
     void launcher_loop()
     {
         cudaSetDevice(cfg.device);
         std::vector<Job*> running;
+        std::vector<Group*> groups;
         for (;;) {
+            std::vector<Job*> grouping;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (running.empty())
-                    cv_launcher.wait_for(lk, std::chrono::milliseconds(2),
-                                         [&] { return stopping || !admitted.empty(); });
+                if (running.empty() && groups.empty())
+                    cv_launcher.wait_for(lk, std::chrono::milliseconds(2), [&] {
+                        return stopping || !admitted.empty() || !pending_batch.empty();
+                    });
                 for (Job* j : admitted) running.push_back(j);
                 admitted.clear();
-                if (stopping && running.empty() && resident == 0 && queue.empty() &&
-                    admitted.empty())
+                grouping.swap(pending_batch);
+                if (stopping && running.empty() && groups.empty() && grouping.empty() &&
+                    resident == 0 && queue.empty() && admitted.empty())
                     break;
             }
+            if (!grouping.empty()) form_group(grouping, groups, running);
             bool progressed = false;
             std::vector<Job*> finished, failed;
+            for (auto it = groups.begin(); it != groups.end();) {
+                Group* g = *it;
+                std::string err;
+                const bool ok = service_group(g, progressed, finished, err);
+                const bool all = std::all_of(g->done.begin(), g->done.end(),
+                                             [](char d) { return d != 0; });
+                if (!ok || all) {
+                    if (!finished.empty()) {
+                        // Hand the finished jobs to the workers before the
+                        // group's batch goes.
+                        std::lock_guard<std::mutex> lk(mu);
+                        for (Job* j : finished) retire.push_back(j);
+                        finished.clear();
+                        cv_worker.notify_one();
+                    }
+                    close_group(g, ok ? std::string() : err);
+                    it = groups.erase(it);
+                } else {
+                    ++it;
+                }
+            }
             for (auto it = running.begin(); it != running.end();) {
                 Job* j = *it;
                 bool bad = false;
@@ -488,7 +665,7 @@ struct cpd_server {
                 }
                 cv_worker.notify_one();
             }
-            if (!progressed && !running.empty())
+            if (!progressed && (!running.empty() || !groups.empty()))
                 std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
     }

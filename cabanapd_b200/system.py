@@ -69,7 +69,7 @@ class ServerConfig(ctypes.Structure):
         ("use_graphs", ctypes.c_int32),
         ("hbm_budget_bytes", ctypes.c_uint64),
         ("setup_threads", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("batch_max_particles", ctypes.c_int32),
     ]
 
 
@@ -157,6 +157,17 @@ SIGNATURES = {
     "cpd_kernel_time": (_I32, [_P, _DP, ctypes.POINTER(_I64), _DP]),
     "cpd_kernel_launches": (_I64, [_P]),
     "cpd_device_bytes": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "cpd_batch_create": (_I32, [ctypes.POINTER(_P), _I32, ctypes.POINTER(_I32),
+                                ctypes.POINTER(_P)]),
+    "cpd_batch_destroy": (_I32, [_P]),
+    "cpd_batch_step": (_I32, [_P, _I32]),
+    "cpd_batch_remaining": (_I32, [_P, _I32, ctypes.POINTER(_I32)]),
+    "cpd_batch_release": (_I32, [_P, _I32]),
+    "cpd_batch_synchronize": (_I32, [_P]),
+    "cpd_batch_set_candidate": (_I32, [_P, _I32]),
+    "cpd_batch_tuning": (_I32, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                                ctypes.POINTER(_I32), ctypes.POINTER(_I32), _DP]),
+    "cpd_batch_launches": (_I64, [_P]),
     "cpd_job_create": (_I32, [ctypes.POINTER(CpdParams), _I32, ctypes.POINTER(_P)]),
     "cpd_job_destroy": (_I32, [_P]),
     "cpd_job_set_particles": (_I32, [_P, _I64, _I64, _P, _P, _P, _P, _P]),
@@ -395,6 +406,81 @@ class System:
         self._check(self._lib.cpd_load_state(self._h, buf.ctypes.data, buf.size))
 
 
+class Batch:
+    """Many set-up systems advanced together (a cpd_batch handle): per time
+    step one persistent-block launch covers every instance, and k-step chunks
+    replay from a CUDA graph. The systems stay usable for reads (energy,
+    fields); state-changing calls on them fail until the batch is closed.
+    steps[i]: the total number of steps system i is to take."""
+
+    def __init__(self, systems, steps):
+        lib = load()
+        self._lib = lib
+        self.systems = list(systems)
+        n = len(self.systems)
+        hs = (_P * n)(*[s.handle for s in self.systems])
+        st = (_I32 * n)(*[int(k) for k in steps])
+        h = _P()
+        self._check(lib.cpd_batch_create(hs, n, st, ctypes.byref(h)))
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CpdError(f"cabanapd_b200 error {rc}: {self._lib.cpd_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cpd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, chunk_steps):
+        """One chunk: every instance takes min(chunk_steps, its steps left)."""
+        self._check(self._lib.cpd_batch_step(self._h, int(chunk_steps)))
+
+    def run(self, chunk_steps=32):
+        """Chunks until every instance has taken its steps; synchronises."""
+        while max(self.remaining(i) for i in range(len(self.systems))) > 0:
+            self.step(chunk_steps)
+        self.synchronize()
+
+    def release(self, instance):
+        """Hand back a finished instance's system (it may step or be
+        destroyed again) while the batch runs on."""
+        self._check(self._lib.cpd_batch_release(self._h, int(instance)))
+
+    def remaining(self, instance):
+        r = _I32()
+        self._check(self._lib.cpd_batch_remaining(self._h, int(instance), ctypes.byref(r)))
+        return r.value
+
+    def synchronize(self):
+        self._check(self._lib.cpd_batch_synchronize(self._h))
+
+    def set_candidate(self, candidate):
+        """Fix the launch shape (-1: the autotuner chooses)."""
+        self._check(self._lib.cpd_batch_set_candidate(self._h, int(candidate)))
+
+    def tuning(self):
+        """(chosen, [(blocks_per_sm, order, bond-updates/s), ...])."""
+        n, chosen = _I32(), _I32()
+        self._check(self._lib.cpd_batch_tuning(self._h, ctypes.byref(n), None, None, None, None))
+        g = (_I32 * n.value)()
+        o = (_I32 * n.value)()
+        t = (_D * n.value)()
+        self._check(self._lib.cpd_batch_tuning(self._h, ctypes.byref(n), ctypes.byref(chosen),
+                                               g, o, t))
+        return chosen.value, [(g[k], o[k], t[k]) for k in range(n.value)]
+
+    def launches(self):
+        return int(self._lib.cpd_batch_launches(self._h))
+
+
 def _params_struct(params, precision=FP64_EXACT, ordering=ORDER_INPUT, device=0):
     p = CpdParams()
     p.influence_type = -1
@@ -416,11 +502,11 @@ class Server:
     and returns a job id; results stay on the host until release()."""
 
     def __init__(self, device=0, max_active=16, steps_per_launch=32, use_graphs=True,
-                 hbm_budget_bytes=150 * 10**9, setup_threads=4):
+                 hbm_budget_bytes=150 * 10**9, setup_threads=4, batch_max_particles=0):
         lib = load()
         self._lib = lib
         cfg = ServerConfig(device, max_active, steps_per_launch, 1 if use_graphs else 0,
-                           int(hbm_budget_bytes), int(setup_threads), 0)
+                           int(hbm_budget_bytes), int(setup_threads), int(batch_max_particles))
         h = _P()
         self._check(lib.cpd_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -47,8 +47,8 @@
  * Entry points without a reference counterpart (each says so where it is
  * declared): cpd_step_stage, cpd_device_field, cpd_set_stream, the kernel
  * timing calls, cpd_compute_energy_noalloc, the state snapshots
- * (cpd_state_bytes / cpd_save_state / cpd_load_state), and the job server
- * (cpd_job_*, cpd_server_*).
+ * (cpd_state_bytes / cpd_save_state / cpd_load_state), the batched step
+ * (cpd_batch_*) and the job server (cpd_job_*, cpd_server_*).
  *
  * Errors: every call returns a cpd_status; cpd_last_error() gives the
  * message of the last failure on the calling thread. The reference throws
@@ -354,6 +354,60 @@ int64_t cpd_kernel_launches(const cpd_system* sys);
 cpd_status cpd_device_bytes(const cpd_system* sys, uint64_t* bytes);
 
 /* ===========================================================================
+ * Batched step. No counterpart in the reference, which advances one
+ * specimen per process with one kernel per phase (CabanaPD_Solver.hpp:332-404).
+ * A batch advances many set-up systems together: one table of per-instance
+ * device views (offsets into the device memory pool) and one tile list over
+ * all their particle rows; per time step one launch of a persistent-block
+ * kernel runs the bond force, bond breaking and both velocity-Verlet half
+ * steps of every instance (two launches when an LPS instance needs its
+ * dilatation pass), and a chunk of k steps is replayed from a CUDA graph.
+ * Each instance runs the arithmetic of its system's general (non-stencil)
+ * kernels: CPD_FP64 systems the FP64 throughput kernels, CPD_MIXED systems
+ * the mixed ones, so results do not depend on the other instances or on the
+ * launch shape. An autotuner picks the persistent grid (blocks per SM) and
+ * the tile order by timing the first chunks, one candidate each (all
+ * candidates give identical results), and keeps the fastest.
+ *
+ * Systems must be set up and initialised (cpd_init), peridynamic without
+ * contact, CPD_FP64 or CPD_MIXED, on one device, with boundary conditions
+ * that fit the fused step. While a system belongs to a batch, calls that
+ * change its state (cpd_step*, cpd_set_state, cpd_load_state, cpd_init, set-up
+ * calls, cpd_system_destroy) return CPD_ERR_STATE; reads (cpd_compute_energy,
+ * cpd_download, cpd_save_state, ...) are ordered after the batch's chunks.
+ * cpd_batch_destroy releases the systems (it does not destroy them).
+ */
+typedef struct cpd_batch cpd_batch;
+
+/* steps[i]: the number of time steps instance i is to take in total. */
+cpd_status cpd_batch_create(cpd_system* const* systems, int32_t count, const int32_t* steps,
+                            cpd_batch** out);
+cpd_status cpd_batch_destroy(cpd_batch* batch);
+/* One chunk: every instance with steps left advances min(chunk_steps, its
+ * steps left) steps. Asynchronous with respect to the host. */
+cpd_status cpd_batch_step(cpd_batch* batch, int32_t chunk_steps);
+/* Hands back instance i once it has no steps left: its system takes
+ * state-changing calls again (and may be destroyed) while the batch runs
+ * on; work later issued on the system's stream still follows the chunk that
+ * finished it. */
+cpd_status cpd_batch_release(cpd_batch* batch, int32_t instance);
+/* Steps instance i still has to take (as of the chunks issued so far). */
+cpd_status cpd_batch_remaining(const cpd_batch* batch, int32_t instance, int32_t* steps);
+cpd_status cpd_batch_synchronize(cpd_batch* batch);
+/* Fix the launch shape to candidate `candidate` (0 <= candidate <
+ * *count), or -1 to let the autotuner choose. */
+cpd_status cpd_batch_set_candidate(cpd_batch* batch, int32_t candidate);
+/* The autotuner's state: candidates, the chosen one (-1 while tuning), and
+ * per candidate its persistent grid in blocks per SM, its tile order (0 by
+ * instance, 1 interleaved across instances) and its measured throughput in
+ * bond-updates/s (0 if not timed). Arrays hold at least *count entries when
+ * non-NULL (query *count first with NULL arrays). */
+cpd_status cpd_batch_tuning(const cpd_batch* batch, int32_t* count, int32_t* chosen,
+                            int32_t* blocks_per_sm, int32_t* order, double* throughput);
+/* Kernels the batch launched (graph replays count each kernel node). */
+int64_t cpd_batch_launches(const cpd_batch* batch);
+
+/* ===========================================================================
  * Job server. No counterpart in the reference, which runs one simulation per
  * process. Continuous batching of independent simulations on one GPU: jobs
  * are described on the host (cpd_job_*: the same inputs as a cpd_system),
@@ -381,7 +435,12 @@ typedef struct cpd_server_config {
     uint64_t hbm_budget_bytes;  /* admission budget on resident device bytes */
     int32_t setup_threads;      /* host threads that admit / set up / retire
                                    jobs concurrently; 0 = 4 */
-    int32_t reserved;
+    int32_t batch_max_particles; /* > 0: peridynamic jobs without contact in
+                                   CPD_FP64 / CPD_MIXED with at most this many
+                                   particles are advanced in batch groups
+                                   (cpd_batch_*: one launch per step for the
+                                   group, jobs set up together form a group);
+                                   0: every job on its own */
 } cpd_server_config;
 
 typedef struct cpd_job_status {

@@ -173,3 +173,22 @@ def test_thin_plate_with_stencil_entries_no_row_holds(cuda, oracle, precision):
     prob = _plate((40, 20, 2))
     g, o = _run(cuda, oracle, prob, precision, 30)
     _check(g, o, precision)
+
+
+@pytest.mark.parametrize("precision", [FAST, MIXED])
+def test_count_pass_spacing_equals_list_spacing(cuda, precision, monkeypatch):
+    """The stencil set-up takes the lattice spacing from the neighbour
+    build's count pass; with CPD_CHECK_SPACING=1 it also walks the list and
+    fails the set-up if the two differ in any bit. A notched plate and an
+    LPS box whose first layer (and a few more rows) is frozen."""
+    monkeypatch.setenv("CPD_CHECK_SPACING", "1")
+    plate = P.plate_impact(num_cells=(60, 30, 4), steps=4, v0=60.0)
+    box = P.lps_random_notches(num_cells=(80, 32, 4), steps=4)
+    nf = 80 * 32 + 7
+    box = dict(box, n_frozen=nf)
+    box["bcs"] = [(k, c, idx[idx >= nf], v) for k, c, idx, v in box["bcs"]]
+    for prob in (plate, box):
+        s = cuda.System(dict(prob["params"], precision=precision))
+        P.setup(s, prob)
+        s.run(prob["num_steps"])
+        assert np.all(np.isfinite(s.get("u")))

@@ -78,6 +78,38 @@ def test_each_job_same_alone_and_in_the_mix(lib, precision):
     srv.close()
 
 
+def _solo_batch(lib, prob, precision, chunk=16):
+    s = lib.System(dict(prob["params"], precision=precision))
+    P.setup(s, prob)
+    b = lib.Batch([s], [prob["num_steps"]])
+    b.run(chunk_steps=chunk)
+    b.close()
+    W, D = s.compute_energy()
+    return s.get("u"), s.get("v"), W, D
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [1, 2])
+def test_batched_jobs_same_alone_and_in_the_mix(lib, precision):
+    """Batch groups on (every job small enough): jobs set up together share
+    one batch, and each job's fields and totals equal the same job advanced
+    alone in a batch of its own, bit for bit."""
+    jobs = _mix(count=10, seed=13)
+    srv = lib.Server(max_active=10, steps_per_launch=16, batch_max_particles=10**6)
+    ids = [srv.submit(j, precision=precision, keep=("u", "v")) for j in jobs]
+    srv.drain(timeout=600)
+    stats = srv.stats()
+    assert stats["done"] == len(jobs) and stats["failed"] == 0
+    for jid, prob in zip(ids, jobs):
+        st = srv.status(jid)
+        assert st["state"] == lib.system.JOB_DONE and st["steps_done"] == prob["num_steps"]
+        u, v, W, D = _solo_batch(lib, prob, precision)
+        assert np.array_equal(srv.get(jid, "u"), u), prob["kind"]
+        assert np.array_equal(srv.get(jid, "v"), v), prob["kind"]
+        assert (st["total_strain_energy"], st["total_damage"]) == (W, D)
+    srv.close()
+
+
 @pytest.mark.gpu
 def test_jobs_admitted_while_others_run(lib):
     """Continuous batching: short jobs submitted after a long one are
