@@ -946,6 +946,22 @@ int orc_set_state(orc_system* s, const double* u, const double* v)
     return 0;
 }
 
+// Overwrites a whole vector field (u, v or f): the sharding tests write
+// ghost rows between steps.
+int orc_set_field(orc_system* s, int32_t field, const double* in)
+{
+    if (s->n == 0) return fail("orc_set_field: no particles");
+    std::vector<double>* dst = nullptr;
+    switch (field) {
+    case ORC_FIELD_U: dst = &s->u; break;
+    case ORC_FIELD_V: dst = &s->v; break;
+    case ORC_FIELD_F: dst = &s->f; break;
+    default: return fail("orc_set_field: only u, v and f");
+    }
+    dst->assign(in, in + 3 * s->n);
+    return 0;
+}
+
 int orc_build_neighbors(orc_system* s)
 {
     if (s->n == 0) return fail("orc_build_neighbors: no particles");

@@ -93,6 +93,7 @@ int orc_set_particles(orc_system* s, int64_t n, int64_t n_frozen,
                       const double* x, const double* vol, const double* rho,
                       const int32_t* nofail, const double* radius);
 int orc_set_state(orc_system* s, const double* u, const double* v);
+int orc_set_field(orc_system* s, int32_t field, const double* in);
 int orc_build_neighbors(orc_system* s);
 int orc_neighbor_stats(const orc_system* s, int32_t* max_n, int64_t* total);
 /* counts[n]; idx/mu padded [n][max_n] */

@@ -67,6 +67,7 @@ def load():
     lib.orc_set_particles.argtypes = [P, ctypes.c_int64, ctypes.c_int64, dp, dp,
                                       dp, ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_set_state.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
+    lib.orc_set_field.argtypes = [P, ctypes.c_int32, dp]
     lib.orc_build_neighbors.argtypes = [P]
     lib.orc_neighbor_stats.argtypes = [P, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_int64)]
@@ -158,6 +159,11 @@ class OracleSystem:
         self._check(self._lib.orc_set_state(
             self._h, ua.ctypes.data if ua is not None else None,
             va.ctypes.data if va is not None else None))
+
+    def set_field(self, field, values):
+        """Overwrite a whole vector field ("u", "v" or "f"), [n][3]."""
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, 3)
+        self._check(self._lib.orc_set_field(self._h, FIELDS[field], _dptr(a)))
 
     def build_neighbors(self):
         self._check(self._lib.orc_build_neighbors(self._h))
