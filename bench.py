@@ -458,6 +458,89 @@ def measure_other(name, device, stream, steps, warmup):
     return out
 
 
+def measure_batch(device, count=64, chunk=16, chunks=10, precision="mixed"):
+    """Many small jobs (PMB / LPS, 1e3-3e4 particles) advanced as one batch
+    (cpd_batch: one persistent-block launch per step for all of them, after
+    the autotuner has timed its candidates) beside the same systems each
+    replaying its own CUDA graph of `chunk` steps on its own stream (the
+    per-job form). Host-timed over `chunks` chunks, synchronised."""
+    import torch
+
+    import cabanapd_b200
+    jobs = P.served_jobs(count=count, n_range=(1e3, 3e4), steps_range=(4000, 4000), seed=77)
+
+    def build():
+        out = []
+        for j in jobs:
+            s = cabanapd_b200.System(dict(j["params"], device=device,
+                                          precision=PRECISION[precision]))
+            P.setup(s, j)
+            out.append(s)
+        return out
+
+    systems = build()
+    bonds = sum(s.neighbor_stats()[1] for s in systems)
+    b = cabanapd_b200.Batch(systems, [4000] * count)
+    ncand = len(b.tuning()[1])
+    for _ in range(ncand):
+        b.step(chunk)
+        b.synchronize()
+    b.step(chunk)
+    b.synchronize()
+    l0 = b.launches()
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        b.step(chunk)
+    b.synchronize()
+    t_batch = time.perf_counter() - t0
+    launches_batch = b.launches() - l0
+    chosen, cands = b.tuning()
+    b.close()
+    for s in systems:
+        s.close()
+
+    systems = build()
+    streams, graphs = [], []
+    for s in systems:
+        st = torch.cuda.Stream(device=device)
+        s.set_stream(st.cuda_stream)
+        s.step(chunk)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            s.step(chunk)
+        streams.append(st)
+        graphs.append(g)
+    for g, st in zip(graphs, streams):
+        with torch.cuda.stream(st):
+            g.replay()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        for g, st in zip(graphs, streams):
+            with torch.cuda.stream(st):
+                g.replay()
+    torch.cuda.synchronize(device)
+    t_graphs = time.perf_counter() - t0
+    del graphs
+    for s in systems:
+        s.close()
+    work = bonds * chunk * chunks
+    return {"workload": f"{count} independent jobs (PMB elastic cubes, PMB notched plates, "
+                        "LPS random-notch boxes), particles log-uniform in [1000, 30000], "
+                        "seed 77",
+            "precision": precision, "bonds": bonds, "steps": chunk * chunks,
+            "batched": {"bond_updates_per_s": work / t_batch, "s": t_batch,
+                        "launches": launches_batch,
+                        "tuner": {"chosen": chosen,
+                                  "candidates": [{"blocks_per_sm": g, "order": o,
+                                                  "bond_updates_per_s": t}
+                                                 for g, o, t in cands]}},
+            "per_system_graphs": {"bond_updates_per_s": work / t_graphs, "s": t_graphs},
+            "batched_vs_per_system": t_graphs / t_batch,
+            "timing": "host clock around synchronised chunks"}
+
+
 E2E_JOBS = 3
 OTHER_STEPS = {"lps": 20, "plate_1p2m": 100, "wave": 100, "dem": 50}
 DEM_FULL_STEPS = 5000  # the packing's full run, for its mixed-vs-FP64 error
@@ -543,6 +626,7 @@ def run_gpu(args, world, rank, local, pg):
     if world == 1 and not args.skip_others:
         line["other_workloads"] = [measure_other(w, device, stream, OTHER_STEPS[w], 3)
                                    for w in ("plate_1p2m", "lps", "dem", "wave")]
+        line["small_jobs_batch"] = measure_batch(device)
     if world == 1 and not args.skip_serve:
         line["serving"] = run_serving(args, device)
     if world == 1 and not args.skip_cpu:
@@ -753,7 +837,8 @@ def main():
     ap.add_argument("--skip-serve", action="store_true", help="omit the served-stream leg")
     ap.add_argument("--skip-others", action="store_true",
                     help="omit the LPS-box and DEM-packing measurements")
-    ap.add_argument("--only-other", choices=["lps", "dem", "plate_1p2m", "wave"], default=None,
+    ap.add_argument("--only-other", choices=["lps", "dem", "plate_1p2m", "wave", "batch"],
+                    default=None,
                     help="measure only that workload (for profiling) and print it")
     ap.add_argument("--serve-jobs", type=int, default=512, help="served stream: number of jobs")
     ap.add_argument("--serve-n", type=float, nargs=2, default=[1e3, 2e6],
@@ -794,8 +879,11 @@ def main():
         import torch
         torch.cuda.set_device(local)
         stream = torch.cuda.Stream(device=local)
-        print(json.dumps(measure_other(args.only_other, local, stream, args.steps, args.warmup)),
-              flush=True)
+        if args.only_other == "batch":
+            out = measure_batch(local, precision=args.precision)
+        else:
+            out = measure_other(args.only_other, local, stream, args.steps, args.warmup)
+        print(json.dumps(out), flush=True)
         return
     world, rank, local, pg = dist_setup()
     try:

@@ -1200,7 +1200,8 @@ cpd_status cpd_build_neighbors(cpd_system* s)
         tr.mark("list", s->stream);
         if (wants_mixed(s)) {
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
-                              s->stream, err, nullptr, &s->md);
+                              s->stream, err, nullptr,
+                              s->md.pd == CPD_PD_PMB ? &s->md : nullptr);
             if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
             s->launches += l;
         } else if (wants_stencil64(s)) {

@@ -350,31 +350,6 @@ struct StencilL64 {
     double hw[kStencilPoly];  // W(q)
     StencilEntryL64 e[kStencilMax];  // past ntab: zero (no contribution, never deferred)
 };
-// Mixed LPS form (FP32 table walk on the FP32 split, one particle volume, no
-// frozen particles): S(q) = 1/2 + q GS(q), W(q) = 1 + q GW(q) with FP32
-// polynomials GS, GW (anchored, so S(0) and W(0) are exact); the weighted
-// volume sums the FP64 weights, the dilatation terms FP32 chunks of 8 bonds.
-constexpr int kStencilPolyL32 = 4;  // coefficients of GS and GW
-struct __align__(16) StencilEntryL32 {
-    float2 exy;               // bond reference vector (FP32 of the lattice offset)
-    float ez, tz;             // its z, 2 xi z
-    float2 txy;               // 2 xi (x, y)
-    float ixi2;               // 1 / xi^2
-    float wv32;               // omega xi^2 v (FP32, dilatation terms)
-    double wv;                // omega xi^2 v (FP64, weighted volume)
-    float fv;                 // omega v
-    uint32_t kwin;            // |num| bits below kwin: inside the polynomials' window
-    uint32_t kbrk;            // ... and below the break band (force pass)
-    int32_t doff;             // neighbour index - particle index
-    int64_t boff;             // doff * 32: record bytes
-};
-struct StencilL32 {
-    int32_t ntab = 0, nwords = 0;
-    double bbc = 0, theta_coeff = 0, s_coeff = 0;
-    float gs[kStencilPolyL32];
-    float gw[kStencilPolyL32];
-    StencilEntryL32 e[kStencilMax];  // past ntab: zero
-};
 // The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
 constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial
 struct __align__(16) StencilEntry32 {
@@ -464,10 +439,6 @@ struct MixedState {
     // theta / m, s_coeff / m) as one 16-byte gather record, with the guard
     // records of u4 on either side.
     StencilL64* stl64 = nullptr;
-    // Mixed LPS stencil path: its table; u2ab then carries guard records
-    // (u2ab = u2ab_base + guard).
-    StencilL32* stl32 = nullptr;
-    MixedU* u2ab_base = nullptr;
     double2* ab64 = nullptr;       // record of particle 0
     double2* ab64_base = nullptr;  // allocation
     // Mixed PMB stencil kernel: its table, and the allocation behind u2
@@ -486,11 +457,10 @@ struct MixedState {
 };
 // lps: set up the LPS mixed kernels too (lps_ok, ab). fp64_stencil: set up
 // the stencil data for the FP64 stencil kernel only (no FP32 copies).
-// md_stencil (mixed): the model, for the tables of the mixed stencil kernels
-// (PMB; LPS with one particle volume and no frozen particles).
+// md_pmb (mixed PMB): also the table of the mixed stencil kernel.
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err,
-                  const Model* fp64_stencil = nullptr, const Model* md_stencil = nullptr);
+                  const Model* fp64_stencil = nullptr, const Model* md_pmb = nullptr);
 // FP64 stencil path (cpd_kernels_stencil.cu).
 // Builds m.st64 and the gather records (false: the stencil does not apply).
 bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
@@ -501,16 +471,6 @@ bool stencil64_ready(const MixedState& m);
 // Mixed PMB: builds m.st32 (false: the stencil kernel does not apply).
 bool prepare_stencil32(const Model& md, const double* h, const MixedStencil* tab, int ntab,
                        MixedState& m);
-// Mixed LPS: builds m.stl32 and the packed records with guards (false: the
-// mixed LPS kernels keep every row). Needs m.lps_ok, one particle volume and
-// no frozen particles.
-bool prepare_stencil32_lps(const ParticleView& p, const Model& md, const double* h,
-                           const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
-                           std::string& err);
-int launch_lps_mtheta_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
-                                const MixedState& m, bool with_m, cudaStream_t st);
-int launch_lps_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
-                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 // Gather records of rows [begin, end) from the displacement u (SoA).

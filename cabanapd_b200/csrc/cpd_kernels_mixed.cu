@@ -1498,8 +1498,7 @@ void free_mixed(MixedState& m, cudaStream_t st)
     delete m.st32;
     m.st32 = nullptr;
     void* ptrs[] = {m.xh, m.xl, m.u2_base, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
-                    m.ab, m.lean_list, m.rest_list, m.vol_sums,
-                    m.u2ab_base ? m.u2ab_base : m.u2ab, m.stencil_list,
+                    m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab, m.stencil_list,
                     m.irregular_list};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
@@ -1508,7 +1507,7 @@ void free_mixed(MixedState& m, cudaStream_t st)
 
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil,
-                  const Model* md_stencil)
+                  const Model* md_pmb)
 {
     int launches = 0;
     PhaseTrace tr("mixed");
@@ -1714,12 +1713,8 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                     }
                     CPD_TRY(cudaStreamSynchronize(st));
                 }
-                if (fp32 && !lps && md_stencil)
-                    prepare_stencil32(*md_stencil, h, tab.data(), m.ntab, m);
-                if (fp32 && lps && md_stencil &&
-                    !prepare_stencil32_lps(p, *md_stencil, h, tab.data(), m.ntab, m, st, err) &&
-                    !err.empty())
-                    return -1;
+                if (fp32 && !lps && md_pmb)
+                    prepare_stencil32(*md_pmb, h, tab.data(), m.ntab, m);
                 if (!fp32) {
                     if (!prepare_stencil64(p, *fp64_stencil, h, tab.data(), m.ntab, m, st, err) &&
                         !err.empty())
@@ -1736,7 +1731,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
     if (fp32) {
         // The split of u, with zero guard records on either side for the
         // stencil kernel's reads at i + delta of absent entries.
-        if (!m.st32 && !m.stl32) m.guard = 0;
+        if (!m.st32) m.guard = 0;
         const size_t recs = (size_t)(np + 2 * m.guard);
         CPD_TRY(dev_alloc(&m.u2_base, sizeof(MixedU) * recs, st));
         CPD_TRY(cudaMemsetAsync(m.u2_base, 0, sizeof(MixedU) * recs, st));
@@ -1820,7 +1815,6 @@ int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Mode
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    if (m.stl32) return launch_lps_mtheta_stencil32(p, nl, md, m, with_m, st);
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
@@ -1871,7 +1865,6 @@ int launch_lps_force_mixed(const ParticleView& p, const EllView& nl, const Model
 {
     const int64_t rows = p.n - p.frozen;
     if (rows <= 0) return 0;
-    if (m.stl32) return launch_lps_force_stencil32(p, nl, md, m, ep, st);
     const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
     const MixedLps l = to_mixed_lps(md, m);
     const size_t lean_bytes = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;

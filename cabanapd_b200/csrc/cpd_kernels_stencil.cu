@@ -245,11 +245,15 @@ __device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilR
         for (int w = 0; w < 4; ++w) ew[w] = pm[w];
         return;
     }
+    // The list holds ceil(max_n / 32) bond-state words per row, which can be
+    // fewer than the table's words (a thin body holds only part of the
+    // table): words past the list's are absent, not read.
+    const int lwords = (nl.max_n + 31) >> 5;
     uint32_t mw[4];
     int cnt = 0, intact = 0;
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
-        mw[w] = w < nwords ? nl.mu[(int64_t)w * np + i] : 0u;
+        mw[w] = (w < nwords && w < lwords) ? nl.mu[(int64_t)w * np + i] : 0u;
         cnt += __popc(pm[w]);
         intact += __popc(mw[w]);
     }
@@ -636,186 +640,6 @@ __global__ void __launch_bounds__(kBlock, 3)
     step_epilogue<false>(p, ep, i, fx, fy, fz);
 }
 
-// ---------------------------------------------------------------------------
-// LPS, mixed precision, on the stencil (one particle volume, every row a
-// stencil row, no frozen particles): the table walk of k_lps_stencil64 in
-// FP32 on the split records. S(q) = 1/2 + q GS(q) and W(q) = 1 + q GW(q)
-// with FP32 polynomials; dilatation terms and pair forces summed in FP32
-// over chunks of 8 entries into FP64 row totals; the weighted volume sums
-// the FP64 weights of the intact bonds. The dilatation pass writes, per
-// particle, the split of u with a = theta_coeff theta / m and b = s_coeff /
-// m in the w lanes (one 32-byte record per neighbour for the force pass).
-// Bonds outside the window take the FP64 exact expressions; in the force
-// pass the window ends 1e-4 s0 below the break, so every bond near it gets
-// the reference's FP64 break test.
-
-template <int N>
-__device__ __forceinline__ float poly32(const float* c, float q)
-{
-    float t = c[N - 1];
-#pragma unroll
-    for (int k = N - 2; k >= 0; --k) t = fmaf(t, q, c[k]);
-    return t;
-}
-
-template <bool FRACTURE, bool WITH_M, int INFL>
-__global__ void __launch_bounds__(kBlock, 3)
-    k_lps_stencil32_mtheta(ParticleView p, EllView nl, StencilRows sr,
-                           const MixedU* __restrict__ U2, MixedU* __restrict__ PACK,
-                           float2* __restrict__ AB, const StencilL32 st)
-{
-    const int lane = threadIdx.x & 31;
-    const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-    if (slot >= sr.wcount) return;
-    const int64_t warp = sr.wlist[slot];
-    const int64_t i = p.frozen + 32 * warp + lane;
-    if (i >= p.n) return;
-    const int64_t np = p.npad;
-    const int kind = sr.warp_kind[warp];
-    uint32_t ew[4];
-    row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
-    const MixedU ui = U2[i];
-    const float2 nh_xy = f2(-ui.hi.x, -ui.hi.y), nl_xy = f2(-ui.lo.x, -ui.lo.y);
-    const float nh_z = -ui.hi.z, nl_z = -ui.lo.z;
-    const char* __restrict__ rb = reinterpret_cast<const char*>(U2 + i);
-    double m = 0.0, th = 0.0;
-    float tc = 0.f;
-    uint32_t pend[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-    for (int k = 0; k < kStencilMax; ++k) {
-        const int w = k >> 5;
-        const uint32_t bit = 1u << (k & 31);
-        const StencilEntryL32& e = st.e[k];
-        const MixedU uj = *reinterpret_cast<const MixedU*>(rb + e.boff);
-        const float2 hxy = __fadd2_rn(__fadd2_rn(f2(uj.hi.x, uj.hi.y), nh_xy),
-                                      __fadd2_rn(f2(uj.lo.x, uj.lo.y), nl_xy));
-        const float hz = (uj.hi.z + nh_z) + (uj.lo.z + nl_z);
-        const float2 pxy = __fmul2_rn(hxy, __fadd2_rn(hxy, e.txy));
-        const float num = fmaf(hz, hz + e.tz, pxy.x + pxy.y);
-        const float q = num * e.ixi2;
-        const float sv = q * fmaf(q, poly32<kStencilPolyL32>(st.gs, q), 0.5f);
-        const bool on = (ew[w] & bit) != 0u;
-        const bool in = (__float_as_uint(num) & 0x7fffffffu) < e.kwin;
-        if (on && !in) pend[w] |= bit;
-        if (WITH_M) m += on ? e.wv : 0.0;
-        tc = fmaf((on && in) ? e.wv32 : 0.f, sv, tc);
-        if ((k & 7) == 7) {
-            th += (double)tc;
-            tc = 0.f;
-        }
-    }
-    if (pend[0] | pend[1] | pend[2] | pend[3]) {
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            uint32_t q = pend[w];
-            while (q) {
-                const int b = __ffs(q) - 1;
-                q &= q - 1;
-                const int k = 32 * w + b;
-                const ExactBond eb = exact_geometry(p, i, i + st.e[k].doff);
-                th = fma(st.e[k].wv, eb.s, th);
-            }
-        }
-    }
-    if (!WITH_M) m = p.m[i];
-    th = (!FRACTURE || m > 0) ? 3.0 * th / m : 0.0;
-    if (WITH_M) p.m[i] = m;
-    p.theta[i] = th;
-    const double a = st.theta_coeff * th / m, bb = st.s_coeff / m;
-    p.lps_a[i] = a;
-    p.lps_b[i] = bb;
-    AB[i] = make_float2((float)a, (float)bb);
-    PACK[i] = MixedU{make_float4(ui.hi.x, ui.hi.y, ui.hi.z, (float)a),
-                     make_float4(ui.lo.x, ui.lo.y, ui.lo.z, (float)bb)};
-}
-
-template <bool FRACTURE, int INFL>
-__global__ void __launch_bounds__(kBlock, 3)
-    k_lps_stencil32_force(ParticleView p, EllView nl, StencilRows sr,
-                          const MixedU* __restrict__ PACK, StepEpilogue ep, const StencilL32 st)
-{
-    const int lane = threadIdx.x & 31;
-    const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-    if (slot >= sr.wcount) return;
-    const int64_t warp = sr.wlist[slot];
-    const int64_t i = p.frozen + 32 * warp + lane;
-    if (i >= p.n) return;
-    const int64_t np = p.npad;
-    const int kind = sr.warp_kind[warp];
-    uint32_t ew[4];
-    row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
-    const MixedU ui = PACK[i];
-    const float ai = ui.hi.w, bi = ui.lo.w;
-    const float2 nh_xy = f2(-ui.hi.x, -ui.hi.y), nl_xy = f2(-ui.lo.x, -ui.lo.y);
-    const float nh_z = -ui.hi.z, nl_z = -ui.lo.z;
-    const char* __restrict__ rb = reinterpret_cast<const char*>(PACK + i);
-    double f[3] = {0.0, 0.0, 0.0};
-    float2 cxy = f2(0.f, 0.f);
-    float cz = 0.f;
-    uint32_t pend[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-    for (int k = 0; k < kStencilMax; ++k) {
-        const int w = k >> 5;
-        const uint32_t bit = 1u << (k & 31);
-        const StencilEntryL32& e = st.e[k];
-        const MixedU uj = *reinterpret_cast<const MixedU*>(rb + e.boff);
-        const float2 hxy = __fadd2_rn(__fadd2_rn(f2(uj.hi.x, uj.hi.y), nh_xy),
-                                      __fadd2_rn(f2(uj.lo.x, uj.lo.y), nl_xy));
-        const float hz = (uj.hi.z + nh_z) + (uj.lo.z + nl_z);
-        const float2 pxy = __fmul2_rn(hxy, __fadd2_rn(hxy, e.txy));
-        const float num = fmaf(hz, hz + e.tz, pxy.x + pxy.y);
-        const float q = num * e.ixi2;
-        const float sv = q * fmaf(q, poly32<kStencilPolyL32>(st.gs, q), 0.5f);
-        const float W = fmaf(q, poly32<kStencilPolyL32>(st.gw, q), 1.0f);
-        const bool on = (ew[w] & bit) != 0u;
-        const bool in = (__float_as_uint(num) & 0x7fffffffu) < e.kbrk;
-        if (on && !in) pend[w] |= bit;
-        float F = fmaf(sv, bi + uj.lo.w, ai + uj.hi.w) * (e.fv * W);
-        F = (on && in) ? F : 0.f;
-        cxy = __ffma2_rn(f2(F, F), __fadd2_rn(e.exy, hxy), cxy);
-        cz = fmaf(F, e.ez + hz, cz);
-        if ((k & 7) == 7) {
-            f[0] += (double)cxy.x;
-            f[1] += (double)cxy.y;
-            f[2] += (double)cz;
-            cxy = f2(0.f, 0.f);
-            cz = 0.f;
-        }
-    }
-    if (pend[0] | pend[1] | pend[2] | pend[3]) {
-        // Deferred bonds: the reference's break test (the row's no-fail flag
-        // only, force/CabanaPD_LPS.hpp:417-418) and FP64 pair force.
-        const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
-        const double a_i = p.lps_a[i], b_i = p.lps_b[i];
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            uint32_t q = pend[w];
-            while (q) {
-                const int b = __ffs(q) - 1;
-                q &= q - 1;
-                const int k = 32 * w + b;
-                const int64_t j = i + st.e[k].doff;
-                const ExactBond eb = exact_geometry(p, i, j);
-                if (FRACTURE && !nofail_i &&
-                    __dmul_rn(eb.r, eb.r) >= __dmul_rn(__dmul_rn(st.bbc, eb.xi), eb.xi)) {
-                    clear_bond_bit(nl, sr, kind, i, np, w, b);
-                    continue;
-                }
-                const double oxi = INFL == 1 ? 1.0 : eb.xi;
-                const double coeff = __dmul_rn(
-                    __dmul_rn(__dadd_rn(__dadd_rn(a_i, p.lps_a[j]),
-                                        __dmul_rn(eb.s, __dadd_rn(b_i, p.lps_b[j]))),
-                              oxi),
-                    p.vol[j]);
-                f[0] += __ddiv_rn(__dmul_rn(coeff, eb.rx), eb.r);
-                f[1] += __ddiv_rn(__dmul_rn(coeff, eb.ry), eb.r);
-                f[2] += __ddiv_rn(__dmul_rn(coeff, eb.rz), eb.r);
-            }
-        }
-    }
-    step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
-}
-
 }  // namespace
 
 void free_stencil64(MixedState& m, cudaStream_t st)
@@ -824,8 +648,6 @@ void free_stencil64(MixedState& m, cudaStream_t st)
     m.st64 = nullptr;
     delete m.stl64;
     m.stl64 = nullptr;
-    delete m.stl32;
-    m.stl32 = nullptr;
     if (m.u4_base) dev_free(m.u4_base, st);
     if (m.u4_alt_base) dev_free(m.u4_alt_base, st);
     if (m.ab64_base) dev_free(m.ab64_base, st);
@@ -1075,139 +897,6 @@ int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Mo
         if (t122) CPD_ST32(false, true, 122); else CPD_ST32(false, true, 128);
     }
 #undef CPD_ST32
-    return 1;
-}
-
-bool prepare_stencil32_lps(const ParticleView& p, const Model& md, const double* h,
-                           const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
-                           std::string& err)
-{
-    delete m.stl32;
-    m.stl32 = nullptr;
-    if (md.pd != CPD_PD_LPS || !m.lps_ok || m.vol_sums == nullptr || p.frozen > 0 ||
-        ntab <= 0 || ntab > kStencilMax || m.nstencil == 0)
-        return false;
-    // Window |q| < qwin: the polynomials' range and (fracture) the break band
-    // of the FP32 kernels (stretch within 1e-4 s0 of s0).
-    const double s_lo = md.s0 * (1.0 - 1e-4);
-    const double qc_lo = (1.0 + s_lo) * (1.0 + s_lo) - 1.0;
-    const double qwin = md.fracture ? std::min(kStencilQ, qc_lo) : kStencilQ;
-    if (!(qwin > 1e-8)) return false;
-    // Anchored forms: (S(q) - 1/2) / q = -1 / (2 (1 + s)^2) and (W(q) - 1) / q
-    // = -1 / (s (1 + s)), s = sqrt(1 + q).
-    auto GS = [](long double q) {
-        const long double r = sqrtl(1.0L + q);
-        return -1.0L / (2.0L * (1.0L + r) * (1.0L + r));
-    };
-    auto GW = [](long double q) {
-        const long double r = sqrtl(1.0L + q);
-        return -1.0L / (r * (1.0L + r));
-    };
-    long double cs[kStencilPoly], cw[kStencilPoly];
-    fit_poly((long double)qwin, kStencilPolyL32, GS, cs);
-    fit_poly((long double)qwin, kStencilPolyL32, GW, cw);
-    StencilL32* S = new StencilL32();
-    S->ntab = ntab;
-    S->nwords = (ntab + 31) / 32;
-    S->bbc = md.bond_break_coeff;
-    S->theta_coeff = md.theta_coeff;
-    S->s_coeff = md.s_coeff;
-    for (int k = 0; k < kStencilPolyL32; ++k) {
-        S->gs[k] = (float)cs[k];
-        S->gw[k] = (float)cw[k];
-    }
-    const long double v = m.vol_uniform;
-    int64_t G = 0;
-    for (int k = 0; k < ntab; ++k) {
-        StencilEntryL32& e = S->e[k];
-        const double a = std::nearbyint((double)tab[k].x / h[0]);
-        const double b = std::nearbyint((double)tab[k].y / h[1]);
-        const double c = std::nearbyint((double)tab[k].z / h[2]);
-        e.exy = make_float2((float)(a * h[0]), (float)(b * h[1]));
-        e.ez = (float)(c * h[2]);
-        e.txy = make_float2(2.f * e.exy.x, 2.f * e.exy.y);
-        e.tz = 2.f * e.ez;
-        // Lengths of the FP32 vectors the kernel works with (as the PMB
-        // form): the force law stays consistent with the geometry it sees.
-        const long double fx = e.exy.x, fy = e.exy.y, fz = e.ez;
-        const long double x2 = fx * fx + fy * fy + fz * fz;
-        const long double xi = sqrtl(x2);
-        e.ixi2 = (float)(1.0L / x2);
-        const long double wv = (md.influence == 1 ? xi : x2) * v;
-        e.wv = (double)wv;
-        e.wv32 = (float)wv;
-        e.fv = (float)(md.influence == 1 ? v / xi : v);
-        e.doff = tab[k].delta == INT32_MAX ? 0 : tab[k].delta;
-        e.boff = (int64_t)e.doff * (int64_t)sizeof(MixedU);
-        const float T = (float)(qwin * (double)x2);
-        uint32_t tb;
-        std::memcpy(&tb, &T, sizeof tb);
-        e.kwin = tb;
-        e.kbrk = tb;
-        G = std::max<int64_t>(G, std::abs((int64_t)e.doff));
-    }
-    // The packed records with zero guard records on either side (reads at
-    // i + delta of absent entries stay inside the allocation).
-    const int64_t guard = G + 32;
-    const size_t recs = (size_t)(p.npad + 2 * guard);
-    MixedU* base = nullptr;
-    if (dev_alloc(&base, sizeof(MixedU) * recs, st) != cudaSuccess ||
-        cudaMemsetAsync(base, 0, sizeof(MixedU) * recs, st) != cudaSuccess) {
-        err = std::string("LPS packed records: ") + cudaGetErrorString(cudaGetLastError());
-        if (base) dev_free(base, st);
-        delete S;
-        return false;
-    }
-    if (m.u2ab_base) {
-        dev_free(m.u2ab_base, st);
-    } else if (m.u2ab) {
-        dev_free(m.u2ab, st);
-        m.bytes -= sizeof(MixedU) * (size_t)p.npad;
-    }
-    m.u2ab_base = base;
-    m.u2ab = base + guard;
-    m.bytes += sizeof(MixedU) * recs;
-    m.guard = guard;
-    m.stl32 = S;
-    return true;
-}
-
-int launch_lps_mtheta_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
-                                const MixedState& m, bool with_m, cudaStream_t st)
-{
-    if (p.n - p.frozen <= 0 || m.nstencil <= 0 || !m.stl32) return 0;
-    const StencilRows sr{m.warp_kind, m.pmask, m.stencil_list, m.nstencil};
-    const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
-    const StencilL32& S = *m.stl32;
-    const bool i1 = md.influence == 1;
-#define CPD_LM32(F, W, I) \
-    k_lps_stencil32_mtheta<F, W, I><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2, m.u2ab, m.ab, S)
-    if (md.fracture) {
-        if (i1) CPD_LM32(true, true, 1); else CPD_LM32(true, true, 0);
-    } else if (with_m) {
-        if (i1) CPD_LM32(false, true, 1); else CPD_LM32(false, true, 0);
-    } else {
-        if (i1) CPD_LM32(false, false, 1); else CPD_LM32(false, false, 0);
-    }
-#undef CPD_LM32
-    return 1;
-}
-
-int launch_lps_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
-                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st)
-{
-    if (p.n - p.frozen <= 0 || m.nstencil <= 0 || !m.stl32) return 0;
-    const StencilRows sr{m.warp_kind, m.pmask, m.stencil_list, m.nstencil};
-    const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
-    const StencilL32& S = *m.stl32;
-    const bool i1 = md.influence == 1;
-#define CPD_LF32(F, I) k_lps_stencil32_force<F, I><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2ab, ep, S)
-    if (md.fracture) {
-        if (i1) CPD_LF32(true, 1); else CPD_LF32(true, 0);
-    } else {
-        if (i1) CPD_LF32(false, 1); else CPD_LF32(false, 0);
-    }
-#undef CPD_LF32
     return 1;
 }
 

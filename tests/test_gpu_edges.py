@@ -192,3 +192,29 @@ def test_count_pass_spacing_equals_list_spacing(cuda, precision, monkeypatch):
         P.setup(s, prob)
         s.run(prob["num_steps"])
         assert np.all(np.isfinite(s.get("u")))
+
+
+@pytest.mark.parametrize("precision", [FAST, MIXED])
+@pytest.mark.parametrize("model", ["lps", "pmb"])
+def test_notched_two_layer_bodies(cuda, oracle, precision, model):
+    """Two lattice layers (rows hold part of the stencil table and fewer
+    bond-state words than the table has) with notches cutting bonds: the
+    stencil kernels read only the list's words. LPS box 102 x 41 x 2 with
+    20 random notches (a slightly non-cubic lattice), PMB plate 60 x 30 x 2
+    with its two notches; 30 steps against the oracle."""
+    if model == "lps":
+        prob = P.lps_random_notches(num_cells=(102, 41, 2), steps=30, seed=20261209)
+    else:
+        prob = P.plate_impact(num_cells=(60, 30, 2), steps=30, v0=60.0)
+    g = cuda.System(dict(prob["params"], precision=precision))
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(g, prob)
+    P.setup(o, prob)
+    tu = TOL[precision][0]
+    assert _nrel(g.get("m"), o.get("m")) <= (1e-13 if precision == FAST else 1e-6) \
+        if model == "lps" else True
+    g.run(prob["num_steps"])
+    o.run(prob["num_steps"])
+    _check(g, o, precision)
+    assert (o.neighbors()[2] == 0).sum() > 0
+    assert _nrel(g.get("u"), o.get("u")) <= tu
