@@ -105,6 +105,12 @@ struct Job {
     std::deque<Chunk> inflight;
     std::vector<cudaEvent_t> spare;
     std::map<int32_t, std::vector<double>> results;
+    // Eviction: requested (the launcher stops issuing chunks and hands the
+    // job to a worker once its chunks are done), and the host snapshot of
+    // the evolving state it resumes from when set up again.
+    std::atomic<bool> evict_request{false};
+    int32_t evictions = 0;
+    std::vector<uint8_t> snapshot;
 };
 
 // A batch group: small jobs advanced together by one cpd_batch (one
@@ -180,6 +186,8 @@ struct cpd_server {
     std::vector<Job*> admitted; // set up, not yet picked by the launcher
     std::vector<Job*> pending_batch;  // set up small jobs for the next batch group
     std::vector<Job*> retire;   // all steps done, not yet finalised
+    std::vector<Job*> evicting; // chunks drained, to be saved and freed
+    int evictions_pending = 0;
     int64_t resident = 0;
     uint64_t resident_bytes = 0, peak_bytes = 0;
     int64_t n_submitted = 0, n_done = 0, n_failed = 0, launches = 0;
@@ -311,9 +319,86 @@ struct cpd_server {
                 return "event creation failed";
             j->spare.push_back(ev);
         }
+        // A resumed job continues from its snapshot (the state it was evicted
+        // with), bit-identical to an uninterrupted run.
+        if (!j->snapshot.empty()) {
+            if (cpd_load_state(j->sys, j->snapshot.data(), (uint64_t)j->snapshot.size()) != CPD_OK)
+                return lib_error("cpd_load_state");
+            std::vector<uint8_t>().swap(j->snapshot);
+        }
         cpd_device_bytes(j->sys, &j->bytes);
-        j->spec.reset();  // the host copy of the input is no longer needed
+        // The host copy of the input stays for jobs that may be evicted (a
+        // resumed job is set up again from it).
+        if (j->batched) j->spec.reset();
         return std::string();
+    }
+
+    // Saves an evicted job's state to the host, frees its device memory and
+    // queues it again right behind the queue's head (the job it made room
+    // for). Caller holds no lock.
+    void evict(Job* j)
+    {
+        std::string err;
+        uint64_t bytes = 0;
+        std::vector<uint8_t> snap;
+        if (cpd_state_bytes(j->sys, &bytes) != CPD_OK)
+            err = std::string("cpd_state_bytes: ") + cpd_last_error();
+        if (err.empty()) {
+            snap.resize((size_t)bytes);
+            if (cpd_save_state(j->sys, snap.data(), bytes) != CPD_OK)
+                err = std::string("cpd_save_state: ") + cpd_last_error();
+        }
+        const int64_t direct = j->sys ? cpd_kernel_launches(j->sys) - j->captured : 0;
+        release_device(j);
+        std::lock_guard<std::mutex> lk(mu);
+        evictions_pending--;
+        resident--;
+        resident_bytes -= std::max(j->bytes, j->est_bytes);
+        j->launches += direct;
+        j->evict_request = false;
+        if (!err.empty()) {
+            finish_failed(j, err);
+            return;
+        }
+        j->snapshot.swap(snap);
+        j->evictions++;
+        j->state = CPD_JOB_QUEUED;
+        j->captured = 0;
+        j->inflight.clear();
+        queue.insert(queue.empty() ? queue.end() : queue.begin() + 1, j);
+        cv_worker.notify_all();
+    }
+
+    // Automatic eviction (cfg.evict_after_s > 0): when the queue's head has
+    // waited that long for memory, the resident job with the most work left
+    // (particles x steps, larger than the head's, never evicted before) is
+    // asked to make room. One eviction at a time. Caller holds mu.
+    void consider_eviction()
+    {
+        if (cfg.evict_after_s <= 0.0 || evictions_pending > 0 || queue.empty()) return;
+        Job* head = queue.front();
+        if (head->est_bytes > cfg.hbm_budget_bytes || resident == 0 ||
+            resident_bytes + head->est_bytes <= cfg.hbm_budget_bytes)
+            return;
+        if (now() - head->t_submit < cfg.evict_after_s) return;
+        const double head_work = (double)head->n * std::max(1, head->steps);
+        Job* victim = nullptr;
+        double most = head_work;
+        for (auto& kv : jobs) {
+            Job* j = kv.second.get();
+            if (j->state != CPD_JOB_RUNNING || j->batched || j->evictions > 0 ||
+                j->evict_request || !j->spec)
+                continue;
+            const double left = (double)j->n * std::max(0, j->steps - j->steps_done.load());
+            if (left > most) {
+                most = left;
+                victim = j;
+            }
+        }
+        if (victim) {
+            victim->evict_request = true;
+            evictions_pending++;
+        }
     }
 
     void finalize(Job* j)
@@ -372,9 +457,18 @@ struct cpd_server {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
             cv_worker.wait_for(lk, std::chrono::milliseconds(50), [&] {
-                return (stopping && resident == 0) || !retire.empty() || admissible() ||
-                       (!accepting && !queue.empty());
+                return (stopping && resident == 0) || !retire.empty() || !evicting.empty() ||
+                       admissible() || (!accepting && !queue.empty());
             });
+            if (!evicting.empty()) {
+                std::vector<Job*> out;
+                out.swap(evicting);
+                lk.unlock();
+                for (Job* j : out) evict(j);
+                lk.lock();
+                continue;
+            }
+            if (accepting && !stopping) consider_eviction();
             if (!retire.empty()) {
                 std::vector<Job*> done;
                 done.swap(retire);
@@ -636,7 +730,9 @@ struct cpd_server {
                     j->inflight.pop_front();
                     progressed = true;
                 }
-                while (!bad && j->steps_launched < j->steps && (int)j->inflight.size() < kInflight) {
+                const bool evicting_now = j->evict_request.load();
+                while (!bad && !evicting_now && j->steps_launched < j->steps &&
+                       (int)j->inflight.size() < kInflight) {
                     if (j->t_start < 0) j->t_start = now();
                     if (!launch_chunk(j)) bad = true;
                     progressed = true;
@@ -645,7 +741,21 @@ struct cpd_server {
                     failed.push_back(j);
                     it = running.erase(it);
                 } else if (j->steps_done == j->steps) {
+                    if (evicting_now) {
+                        // Finished before it could be evicted.
+                        j->evict_request = false;
+                        std::lock_guard<std::mutex> lk(mu);
+                        evictions_pending--;
+                    }
                     finished.push_back(j);
+                    it = running.erase(it);
+                } else if (evicting_now && j->inflight.empty()) {
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        evicting.push_back(j);
+                        cv_worker.notify_one();
+                    }
+                    progressed = true;
                     it = running.erase(it);
                 } else {
                     ++it;
@@ -759,7 +869,7 @@ cpd_status cpd_server_create(const cpd_server_config* cfg, cpd_server** out)
     if (!cfg || !out) return fail(CPD_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
     if (cfg->max_active < 1 || cfg->steps_per_launch < 1 || cfg->hbm_budget_bytes == 0 ||
-        cfg->setup_threads < 0)
+        cfg->setup_threads < 0 || cfg->evict_after_s < 0.0)
         return fail(CPD_ERR_INVALID_ARGUMENT,
                     "max_active, steps_per_launch and hbm_budget_bytes must be positive");
     int ndev = 0;
@@ -868,6 +978,7 @@ cpd_status cpd_server_job_status(cpd_server* s, int64_t id, cpd_job_status* out)
     st.total_strain_energy = j.W;
     st.total_damage = j.D;
     st.kernel_launches = j.launches;
+    st.evictions = j.evictions;
     *out = st;
     return CPD_OK;
 }
@@ -896,6 +1007,21 @@ cpd_status cpd_server_download(cpd_server* s, int64_t id, int32_t field, double*
     auto r = j.results.find(field);
     if (r == j.results.end()) return fail(CPD_ERR_STATE, "field was not kept for this job");
     std::memcpy(host_out, r->second.data(), sizeof(double) * r->second.size());
+    return CPD_OK;
+}
+
+cpd_status cpd_server_evict(cpd_server* s, int64_t id)
+{
+    if (!s) return fail(CPD_ERR_INVALID_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail(CPD_ERR_INVALID_ARGUMENT, "unknown job id");
+    Job* j = it->second.get();
+    if (j->state != CPD_JOB_RUNNING || j->batched || !j->spec)
+        return fail(CPD_ERR_STATE, "only a running job that is not in a batch group is evicted");
+    if (j->evict_request) return CPD_OK;
+    j->evict_request = true;
+    s->evictions_pending++;
     return CPD_OK;
 }
 

@@ -70,6 +70,7 @@ class ServerConfig(ctypes.Structure):
         ("hbm_budget_bytes", ctypes.c_uint64),
         ("setup_threads", ctypes.c_int32),
         ("batch_max_particles", ctypes.c_int32),
+        ("evict_after_s", ctypes.c_double),
     ]
 
 
@@ -90,6 +91,7 @@ class JobStatus(ctypes.Structure):
         ("total_strain_energy", ctypes.c_double),
         ("total_damage", ctypes.c_double),
         ("kernel_launches", ctypes.c_int64),
+        ("evictions", ctypes.c_int64),
     ]
 
 
@@ -185,6 +187,7 @@ SIGNATURES = {
     "cpd_server_job_error": (_I32, [_P, _I64, ctypes.c_char_p, _I64]),
     "cpd_server_download": (_I32, [_P, _I64, _I32, _P]),
     "cpd_server_release": (_I32, [_P, _I64]),
+    "cpd_server_evict": (_I32, [_P, _I64]),
     "cpd_server_stats_get": (_I32, [_P, ctypes.POINTER(ServerStats)]),
 }
 
@@ -502,11 +505,13 @@ class Server:
     and returns a job id; results stay on the host until release()."""
 
     def __init__(self, device=0, max_active=16, steps_per_launch=32, use_graphs=True,
-                 hbm_budget_bytes=150 * 10**9, setup_threads=4, batch_max_particles=0):
+                 hbm_budget_bytes=150 * 10**9, setup_threads=4, batch_max_particles=0,
+                 evict_after_s=0.0):
         lib = load()
         self._lib = lib
         cfg = ServerConfig(device, max_active, steps_per_launch, 1 if use_graphs else 0,
-                           int(hbm_budget_bytes), int(setup_threads), int(batch_max_particles))
+                           int(hbm_budget_bytes), int(setup_threads), int(batch_max_particles),
+                           float(evict_after_s))
         h = _P()
         self._check(lib.cpd_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -596,6 +601,11 @@ class Server:
         self._check(self._lib.cpd_server_download(self._h, int(job_id), FIELDS[field],
                                                   out.ctypes.data))
         return out
+
+    def evict(self, job_id):
+        """Save a running job's state to the host, free its device memory and
+        queue it again; it resumes from the snapshot."""
+        self._check(self._lib.cpd_server_evict(self._h, int(job_id)))
 
     def release(self, job_id):
         self._check(self._lib.cpd_server_release(self._h, int(job_id)))

@@ -65,7 +65,7 @@
 extern "C" {
 #endif
 
-#define CPD_ABI_VERSION 2
+#define CPD_ABI_VERSION 3
 
 typedef struct cpd_system cpd_system;
 typedef int32_t cpd_status;
@@ -441,6 +441,15 @@ typedef struct cpd_server_config {
                                    (cpd_batch_*: one launch per step for the
                                    group, jobs set up together form a group);
                                    0: every job on its own */
+    double evict_after_s;       /* > 0: when the queue's head has waited this
+                                   long for memory, the resident job with the
+                                   most work left (more than the head's) is
+                                   evicted: its state is saved to the host
+                                   (cpd_save_state), its device memory freed,
+                                   and it is queued again right behind the
+                                   head; set up again later, it resumes from
+                                   the snapshot (cpd_load_state), bit-identical
+                                   to an uninterrupted run. 0: never */
 } cpd_server_config;
 
 typedef struct cpd_job_status {
@@ -456,6 +465,7 @@ typedef struct cpd_job_status {
     double submit_time, admit_time, ready_time, start_time, finish_time;
     double total_strain_energy, total_damage;                 /* at the end */
     int64_t kernel_launches;    /* kernels run (graph replays count each node) */
+    int64_t evictions;          /* times the job was evicted and resumed */
 } cpd_job_status;
 
 typedef struct cpd_server_stats {
@@ -498,6 +508,11 @@ cpd_status cpd_server_job_error(cpd_server* server, int64_t job_id, char* buf, i
 /* A kept field of a DONE job, in the caller's particle order. */
 cpd_status cpd_server_download(cpd_server* server, int64_t job_id, int32_t field,
                                double* host_out);
+/* Evict a running job (not one in a batch group): once its chunks in
+ * flight complete, its state is saved to the host and its device memory
+ * freed; it is queued again behind the queue's head and resumes from the
+ * snapshot, bit-identical to an uninterrupted run. */
+cpd_status cpd_server_evict(cpd_server* server, int64_t job_id);
 cpd_status cpd_server_release(cpd_server* server, int64_t job_id);
 cpd_status cpd_server_stats_get(cpd_server* server, cpd_server_stats* out);
 

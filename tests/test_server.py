@@ -188,3 +188,61 @@ def test_failures_stay_with_their_job(lib):
     with pytest.raises(lib.CpdError):
         srv.status(ids[1])
     srv.close()
+
+
+def _wait_steps(srv, jid, steps, timeout=120.0):
+    t_end = time.time() + timeout
+    while srv.status(jid)["steps_done"] < steps and time.time() < t_end:
+        time.sleep(0.002)
+    return srv.status(jid)
+
+
+@pytest.mark.gpu
+def test_evicted_job_resumes_bit_identical(lib):
+    """A running job evicted on request (its state saved to the host, its
+    device memory freed) is set up again and resumes from the snapshot: its
+    fields and totals equal the uninterrupted run bit for bit."""
+    prob = P.plate_impact(num_cells=(120, 60, 6), steps=600)
+    srv = lib.Server(max_active=2, steps_per_launch=16)
+    jid = srv.submit(prob, precision=1, keep=("u", "v"))
+    st = _wait_steps(srv, jid, 64)
+    assert st["state"] == lib.system.JOB_RUNNING and st["steps_done"] < prob["num_steps"]
+    srv.evict(jid)
+    srv.drain(timeout=600)
+    st = srv.status(jid)
+    assert st["state"] == lib.system.JOB_DONE and st["steps_done"] == prob["num_steps"]
+    assert st["evictions"] == 1
+    u, v, W, D = _solo(lib, prob, 1)
+    assert np.array_equal(srv.get(jid, "u"), u)
+    assert np.array_equal(srv.get(jid, "v"), v)
+    assert (st["total_strain_energy"], st["total_damage"]) == (W, D)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_budget_pressure_evicts_the_long_job(lib):
+    """A budget that holds one of two jobs: the short job that arrives while
+    the long one runs waits evict_after_s, then the long job is evicted,
+    the short one runs and finishes first, and the long one resumes; both
+    equal their uninterrupted runs bit for bit."""
+    long_job = P.plate_impact(num_cells=(200, 100, 9), steps=2000)
+    short = P.plate_impact(num_cells=(80, 40, 4), steps=100)
+    probe = lib.Server(max_active=1)
+    sizes = [probe.wait(probe.submit(j, precision=2))["device_bytes"] for j in (long_job, short)]
+    probe.close()
+    budget = sizes[0] + sizes[1] // 2
+    srv = lib.Server(max_active=4, steps_per_launch=16, hbm_budget_bytes=budget,
+                     evict_after_s=0.05)
+    a = srv.submit(long_job, precision=2, keep=("u",))
+    _wait_steps(srv, a, 64)
+    b = srv.submit(short, precision=2, keep=("u",))
+    srv.drain(timeout=600)
+    sa, sb = srv.status(a), srv.status(b)
+    assert sa["state"] == sb["state"] == lib.system.JOB_DONE
+    assert sa["evictions"] == 1 and sb["evictions"] == 0
+    assert sb["finish_time"] < sa["finish_time"]
+    assert srv.stats()["peak_resident_bytes"] <= budget
+    for jid, prob in ((a, long_job), (b, short)):
+        u, _, _, _ = _solo(lib, prob, 2)
+        assert np.array_equal(srv.get(jid, "u"), u)
+    srv.close()
