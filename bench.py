@@ -381,6 +381,16 @@ def other_workload(name, steps):
             {"workload": "dem_hertz_packing", "lattice": list(DEM_DIMS), "rebuild_every": 10})
 
 
+def check_mixed_error(workload, err):
+    """A mixed-precision run that left finite values or the mixed bars far
+    behind (relative error above 1e-3 in a field against FP64) has broken
+    arithmetic: no throughput is reported for it."""
+    bad = {k: v for k, v in err.items()
+           if k in ("u", "v", "f", "theta") and not (np.isfinite(v) and v <= 1e-3)}
+    if bad:
+        raise SystemExit(f"{workload}: mixed precision departs from FP64: {bad}")
+
+
 def measure_other(name, device, stream, steps, warmup):
     """A short measurement of another hot-path workload: the LPS fracture
     box (8.0 M particles), the 1.2 M-particle variant of the notched plate or
@@ -450,6 +460,7 @@ def measure_other(name, device, stream, steps, warmup):
         if name == "dem":
             err["contact_rebuilds"] = [a.contact_rebuilds(), b.contact_rebuilds()]
             err["contacts"] = [a.neighbor_stats()[1], b.neighbor_stats()[1]]
+        check_mixed_error(name, err)
         out["plain_fp64"] = res["fp64"]
         out["mixed_vs_plain"] = res["fp64"]["ms_per_step"] / res[head]["ms_per_step"]
         out["mixed_error_vs_fp64"] = err
@@ -583,6 +594,7 @@ def run_gpu(args, world, rank, local, pg):
         err["strain_energy"] = abs(wa - wb) / abs(wb)
         err["damage_identical"] = bool(np.array_equal(a.get("phi"), b.get("phi")))
         err["total_damage"] = [da, db]
+        check_mixed_error("plate", err)
         plain = {"value": pv, "ms_per_step": pms / args.steps,
                  "roofline": roofline("fp64", res["fp64"], bonds),
                  "gpu_launches": res["fp64"]["launches"]}

@@ -443,13 +443,15 @@ bool use_mixed(const cpd_system* s)
     return wants_mixed(s) && (s->md.pd == CPD_PD_PMB || s->mixed.lps_ok);
 }
 
-// CPD_FP64 PMB or LPS without contact on a lattice: the stencil kernels take
-// the stencil rows (set up with the neighbour list when wants_stencil64; LPS
-// needs one particle volume and every row a stencil row).
+// CPD_FP64 PMB without contact on a lattice: the stencil kernel takes the
+// stencil rows (set up with the neighbour list when wants_stencil64). LPS
+// keeps the FP64 throughput kernels: its dilatation and force sum strongly
+// cancelling bond terms, which would turn the lattice offsets' departure
+// from the positions' rounded differences (~1e-14) into errors above 1e-12.
 bool wants_stencil64(const cpd_system* s)
 {
     return s->params.precision == CPD_FP64 && s->md.contact == CPD_CONTACT_NONE &&
-           (s->md.pd == CPD_PD_PMB || s->md.pd == CPD_PD_LPS);
+           s->md.pd == CPD_PD_PMB;
 }
 
 bool use_stencil64(const cpd_system* s)
@@ -497,12 +499,6 @@ cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, const MixedState
         CPD_LAUNCHED(launch_lps_mtheta_mixed(p, pd_view(s), s->md, m, compute_m, s->stream));
         return CPD_OK;
     }
-    if (use_stencil64(s)) {
-        // m.u4 holds p.u (the fused step keeps it so; lps_prepare packs it).
-        CPD_LAUNCHED(launch_lps_mtheta_stencil64(p, pd_view(s), s->md, m, compute_m,
-                                                 s->stream));
-        return CPD_OK;
-    }
     if (use_fast(s)) {
         CPD_LAUNCHED(launch_lps_m_theta_fast(p, pd_view(s), s->md, compute_m, s->stream));
         return CPD_OK;
@@ -514,9 +510,7 @@ cpd_status lps_prepare_on(cpd_system* s, const ParticleView& p, const MixedState
 
 cpd_status lps_prepare(cpd_system* s, bool compute_m)
 {
-    const ParticleView p = view(s);
-    if (use_stencil64(s)) CPD_LAUNCHED(launch_pack_u4(p, p.u, 0, p.n, s->mixed.u4, s->stream));
-    return lps_prepare_on(s, p, s->mixed, compute_m);
+    return lps_prepare_on(s, view(s), s->mixed, compute_m);
 }
 
 cpd_status contact_force(cpd_system* s, bool reset)

@@ -325,31 +325,6 @@ struct Stencil64 {
     double h[kStencilPoly];
     StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
 };
-// LPS form of the FP64 stencil table (one particle volume v). With q = (r^2 -
-// xi^2) / xi^2 the stretch is s = q S(q), S(q) = 1 / (1 + sqrt(1 + q)), and
-// xi / r = W(q) = 1 / sqrt(1 + q), both as polynomials on the entry window;
-// the weighted-volume weight omega xi^2 v and the force factor omega xi v /
-// xi (times W = xi / r gives omega xi v / r) are entry constants
-// (force_models/CabanaPD_LPS.hpp:85-134).
-struct __align__(16) StencilEntryL64 {
-    double ex, ey, ez;        // bond reference vector xi (FP64 lattice offset)
-    double tx, ty, tz;        // 2 xi
-    double ixi2;              // 1 / xi^2
-    double wv;                // omega xi^2 v (influence 0: xi^2 v; 1: xi v)
-    double fv;                // omega v (influence 0: v; 1: v / xi)
-    int64_t boff;             // (neighbour index - particle index) * 32: record bytes
-    int32_t doff;             // neighbour index - particle index
-    uint32_t kwin;            // |num| inside the polynomials' window: high word below kwin
-    uint32_t kbrk;            // ... and below the break band (force pass)
-    uint32_t pad;
-};
-struct StencilL64 {
-    int32_t ntab = 0, nwords = 0;
-    double bbc = 0, theta_coeff = 0, s_coeff = 0;
-    double hs[kStencilPoly];  // S(q), monomial coefficients (past the degree: 0)
-    double hw[kStencilPoly];  // W(q)
-    StencilEntryL64 e[kStencilMax];  // past ntab: zero (no contribution, never deferred)
-};
 // The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
 constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial
 struct __align__(16) StencilEntry32 {
@@ -435,12 +410,9 @@ struct MixedState {
     // records (u_x, u_y, u_z, vol) with `guard` zero records on either side,
     // so i + delta of an absent stencil entry stays inside the allocation.
     Stencil64* st64 = nullptr;
-    // FP64 LPS stencil path: its table, and per particle (a, b) = (theta_coeff
-    // theta / m, s_coeff / m) as one 16-byte gather record, with the guard
-    // records of u4 on either side.
-    StencilL64* stl64 = nullptr;
-    double2* ab64 = nullptr;       // record of particle 0
-    double2* ab64_base = nullptr;  // allocation
+    // The FP64 stencil walk runs in two launches: the first one's force sum
+    // per row (x, y, z; w unused), which the second one continues.
+    double4* f64part = nullptr;
     // Mixed PMB stencil kernel: its table, and the allocation behind u2
     // (u2 = u2_base + guard; `guard` zero records on either side).
     Stencil32* st32 = nullptr;
@@ -478,10 +450,6 @@ int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_
                    double4* u4, cudaStream_t st);
 int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
-// FP64 LPS stencil path: weighted volume (with_m) and dilatation of every
-// row from the gather records m.u4 (which must hold p.u).
-int launch_lps_mtheta_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
-                                const MixedState& m, bool with_m, cudaStream_t st);
 int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                             const MixedState& m, bool with_m, cudaStream_t st);
 double mixed_wscale(const Model& md);

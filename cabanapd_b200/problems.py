@@ -166,14 +166,16 @@ def displacement_profile(prob, u, profile_dim=0, displacement_dim=None):
     return x[on, profile_dim], u[on, displacement_dim]
 
 
-def plate_impact(num_cells=(800, 400, 36), steps=2000, v0=16.5):
+def plate_impact(num_cells=(800, 400, 36), steps=2000, v0=16.5, size=(0.2, 0.1, 0.009)):
     """PMB brittle fracture, double-notched plate impact (Kalthoff-Winkler
     layout of examples/mechanics/kalthoff_winkler.cpp): plate
     0.2 x 0.1 x 0.009 m, delta = 3.01 dx, E = 191 GPa, nu = 0.25,
     rho = 8000, G0 = 22170, two 0.05 m notches from the left edge at
     y = +-0.025, v_x = v0 on the strip between them held by a zero-force BC.
+    `size` scales the plate (notches and strip in proportion), e.g. for a
+    small plate at the full plate's spacing.
     """
-    size = [0.2, 0.1, 0.009]
+    size = [float(s) for s in size]
     low = [-0.5 * s for s in size]
     high = [0.5 * s for s in size]
     x, vol, h = lattice(low, high, num_cells)

@@ -27,10 +27,12 @@ def _nrel(a, b):
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
 
 
-def _check(g, o, precision):
+def _check(g, o, precision, tol_fields=None):
     tu, tf = TOL[precision]
-    for fld, tol in (("u", tu), ("v", tf), ("f", tf)):
-        a, b = g.get(fld), o.get(fld)
+    tols = {"u": tu, "v": tf, "f": tf}
+    tols.update(tol_fields or {})
+    for fld in ("u", "v", "f"):
+        a, b, tol = g.get(fld), o.get(fld), tols[fld]
         if tol == 0.0:
             assert np.array_equal(a, b), fld
         else:
@@ -201,7 +203,13 @@ def test_notched_two_layer_bodies(cuda, oracle, precision, model):
     bond-state words than the table has) with notches cutting bonds: the
     stencil kernels read only the list's words. LPS box 102 x 41 x 2 with
     20 random notches (a slightly non-cubic lattice), PMB plate 60 x 30 x 2
-    with its two notches; 30 steps against the oracle."""
+    with its two notches; 30 steps against the oracle.
+
+    The LPS forces of a two-layer body cancel far more than a bulk body's
+    (every row is a surface row): the oracle itself, started from positions
+    moved by one ulp, ends 30 steps later ~1e-11 away in f and ~2e-12 in v.
+    FP64 is held to that spread (measured here, and at least 1e-12) in v
+    and f, and to 1e-12 in u."""
     if model == "lps":
         prob = P.lps_random_notches(num_cells=(102, 41, 2), steps=30, seed=20261209)
     else:
@@ -215,6 +223,16 @@ def test_notched_two_layer_bodies(cuda, oracle, precision, model):
         assert _nrel(g.get("m"), o.get("m")) <= (1e-13 if precision == FAST else 1e-6)
     g.run(prob["num_steps"])
     o.run(prob["num_steps"])
-    _check(g, o, precision)
+    tol_fields = None
+    if model == "lps" and precision == FAST:
+        moved = dict(prob)
+        rng = np.random.default_rng(5)
+        x = np.asarray(prob["x"], dtype=np.float64)
+        moved["x"] = np.nextafter(x, np.where(rng.random(x.shape) < 0.5, -np.inf, np.inf))
+        o2 = oracle.OracleSystem(prob["params"])
+        P.setup(o2, moved)
+        o2.run(prob["num_steps"])
+        tol_fields = {fld: max(1e-12, _nrel(o2.get(fld), o.get(fld))) for fld in ("v", "f")}
+    _check(g, o, precision, tol_fields)
     assert (o.neighbors()[2] == 0).sum() > 0
     assert _nrel(g.get("u"), o.get("u")) <= tu

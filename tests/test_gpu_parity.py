@@ -450,6 +450,25 @@ def test_mixed_plate_impact(cuda, oracle, ordering):
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
+def test_mixed_plate_at_the_full_plates_spacing(cuda):
+    """The FP32 table constants at the 800 x 400 x 36 plate's spacing
+    (dx = 2.5e-4 m: c vol / xi^3 ~ 1e22) stay finite: a 20 x 10 x 2.5 mm
+    plate of 80 x 40 x 10 cells, mixed against FP64 over 40 steps."""
+    prob = P.plate_impact(num_cells=(80, 40, 10), steps=40, v0=60.0, size=(0.02, 0.01, 0.0025))
+    runs = {}
+    for prec in (MIXED, 1):
+        s = cuda.System(dict(prob["params"], precision=prec))
+        P.setup(s, prob)
+        s.run(40)
+        runs[prec] = s
+    g, f = runs[MIXED], runs[1]
+    assert np.all(np.isfinite(g.get("f")))
+    assert _nrel(g.get("u"), f.get("u")) <= 1e-6
+    assert _nrel(g.get("v"), f.get("v")) <= 1e-5
+    assert _nrel(g.get("f"), f.get("f")) <= 1e-5
+    assert np.array_equal(g.neighbors()[2], f.neighbors()[2])
+
+
 def test_mixed_elastic_wave(cuda, oracle):
     prob = P.elastic_wave_pmb(n=41, steps=100)
     g, o = _pair_mixed(cuda, oracle, prob)
