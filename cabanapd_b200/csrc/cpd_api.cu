@@ -702,6 +702,14 @@ bool fused_ready(const cpd_system* s)
            (!use_mixed(s) || s->u2_alt) && (!contact_fusable(s) || s->v_alt);
 }
 
+// Whether the last step of cpd_step_energy forms the energy itself: the
+// mixed PMB stencil kernel with one particle volume.
+bool fused_energy_ok(const cpd_system* s)
+{
+    return use_mixed(s) && s->md.pd == CPD_PD_PMB && s->mixed.st32 && s->mixed.vol_sums &&
+           s->mixed.nstencil > 0 && s->mixed.u2;
+}
+
 // num_steps steps as: first half step, then one bond kernel per step whose
 // epilogue applies the boundary conditions, the second half step and (but
 // for the last step) the next first half step, alternating displacement
@@ -768,7 +776,10 @@ cpd_status step_fused_contact(cpd_system* s, int32_t num_steps)
     return CPD_OK;
 }
 
-cpd_status step_fused(cpd_system* s, int32_t num_steps)
+// energy_part (mixed stencil path, one particle volume): the last step's
+// bond kernel also forms W and phi of the stencil rows and their per-warp
+// partial sums there.
+cpd_status step_fused(cpd_system* s, int32_t num_steps, double* energy_part = nullptr)
 {
     if (contact_fusable(s)) return step_fused_contact(s, num_steps);
     const bool mixed = use_mixed(s);
@@ -822,6 +833,7 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps)
         ep.u_next = unxt;
         ep.u2_next = u2nxt;
         ep.u4_next = u4nxt;
+        ep.energy_part = k + 1 < num_steps ? nullptr : energy_part;
         if (is_lps(s)) CPD_OK_OR_RETURN(lps_prepare_on(s, pk, mk, s->md.fracture != 0));
         CPD_OK_OR_RETURN(pd_force_on(s, pk, mk, ep));
         std::swap(ucur, unxt);
@@ -924,6 +936,17 @@ int64_t system_rows(const cpd_system* s) { return s->n - s->frozen; }
 extern "C" {
 
 int32_t cpd_abi_version(void) { return CPD_ABI_VERSION; }
+
+cpd_status cpd_stencil_stats(const cpd_system* s, int64_t* stencil_warps,
+                             int64_t* irregular_warps, int32_t* table_entries)
+{
+    if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
+    const bool sten = (use_mixed(s) && s->mixed.st32) || (use_stencil64(s) && s->mixed.st64);
+    if (stencil_warps) *stencil_warps = sten ? s->mixed.nstencil : 0;
+    if (irregular_warps) *irregular_warps = sten ? s->mixed.nirregular : 0;
+    if (table_entries) *table_entries = sten ? s->mixed.ntab : 0;
+    return CPD_OK;
+}
 const char* cpd_last_error(void) { return g_last_error.c_str(); }
 
 cpd_status cpd_system_create(const cpd_params* params, cpd_system** out)
@@ -1418,25 +1441,31 @@ static int launch_energy(cpd_system* s, const ParticleView& p, double* partials,
     return nb;
 }
 
+// Totals from rows of (W_i vol_i, phi_i) partial sums in s->red.
+static cpd_status sum_energy_partials(cpd_system* s, int rows, double* total_W, double* total_D)
+{
+    CPD_CUDA(cudaGetLastError());
+    CPD_LAUNCHED(launch_sum_partials(s->red, rows, 2, s->red_out + 2, s->stream));
+    CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
+                             cudaMemcpyDeviceToHost, s->stream));
+    CPD_CUDA(cudaStreamSynchronize(s->stream));
+    if (total_W) *total_W = s->h_red[2];
+    if (total_D) *total_D = s->h_red[3];
+    return CPD_OK;
+}
+
 cpd_status cpd_compute_energy(cpd_system* s, double* total_W, double* total_D)
 {
     CPD_OK_OR_RETURN(check_ready(s, true));
     CPD_CUDA(cudaSetDevice(s->device));
-    double Wt = 0.0, Dt = 0.0;
     if (has_pd(s)) {
         const int nb = energy_blocks(s->n - s->frozen);
         CPD_OK_OR_RETURN(ensure_reduction(s, nb + 1));
         const int rows = launch_energy(s, view(s), s->red, nb, nb + 1);
-        CPD_CUDA(cudaGetLastError());
-        CPD_LAUNCHED(launch_sum_partials(s->red, rows, 2, s->red_out + 2, s->stream));
-        CPD_CUDA(cudaMemcpyAsync(s->h_red + 2, s->red_out + 2, sizeof(double) * 2,
-                                 cudaMemcpyDeviceToHost, s->stream));
-        CPD_CUDA(cudaStreamSynchronize(s->stream));
-        Wt = s->h_red[2];
-        Dt = s->h_red[3];
+        return sum_energy_partials(s, rows, total_W, total_D);
     }
-    if (total_W) *total_W = Wt;
-    if (total_D) *total_D = Dt;
+    if (total_W) *total_W = 0.0;
+    if (total_D) *total_D = 0.0;
     return CPD_OK;
 }
 
@@ -1525,6 +1554,28 @@ cpd_status cpd_step_energy(cpd_system* s, int32_t num_steps, double* total_W, do
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         CPD_CUDA(cudaStreamIsCapturing(s->stream, &cs));
         if (cs == cudaStreamCaptureStatusNone) CPD_OK_OR_RETURN(prepare_fused(s));
+    }
+    if (num_steps > 0 && fused_ready(s) && fused_energy_ok(s)) {
+        // The last step's mixed stencil kernel forms W and phi of its rows
+        // (after that step's bond breaking, on the displacement the step
+        // ends with) and one partial row per stencil warp; the irregular
+        // rows take the energy kernel afterwards, on the same final state.
+        const int64_t wrows = s->mixed.nstencil;
+        const int64_t gi = (s->mixed.nirregular + 7) / 8;
+        CPD_OK_OR_RETURN(ensure_reduction(s, (int)(wrows + gi + 1)));
+        CPD_OK_OR_RETURN(step_fused(s, num_steps, s->red));
+        int rows = (int)wrows;
+        if (s->mixed.nirregular > 0) {
+            int l = 0;
+            const int r = launch_energy_mixed_rows(view(s), pd_view(s), s->md, s->mixed,
+                                                   s->mixed.irregular_list,
+                                                   s->mixed.nirregular, s->red + 2 * wrows, &l,
+                                                   s->stream);
+            s->launches += l;
+            if (r < 0) return set_error(CPD_ERR_STATE, "energy of the irregular rows");
+            rows += r;
+        }
+        return sum_energy_partials(s, rows, total_W, total_D);
     }
     CPD_OK_OR_RETURN(cpd_step(s, num_steps));
     return cpd_compute_energy(s, total_W, total_D);

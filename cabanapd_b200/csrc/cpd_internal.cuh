@@ -343,6 +343,9 @@ struct Stencil32 {
     double bbc = 0, c = 0;
     float h[kStencilPoly32];  // H(q) ~ 1 / (sqrt(1+q) (1 + sqrt(1+q))), FP32
     StencilEntry32 e[kStencilMax];  // past ntab: zero (no force, never deferred)
+    // Energy factor of each entry, c vol xi / 4 (one particle volume; the
+    // bond's strain energy is kw s^2, force/CabanaPD_PMB.hpp:127-155).
+    float kw[kStencilMax];
 };
 
 // Where the stencil kernels find their rows: the warp list (kinds 1-3, tile
@@ -376,6 +379,10 @@ struct StepEpilogue {
     double* v_next = nullptr;
     // FP64 stencil path: the next displacement's gather records as well.
     double4* u4_next = nullptr;
+    // Mixed stencil kernel on an output step: also the rows' strain energy
+    // density and damage (W, phi), and per stencil warp the partial sums
+    // (sum W_i vol_i, sum phi_i) at energy_part[2 slot], [2 slot + 1].
+    double* energy_part = nullptr;
 };
 
 struct MixedState {
@@ -450,6 +457,13 @@ int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_
                    double4* u4, cudaStream_t st);
 int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
+// Energy and damage of the listed warps' rows on the mixed path (the rows
+// the mixed stencil kernel does not hold, after its output step): block
+// partials at partials; returns the partial rows written, -1 when the
+// mixed energy kernels do not serve the model.
+int launch_energy_mixed_rows(const ParticleView& p, const EllView& nl, const Model& md,
+                             const MixedState& m, const int32_t* wlist, int64_t wcount,
+                             double* partials, int* launches, cudaStream_t st);
 int launch_lps_mtheta_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                             const MixedState& m, bool with_m, cudaStream_t st);
 double mixed_wscale(const Model& md);

@@ -1967,6 +1967,31 @@ int launch_hertz_force_mixed(const ParticleView& p, const EllView& nl, const Mod
     return 1;
 }
 
+namespace {
+
+// Energy kernel of the model over the listed warps (all rows: wlist null),
+// grid blocks of 8 warps, partials per block.
+void energy_mixed_launch(const ParticleView& p, const EllView& nl, const Model& md,
+                         const MixedState& m, int grid, double* part, const int32_t* list,
+                         int64_t count, bool lean, cudaStream_t st);
+
+}  // namespace
+
+int launch_energy_mixed_rows(const ParticleView& p, const EllView& nl, const Model& md,
+                             const MixedState& m, const int32_t* wlist, int64_t wcount,
+                             double* partials, int* launches, cudaStream_t st)
+{
+    *launches = 0;
+    const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    if (m.ntab == 0 || sb > 48 * 1024 || !m.warp_kind) return -1;
+    if (!(md.pd == CPD_PD_PMB || (md.pd == CPD_PD_LPS && m.lps_ok))) return -1;
+    if (wcount <= 0) return 0;
+    const int grid = (int)((wcount + kBlock / 32 - 1) / (kBlock / 32));
+    energy_mixed_launch(p, nl, md, m, grid, partials, wlist, wcount, false, st);
+    *launches = 1;
+    return grid;
+}
+
 int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& md,
                         const MixedState& m, double* partials, int nblocks, int capacity,
                         int* launches, cudaStream_t st)
@@ -1975,41 +2000,13 @@ int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& m
     const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
     if (m.ntab == 0 || sb > 48 * 1024 || !m.warp_kind) return -1;
     if (!(md.pd == CPD_PD_PMB || (md.pd == CPD_PD_LPS && m.lps_ok))) return -1;
-    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
-    const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
-    const int key = (md.pd == CPD_PD_LPS ? 4 : 0) + (md.influence == 1 ? 2 : 0) +
-                    (md.fracture ? 1 : 0);
     // Large systems: the lean warps in their tile order, then the others,
     // when the partials buffer holds both launches' blocks.
     const int64_t wpb = kBlock / 32;
     const int gl = (int)((m.nlean + wpb - 1) / wpb), gr = (int)((m.nrest + wpb - 1) / wpb);
     const bool split = m.lean_list && p.n - p.frozen >= split_min_rows() && gl + gr <= capacity;
-    const double* vs = md.fracture ? m.vol_sums : nullptr;
     auto launch = [&](int grid, double* part, const int32_t* list, int64_t count, bool lean) {
-#define CPD_EN(L, I, F, U)                                                                   \
-    if (lean)                                                                                \
-        k_energy_mixed<L, I, F, U, true><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, \
-                                                                   count, vs);               \
-    else                                                                                     \
-        k_energy_mixed<L, I, F, U, false><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, \
-                                                                    count, vs)
-        if (vs) {
-            switch (key) {
-            case 1: case 3: CPD_EN(false, 0, true, true); break;
-            case 5: CPD_EN(true, 0, true, true); break;
-            default: CPD_EN(true, 1, true, true); break;
-            }
-            return;
-        }
-        switch (key) {
-        case 0: case 2: CPD_EN(false, 0, false, false); break;
-        case 1: case 3: CPD_EN(false, 0, true, false); break;
-        case 4: CPD_EN(true, 0, false, false); break;
-        case 5: CPD_EN(true, 0, true, false); break;
-        case 6: CPD_EN(true, 1, false, false); break;
-        default: CPD_EN(true, 1, true, false); break;
-        }
-#undef CPD_EN
+        energy_mixed_launch(p, nl, md, m, grid, part, list, count, lean, st);
     };
     if (!split) {
         launch(nblocks, partials, nullptr, 0, false);
@@ -2021,5 +2018,45 @@ int launch_energy_mixed(const ParticleView& p, const EllView& nl, const Model& m
     *launches = gr > 0 ? 2 : 1;
     return gl + gr;
 }
+
+namespace {
+
+void energy_mixed_launch(const ParticleView& p, const EllView& nl, const Model& md,
+                         const MixedState& m, int grid, double* part, const int32_t* list,
+                         int64_t count, bool lean, cudaStream_t st)
+{
+    const size_t sb = (1 + kBlock / 32) * sizeof(MixedStencil) * m.ntab;
+    const MixedView mv{m.xh, m.xl, m.u2, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask};
+    const MixedEnergy e{md.c, md.theta_coeff, md.s_coeff, m.ntab};
+    const int key = (md.pd == CPD_PD_LPS ? 4 : 0) + (md.influence == 1 ? 2 : 0) +
+                    (md.fracture ? 1 : 0);
+    const double* vs = md.fracture ? m.vol_sums : nullptr;
+#define CPD_EN(L, I, F, U)                                                                   \
+    if (lean)                                                                                \
+        k_energy_mixed<L, I, F, U, true><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, \
+                                                                   count, vs);               \
+    else                                                                                     \
+        k_energy_mixed<L, I, F, U, false><<<grid, kBlock, sb, st>>>(p, nl, mv, e, part, list, \
+                                                                    count, vs)
+    if (vs) {
+        switch (key) {
+        case 1: case 3: CPD_EN(false, 0, true, true); break;
+        case 5: CPD_EN(true, 0, true, true); break;
+        default: CPD_EN(true, 1, true, true); break;
+        }
+        return;
+    }
+    switch (key) {
+    case 0: case 2: CPD_EN(false, 0, false, false); break;
+    case 1: case 3: CPD_EN(false, 0, true, false); break;
+    case 4: CPD_EN(true, 0, false, false); break;
+    case 5: CPD_EN(true, 0, true, false); break;
+    case 6: CPD_EN(true, 1, false, false); break;
+    default: CPD_EN(true, 1, true, false); break;
+    }
+#undef CPD_EN
+}
+
+}  // namespace
 
 }  // namespace cpd

@@ -121,9 +121,12 @@ __global__ void __launch_bounds__(kBlock)
 // (CabanaPD_Force.hpp:74-93 getDistance, CabanaPD_ForceModels.hpp:123-128,
 // force/CabanaPD_PMB.hpp:259-279). Returns true when the bond breaks;
 // otherwise adds its force to f.
+// With w: the bond's strain energy c s^2 xi vol_j / 4 is added to *w when it
+// stays intact (force/CabanaPD_PMB.hpp:127-155).
 template <bool FRACTURE>
 __device__ __forceinline__ bool exact_bond(const ParticleView& p, int64_t i, int64_t j, double c,
-                                           double bbc, bool nofail_i, double (&f)[3])
+                                           double bbc, bool nofail_i, double (&f)[3],
+                                           double* w)
 {
     const int64_t np = p.npad;
     const double xx = __dsub_rn(p.x[j], p.x[i]);
@@ -141,6 +144,7 @@ __device__ __forceinline__ bool exact_bond(const ParticleView& p, int64_t i, int
         return true;
     const double s = __ddiv_rn(__dsub_rn(r, xi), xi);
     const double coeff = __dmul_rn(__dmul_rn(c, s), p.vol[j]);
+    if (w) *w += 0.25 * c * s * s * xi * p.vol[j];
     f[0] += __ddiv_rn(__dmul_rn(coeff, rx), r);
     f[1] += __ddiv_rn(__dmul_rn(coeff, ry), r);
     f[2] += __ddiv_rn(__dmul_rn(coeff, rz), r);
@@ -315,7 +319,8 @@ __global__ void __launch_bounds__(kBlock, 4)
                 const int b = __ffs(q) - 1;
                 q &= q - 1;
                 const int k = 32 * w + b;
-                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
+                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f,
+                                         nullptr))
                     clear_bond_bit(nl, sr, kind, i, np, w, b);
             }
         }
@@ -341,12 +346,15 @@ __global__ void __launch_bounds__(kBlock, 4)
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 // x and y in paired FP32 operations (FADD2 / FMUL2 / FFMA2), z alone.
-template <bool UNIFORM>
+// ENERGY: the bond's strain energy kw s^2 into cw as well, with the stretch
+// s = a / (1 - a) from a = q H(q) = 1 - xi / r.
+template <bool UNIFORM, bool ENERGY = false>
 __device__ __forceinline__ void stencil_bond32(const StencilEntry32& e, const float* h,
                                                const MixedU& uj, const float2& nh_xy,
                                                float nh_z, const float2& nl_xy, float nl_z,
                                                bool on, uint32_t bit, uint32_t& pend,
-                                               float2& cxy, float& cz)
+                                               float2& cxy, float& cz, float kw = 0.f,
+                                               float* cw = nullptr)
 {
     const float2 hxy = __fadd2_rn(__fadd2_rn(f2(uj.hi.x, uj.hi.y), nh_xy),
                                   __fadd2_rn(f2(uj.lo.x, uj.lo.y), nl_xy));
@@ -362,19 +370,34 @@ __device__ __forceinline__ void stencil_bond32(const StencilEntry32& e, const fl
     F = (on && in) ? F : 0.f;
     cxy = __ffma2_rn(f2(F, F), __fadd2_rn(e.exy, hxy), cxy);
     cz = fmaf(F, e.ez + hz, cz);
+    if (ENERGY) {
+        const float a = q * t;
+        const float sv = __fdividef(a, 1.f - a);
+        *cw += (on && in) ? kw * sv * sv : 0.f;
+    }
 }
 
-template <bool FRACTURE, bool UNIFORM, int NT>
+// ENERGY (output steps; one particle volume): the rows' strain energy
+// density W_i (the bond terms kw s^2 in the force's FP32 chunks of 8 into
+// FP64, the deferred bonds' in FP64) and damage phi_i = 1 - vol_sums[intact]
+// / vol_sums[bonds] (the ordered FP64 sums of the damage formula,
+// force/CabanaPD_PMB.hpp:289-339), after this step's bond breaking; the
+// warp's sums of W_i vol_i and phi_i go to ep.energy_part.
+template <bool FRACTURE, bool UNIFORM, int NT, bool ENERGY = false>
 __global__ void __launch_bounds__(kBlock, 3)
     k_pmb_stencil32(ParticleView p, EllView nl, StencilRows sr, const MixedU* __restrict__ U2,
-                    StepEpilogue ep, const Stencil32 st)
+                    StepEpilogue ep, const Stencil32 st, const double* __restrict__ vol_sums)
 {
     const int lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     if (slot >= sr.wcount) return;
     const int64_t warp = sr.wlist[slot];
     const int64_t i = p.frozen + 32 * warp + lane;
-    if (i >= p.n) return;
+    // Without ENERGY a lane past the last row leaves; with it every lane of
+    // the warp reaches the warp's sums.
+    if (!ENERGY && i >= p.n) return;
+    double Phi_i = 0.0, dmg_i = 0.0;
+    if (i < p.n) {
     const int64_t np = p.npad;
     const int kind = sr.warp_kind[warp];
     uint32_t ew[4];
@@ -386,6 +409,8 @@ __global__ void __launch_bounds__(kBlock, 3)
     double f[3] = {0.0, 0.0, 0.0};
     float2 cxy = f2(0.f, 0.f);
     float cz = 0.f;
+    double wsum = 0.0;
+    float cw = 0.f;
     uint32_t pend[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
@@ -393,16 +418,22 @@ __global__ void __launch_bounds__(kBlock, 3)
         const uint32_t bit = 1u << (k & 31);
         const StencilEntry32& e = st.e[k];
         const MixedU uj = *reinterpret_cast<const MixedU*>(rb + e.boff);
-        stencil_bond32<UNIFORM>(e, st.h, uj, nh_xy, nh_z, nl_xy, nl_z, (ew[w] & bit) != 0u, bit,
-                                pend[w], cxy, cz);
+        stencil_bond32<UNIFORM, ENERGY>(e, st.h, uj, nh_xy, nh_z, nl_xy, nl_z,
+                                        (ew[w] & bit) != 0u, bit, pend[w], cxy, cz,
+                                        ENERGY ? st.kw[k] : 0.f, &cw);
         if ((k & 7) == 7 || k == NT - 1) {
             f[0] += (double)cxy.x;
             f[1] += (double)cxy.y;
             f[2] += (double)cz;
             cxy = f2(0.f, 0.f);
             cz = 0.f;
+            if (ENERGY) {
+                wsum += (double)cw;
+                cw = 0.f;
+            }
         }
     }
+    int broken = 0;
     if (pend[0] | pend[1] | pend[2] | pend[3]) {
         const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
 #pragma unroll
@@ -412,12 +443,37 @@ __global__ void __launch_bounds__(kBlock, 3)
                 const int b = __ffs(q) - 1;
                 q &= q - 1;
                 const int k = 32 * w + b;
-                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f))
+                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f,
+                                         ENERGY ? &wsum : nullptr)) {
                     clear_bond_bit(nl, sr, kind, i, np, w, b);
+                    ++broken;
+                }
             }
         }
     }
     step_epilogue<true>(p, ep, i, f[0], f[1], f[2]);
+    if (ENERGY) {
+        p.W[i] = wsum;
+        Phi_i = wsum * p.vol[i];
+        if (FRACTURE) {
+            const int intact =
+                __popc(ew[0]) + __popc(ew[1]) + __popc(ew[2]) + __popc(ew[3]) - broken;
+            dmg_i = 1 - vol_sums[intact] / vol_sums[nl.count[i]];
+            p.phi[i] = dmg_i;
+        }
+    }
+    }
+    if (ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            Phi_i += __shfl_xor_sync(0xffffffffu, Phi_i, o);
+            dmg_i += __shfl_xor_sync(0xffffffffu, dmg_i, o);
+        }
+        if (lane == 0) {
+            ep.energy_part[2 * slot] = Phi_i;
+            ep.energy_part[2 * slot + 1] = dmg_i;
+        }
+    }
 }
 
 }  // namespace
@@ -550,6 +606,7 @@ bool prepare_stencil32(const Model& md, const double* h, const MixedStencil* tab
         const long double x2 = fx * fx + fy * fy + fz * fz;
         e.ixi2 = (float)(1.0L / x2);
         e.K = (float)(scale / (sqrtl(x2) * x2));
+        S->kw[k] = (float)(0.25L * scale * sqrtl(x2));
         e.doff = tab[k].delta == INT32_MAX ? 0 : tab[k].delta;  // (as in the FP64 table)
         e.boff = (int64_t)e.doff * (int64_t)sizeof(MixedU);
         const float T = (float)(qwin * (double)x2);
@@ -572,8 +629,21 @@ int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Mo
     const bool uniform = m.vol_sums != nullptr;
     const Stencil32& S = *m.st32;
     const bool t122 = S.ntab == 122;
+    if (ep.energy_part) {
+        // Output step: the energy forms (one particle volume only).
+        if (!uniform) return -1;
+#define CPD_ST32E(F, NT) \
+    k_pmb_stencil32<F, true, NT, true><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2, ep, S, m.vol_sums)
+        if (md.fracture) {
+            if (t122) CPD_ST32E(true, 122); else CPD_ST32E(true, 128);
+        } else {
+            if (t122) CPD_ST32E(false, 122); else CPD_ST32E(false, 128);
+        }
+#undef CPD_ST32E
+        return 1;
+    }
 #define CPD_ST32(F, U, NT) \
-    k_pmb_stencil32<F, U, NT><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2, ep, S)
+    k_pmb_stencil32<F, U, NT><<<g, kBlock, 0, st>>>(p, nl, sr, m.u2, ep, S, nullptr)
     if (!uniform) {
         if (md.fracture) CPD_ST32(true, false, 128); else CPD_ST32(false, false, 128);
     } else if (md.fracture) {

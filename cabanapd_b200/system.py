@@ -158,6 +158,9 @@ SIGNATURES = {
     "cpd_set_kernel_timing": (_I32, [_P, _I32]),
     "cpd_kernel_time": (_I32, [_P, _DP, ctypes.POINTER(_I64), _DP]),
     "cpd_kernel_launches": (_I64, [_P]),
+    "cpd_stencil_stats": (_I32, [_P, ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(ctypes.c_int32)]),
     "cpd_device_bytes": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
     "cpd_batch_create": (_I32, [ctypes.POINTER(_P), _I32, ctypes.POINTER(_I32),
                                 ctypes.POINTER(_P)]),
@@ -394,6 +397,15 @@ class System:
 
     def kernel_launches(self):
         return self._lib.cpd_kernel_launches(self._h)
+
+    def stencil_stats(self):
+        """(warps on the lattice-stencil bond kernels, warps on the general
+        kernels beside them, offset-table entries); zeros when the general
+        kernels take every row."""
+        w, r, t = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        self._check(self._lib.cpd_stencil_stats(self._h, ctypes.byref(w), ctypes.byref(r),
+                                                ctypes.byref(t)))
+        return w.value, r.value, t.value
 
     def save_state(self):
         """Snapshot of the evolving state (cpd_save_state) as a uint8 array."""

@@ -65,7 +65,7 @@
 extern "C" {
 #endif
 
-#define CPD_ABI_VERSION 3
+#define CPD_ABI_VERSION 4
 
 typedef struct cpd_system cpd_system;
 typedef int32_t cpd_status;
@@ -348,6 +348,14 @@ cpd_status cpd_kernel_time(cpd_system* sys, double* total_ms,
                            int64_t* launches, double* bytes_per_launch);
 /* Number of kernels this library launched on the system since creation. */
 int64_t cpd_kernel_launches(const cpd_system* sys);
+/* No counterpart in the reference. Which bond kernels hold the rows (after
+ * cpd_build_neighbors): the warps of 32 rows the lattice-stencil kernels
+ * walk (CPD_FP64 and CPD_MIXED PMB on a lattice whose offset table fits the
+ * unrolled kernels), the warps the general kernels take beside them, and
+ * the entries of the offset table; all 0 when the general kernels run
+ * every row. */
+cpd_status cpd_stencil_stats(const cpd_system* sys, int64_t* stencil_warps,
+                             int64_t* irregular_warps, int32_t* table_entries);
 /* No counterpart in the reference. Device bytes the system holds (particle
  * fields, neighbour and contact lists, mixed-precision copies, boundary
  * lists), for admission against a memory budget. */

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_params_layout():
     from cabanapd_b200 import system
     lib = system.load()
-    assert lib.cpd_abi_version() == 3
+    assert lib.cpd_abi_version() == 4
     # cpd_params: 4 int32, 10 double, 5 int32 (+4 padding), 2 double
     # -> 16 + 80 + 20 + 4 + 16
     assert ctypes.sizeof(system.CpdParams) == 136

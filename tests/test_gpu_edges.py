@@ -203,7 +203,8 @@ def test_notched_two_layer_bodies(cuda, oracle, precision, model):
     bond-state words than the table has) with notches cutting bonds: the
     stencil kernels read only the list's words. LPS box 102 x 41 x 2 with
     20 random notches (a slightly non-cubic lattice), PMB plate 60 x 30 x 2
-    with its two notches; 30 steps against the oracle.
+    on a cubic lattice (the plate 6.7 mm thick) with its two notches; 30
+    steps against the oracle.
 
     The LPS forces of a two-layer body cancel far more than a bulk body's
     (every row is a surface row): the oracle itself, started from positions
@@ -213,12 +214,16 @@ def test_notched_two_layer_bodies(cuda, oracle, precision, model):
     if model == "lps":
         prob = P.lps_random_notches(num_cells=(102, 41, 2), steps=30, seed=20261209)
     else:
-        prob = P.plate_impact(num_cells=(60, 30, 2), steps=30, v0=60.0)
+        prob = P.plate_impact(num_cells=(60, 30, 2), steps=30, v0=60.0,
+                              size=(0.2, 0.1, 0.2 * 2 / 60))
     g = cuda.System(dict(prob["params"], precision=precision))
     o = oracle.OracleSystem(prob["params"])
     P.setup(g, prob)
     P.setup(o, prob)
     tu = TOL[precision][0]
+    if model == "pmb":
+        # A cubic lattice: the stencil kernels hold the rows.
+        assert g.stencil_stats()[0] > 0
     if model == "lps":
         assert _nrel(g.get("m"), o.get("m")) <= (1e-13 if precision == FAST else 1e-6)
     g.run(prob["num_steps"])
