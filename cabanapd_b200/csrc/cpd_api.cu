@@ -703,11 +703,14 @@ bool fused_ready(const cpd_system* s)
 }
 
 // Whether the last step of cpd_step_energy forms the energy itself: the
-// mixed PMB stencil kernel with one particle volume.
+// PMB stencil kernels with one particle volume (mixed: beside any warps on
+// the general kernels; FP64: when the stencil kernel holds every row).
 bool fused_energy_ok(const cpd_system* s)
 {
-    return use_mixed(s) && s->md.pd == CPD_PD_PMB && s->mixed.st32 && s->mixed.vol_sums &&
-           s->mixed.nstencil > 0 && s->mixed.u2;
+    const MixedState& m = s->mixed;
+    if (s->md.pd != CPD_PD_PMB || !m.vol_sums || m.nstencil <= 0) return false;
+    if (use_mixed(s)) return m.st32 && m.u2;
+    return use_stencil64(s) && m.st64 && m.nirregular == 0;
 }
 
 // num_steps steps as: first half step, then one bond kernel per step whose

@@ -323,7 +323,12 @@ struct Stencil64 {
     // H(q) = sum_k h[k] q^k ~ 1 / (sqrt(1+q) (1 + sqrt(1+q))) on |q| <= kStencilQ,
     // so that 1 - xi / r = q H(q) with q = (r^2 - xi^2) / xi^2.
     double h[kStencilPoly];
+    // S(q) = sum_k sh[k] q^k ~ 1 / (1 + sqrt(1+q)), the stretch s = q S(q)
+    // (output steps' energy).
+    double sh[kStencilPoly];
     StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
+    // Energy factor of each entry, c vol xi / 4 (one particle volume).
+    double kw[kStencilMax];
 };
 // The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
 constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial

@@ -70,7 +70,10 @@ inline uint32_t hi_word(double v)
 // error vanishes as q -> 0 instead of leaving a uniform bias of the size of
 // the interpolation error (which the FP32 kernel's 4 coefficients would
 // turn into a systematic stiffness error of ~5e-8).
-void fit_stretch_poly(long double Q, int n, long double* out, bool anchored = false)
+// stretch: S(q) = 1 / (1 + sqrt(1+q)) instead (unanchored), so that the
+// stretch is s = r / xi - 1 = q S(q).
+void fit_stretch_poly(long double Q, int n, long double* out, bool anchored = false,
+                      bool stretch = false)
 {
     const int m = anchored ? n - 1 : n;
     long double A[kStencilPoly][kStencilPoly + 1];
@@ -82,8 +85,9 @@ void fit_stretch_poly(long double Q, int n, long double* out, bool anchored = fa
             A[r][c] = pw;
             pw *= t;
         }
-        A[r][m] = anchored ? -(s + 2.0L) / (2.0L * s * (1.0L + s) * (1.0L + s))
-                           : 1.0L / (s * (1.0L + s));
+        A[r][m] = stretch    ? 1.0L / (1.0L + s)
+                  : anchored ? -(s + 2.0L) / (2.0L * s * (1.0L + s) * (1.0L + s))
+                             : 1.0L / (s * (1.0L + s));
     }
     for (int c = 0; c < m; ++c) {
         int piv = c;
@@ -154,11 +158,13 @@ __device__ __forceinline__ bool exact_bond(const ParticleView& p, int64_t i, int
 // One bond of the unrolled table walk: entry e of row i, gather record uj.
 // Adds F r_vec to f when the bond is present and intact (bit on) and num is
 // inside the entry's window; a present bond outside it is deferred (pend).
-template <bool UNIFORM, int NP>
+// ENERGY: the bond's strain energy kw s^2 into w as well, s = q S(q).
+template <bool UNIFORM, int NP, bool ENERGY = false>
 __device__ __forceinline__ void stencil_bond64(const StencilEntry64& e, const double* h,
                                                const double4& uj, const double4& ui, bool on,
                                                uint32_t bit, uint32_t& pend, double& fx,
-                                               double& fy, double& fz)
+                                               double& fy, double& fz, const double* sh = nullptr,
+                                               double kw = 0.0, double* w = nullptr)
 {
     const double hx = uj.x - ui.x, hy = uj.y - ui.y, hz = uj.z - ui.z;
     const double num = fma(hz, hz + e.tz, fma(hy, hy + e.ty, hx * (hx + e.tx)));
@@ -174,6 +180,13 @@ __device__ __forceinline__ void stencil_bond64(const StencilEntry64& e, const do
     fx = fma(F, e.ex + hx, fx);
     fy = fma(F, e.ey + hy, fy);
     fz = fma(F, e.ez + hz, fz);
+    if (ENERGY) {
+        double sv = sh[NP - 1];
+#pragma unroll
+        for (int k = NP - 2; k >= 0; --k) sv = fma(sv, q, sh[k]);
+        sv *= q;
+        *w += (on && in) ? kw * sv * sv : 0.0;
+    }
 }
 
 // Row i's present and intact table entries as entry-order bits (bit k of
@@ -264,30 +277,40 @@ __device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilR
 // not start at entry 0 continues from the partial force record FPART of the
 // previous part, and a part that is not the last stores its sum there;
 // the last part applies the step epilogue.
-template <bool FRACTURE, bool UNIFORM, int K0, int K1, int NP, bool LAST>
+// ENERGY (output steps; one particle volume): the parts also sum the rows'
+// strain energy density W_i (the first part's in FPART's w), and the last
+// part writes W_i and phi_i = 1 - vol_sums[intact] / vol_sums[bonds] after
+// the step's bond breaking, and per warp the sums of W_i vol_i and phi_i to
+// ep.energy_part, as k_pmb_stencil32 does.
+template <bool FRACTURE, bool UNIFORM, int K0, int K1, int NP, bool LAST, bool ENERGY = false>
 __global__ void __launch_bounds__(kBlock, 4)
     k_pmb_stencil64(ParticleView p, EllView nl, StencilRows sr,
                     const double4* __restrict__ U4, double4* __restrict__ FPART,
-                    StepEpilogue ep, const Stencil64 st)
+                    StepEpilogue ep, const Stencil64 st, const double* __restrict__ vol_sums)
 {
+    constexpr bool SUMS = ENERGY && LAST;
     const int lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     if (slot >= sr.wcount) return;
     const int64_t warp = sr.wlist[slot];
     const int64_t i = p.frozen + 32 * warp + lane;
-    if (i >= p.n) return;
+    // With the warp sums every lane of the warp reaches them.
+    if (!SUMS && i >= p.n) return;
+    double Phi_i = 0.0, dmg_i = 0.0;
+    if (i < p.n) {
     const int64_t np = p.npad;
     const int kind = sr.warp_kind[warp];
     uint32_t ew[4];
     row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
     const double4 ui = U4[i];
     const char* __restrict__ rb = reinterpret_cast<const char*>(U4 + i);
-    double fx = 0.0, fy = 0.0, fz = 0.0;
+    double fx = 0.0, fy = 0.0, fz = 0.0, wsum = 0.0;
     if (K0 > 0) {
         const double4 fp = FPART[i];
         fx = fp.x;
         fy = fp.y;
         fz = fp.z;
+        if (ENERGY) wsum = fp.w;
     }
     uint32_t pend[4] = {0u, 0u, 0u, 0u};
     // Fully unrolled, every entry of the range for every row: an absent entry
@@ -305,9 +328,10 @@ __global__ void __launch_bounds__(kBlock, 4)
         const uint32_t bit = 1u << (k & 31);
         const StencilEntry64& e = st.e[k];
         const double4 uj = *reinterpret_cast<const double4*>(rb + e.boff);
-        stencil_bond64<UNIFORM, NP>(e, st.h, uj, ui, (ew[w] & bit) != 0u, bit, pend[w], fx, fy,
-                                    fz);
+        stencil_bond64<UNIFORM, NP, ENERGY>(e, st.h, uj, ui, (ew[w] & bit) != 0u, bit, pend[w],
+                                            fx, fy, fz, st.sh, ENERGY ? st.kw[k] : 0.0, &wsum);
     }
+    int broken = 0;
     if (pend[0] | pend[1] | pend[2] | pend[3]) {
         // Deferred bonds: the reference's exact test and force.
         double f[3] = {fx, fy, fz};
@@ -320,18 +344,44 @@ __global__ void __launch_bounds__(kBlock, 4)
                 q &= q - 1;
                 const int k = 32 * w + b;
                 if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f,
-                                         nullptr))
+                                         ENERGY ? &wsum : nullptr)) {
                     clear_bond_bit(nl, sr, kind, i, np, w, b);
+                    ++broken;
+                }
             }
         }
         fx = f[0];
         fy = f[1];
         fz = f[2];
     }
-    if (LAST)
+    if (LAST) {
         step_epilogue<false>(p, ep, i, fx, fy, fz);
-    else
-        FPART[i] = make_double4(fx, fy, fz, 0.0);
+        if (ENERGY) {
+            // ew covers every entry (the first part's breaking included).
+            p.W[i] = wsum;
+            Phi_i = wsum * p.vol[i];
+            if (FRACTURE) {
+                const int intact =
+                    __popc(ew[0]) + __popc(ew[1]) + __popc(ew[2]) + __popc(ew[3]) - broken;
+                dmg_i = 1 - vol_sums[intact] / vol_sums[nl.count[i]];
+                p.phi[i] = dmg_i;
+            }
+        }
+    } else {
+        FPART[i] = make_double4(fx, fy, fz, ENERGY ? wsum : 0.0);
+    }
+    }
+    if (SUMS) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            Phi_i += __shfl_xor_sync(0xffffffffu, Phi_i, o);
+            dmg_i += __shfl_xor_sync(0xffffffffu, dmg_i, o);
+        }
+        if (lane == 0) {
+            ep.energy_part[2 * slot] = Phi_i;
+            ep.energy_part[2 * slot + 1] = dmg_i;
+        }
+    }
 }
 
 // Mixed precision (CPD_MIXED, PMB): the same table walk in FP32 on the FP32
@@ -516,9 +566,13 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
     // 9 up to kStencilQ.
     const long double qfit = qwin > 1e-6 ? (long double)qwin : 1e-6L;
     S->np = qfit <= 0.0231L ? 8 : 9;
-    long double hc[kStencilPoly] = {};
+    long double hc[kStencilPoly] = {}, sc[kStencilPoly] = {};
     fit_stretch_poly(qfit, S->np, hc);
-    for (int k = 0; k < kStencilPoly; ++k) S->h[k] = (double)hc[k];
+    fit_stretch_poly(qfit, S->np, sc, false, true);
+    for (int k = 0; k < kStencilPoly; ++k) {
+        S->h[k] = (double)hc[k];
+        S->sh[k] = (double)sc[k];
+    }
     int64_t G = 0;
     for (int k = 0; k < ntab; ++k) {
         StencilEntry64& e = S->e[k];
@@ -538,6 +592,7 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
         const long double xi = sqrtl(x2);
         e.ixi2 = (double)(1.0L / x2);
         e.K = (double)(scale / (xi * x2));
+        S->kw[k] = (double)(0.25L * scale * xi);
         // An entry that no row holds (a thin body) has no index delta: its
         // bonds are absent everywhere, and it reads the row's own record.
         e.doff = tab[k].delta == INT32_MAX ? 0 : tab[k].delta;
@@ -678,17 +733,31 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
         // second adds its own and runs the epilogue. Each is a shorter
         // unrolled walk that stays in the instruction cache (B200, 11.52 M
         // row plate: 3.14 ms per step for the two, 3.30 ms for one walk).
-#define CPD_ST64(F, U, NT, NP)                                                               \
+#define CPD_ST64X(F, U, NT, NP, E)                                                           \
     do {                                                                                     \
-        k_pmb_stencil64<F, U, 0, 64, NP, false><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4,       \
-                                                                      m.f64part, ep, S);    \
-        k_pmb_stencil64<F, U, 64, NT, NP, true><<<g, kBlock, 0, st>>>(p, nl, sr, m.u4,       \
-                                                                      m.f64part, ep, S);    \
+        k_pmb_stencil64<F, U, 0, 64, NP, false, E><<<g, kBlock, 0, st>>>(                    \
+            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums);                                  \
+        k_pmb_stencil64<F, U, 64, NT, NP, true, E><<<g, kBlock, 0, st>>>(                    \
+            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums);                                  \
     } while (0)
+#define CPD_ST64(F, U, NT, NP) CPD_ST64X(F, U, NT, NP, false)
         // Unrolled forms: the 122-entry table of a cubic lattice at a
         // 3.01-spacing horizon, else 128 entries (zero past ntab).
         const bool t122 = S.ntab == 122;
-        if (!uniform) {
+        if (ep.energy_part && uniform) {
+            // Output step: the energy forms.
+            if (md.fracture) {
+                if (S.np == 8) {
+                    if (t122) CPD_ST64X(true, true, 122, 8, true);
+                    else CPD_ST64X(true, true, 128, 8, true);
+                } else {
+                    CPD_ST64X(true, true, 128, 9, true);
+                }
+            } else {
+                if (t122) CPD_ST64X(false, true, 122, 9, true);
+                else CPD_ST64X(false, true, 128, 9, true);
+            }
+        } else if (!uniform) {
             if (md.fracture) CPD_ST64(true, false, 128, 9); else CPD_ST64(false, false, 128, 9);
         } else if (md.fracture) {
             if (S.np == 8) {
@@ -700,6 +769,7 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
             if (t122) CPD_ST64(false, true, 122, 9); else CPD_ST64(false, true, 128, 9);
         }
 #undef CPD_ST64
+#undef CPD_ST64X
         launched += 2;
     }
     if (m.nirregular > 0)

@@ -669,17 +669,18 @@ def _with_offlattice_pair(prob):
     return out
 
 
-def test_step_energy_equals_step_then_energy(cuda, oracle):
+@pytest.mark.parametrize("precision", [1, MIXED])
+def test_step_energy_equals_step_then_energy(cuda, oracle, precision):
     """cpd_step_energy (the Solver's output step in one call) against
     cpd_step + cpd_compute_energy on the same system, and the oracle's
     totals. On this lattice (one particle volume) the last step's stencil
     kernel forms the energy itself: states, bonds and phi bit for bit (phi
-    from the same ordered volume sums), W to the FP32 rounding of its bond
-    terms (a different FP32 form of the stretch), the totals summed in
-    another order."""
+    from the same ordered volume sums), W to the rounding of its bond terms
+    (FP32 on the mixed path, FP64 on the FP64 path; another form of the
+    stretch), the totals summed in another order."""
     prob = _cubic_plate(96, 8, steps=120)
-    a = cuda.System(dict(prob["params"], precision=MIXED))
-    b = cuda.System(dict(prob["params"], precision=MIXED))
+    a = cuda.System(dict(prob["params"], precision=precision))
+    b = cuda.System(dict(prob["params"], precision=precision))
     o = oracle.OracleSystem(prob["params"])
     for s in (a, b, o):
         P.setup(s, prob)
@@ -704,11 +705,12 @@ def test_step_energy_equals_step_then_energy(cuda, oracle):
         for fld in ("u", "v", "f", "phi"):
             assert np.array_equal(a.get(fld), b.get(fld)), fld
         assert np.array_equal(a.neighbors()[2], b.neighbors()[2])
-        # W from the stencil kernel's own FP32 terms, not the energy pass's.
+        # W from the stencil kernel's own terms, not the energy pass's.
         assert not np.array_equal(a.get("W"), b.get("W"))
-        assert _nrel(a.get("W"), b.get("W")) <= 1e-6
-        assert _rel(wa, wb) <= 1e-6 and _rel(da, db) <= 1e-13
-        assert _rel(da, do) <= 1e-12 and _rel(wa, wo) <= 1e-6
+        tw = 1e-6 if precision == MIXED else 1e-13
+        assert _nrel(a.get("W"), b.get("W")) <= tw
+        assert _rel(wa, wb) <= tw and _rel(da, db) <= 1e-13
+        assert _rel(da, do) <= 1e-12 and _rel(wa, wo) <= (1e-6 if precision == MIXED else 1e-12)
     assert da > 0
 
 
@@ -791,4 +793,4 @@ def test_split_forms_on_small_systems():
                         os.path.join(here, "test_gpu_parity.py"), "-k", sel],
                        env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
-    assert "9 passed" in r.stdout, r.stdout[-500:]
+    assert "10 passed" in r.stdout, r.stdout[-500:]
