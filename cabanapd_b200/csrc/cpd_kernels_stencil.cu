@@ -415,7 +415,9 @@ __device__ __forceinline__ void stencil_bond32(const StencilEntry32& e, const fl
     const float t = fmaf(fmaf(fmaf(h[3], q, h[2]), q, h[1]), q, h[0]);
     float F = (num * e.K) * t;
     if (!UNIFORM) F *= uj.hi.w;
-    const bool in = (__float_as_uint(num) & 0x7fffffffu) < e.khi;
+    // |num| below the window's bound T (khi holds T's bits): one compare
+    // with the absolute-value operand; false for NaN, as the integer form.
+    const bool in = fabsf(num) < __uint_as_float(e.khi);
     if (on && !in) pend |= bit;
     F = (on && in) ? F : 0.f;
     cxy = __ffma2_rn(f2(F, F), __fadd2_rn(e.exy, hxy), cxy);
