@@ -172,6 +172,25 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// Sample rows for the index deltas: row r_s = lo + (2 s + 1) span / (2 S) of
+// each block s writes its bonds' codes and index deltas (code kMixedGeneric
+// past its count) at out[s][k], k < max_n.
+__global__ void k_sample_rows(EllView nl, int64_t np, const uint8_t* __restrict__ code,
+                              int64_t lo, int64_t span, int nsamples, int2* out)
+{
+    const int s = blockIdx.x;
+    const int64_t r = lo + ((2 * (int64_t)s + 1) * span) / (2 * (int64_t)nsamples);
+    const int cnt = nl.count[r];
+    for (int k = threadIdx.x; k < nl.max_n; k += blockDim.x) {
+        int2 v = make_int2(kMixedGeneric, 0);
+        if (k < cnt) {
+            v.x = code[(int64_t)k * np + r];
+            v.y = (int)(nl.idx[(int64_t)k * np + r] - r);
+        }
+        out[(int64_t)s * nl.max_n + k] = v;
+    }
+}
+
 // Per row: first the delta check of every coded bond (a bond whose code's
 // index delta is not its own j - i becomes generic), then the presence bits
 // of the stencil entries the row holds (its codes are a strictly increasing
@@ -1633,11 +1652,53 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 L.lut = d_lut;
                 tr.mark("spacing+table", st);
                 k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
-                tr.mark("code", st);
                 launches++;
+                tr.mark("code", st);
                 std::vector<unsigned int> delta(kMixedGeneric);
                 CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
                                         cudaMemcpyDeviceToHost, st));
+                {
+                    // Each code's index delta is the one most of 256 rows spread
+                    // over the body hold (the minimum over all bonds where no
+                    // sample holds the code). In a body with voids or holes the
+                    // rows whose neighbours lie across one see shifted deltas;
+                    // the minimum would take a shifted one and leave every other
+                    // row irregular.
+                    const int S = (int)std::min<int64_t>(256, rows);
+                    const int mn = std::max(pd.max_n, 1);
+                    if (S > 0) {
+                        int2* d_samp = nullptr;
+                        CPD_TRY(dev_alloc(&d_samp, sizeof(int2) * (size_t)S * mn, st));
+                        k_sample_rows<<<S, kBlock, 0, st>>>(pd.view(), np, m.code, p.frozen,
+                                                            rows, S, d_samp);
+                        launches++;
+                        std::vector<int2> samp((size_t)S * mn);
+                        CPD_TRY(cudaMemcpyAsync(samp.data(), d_samp, sizeof(int2) * samp.size(),
+                                                cudaMemcpyDeviceToHost, st));
+                        CPD_TRY(cudaStreamSynchronize(st));
+                        CPD_TRY(dev_free(d_samp, st));
+                        std::vector<std::vector<int>> seen(tab.size());
+                        for (const int2& v : samp)
+                            if (v.x < (int)tab.size()) seen[v.x].push_back(v.y);
+                        for (size_t t = 0; t < tab.size(); ++t) {
+                            std::vector<int>& d = seen[t];
+                            if (d.empty()) continue;
+                            std::sort(d.begin(), d.end());
+                            int best = d[0], run = 0, best_run = 0;
+                            for (size_t q = 0; q < d.size(); ++q) {
+                                run = (q > 0 && d[q] == d[q - 1]) ? run + 1 : 1;
+                                if (run > best_run) {
+                                    best_run = run;
+                                    best = d[q];
+                                }
+                            }
+                            delta[t] = (unsigned int)((long long)best + (1LL << 31));
+                        }
+                        CPD_TRY(cudaMemcpyAsync(d_delta, delta.data(),
+                                                sizeof(unsigned int) * kMixedGeneric,
+                                                cudaMemcpyHostToDevice, st));
+                    }
+                }
                 CPD_TRY(cudaStreamSynchronize(st));
                 for (size_t t = 0; t < tab.size(); ++t)
                     tab[t].delta = (int32_t)((long long)delta[t] - (1LL << 31));

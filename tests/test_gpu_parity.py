@@ -470,20 +470,43 @@ def test_mixed_plate_at_the_full_plates_spacing(cuda):
     assert np.array_equal(g.neighbors()[2], f.neighbors()[2])
 
 
+def _with_void(prob, sites):
+    """The problem with the given lattice sites left empty (index deltas
+    across them shift: the rows whose neighbours lie across them take the
+    general kernels)."""
+    from cabanapd_b200 import shard
+    keep = np.setdiff1d(np.arange(len(prob["x"])), sites)
+    return shard.local_problem(prob, keep, np.ones(keep.size, dtype=bool))
+
+
+@pytest.mark.parametrize("body", ["pair", "void"])
 @pytest.mark.parametrize("precision", [1, MIXED])
-def test_stencil_kernels_plate_against_oracle(cuda, oracle, precision):
+def test_stencil_kernels_plate_against_oracle(cuda, oracle, precision, body):
     """The lattice-stencil bond kernels (FP64: the two-launch walk; MIXED:
-    the FP32 walk on the split records) on a cubic notched plate, with an
-    off-lattice pair whose warp takes the general kernels: FP64 within
-    1e-12 of the oracle with identical bonds over 160 steps; MIXED within
-    the mixed bars, bonds identical."""
-    prob = _with_offlattice_pair(_cubic_plate(96, 8, steps=160))
+    the FP32 walk on the split records) on a cubic notched plate beside
+    warps on the general kernels: an off-lattice pair (one warp), or two
+    empty lattice sites in the plate (the warps of rows whose neighbours lie
+    across them; the index deltas come from the rows around the middle).
+    FP64 within 1e-12 of the oracle with identical bonds over 160 steps;
+    MIXED within the mixed bars, bonds identical."""
+    plate = _cubic_plate(96, 8, steps=160)
+    if body == "pair":
+        prob = _with_offlattice_pair(plate)
+    else:
+        prob = _with_void(plate, [13000, 13001])
     g = cuda.System(dict(prob["params"], precision=precision))
     o = oracle.OracleSystem(prob["params"])
     P.setup(g, prob)
     P.setup(o, prob)
     warps, irregular, entries = g.stencil_stats()
-    assert warps > 0 and irregular == 1 and entries == 122
+    assert entries == 122
+    if body == "pair":
+        assert warps == len(plate["x"]) // 32 and irregular == 1
+    else:
+        # The rows within three planes of the void in index order (most of
+        # this 8-plane plate) leave the stencil kernels, the others stay
+        # (with the smallest delta over all bonds as the table's, none did).
+        assert irregular > 0 and warps > 0.1 * (warps + irregular)
     for _ in range(4):
         g.run(40)
         o.run(40)
