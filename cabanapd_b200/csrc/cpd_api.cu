@@ -479,7 +479,8 @@ cpd_status pd_force_on(cpd_system* s, const ParticleView& p, const MixedState& m
         CPD_LAUNCHED(launch_pd_force_mixed(p, pd_view(s), s->md, m, ep, s->stream));
     } else if (use_stencil64(s)) {
         // Outside the fused step the gather records follow p.u here.
-        if (ep.mode == 0) CPD_LAUNCHED(launch_pack_u4(p, p.u, 0, p.n, m.u4, s->stream));
+        if (ep.mode == 0)
+            CPD_LAUNCHED(launch_pack_u4(p, p.u, 0, p.n, m.u4, s->stream, m.gcell));
         CPD_LAUNCHED(launch_pd_force_stencil64(p, pd_view(s), s->md, m, ep, s->stream));
     } else if (use_fast(s))
         CPD_LAUNCHED(launch_pd_force_fast(p, pd_view(s), s->md, ep, s->stream));
@@ -814,8 +815,8 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, double* energy_part = nu
     if (sten) {
         // Gather records of the first step's displacement, and the frozen
         // rows of the second buffer (the kernels write rows from frozen on).
-        CPD_LAUNCHED(launch_pack_u4(p, ucur, 0, s->n, u4cur, s->stream));
-        CPD_LAUNCHED(launch_pack_u4(p, s->u, 0, s->frozen, u4nxt, s->stream));
+        CPD_LAUNCHED(launch_pack_u4(p, ucur, 0, s->n, u4cur, s->stream, s->mixed.gcell));
+        CPD_LAUNCHED(launch_pack_u4(p, s->u, 0, s->frozen, u4nxt, s->stream, s->mixed.gcell));
     }
     StepEpilogue ep;
     ep.dt = s->params.dt;
@@ -826,6 +827,7 @@ cpd_status step_fused(cpd_system* s, int32_t num_steps, double* energy_part = nu
     ep.bc_keep = s->bc_keep;
     ep.bc_add = s->bc_add;
     ep.nbc = s->nbc;
+    ep.u4_cell = sten ? s->mixed.gcell : nullptr;
     for (int32_t k = 0; k < num_steps; ++k) {
         ParticleView pk = p;
         pk.u = ucur;

@@ -87,7 +87,9 @@ __device__ __forceinline__ void step_epilogue(const ParticleView& p, const StepE
         ep.u_next[d * np + i] = u[d];
     }
     if (MIXED) ep.u2_next[i] = split_u(u[0], u[1], u[2], ep.c * p.vol[i], p.nofail[i]);
-    if (!MIXED && ep.u4_next) ep.u4_next[i] = make_double4(u[0], u[1], u[2], p.vol[i]);
+    if (!MIXED && ep.u4_next)
+        ep.u4_next[ep.u4_cell ? (int64_t)ep.u4_cell[i] : i] =
+            make_double4(u[0], u[1], u[2], p.vol[i]);
 }
 
 }  // namespace cpd

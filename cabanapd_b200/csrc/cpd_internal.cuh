@@ -382,8 +382,10 @@ struct StepEpilogue {
     // Contact steps: neighbours read this row's velocity during the pass
     // (Hertz damping), so the new velocity goes to this second buffer.
     double* v_next = nullptr;
-    // FP64 stencil path: the next displacement's gather records as well.
+    // FP64 stencil path: the next displacement's gather records as well, at
+    // record u4_cell[i] of row i (the lattice-cell layout) or at i (null).
     double4* u4_next = nullptr;
+    const int32_t* u4_cell = nullptr;
     // Mixed stencil kernel on an output step: also the rows' strain energy
     // density and damage (W, phi), and per stencil warp the partial sums
     // (sum W_i vol_i, sum phi_i) at energy_part[2 slot], [2 slot + 1].
@@ -425,6 +427,14 @@ struct MixedState {
     // The FP64 stencil walk runs in two launches: the first one's force sum
     // per row (x, y, z; w unused), which the second one continues.
     double4* f64part = nullptr;
+    // Lattice-cell layout of the FP64 gather records (a lattice body whose
+    // particle order is not one box of lattice lines, e.g. with holes): row
+    // i's record is u4[gcell[i]], gcell[i] = a + nx (b + ny c) from its
+    // lattice coordinates, so that entry k is always record gcell[i] +
+    // delta_k; cells without a particle hold zero records. Null: records by
+    // row (u4[i]), the table's deltas then being index deltas.
+    int32_t* gcell = nullptr;
+    int64_t grid_cells = 0;
     // Mixed PMB stencil kernel: its table, and the allocation behind u2
     // (u2 = u2_base + guard; `guard` zero records on either side).
     Stencil32* st32 = nullptr;
@@ -458,8 +468,10 @@ bool prepare_stencil32(const Model& md, const double* h, const MixedStencil* tab
 int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 // Gather records of rows [begin, end) from the displacement u (SoA).
+// Rows [begin, end) of u (and vol) as gather records: u4[cell[i]], or u4[i]
+// when cell is null.
 int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_t end,
-                   double4* u4, cudaStream_t st);
+                   double4* u4, cudaStream_t st, const int32_t* cell = nullptr);
 int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Model& md,
                               const MixedState& m, const StepEpilogue& ep, cudaStream_t st);
 // Energy and damage of the listed warps' rows on the mixed path (the rows

@@ -191,6 +191,82 @@ __global__ void k_sample_rows(EllView nl, int64_t np, const uint8_t* __restrict_
     }
 }
 
+// Order-preserving unsigned image of a double (for atomicMin / atomicMax).
+__device__ __forceinline__ unsigned long long ordered_bits(double v)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// Per axis the smallest and largest position of rows [0, n) (ordered_bits:
+// out[0..2] minima, out[3..5] maxima; grid-stride rows, one atomic per block
+// and value).
+__global__ void __launch_bounds__(kBlock)
+    k_bounds(const double* __restrict__ x, int64_t n, int64_t np, unsigned long long* out)
+{
+    __shared__ unsigned long long s[6][kBlock];
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        for (int d = 0; d < 3; ++d) {
+            const unsigned long long b = ordered_bits(x[d * np + i]);
+            lo[d] = b < lo[d] ? b : lo[d];
+            hi[d] = b > hi[d] ? b : hi[d];
+        }
+    for (int d = 0; d < 3; ++d) {
+        s[d][threadIdx.x] = lo[d];
+        s[3 + d][threadIdx.x] = hi[d];
+    }
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int d = 0; d < 3; ++d) {
+                s[d][threadIdx.x] = min(s[d][threadIdx.x], s[d][threadIdx.x + w]);
+                s[3 + d][threadIdx.x] = max(s[3 + d][threadIdx.x], s[3 + d][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(out + d, s[d][0]);
+            atomicMax(out + 3 + d, s[3 + d][0]);
+        }
+}
+
+// Lattice cell of every row [0, n): cell = a + nc0 (b + nc1 c) from
+// (x - x0) / h rounded per axis. flags[0] counts positions more than 1e-6
+// spacings off the lattice, flags[1] cells taken twice; ext[0] / ext[1] are
+// the smallest and largest cell - row (biased by 2^62).
+__global__ void __launch_bounds__(kBlock)
+    k_lattice_cells(const double* __restrict__ x, int64_t n, int64_t np, double3 x0,
+                    double3 hinv, int3 nc, int32_t* __restrict__ cell,
+                    uint32_t* __restrict__ occ, unsigned int* flags, unsigned long long* ext)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t[3] = {(x[i] - x0.x) * hinv.x, (x[np + i] - x0.y) * hinv.y,
+                         (x[2 * np + i] - x0.z) * hinv.z};
+    const int ncs[3] = {nc.x, nc.y, nc.z};
+    long long a[3];
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        const double r = rint(t[d]);
+        if (fabs(t[d] - r) > 1e-6 || r < 0.0 || r >= (double)ncs[d]) ok = false;
+        a[d] = (long long)r;
+    }
+    if (!ok) {
+        atomicAdd(flags, 1u);
+        cell[i] = 0;
+        return;
+    }
+    const long long g = a[0] + (long long)nc.x * (a[1] + (long long)nc.y * a[2]);
+    cell[i] = (int32_t)g;
+    if (atomicAdd(occ + g, 1u) != 0u) atomicAdd(flags + 1, 1u);
+    const unsigned long long e = (unsigned long long)(g - i + (1LL << 62));
+    atomicMin(ext, e);
+    atomicMax(ext + 1, e);
+}
+
 // Per row: first the delta check of every coded bond (a bond whose code's
 // index delta is not its own j - i becomes generic), then the presence bits
 // of the stencil entries the row holds (its codes are a strictly increasing
@@ -199,7 +275,8 @@ __global__ void k_sample_rows(EllView nl, int64_t np, const uint8_t* __restrict_
 // 1 if every row is a table subset, else 0.
 __global__ void __launch_bounds__(kBlock)
     k_row_masks(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code, int ntab,
-                uint32_t* pmask, uint8_t* kind, uint32_t* warp_pmask)
+                uint32_t* pmask, uint8_t* kind, uint32_t* warp_pmask,
+                const int32_t* __restrict__ gcell)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int nmask = (ntab + 31) / 32;
@@ -215,8 +292,10 @@ __global__ void __launch_bounds__(kBlock)
         for (int k = 0; k < cnt; ++k) {
             const int64_t o = (int64_t)k * np + i;
             int c = code[o];
-            if (c != kMixedGeneric &&
-                (long long)delta[c] - (1LL << 31) != (long long)(nl.idx[o] - i)) {
+            // The delta of the records' layout: lattice cells or rows.
+            const long long dij = gcell ? (long long)gcell[nl.idx[o]] - (long long)gcell[i]
+                                        : (long long)(nl.idx[o] - i);
+            if (c != kMixedGeneric && (long long)delta[c] - (1LL << 31) != dij) {
                 c = kMixedGeneric;
                 code[o] = (uint8_t)c;
             }
@@ -1518,11 +1597,102 @@ void free_mixed(MixedState& m, cudaStream_t st)
     m.st32 = nullptr;
     void* ptrs[] = {m.xh, m.xl, m.u2_base, m.code, m.table, m.warp_kind, m.pmask, m.warp_pmask,
                     m.ab, m.lean_list, m.rest_list, m.vol_sums, m.u2ab, m.stencil_list,
-                    m.irregular_list};
+                    m.irregular_list, m.gcell};
     for (void* q : ptrs)
         if (q) dev_free(q, st);
     m = MixedState{};
 }
+
+namespace {
+
+// The FP64 stencil records' layout: when every particle sits on one lattice
+// cell of the bounding box (no two in one) but the particle order is not one
+// box of lattice lines (cell - row not constant: a body with holes or a
+// non-box outline), the records go by lattice cell (m.gcell) and each table
+// entry's delta becomes its cell delta a + nc0 (b + nc1 c), so that every
+// lattice row keeps the stencil kernel. Otherwise nothing changes (the row
+// layout, whose index deltas equal the cell deltas in a box).
+#define CPD_RET(call)                   \
+    do {                                \
+        const cudaError_t e_ = (call);  \
+        if (e_ != cudaSuccess) return e_; \
+    } while (0)
+cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
+                                const std::vector<MixedStencil>& tab, int64_t rows,
+                                MixedState& m, std::vector<unsigned int>& delta,
+                                unsigned int* d_delta, int& launches, cudaStream_t st)
+{
+    if (p.n <= 0 || rows <= 0) return cudaSuccess;
+    unsigned long long* d_b = nullptr;
+    cudaError_t e = dev_alloc(&d_b, sizeof(unsigned long long) * 8, st);
+    if (e != cudaSuccess) return e;
+    const unsigned long long init[8] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, ~0ull, 0ull};
+    CPD_RET(cudaMemcpyAsync(d_b, init, sizeof init, cudaMemcpyHostToDevice, st));
+    const int nb = (int)std::min<int64_t>(blocks_for(p.n), 148 * 8);
+    k_bounds<<<nb, kBlock, 0, st>>>(p.x, p.n, p.npad, d_b);
+    launches++;
+    unsigned long long hb[8];
+    CPD_RET(cudaMemcpyAsync(hb, d_b, sizeof hb, cudaMemcpyDeviceToHost, st));
+    CPD_RET(cudaStreamSynchronize(st));
+    auto from_bits = [](unsigned long long k) {
+        const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double v;
+        std::memcpy(&v, &b, sizeof v);
+        return v;
+    };
+    double lo[3];
+    int64_t nc[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = from_bits(hb[d]);
+        nc[d] = (int64_t)std::llround((from_bits(hb[3 + d]) - lo[d]) / h[d]) + 1;
+    }
+    const int64_t cells = nc[0] * nc[1] * nc[2];
+    // A sparse outline would need too many empty records.
+    if (cells > 4 * p.n + 4096 || cells >= ((int64_t)1 << 31)) {
+        dev_free(d_b, st);
+        return cudaSuccess;
+    }
+    int32_t* cell = nullptr;
+    uint32_t* occ = nullptr;
+    unsigned int* flags = nullptr;
+    CPD_RET(dev_alloc(&cell, sizeof(int32_t) * (size_t)p.npad, st));
+    CPD_RET(dev_alloc(&occ, sizeof(uint32_t) * (size_t)cells, st));
+    CPD_RET(dev_alloc(&flags, sizeof(unsigned int) * 2, st));
+    CPD_RET(cudaMemsetAsync(occ, 0, sizeof(uint32_t) * (size_t)cells, st));
+    CPD_RET(cudaMemsetAsync(flags, 0, sizeof(unsigned int) * 2, st));
+    k_lattice_cells<<<blocks_for(p.n), kBlock, 0, st>>>(
+        p.x, p.n, p.npad, make_double3(lo[0], lo[1], lo[2]),
+        make_double3(1.0 / h[0], 1.0 / h[1], 1.0 / h[2]),
+        make_int3((int)nc[0], (int)nc[1], (int)nc[2]), cell, occ, flags, d_b + 6);
+    launches++;
+    unsigned int hf[2];
+    CPD_RET(cudaMemcpyAsync(hf, flags, sizeof hf, cudaMemcpyDeviceToHost, st));
+    CPD_RET(cudaMemcpyAsync(hb + 6, d_b + 6, sizeof(unsigned long long) * 2,
+                            cudaMemcpyDeviceToHost, st));
+    CPD_RET(cudaStreamSynchronize(st));
+    dev_free(occ, st);
+    dev_free(flags, st);
+    dev_free(d_b, st);
+    if (hf[0] != 0u || hf[1] != 0u || hb[6] == hb[7]) {
+        // Off the lattice, two particles in a cell, or one box in row order.
+        dev_free(cell, st);
+        return cudaSuccess;
+    }
+    m.gcell = cell;
+    m.grid_cells = cells;
+    m.bytes += sizeof(int32_t) * (size_t)p.npad;
+    for (size_t t = 0; t < tab.size(); ++t) {
+        const long long a = std::llround(tab[t].x / h[0]);
+        const long long b = std::llround(tab[t].y / h[1]);
+        const long long c = std::llround(tab[t].z / h[2]);
+        delta[t] = (unsigned int)(a + nc[0] * (b + nc[1] * c) + (1LL << 31));
+    }
+    return cudaMemcpyAsync(d_delta, delta.data(), sizeof(unsigned int) * kMixedGeneric,
+                           cudaMemcpyHostToDevice, st);
+}
+
+#undef CPD_RET
+}  // namespace
 
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil,
@@ -1699,6 +1869,8 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                                                 cudaMemcpyHostToDevice, st));
                     }
                 }
+                if (!fp32)
+                    CPD_TRY(lattice_cell_layout(p, h, tab, rows, m, delta, d_delta, launches, st));
                 CPD_TRY(cudaStreamSynchronize(st));
                 for (size_t t = 0; t < tab.size(); ++t)
                     tab[t].delta = (int32_t)((long long)delta[t] - (1LL << 31));
@@ -1715,7 +1887,7 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 m.bytes += sizeof(uint32_t) * nmask * nwarps;
                 k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code,
                                                                  m.ntab, m.pmask, m.warp_kind,
-                                                                 m.warp_pmask);
+                                                                 m.warp_pmask, m.gcell);
                 launches++;
                 CPD_TRY(dev_free(d_delta, st));
                 tr.mark("masks", st);

@@ -113,11 +113,12 @@ void fit_stretch_poly(long double Q, int n, long double* out, bool anchored = fa
 
 __global__ void __launch_bounds__(kBlock)
     k_pack_u4(const double* __restrict__ u, const double* __restrict__ vol, int64_t np,
-              int64_t begin, int64_t end, double4* __restrict__ u4)
+              int64_t begin, int64_t end, double4* __restrict__ u4,
+              const int32_t* __restrict__ cell)
 {
     const int64_t i = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= end) return;
-    u4[i] = make_double4(u[i], u[np + i], u[2 * np + i], vol[i]);
+    u4[cell ? (int64_t)cell[i] : i] = make_double4(u[i], u[np + i], u[2 * np + i], vol[i]);
 }
 
 // The reference's exact break test and pair force of bond (i, j) from
@@ -255,10 +256,10 @@ __device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilR
     }
 }
 
-// Marks broken the bond of row i at table entry 32 w + b (its slot: the
-// row's present entries before it).
-__device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilRows& sr,
-                                               int kind, int64_t i, int64_t np, int w, int b)
+// Bond slot of row i's table entry 32 w + b: the row's present entries
+// before it (kind 2: the entry itself).
+__device__ __forceinline__ int entry_slot(const StencilRows& sr, int kind, int64_t i,
+                                          int64_t np, int w, int b)
 {
     int s = 32 * w + b;
     if (kind != 2) {
@@ -266,6 +267,14 @@ __device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilR
         for (int v = 0; v < w; ++v) s += __popc(sr.pmask[(int64_t)v * np + i]);
         s += __popc(sr.pmask[(int64_t)w * np + i] & ((1u << b) - 1u));
     }
+    return s;
+}
+
+// Marks broken the bond of row i at table entry 32 w + b.
+__device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilRows& sr,
+                                               int kind, int64_t i, int64_t np, int w, int b)
+{
+    const int s = entry_slot(sr, kind, i, np, w, b);
     nl.mu[(int64_t)(s >> 5) * np + i] &= ~(1u << (s & 31));
 }
 
@@ -286,7 +295,8 @@ template <bool FRACTURE, bool UNIFORM, int K0, int K1, int NP, bool LAST, bool E
 __global__ void __launch_bounds__(kBlock, 4)
     k_pmb_stencil64(ParticleView p, EllView nl, StencilRows sr,
                     const double4* __restrict__ U4, double4* __restrict__ FPART,
-                    StepEpilogue ep, const Stencil64 st, const double* __restrict__ vol_sums)
+                    StepEpilogue ep, const Stencil64 st, const double* __restrict__ vol_sums,
+                    const int32_t* __restrict__ CELL)
 {
     constexpr bool SUMS = ENERGY && LAST;
     const int lane = threadIdx.x & 31;
@@ -302,8 +312,10 @@ __global__ void __launch_bounds__(kBlock, 4)
     const int kind = sr.warp_kind[warp];
     uint32_t ew[4];
     row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
-    const double4 ui = U4[i];
-    const char* __restrict__ rb = reinterpret_cast<const char*>(U4 + i);
+    // Row i's gather record: by lattice cell, or by row.
+    const int64_t rec = CELL ? (int64_t)CELL[i] : i;
+    const double4 ui = U4[rec];
+    const char* __restrict__ rb = reinterpret_cast<const char*>(U4 + rec);
     double fx = 0.0, fy = 0.0, fz = 0.0, wsum = 0.0;
     if (K0 > 0) {
         const double4 fp = FPART[i];
@@ -343,7 +355,12 @@ __global__ void __launch_bounds__(kBlock, 4)
                 const int b = __ffs(q) - 1;
                 q &= q - 1;
                 const int k = 32 * w + b;
-                if (exact_bond<FRACTURE>(p, i, i + st.e[k].doff, st.c, st.bbc, nofail_i, f,
+                // The neighbour: from the list when records are by lattice
+                // cell (the table's deltas are then cell deltas).
+                const int64_t j =
+                    CELL ? (int64_t)nl.idx[(int64_t)entry_slot(sr, kind, i, np, w, b) * np + i]
+                         : i + st.e[k].doff;
+                if (exact_bond<FRACTURE>(p, i, j, st.c, st.bbc, nofail_i, f,
                                          ENERGY ? &wsum : nullptr)) {
                     clear_bond_bit(nl, sr, kind, i, np, w, b);
                     ++broken;
@@ -606,7 +623,8 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
     }
     m.st64 = S;
     m.guard = G + 32;
-    const size_t recs = (size_t)(p.npad + 2 * m.guard);
+    // Records by lattice cell (m.gcell) or by row.
+    const size_t recs = (size_t)((m.gcell ? m.grid_cells : p.npad) + 2 * m.guard);
     if (dev_alloc(&m.u4_base, sizeof(double4) * recs, st) != cudaSuccess ||
         dev_alloc(&m.u4_alt_base, sizeof(double4) * recs, st) != cudaSuccess ||
         dev_alloc(&m.f64part, sizeof(double4) * (size_t)p.npad, st) != cudaSuccess ||
@@ -713,10 +731,11 @@ int launch_pd_force_stencil32(const ParticleView& p, const EllView& nl, const Mo
 }
 
 int launch_pack_u4(const ParticleView& p, const double* u, int64_t begin, int64_t end,
-                   double4* u4, cudaStream_t st)
+                   double4* u4, cudaStream_t st, const int32_t* cell)
 {
     if (end <= begin) return 0;
-    k_pack_u4<<<blocks_for(end - begin), kBlock, 0, st>>>(u, p.vol, p.npad, begin, end, u4);
+    k_pack_u4<<<blocks_for(end - begin), kBlock, 0, st>>>(u, p.vol, p.npad, begin, end, u4,
+                                                          cell);
     return 1;
 }
 
@@ -738,9 +757,9 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
 #define CPD_ST64X(F, U, NT, NP, E)                                                           \
     do {                                                                                     \
         k_pmb_stencil64<F, U, 0, 64, NP, false, E><<<g, kBlock, 0, st>>>(                    \
-            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums);                                  \
+            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums, m.gcell);                         \
         k_pmb_stencil64<F, U, 64, NT, NP, true, E><<<g, kBlock, 0, st>>>(                    \
-            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums);                                  \
+            p, nl, sr, m.u4, m.f64part, ep, S, m.vol_sums, m.gcell);                         \
     } while (0)
 #define CPD_ST64(F, U, NT, NP) CPD_ST64X(F, U, NT, NP, false)
         // Unrolled forms: the 122-entry table of a cubic lattice at a
