@@ -946,7 +946,8 @@ cpd_status cpd_stencil_stats(const cpd_system* s, int64_t* stencil_warps,
                              int64_t* irregular_warps, int32_t* table_entries)
 {
     if (!s) return set_error(CPD_ERR_INVALID_ARGUMENT, "null system");
-    const bool sten = (use_mixed(s) && s->mixed.st32) || (use_stencil64(s) && s->mixed.st64);
+    const bool sten = (use_mixed(s) && s->mixed.st32) ||
+                      (use_stencil64(s) && (s->mixed.st64 || s->mixed.st64w));
     if (stencil_warps) *stencil_warps = sten ? s->mixed.nstencil : 0;
     if (irregular_warps) *irregular_warps = sten ? s->mixed.nirregular : 0;
     if (table_entries) *table_entries = sten ? s->mixed.ntab : 0;

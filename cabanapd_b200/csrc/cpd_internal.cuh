@@ -315,7 +315,12 @@ struct __align__(16) StencilEntry64 {
     // high word of |num| is below khi.
     uint32_t khi;
 };
-struct Stencil64 {
+// The FP64 table in two sizes: up to kStencilMax entries (horizons to ~3.5
+// spacings; one struct per launch keeps the parameters small) and up to
+// kStencilMaxWide (a horizon of 4 spacings: 256 entries).
+constexpr int kStencilMaxWide = 256;
+template <int N>
+struct Stencil64T {
     int32_t ntab = 0, nwords = 0;
     int32_t np = 0;        // coefficients of h in use (8 or 9)
     double bbc = 0;        // bond_break_coeff (the exact re-test)
@@ -326,10 +331,12 @@ struct Stencil64 {
     // S(q) = sum_k sh[k] q^k ~ 1 / (1 + sqrt(1+q)), the stretch s = q S(q)
     // (output steps' energy).
     double sh[kStencilPoly];
-    StencilEntry64 e[kStencilMax];  // past ntab: zero (no force, never deferred)
+    StencilEntry64 e[N];  // past ntab: zero (no force, never deferred)
     // Energy factor of each entry, c vol xi / 4 (one particle volume).
-    double kw[kStencilMax];
+    double kw[N];
 };
+using Stencil64 = Stencil64T<kStencilMax>;
+using Stencil64W = Stencil64T<kStencilMaxWide>;
 // The mixed-precision form (FP32 bond arithmetic on the FP32 split of u).
 constexpr int kStencilPoly32 = 4;  // coefficients of the FP32 stretch polynomial
 struct __align__(16) StencilEntry32 {
@@ -424,6 +431,7 @@ struct MixedState {
     // records (u_x, u_y, u_z, vol) with `guard` zero records on either side,
     // so i + delta of an absent stencil entry stays inside the allocation.
     Stencil64* st64 = nullptr;
+    Stencil64W* st64w = nullptr;  // tables past kStencilMax entries
     // The FP64 stencil walk runs in two launches: the first one's force sum
     // per row (x, y, z; w unused), which the second one continues.
     double4* f64part = nullptr;

@@ -112,6 +112,9 @@ __global__ void __launch_bounds__(kBlock)
         for (int d = 0; d < 3; ++d) atomicMin(out + d, s[d][0]);
 }
 
+// Slots of the per-entry delta arrays (byte codes and the wide FP64 table).
+constexpr int kDeltaSlots = kStencilMaxWide > kMixedGeneric ? kStencilMaxWide : kMixedGeneric;
+
 struct LatticeLut {
     double h[3];
     double hinv[3];  // 1 / h
@@ -273,10 +276,13 @@ __global__ void __launch_bounds__(kBlock)
 // subset of the table); per warp: 2 if every row is the whole table, 3 if
 // every row is the same table subset (the subset is recorded for the warp),
 // 1 if every row is a table subset, else 0.
+// LUT: each bond's entry from the positions (L, as k_code_bonds does) with
+// no code array; else from the codes, which the delta check may rewrite.
+template <bool LUT>
 __global__ void __launch_bounds__(kBlock)
     k_row_masks(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code, int ntab,
                 uint32_t* pmask, uint8_t* kind, uint32_t* warp_pmask,
-                const int32_t* __restrict__ gcell)
+                const int32_t* __restrict__ gcell, LatticeLut L)
 {
     const int64_t i = p.frozen + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int nmask = (ntab + 31) / 32;
@@ -289,15 +295,37 @@ __global__ void __launch_bounds__(kBlock)
         const int cnt = nl.count[i];
         full = cnt == ntab;
         int prev = -1;
+        const int nx = 2 * L.half[0] + 1, ny = 2 * L.half[1] + 1;
+        // No entry: the byte codes' generic code, or (positions, where the
+        // table may hold up to kStencilMaxWide entries) a value past it.
+        const int generic = LUT ? (1 << 20) : kMixedGeneric;
         for (int k = 0; k < cnt; ++k) {
             const int64_t o = (int64_t)k * np + i;
-            int c = code[o];
+            const int64_t j = nl.idx[o];
+            int c = generic;
+            if (LUT) {
+                int off[3];
+                bool ok = true;
+                for (int d = 0; d < 3; ++d) {
+                    const double dd = p.x[d * np + j] - p.x[d * np + i];
+                    const double a = rint(dd * L.hinv[d]);
+                    if (fabs(dd - a * L.h[d]) > 1e-6 * L.h[d] || fabs(a) > L.half[d]) ok = false;
+                    off[d] = (int)a;
+                }
+                if (ok) {
+                    const int e = L.lut[(off[0] + L.half[0]) +
+                                        nx * ((off[1] + L.half[1]) + ny * (off[2] + L.half[2]))];
+                    if (e >= 0) c = e;
+                }
+            } else {
+                c = code[o];
+            }
             // The delta of the records' layout: lattice cells or rows.
-            const long long dij = gcell ? (long long)gcell[nl.idx[o]] - (long long)gcell[i]
-                                        : (long long)(nl.idx[o] - i);
-            if (c != kMixedGeneric && (long long)delta[c] - (1LL << 31) != dij) {
-                c = kMixedGeneric;
-                code[o] = (uint8_t)c;
+            const long long dij = gcell ? (long long)gcell[j] - (long long)gcell[i]
+                                        : (long long)(j - i);
+            if (c != generic && (long long)delta[c] - (1LL << 31) != dij) {
+                c = generic;
+                if (!LUT) code[o] = (uint8_t)c;
             }
             if (!subset) continue;
             if (c >= ntab || c <= prev) {
@@ -1605,13 +1633,14 @@ void free_mixed(MixedState& m, cudaStream_t st)
 
 namespace {
 
-// The FP64 stencil records' layout: when every particle sits on one lattice
-// cell of the bounding box (no two in one) but the particle order is not one
-// box of lattice lines (cell - row not constant: a body with holes or a
-// non-box outline), the records go by lattice cell (m.gcell) and each table
-// entry's delta becomes its cell delta a + nc0 (b + nc1 c), so that every
-// lattice row keeps the stencil kernel. Otherwise nothing changes (the row
-// layout, whose index deltas equal the cell deltas in a box).
+// The FP64 stencil records' layout. When every particle sits on its own
+// lattice cell of the bounding box, each table entry's delta is its cell
+// delta a + nc0 (b + nc1 c): layout 1 when the particle order is one box of
+// lattice lines (cell - row constant: records by row, the index deltas being
+// the cell deltas), layout 2 otherwise (a body with holes or a non-box
+// outline: records by lattice cell, m.gcell), so that every lattice row keeps
+// the stencil kernel. Layout 0 (not a lattice of distinct cells, or too
+// sparse a bounding box): deltas from the bond codes.
 #define CPD_RET(call)                   \
     do {                                \
         const cudaError_t e_ = (call);  \
@@ -1619,9 +1648,10 @@ namespace {
     } while (0)
 cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
                                 const std::vector<MixedStencil>& tab, int64_t rows,
-                                MixedState& m, std::vector<unsigned int>& delta,
-                                unsigned int* d_delta, int& launches, cudaStream_t st)
+                                MixedState& m, std::vector<unsigned int>& delta, int& launches,
+                                int& layout, cudaStream_t st)
 {
+    layout = 0;
     if (p.n <= 0 || rows <= 0) return cudaSuccess;
     unsigned long long* d_b = nullptr;
     cudaError_t e = dev_alloc(&d_b, sizeof(unsigned long long) * 8, st);
@@ -1673,22 +1703,29 @@ cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
     dev_free(occ, st);
     dev_free(flags, st);
     dev_free(d_b, st);
-    if (hf[0] != 0u || hf[1] != 0u || hb[6] == hb[7]) {
-        // Off the lattice, two particles in a cell, or one box in row order.
+    if (hf[0] != 0u || hf[1] != 0u) {
+        // Off the lattice, or two particles in a cell.
         dev_free(cell, st);
         return cudaSuccess;
     }
-    m.gcell = cell;
-    m.grid_cells = cells;
-    m.bytes += sizeof(int32_t) * (size_t)p.npad;
+    if (hb[6] == hb[7]) {
+        // One box in row order: records by row, whose index deltas are the
+        // cell deltas.
+        dev_free(cell, st);
+        layout = 1;
+    } else {
+        m.gcell = cell;
+        m.grid_cells = cells;
+        m.bytes += sizeof(int32_t) * (size_t)p.npad;
+        layout = 2;
+    }
     for (size_t t = 0; t < tab.size(); ++t) {
         const long long a = std::llround(tab[t].x / h[0]);
         const long long b = std::llround(tab[t].y / h[1]);
         const long long c = std::llround(tab[t].z / h[2]);
         delta[t] = (unsigned int)(a + nc[0] * (b + nc[1] * c) + (1LL << 31));
     }
-    return cudaMemcpyAsync(d_delta, delta.data(), sizeof(unsigned int) * kMixedGeneric,
-                           cudaMemcpyHostToDevice, st);
+    return cudaSuccess;
 }
 
 #undef CPD_RET
@@ -1788,7 +1825,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                         const double vx = a * h[0], vy = b * h[1], vz = c * h[2];
                         const double len = std::sqrt(vx * vx + vy * vy + vz * vz);
                         if (len > cutoff * (1.0 + 1e-9)) continue;
-                        if ((int)tab.size() >= kMixedGeneric) {
+                        // Codes are bytes below kMixedGeneric; the FP64
+                        // stencil path codes rows from the positions and
+                        // takes up to kStencilMaxWide entries.
+                        if ((int)tab.size() >= (fp32 ? kMixedGeneric : kStencilMaxWide)) {
                             lattice = false;
                             break;
                         }
@@ -1805,14 +1845,24 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                         e.pad = 0;
                         tab.push_back(e);
                     }
+            // FP64: when every particle sits on its own lattice cell, each
+            // entry's delta comes from the geometry and rows are coded from
+            // the positions (no per-bond codes); else the byte codes below.
+            int layout = 0;
+            std::vector<unsigned int> delta(kDeltaSlots, 0xffffffffu);
+            if (lattice && !tab.empty() && !fp32)
+                CPD_TRY(lattice_cell_layout(p, h, tab, rows, m, delta, launches, layout, st));
+            const bool by_codes = layout == 0;
+            if (by_codes && (int)tab.size() >= kMixedGeneric) lattice = false;
             if (lattice && !tab.empty()) {
                 int16_t* d_lut = nullptr;
                 unsigned int* d_delta = nullptr;
                 CPD_TRY(dev_alloc(&d_lut, sizeof(int16_t) * lut.size(), st));
-                CPD_TRY(dev_alloc(&d_delta, sizeof(unsigned int) * kMixedGeneric, st));
+                CPD_TRY(dev_alloc(&d_delta, sizeof(unsigned int) * kDeltaSlots, st));
                 CPD_TRY(cudaMemcpyAsync(d_lut, lut.data(), sizeof(int16_t) * lut.size(),
                                         cudaMemcpyHostToDevice, st));
-                CPD_TRY(cudaMemsetAsync(d_delta, 0xff, sizeof(unsigned int) * kMixedGeneric, st));
+                CPD_TRY(cudaMemcpyAsync(d_delta, delta.data(), sizeof(unsigned int) * kDeltaSlots,
+                                        cudaMemcpyHostToDevice, st));
                 LatticeLut L;
                 for (int d = 0; d < 3; ++d) {
                     L.h[d] = h[d];
@@ -1821,10 +1871,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 }
                 L.lut = d_lut;
                 tr.mark("spacing+table", st);
+                if (by_codes) {
                 k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
                 launches++;
                 tr.mark("code", st);
-                std::vector<unsigned int> delta(kMixedGeneric);
                 CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
                                         cudaMemcpyDeviceToHost, st));
                 {
@@ -1869,15 +1919,15 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                                                 cudaMemcpyHostToDevice, st));
                     }
                 }
-                if (!fp32)
-                    CPD_TRY(lattice_cell_layout(p, h, tab, rows, m, delta, d_delta, launches, st));
+                }
                 CPD_TRY(cudaStreamSynchronize(st));
                 for (size_t t = 0; t < tab.size(); ++t)
                     tab[t].delta = (int32_t)((long long)delta[t] - (1LL << 31));
-                CPD_TRY(cudaMemcpyAsync(m.table, tab.data(), sizeof(MixedStencil) * tab.size(),
-                                        cudaMemcpyHostToDevice, st));
+                if (fp32)
+                    CPD_TRY(cudaMemcpyAsync(m.table, tab.data(),
+                                            sizeof(MixedStencil) * tab.size(),
+                                            cudaMemcpyHostToDevice, st));
                 CPD_TRY(cudaStreamSynchronize(st));
-                CPD_TRY(dev_free(d_lut, st));
                 m.ntab = (int)tab.size();
                 for (int d = 0; d < 3; ++d) m.h[d] = h[d];
                 const int nmask = (m.ntab + 31) / 32;
@@ -1885,10 +1935,16 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 m.bytes += sizeof(uint32_t) * nmask * np;
                 CPD_TRY(dev_alloc(&m.warp_pmask, sizeof(uint32_t) * nmask * nwarps, st));
                 m.bytes += sizeof(uint32_t) * nmask * nwarps;
-                k_row_masks<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), d_delta, m.code,
-                                                                 m.ntab, m.pmask, m.warp_kind,
-                                                                 m.warp_pmask, m.gcell);
+                if (by_codes)
+                    k_row_masks<false><<<blocks_for(rows), kBlock, 0, st>>>(
+                        p, pd.view(), d_delta, m.code, m.ntab, m.pmask, m.warp_kind,
+                        m.warp_pmask, m.gcell, L);
+                else
+                    k_row_masks<true><<<blocks_for(rows), kBlock, 0, st>>>(
+                        p, pd.view(), d_delta, m.code, m.ntab, m.pmask, m.warp_kind,
+                        m.warp_pmask, m.gcell, L);
                 launches++;
+                CPD_TRY(dev_free(d_lut, st));
                 CPD_TRY(dev_free(d_delta, st));
                 tr.mark("masks", st);
                 const int64_t nw = (rows + 31) / 32;

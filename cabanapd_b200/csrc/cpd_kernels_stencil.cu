@@ -194,14 +194,14 @@ __device__ __forceinline__ void stencil_bond64(const StencilEntry64& e, const do
 // ew[w] = entry 32 w + k). Kind-2 rows hold the whole table, so bond slot k
 // is entry k; other stencil rows hold the entries of their presence mask in
 // table order, so their s-th present entry is bond slot s.
-template <bool FRACTURE>
+template <bool FRACTURE, int NW = 4>
 __device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilRows& sr,
                                                int ntab, int nwords, int kind, int64_t i,
-                                               int64_t np, uint32_t (&ew)[4])
+                                               int64_t np, uint32_t (&ew)[NW])
 {
-    uint32_t pm[4];
+    uint32_t pm[NW];
 #pragma unroll
-    for (int w = 0; w < 4; ++w) {
+    for (int w = 0; w < NW; ++w) {
         uint32_t full = 0u;
         if (w < nwords) {
             const int rem = ntab - 32 * w;
@@ -211,34 +211,34 @@ __device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilR
     }
     if (!FRACTURE) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w) ew[w] = pm[w];
+        for (int w = 0; w < NW; ++w) ew[w] = pm[w];
         return;
     }
     // The list holds ceil(max_n / 32) bond-state words per row, which can be
     // fewer than the table's words (a thin body holds only part of the
     // table): words past the list's are absent, not read.
     const int lwords = (nl.max_n + 31) >> 5;
-    uint32_t mw[4];
+    uint32_t mw[NW];
     int cnt = 0, intact = 0;
 #pragma unroll
-    for (int w = 0; w < 4; ++w) {
+    for (int w = 0; w < NW; ++w) {
         mw[w] = (w < nwords && w < lwords) ? nl.mu[(int64_t)w * np + i] : 0u;
         cnt += __popc(pm[w]);
         intact += __popc(mw[w]);
     }
     if (kind == 2) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w) ew[w] = mw[w] & pm[w];
+        for (int w = 0; w < NW; ++w) ew[w] = mw[w] & pm[w];
     } else if (intact == cnt) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w) ew[w] = pm[w];
+        for (int w = 0; w < NW; ++w) ew[w] = pm[w];
     } else {
         // Slot order -> entry order: the s-th present entry takes the s-th
         // bit of the slot-order words.
         int sw = 0, sb = 0;
         uint32_t src = mw[0];
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
+        for (int w = 0; w < NW; ++w) {
             uint32_t out = 0u, q = pm[w];
             while (q) {
                 const int b = __ffs(q) - 1;
@@ -248,7 +248,10 @@ __device__ __forceinline__ void row_entry_bits(const EllView& nl, const StencilR
                 if (++sb == 32) {
                     sb = 0;
                     ++sw;
-                    src = sw == 1 ? mw[1] : (sw == 2 ? mw[2] : mw[3]);
+                    src = 0u;
+#pragma unroll
+                    for (int v = 1; v < NW; ++v)
+                        if (sw == v) src = mw[v];
                 }
             }
             ew[w] = out;
@@ -291,13 +294,16 @@ __device__ __forceinline__ void clear_bond_bit(const EllView& nl, const StencilR
 // part writes W_i and phi_i = 1 - vol_sums[intact] / vol_sums[bonds] after
 // the step's bond breaking, and per warp the sums of W_i vol_i and phi_i to
 // ep.energy_part, as k_pmb_stencil32 does.
-template <bool FRACTURE, bool UNIFORM, int K0, int K1, int NP, bool LAST, bool ENERGY = false>
+// TAB: the table's size (Stencil64 or Stencil64W); its bond-bit words NW.
+template <bool FRACTURE, bool UNIFORM, int K0, int K1, int NP, bool LAST, bool ENERGY = false,
+          class TAB = Stencil64>
 __global__ void __launch_bounds__(kBlock, 4)
     k_pmb_stencil64(ParticleView p, EllView nl, StencilRows sr,
                     const double4* __restrict__ U4, double4* __restrict__ FPART,
-                    StepEpilogue ep, const Stencil64 st, const double* __restrict__ vol_sums,
+                    StepEpilogue ep, const TAB st, const double* __restrict__ vol_sums,
                     const int32_t* __restrict__ CELL)
 {
+    constexpr int NW = (int)(sizeof(st.e) / sizeof(st.e[0])) / 32;
     constexpr bool SUMS = ENERGY && LAST;
     const int lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
@@ -310,8 +316,8 @@ __global__ void __launch_bounds__(kBlock, 4)
     if (i < p.n) {
     const int64_t np = p.npad;
     const int kind = sr.warp_kind[warp];
-    uint32_t ew[4];
-    row_entry_bits<FRACTURE>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
+    uint32_t ew[NW];
+    row_entry_bits<FRACTURE, NW>(nl, sr, st.ntab, st.nwords, kind, i, np, ew);
     // Row i's gather record: by lattice cell, or by row.
     const int64_t rec = CELL ? (int64_t)CELL[i] : i;
     const double4 ui = U4[rec];
@@ -324,7 +330,9 @@ __global__ void __launch_bounds__(kBlock, 4)
         fz = fp.z;
         if (ENERGY) wsum = fp.w;
     }
-    uint32_t pend[4] = {0u, 0u, 0u, 0u};
+    uint32_t pend[NW];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) pend[w] = 0u;
     // Fully unrolled, every entry of the range for every row: an absent entry
     // (no bit in ew) reads the record at i + delta_k (a neighbour, or a zero
     // guard record) and adds nothing, which costs less than a branch per
@@ -344,12 +352,15 @@ __global__ void __launch_bounds__(kBlock, 4)
                                             fx, fy, fz, st.sh, ENERGY ? st.kw[k] : 0.0, &wsum);
     }
     int broken = 0;
-    if (pend[0] | pend[1] | pend[2] | pend[3]) {
+    uint32_t anyp = 0u;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) anyp |= pend[w];
+    if (anyp) {
         // Deferred bonds: the reference's exact test and force.
         double f[3] = {fx, fy, fz};
         const bool nofail_i = FRACTURE ? (p.nofail[i] != 0) : false;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
+        for (int w = 0; w < NW; ++w) {
             uint32_t q = pend[w];
             while (q) {
                 const int b = __ffs(q) - 1;
@@ -378,8 +389,9 @@ __global__ void __launch_bounds__(kBlock, 4)
             p.W[i] = wsum;
             Phi_i = wsum * p.vol[i];
             if (FRACTURE) {
-                const int intact =
-                    __popc(ew[0]) + __popc(ew[1]) + __popc(ew[2]) + __popc(ew[3]) - broken;
+                int intact = -broken;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) intact += __popc(ew[w]);
                 dmg_i = 1 - vol_sums[intact] / vol_sums[nl.count[i]];
                 p.phi[i] = dmg_i;
             }
@@ -551,6 +563,8 @@ void free_stencil64(MixedState& m, cudaStream_t st)
 {
     delete m.st64;
     m.st64 = nullptr;
+    delete m.st64w;
+    m.st64w = nullptr;
     if (m.u4_base) dev_free(m.u4_base, st);
     if (m.u4_alt_base) dev_free(m.u4_alt_base, st);
     if (m.f64part) dev_free(m.f64part, st);
@@ -559,16 +573,20 @@ void free_stencil64(MixedState& m, cudaStream_t st)
     m.guard = 0;
 }
 
-bool stencil64_ready(const MixedState& m) { return m.st64 != nullptr && m.u4 && m.u4_alt; }
-
-
-bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
-                       const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
-                       std::string& err)
+bool stencil64_ready(const MixedState& m)
 {
-    free_stencil64(m, st);
-    if (md.pd != CPD_PD_PMB || ntab <= 0 || ntab > kStencilMax) return false;
-    Stencil64* S = new Stencil64();
+    return (m.st64 != nullptr || m.st64w != nullptr) && m.u4 && m.u4_alt;
+}
+
+
+namespace {
+
+// Fills the FP64 table S from the lattice offsets; returns the largest
+// |delta| of its entries.
+template <int N>
+int64_t fill_stencil64(const Model& md, const double* h, const MixedStencil* tab, int ntab,
+                       const MixedState& m, Stencil64T<N>* S)
+{
     S->ntab = ntab;
     S->nwords = (ntab + 31) / 32;
     S->bbc = md.bond_break_coeff;
@@ -621,7 +639,28 @@ bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
         e.khi = qwin > 0.0 ? hi_word(qwin * (double)x2) : 0u;
         G = std::max<int64_t>(G, std::abs((int64_t)e.doff));
     }
-    m.st64 = S;
+    return G;
+}
+
+}  // namespace
+
+bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
+                       const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
+                       std::string& err)
+{
+    free_stencil64(m, st);
+    if (md.pd != CPD_PD_PMB || ntab <= 0 || ntab > kStencilMaxWide) return false;
+    int64_t G = 0;
+    if (ntab <= kStencilMax) {
+        m.st64 = new Stencil64();
+        G = fill_stencil64(md, h, tab, ntab, m, m.st64);
+    } else {
+        // The wide walk (four launches of 64 entries) takes one particle
+        // volume only.
+        if (m.vol_sums == nullptr) return false;
+        m.st64w = new Stencil64W();
+        G = fill_stencil64(md, h, tab, ntab, m, m.st64w);
+    }
     m.guard = G + 32;
     // Records by lattice cell (m.gcell) or by row.
     const size_t recs = (size_t)((m.gcell ? m.grid_cells : p.npad) + 2 * m.guard);
@@ -748,6 +787,34 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
         const StencilRows sr{m.warp_kind, m.pmask, m.stencil_list, m.nstencil};
         const int g = (int)((m.nstencil + kBlock / 32 - 1) / (kBlock / 32));
         const bool uniform = m.vol_sums != nullptr;
+        if (m.st64w) {
+            // Tables past 128 entries (a horizon of 4 spacings: 256): four
+            // launches of 64 entries, the partial force passed on between
+            // them; one particle volume.
+            const Stencil64W& W = *m.st64w;
+#define CPD_ST64W(F, NP)                                                                      \
+    do {                                                                                      \
+        k_pmb_stencil64<F, true, 0, 64, NP, false, false, Stencil64W>                         \
+            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
+        k_pmb_stencil64<F, true, 64, 128, NP, false, false, Stencil64W>                       \
+            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
+        k_pmb_stencil64<F, true, 128, 192, NP, false, false, Stencil64W>                      \
+            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
+        k_pmb_stencil64<F, true, 192, 256, NP, true, false, Stencil64W>                       \
+            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
+    } while (0)
+            if (md.fracture) {
+                if (W.np == 8) CPD_ST64W(true, 8); else CPD_ST64W(true, 9);
+            } else {
+                CPD_ST64W(false, 9);
+            }
+#undef CPD_ST64W
+            launched += 4;
+            if (m.nirregular > 0)
+                launched += launch_pd_force_fast(p, nl, md, ep, st, m.irregular_list,
+                                                 m.nirregular);
+            return launched;
+        }
         const Stencil64& S = *m.st64;
         // Two launches over the table's halves (entries 0-63, then 64 on):
         // the first stores its partial force and broken count per row, the

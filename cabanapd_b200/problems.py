@@ -166,20 +166,22 @@ def displacement_profile(prob, u, profile_dim=0, displacement_dim=None):
     return x[on, profile_dim], u[on, displacement_dim]
 
 
-def plate_impact(num_cells=(800, 400, 36), steps=2000, v0=16.5, size=(0.2, 0.1, 0.009)):
+def plate_impact(num_cells=(800, 400, 36), steps=2000, v0=16.5, size=(0.2, 0.1, 0.009),
+                 horizon_factor=3.01):
     """PMB brittle fracture, double-notched plate impact (Kalthoff-Winkler
     layout of examples/mechanics/kalthoff_winkler.cpp): plate
     0.2 x 0.1 x 0.009 m, delta = 3.01 dx, E = 191 GPa, nu = 0.25,
     rho = 8000, G0 = 22170, two 0.05 m notches from the left edge at
     y = +-0.025, v_x = v0 on the strip between them held by a zero-force BC.
     `size` scales the plate (notches and strip in proportion), e.g. for a
-    small plate at the full plate's spacing.
+    small plate at the full plate's spacing; `horizon_factor` is delta / dx
+    (the reference's example decks use 4).
     """
     size = [float(s) for s in size]
     low = [-0.5 * s for s in size]
     high = [0.5 * s for s in size]
     x, vol, h = lattice(low, high, num_cells)
-    horizon = 3.01 * h[0]
+    horizon = horizon_factor * h[0]
     E, nu, rho0, G0 = 191e9, 0.25, 8000.0, 22170.0
     K = E / (3.0 * (1.0 - 2.0 * nu))
     dt = 0.5 * critical_timestep(h[0], h[1], h[2], int(math.floor(horizon / h[0])),

@@ -537,6 +537,31 @@ def test_stencil_kernels_plate_against_oracle(cuda, oracle, precision, body):
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
+def test_fp64_stencil_at_a_four_spacing_horizon(cuda, oracle):
+    """A horizon of four spacings (the reference's example decks): 256 table
+    entries, the FP64 stencil walk in four launches of 64, rows coded from
+    the positions; within 1e-12 of the oracle with identical bonds over 120
+    steps, every warp on the stencil kernel."""
+    prob = P.plate_impact(num_cells=(96, 48, 8), steps=120, v0=60.0,
+                          size=(0.2, 0.1, 0.2 * 8 / 96), horizon_factor=4.0)
+    g = cuda.System(dict(prob["params"], precision=1))
+    o = oracle.OracleSystem(prob["params"])
+    P.setup(g, prob)
+    P.setup(o, prob)
+    warps, irregular, entries = g.stencil_stats()
+    assert entries == 256 and irregular == 0 and warps == len(prob["x"]) // 32
+    for _ in range(3):
+        g.run(40)
+        o.run(40)
+        assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
+        for fld in ("u", "v", "f"):
+            assert _nrel(g.get(fld), o.get(fld)) <= 1e-12, fld
+        wg, dg = g.compute_energy()
+        wo, do = o.compute_energy()
+        assert _rel(wg, wo) <= 1e-12 and _rel(dg, do) <= 1e-12
+    assert (o.neighbors()[2] == 0).sum() > 0
+
+
 def test_mixed_elastic_wave(cuda, oracle):
     prob = P.elastic_wave_pmb(n=41, steps=100)
     g, o = _pair_mixed(cuda, oracle, prob)
