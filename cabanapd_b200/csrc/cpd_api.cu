@@ -181,6 +181,9 @@ struct cpd_system {
     MixedU* u2_alt_base = nullptr;  // allocation: u2_alt with the split's guard records
     bool neighbors_built = false;
     bool initialized = false;
+    // CPD_MIXED PMB whose lattice table is past the byte codes (over 253
+    // entries: a horizon of four spacings): the FP64 stencil kernels run it.
+    bool mixed_via_fp64 = false;
     // The batch that advances this system (cpd_batch_create); while set,
     // calls that change the system's state are refused.
     const void* batch = nullptr;
@@ -435,7 +438,7 @@ cpd_status timed_end(cpd_system* s, cudaEvent_t e0)
 bool wants_mixed(const cpd_system* s)
 {
     return s->params.precision == CPD_MIXED && s->md.contact == CPD_CONTACT_NONE &&
-           (s->md.pd == CPD_PD_PMB || s->md.pd == CPD_PD_LPS);
+           (s->md.pd == CPD_PD_PMB || s->md.pd == CPD_PD_LPS) && !s->mixed_via_fp64;
 }
 
 bool use_mixed(const cpd_system* s)
@@ -450,8 +453,8 @@ bool use_mixed(const cpd_system* s)
 // from the positions' rounded differences (~1e-14) into errors above 1e-12.
 bool wants_stencil64(const cpd_system* s)
 {
-    return s->params.precision == CPD_FP64 && s->md.contact == CPD_CONTACT_NONE &&
-           s->md.pd == CPD_PD_PMB;
+    return (s->params.precision == CPD_FP64 || s->mixed_via_fp64) &&
+           s->md.contact == CPD_CONTACT_NONE && s->md.pd == CPD_PD_PMB;
 }
 
 bool use_stencil64(const cpd_system* s)
@@ -1208,6 +1211,7 @@ cpd_status cpd_build_neighbors(cpd_system* s)
     // set up below: it is allocated again when the step is next prepared.
     if (s->u2_alt_base) dev_free(s->u2_alt_base, s->stream);
     s->u2_alt = s->u2_alt_base = nullptr;
+    s->mixed_via_fp64 = false;
     if (has_pd(s)) {
         // CabanaPD_Neighbor.hpp:56-59: reference positions, cutoff + 1e-14.
         double hmin[3];
@@ -1221,13 +1225,33 @@ cpd_status cpd_build_neighbors(cpd_system* s)
             for (int d = 0; d < 3; ++d) s->pd.hmin[d] = hmin[d];
         s->launches += l;
         tr.mark("list", s->stream);
+        const int entries = wants_mixed(s) && s->md.pd == CPD_PD_PMB
+                                ? lattice_table_entries(s->pd.hmin, s->md.horizon + 1e-14)
+                                : 0;
+        if (entries >= kMixedGeneric && entries <= kStencilMaxWide) {
+            // CPD_MIXED PMB at a horizon whose lattice table is past the byte
+            // codes (a horizon of four spacings: 256 entries): the mixed
+            // kernels would take FP32 positions on every bond, the FP64
+            // stencil kernel is faster there (1.04 vs 2.83 ms per step on a
+            // 1.44 M-particle plate) and exact to FP64. It runs when the
+            // lattice allows it.
+            s->mixed_via_fp64 = true;
+            l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, false, s->mixed,
+                              s->stream, err, &s->md);
+            if (l < 0) return set_error(CPD_ERR_CUDA, "stencil set-up: " + err);
+            s->launches += l;
+            if (!stencil64_ready(s->mixed)) {
+                free_mixed(s->mixed, s->stream);
+                s->mixed_via_fp64 = false;
+            }
+        }
         if (wants_mixed(s)) {
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, is_lps(s), s->mixed,
                               s->stream, err, nullptr,
                               s->md.pd == CPD_PD_PMB ? &s->md : nullptr);
             if (l < 0) return set_error(CPD_ERR_CUDA, "mixed-precision set-up: " + err);
             s->launches += l;
-        } else if (wants_stencil64(s)) {
+        } else if (wants_stencil64(s) && !s->mixed_via_fp64) {
             l = prepare_mixed(view(s), s->pd, s->md.horizon + 1e-14, false, s->mixed,
                               s->stream, err, &s->md);
             if (l < 0) return set_error(CPD_ERR_CUDA, "stencil set-up: " + err);

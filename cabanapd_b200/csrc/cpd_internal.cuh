@@ -465,6 +465,9 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                   const Model* fp64_stencil = nullptr, const Model* md_pmb = nullptr);
 // FP64 stencil path (cpd_kernels_stencil.cu).
 // Builds m.st64 and the gather records (false: the stencil does not apply).
+// Entries of the lattice table for per-axis spacings h within cutoff (the
+// offsets prepare_mixed tabulates).
+int lattice_table_entries(const double* h, double cutoff);
 bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
                        const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
                        std::string& err);

@@ -1731,6 +1731,26 @@ cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
 #undef CPD_RET
 }  // namespace
 
+int lattice_table_entries(const double* h, double cutoff)
+{
+    int half[3];
+    for (int d = 0; d < 3; ++d) {
+        if (!(h[d] > 1e-6 * cutoff) || !std::isfinite(h[d])) return 0;
+        half[d] = (int)std::floor(cutoff / h[d] + 1e-9);
+    }
+    int n = 0;
+    for (int c = -half[2]; c <= half[2]; ++c)
+        for (int b = -half[1]; b <= half[1]; ++b)
+            for (int a = -half[0]; a <= half[0]; ++a) {
+                if (a == 0 && b == 0 && c == 0) continue;
+                const double vx = a * h[0], vy = b * h[1], vz = c * h[2];
+                if (std::sqrt(vx * vx + vy * vy + vz * vz) <= cutoff * (1.0 + 1e-9) &&
+                    ++n > kStencilMaxWide)
+                    return n;  // past every table: the count no longer matters
+            }
+    return n;
+}
+
 int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, bool lps,
                   MixedState& m, cudaStream_t st, std::string& err, const Model* fp64_stencil,
                   const Model* md_pmb)

@@ -562,6 +562,25 @@ def test_fp64_stencil_at_a_four_spacing_horizon(cuda, oracle):
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
+def test_mixed_at_a_four_spacing_horizon_runs_the_fp64_stencil(cuda):
+    """CPD_MIXED PMB at a horizon of four spacings (a 256-entry table, past
+    the mixed path's byte codes) runs the FP64 stencil kernels: the same
+    bits as CPD_FP64 on the same plate."""
+    prob = P.plate_impact(num_cells=(96, 48, 8), steps=60, v0=60.0,
+                          size=(0.2, 0.1, 0.2 * 8 / 96), horizon_factor=4.0)
+    runs = {}
+    for prec in (1, MIXED):
+        s = cuda.System(dict(prob["params"], precision=prec))
+        P.setup(s, prob)
+        assert s.stencil_stats()[2] == 256
+        s.run(60)
+        runs[prec] = s
+    for fld in ("u", "v", "f"):
+        assert np.array_equal(runs[1].get(fld), runs[MIXED].get(fld)), fld
+    assert np.array_equal(runs[1].neighbors()[2], runs[MIXED].neighbors()[2])
+    assert runs[1].compute_energy() == runs[MIXED].compute_energy()
+
+
 def test_mixed_elastic_wave(cuda, oracle):
     prob = P.elastic_wave_pmb(n=41, steps=100)
     g, o = _pair_mixed(cuda, oracle, prob)
