@@ -468,6 +468,10 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
 // Entries of the lattice table for per-axis spacings h within cutoff (the
 // offsets prepare_mixed tabulates).
 int lattice_table_entries(const double* h, double cutoff);
+// The FP64 stencil records' layout a body would take (0: not a lattice of
+// distinct cells; 1: one box of lattice lines in row order; 2: by lattice
+// cell), from its positions and spacings h; synchronises the stream.
+int lattice_layout_probe(const ParticleView& p, const double* h, cudaStream_t st);
 bool prepare_stencil64(const ParticleView& p, const Model& md, const double* h,
                        const MixedStencil* tab, int ntab, MixedState& m, cudaStream_t st,
                        std::string& err);

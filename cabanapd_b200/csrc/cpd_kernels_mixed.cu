@@ -1731,6 +1731,20 @@ cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
 #undef CPD_RET
 }  // namespace
 
+int lattice_layout_probe(const ParticleView& p, const double* h, cudaStream_t st)
+{
+    // The layout test alone: no table deltas are kept and the system's
+    // state is left as it was.
+    MixedState probe;
+    std::vector<MixedStencil> none;
+    std::vector<unsigned int> delta;
+    int launches = 0, layout = 0;
+    const cudaError_t e = lattice_cell_layout(p, h, none, p.n - p.frozen, probe, delta,
+                                              launches, layout, st);
+    if (probe.gcell) dev_free(probe.gcell, st);
+    return e == cudaSuccess ? layout : 0;
+}
+
 int lattice_table_entries(const double* h, double cutoff)
 {
     int half[3];

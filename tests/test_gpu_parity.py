@@ -488,25 +488,29 @@ def _with_hole(prob, centre=(0.03, 0.0), radius=0.008):
     return _with_void(prob, np.nonzero(inside)[0])
 
 
-@pytest.mark.parametrize("body", ["pair", "void", "hole"])
+@pytest.mark.parametrize("body", ["pair", "void", "hole", "void_and_pair"])
 @pytest.mark.parametrize("precision", [1, MIXED])
 def test_stencil_kernels_plate_against_oracle(cuda, oracle, precision, body):
     """The lattice-stencil bond kernels (FP64: the two-launch walk; MIXED:
     the FP32 walk on the split records) on a cubic notched plate: beside an
     off-lattice pair (one warp on the general kernels), with two empty
-    lattice sites, and with a cylindrical hole through the plate. With
-    empty sites the particles' index deltas vary: FP64 then gathers its
-    records by lattice cell and keeps every row on the stencil kernel;
-    MIXED keeps the rows whose deltas are the majority's. FP64 within 1e-12
-    of the oracle with identical bonds over 160 steps; MIXED within the
-    mixed bars, bonds identical."""
+    lattice sites, with a cylindrical hole through the plate, and with both
+    empty sites and the pair. With empty sites the particles' index deltas
+    vary: on a lattice of distinct cells FP64 gathers its records by cell
+    and keeps every row on the stencil kernel, and MIXED runs that FP64
+    kernel; with the pair off the lattice as well, both keep the rows whose
+    deltas are the majority's. FP64 (and MIXED on the FP64 kernel) within
+    1e-12 of the oracle with identical bonds over 160 steps; MIXED on its
+    own kernels within the mixed bars, bonds identical."""
     plate = _cubic_plate(96, 8, steps=160)
     if body == "pair":
         prob = _with_offlattice_pair(plate)
     elif body == "void":
         prob = _with_void(plate, [13000, 13001])
-    else:
+    elif body == "hole":
         prob = _with_hole(plate)
+    else:
+        prob = _with_offlattice_pair(_with_void(plate, [13000, 13001]))
     g = cuda.System(dict(prob["params"], precision=precision))
     o = oracle.OracleSystem(prob["params"])
     P.setup(g, prob)
@@ -514,20 +518,21 @@ def test_stencil_kernels_plate_against_oracle(cuda, oracle, precision, body):
     warps, irregular, entries = g.stencil_stats()
     assert entries == 122
     rows_warps = (len(prob["x"]) + 31) // 32
+    fp64_kernels = precision == 1 or body in ("void", "hole")
     if body == "pair":
         assert warps == len(plate["x"]) // 32 and irregular == 1
-    elif precision == 1:
+    elif body in ("void", "hole"):
         assert warps == rows_warps and irregular == 0
     else:
         # The rows whose neighbours lie across an empty site in index
-        # order leave the stencil kernel (for the void: the rows within
-        # three planes of it, most of this 8-plane plate).
+        # order leave the stencil kernel (the rows within three planes of
+        # the void, most of this 8-plane plate).
         assert irregular > 0 and warps > 0.1 * rows_warps
     for _ in range(4):
         g.run(40)
         o.run(40)
         assert np.array_equal(g.neighbors()[2], o.neighbors()[2])
-        if precision == 1:
+        if fp64_kernels:
             for fld in ("u", "v", "f"):
                 assert _nrel(g.get(fld), o.get(fld)) <= 1e-12, fld
         else:
