@@ -792,16 +792,27 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
             // launches of 64 entries, the partial force passed on between
             // them; one particle volume.
             const Stencil64W& W = *m.st64w;
+            // Tables of up to 192 entries (unequal spacings at a 3-spacing
+            // horizon) stop after the third launch.
+            const bool t192 = W.ntab <= 192;
 #define CPD_ST64W(F, NP)                                                                      \
     do {                                                                                      \
         k_pmb_stencil64<F, true, 0, 64, NP, false, false, Stencil64W>                         \
             <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
         k_pmb_stencil64<F, true, 64, 128, NP, false, false, Stencil64W>                       \
             <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
-        k_pmb_stencil64<F, true, 128, 192, NP, false, false, Stencil64W>                      \
-            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
-        k_pmb_stencil64<F, true, 192, 256, NP, true, false, Stencil64W>                       \
-            <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
+        if (t192) {                                                                           \
+            k_pmb_stencil64<F, true, 128, 192, NP, true, false, Stencil64W>                   \
+                <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
+                                       m.gcell);                                              \
+        } else {                                                                              \
+            k_pmb_stencil64<F, true, 128, 192, NP, false, false, Stencil64W>                  \
+                <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
+                                       m.gcell);                                              \
+            k_pmb_stencil64<F, true, 192, 256, NP, true, false, Stencil64W>                   \
+                <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
+                                       m.gcell);                                              \
+        }                                                                                     \
     } while (0)
             if (md.fracture) {
                 if (W.np == 8) CPD_ST64W(true, 8); else CPD_ST64W(true, 9);
@@ -809,7 +820,7 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
                 CPD_ST64W(false, 9);
             }
 #undef CPD_ST64W
-            launched += 4;
+            launched += t192 ? 3 : 4;
             if (m.nirregular > 0)
                 launched += launch_pd_force_fast(p, nl, md, ep, st, m.irregular_list,
                                                  m.nirregular);
