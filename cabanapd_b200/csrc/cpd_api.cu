@@ -714,7 +714,7 @@ bool fused_energy_ok(const cpd_system* s)
     const MixedState& m = s->mixed;
     if (s->md.pd != CPD_PD_PMB || !m.vol_sums || m.nstencil <= 0) return false;
     if (use_mixed(s)) return m.st32 && m.u2;
-    return use_stencil64(s) && m.st64 && m.nirregular == 0;
+    return use_stencil64(s) && (m.st64 || m.st64w) && m.nirregular == 0;
 }
 
 // num_steps steps as: first half step, then one bond kernel per step whose

@@ -795,29 +795,35 @@ int launch_pd_force_stencil64(const ParticleView& p, const EllView& nl, const Mo
             // Tables of up to 192 entries (unequal spacings at a 3-spacing
             // horizon) stop after the third launch.
             const bool t192 = W.ntab <= 192;
-#define CPD_ST64W(F, NP)                                                                      \
+#define CPD_ST64W(F, NP, E)                                                                   \
     do {                                                                                      \
-        k_pmb_stencil64<F, true, 0, 64, NP, false, false, Stencil64W>                         \
+        k_pmb_stencil64<F, true, 0, 64, NP, false, E, Stencil64W>                             \
             <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
-        k_pmb_stencil64<F, true, 64, 128, NP, false, false, Stencil64W>                       \
+        k_pmb_stencil64<F, true, 64, 128, NP, false, E, Stencil64W>                           \
             <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums, m.gcell);   \
         if (t192) {                                                                           \
-            k_pmb_stencil64<F, true, 128, 192, NP, true, false, Stencil64W>                   \
+            k_pmb_stencil64<F, true, 128, 192, NP, true, E, Stencil64W>                       \
                 <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
                                        m.gcell);                                              \
         } else {                                                                              \
-            k_pmb_stencil64<F, true, 128, 192, NP, false, false, Stencil64W>                  \
+            k_pmb_stencil64<F, true, 128, 192, NP, false, E, Stencil64W>                      \
                 <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
                                        m.gcell);                                              \
-            k_pmb_stencil64<F, true, 192, 256, NP, true, false, Stencil64W>                   \
+            k_pmb_stencil64<F, true, 192, 256, NP, true, E, Stencil64W>                       \
                 <<<g, kBlock, 0, st>>>(p, nl, sr, m.u4, m.f64part, ep, W, m.vol_sums,         \
                                        m.gcell);                                              \
         }                                                                                     \
     } while (0)
+            // An output step (ep.energy_part): the energy forms.
+            const bool en = ep.energy_part != nullptr;
             if (md.fracture) {
-                if (W.np == 8) CPD_ST64W(true, 8); else CPD_ST64W(true, 9);
+                if (W.np == 8) {
+                    if (en) CPD_ST64W(true, 8, true); else CPD_ST64W(true, 8, false);
+                } else {
+                    if (en) CPD_ST64W(true, 9, true); else CPD_ST64W(true, 9, false);
+                }
             } else {
-                CPD_ST64W(false, 9);
+                if (en) CPD_ST64W(false, 9, true); else CPD_ST64W(false, 9, false);
             }
 #undef CPD_ST64W
             launched += t192 ? 3 : 4;

@@ -567,6 +567,36 @@ def test_fp64_stencil_at_a_four_spacing_horizon(cuda, oracle):
     assert (o.neighbors()[2] == 0).sum() > 0
 
 
+def test_step_energy_at_a_four_spacing_horizon(cuda, oracle):
+    """The output step in one call on the wide FP64 walk (256 entries, four
+    launches, the partial energy passed on with the partial force): states,
+    bonds and phi as step + energy bit for bit, W to FP64 rounding, totals
+    against the oracle."""
+    prob = P.plate_impact(num_cells=(96, 48, 8), steps=60, v0=60.0,
+                          size=(0.2, 0.1, 0.2 * 8 / 96), horizon_factor=4.0)
+    a = cuda.System(dict(prob["params"], precision=1))
+    b = cuda.System(dict(prob["params"], precision=1))
+    o = oracle.OracleSystem(prob["params"])
+    for s_ in (a, b, o):
+        P.setup(s_, prob)
+    assert a.stencil_stats()[2] == 256
+    for _ in range(3):
+        la, lb = a.kernel_launches(), b.kernel_launches()
+        wa, da = a.step_energy(20)
+        b.step(20)
+        wb, db = b.compute_energy()
+        o.run(20)
+        wo, do = o.compute_energy()
+        assert a.kernel_launches() - la < b.kernel_launches() - lb
+        for fld in ("u", "v", "f", "phi"):
+            assert np.array_equal(a.get(fld), b.get(fld)), fld
+        assert not np.array_equal(a.get("W"), b.get("W"))
+        assert _nrel(a.get("W"), b.get("W")) <= 1e-13
+        assert _rel(wa, wb) <= 1e-13 and _rel(da, db) <= 1e-13
+        assert _rel(wa, wo) <= 1e-12 and _rel(da, do) <= 1e-12
+    assert da > 0
+
+
 def test_mixed_at_a_four_spacing_horizon_runs_the_fp64_stencil(cuda):
     """CPD_MIXED PMB at a horizon of four spacings (a 256-entry table, past
     the mixed path's byte codes) runs the FP64 stencil kernels: the same
