@@ -54,6 +54,7 @@ import numpy as np  # noqa: E402
 from cabanapd_b200 import problems as P  # noqa: E402
 
 PLATE_CELLS = (800, 400, 36)
+HORIZON_FACTOR = 3.01  # delta / dx of the plate
 LPS_CELLS = (1000, 400, 20)   # LPS random-notch box, dx = 1e-4: 8.0 M particles
 PLATE_1P2M_CELLS = (376, 188, 17)  # the ~1.2 M-particle variant of the plate
 WAVE_CELLS = 41               # PMB elastic wave, 41^3 particles
@@ -212,7 +213,7 @@ def visible_index(local):
 
 # ---------------------------------------------------------------------------
 def cpu_sample_problem():
-    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=1)
+    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=1, horizon_factor=HORIZON_FACTOR)
     nx, ny, nz = PLATE_CELLS
     ix = np.arange(prob["x"].shape[0]) % nx
     keep = ix < CPU_SLAB_X
@@ -563,7 +564,8 @@ def run_gpu(args, world, rank, local, pg):
     import cabanapd_b200
     device = local
     torch.cuda.set_device(device)
-    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps)
+    prob = P.plate_impact(num_cells=PLATE_CELLS, steps=args.steps,
+                          horizon_factor=HORIZON_FACTOR)
     stream = torch.cuda.Stream(device=device)
     precs = [args.precision] if args.precision != "mixed" or args.only else ["mixed", "fp64"]
     systems, res = {}, {}
@@ -616,7 +618,8 @@ def run_gpu(args, world, rank, local, pg):
         "dtype": {"mixed": "f32 bonds + f64 state", "fp64": "f64", "exact": "f64"}[head],
         "data": "synthetic",
         "config": {"workload": "pmb_fracture_notched_plate_impact",
-                   "plate_cells": list(PLATE_CELLS), "particles_per_gpu": n,
+                   "plate_cells": list(PLATE_CELLS), "horizon_over_dx": HORIZON_FACTOR,
+                   "particles_per_gpu": n,
                    "bonds_per_gpu": bonds, "precision": head,
                    "l2": "inputs larger than L2 (neighbour list %.1f GB)" % (4 * bonds / 1e9),
                    "particle_steps_per_s": particle_steps},
@@ -846,6 +849,8 @@ def main():
     ap.add_argument("--cells", default=None,
                     help="cells nx,ny,nz of the plate (or, with --only-other, of that "
                          "workload) for profiling on a smaller case")
+    ap.add_argument("--horizon-factor", type=float, default=3.01,
+                    help="delta / dx of the plate (for profiling the wide-table walk: 4)")
     ap.add_argument("--skip-serve", action="store_true", help="omit the served-stream leg")
     ap.add_argument("--skip-others", action="store_true",
                     help="omit the LPS-box and DEM-packing measurements")
@@ -868,7 +873,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    global PLATE_CELLS, LPS_CELLS, DEM_DIMS, PLATE_1P2M_CELLS, WAVE_CELLS
+    global PLATE_CELLS, LPS_CELLS, DEM_DIMS, PLATE_1P2M_CELLS, WAVE_CELLS, HORIZON_FACTOR
+    HORIZON_FACTOR = args.horizon_factor
     if args.cells:
         cells = tuple(int(c) for c in args.cells.split(","))
         if args.only_other == "lps":
