@@ -246,28 +246,39 @@ __global__ void __launch_bounds__(kBlock)
                     uint32_t* __restrict__ occ, unsigned int* flags, unsigned long long* ext)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double t[3] = {(x[i] - x0.x) * hinv.x, (x[np + i] - x0.y) * hinv.y,
-                         (x[2 * np + i] - x0.z) * hinv.z};
-    const int ncs[3] = {nc.x, nc.y, nc.z};
-    long long a[3];
-    bool ok = true;
-    for (int d = 0; d < 3; ++d) {
-        const double r = rint(t[d]);
-        if (fabs(t[d] - r) > 1e-6 || r < 0.0 || r >= (double)ncs[d]) ok = false;
-        a[d] = (long long)r;
+    // Every lane reaches the warp's min / max below (one atomic per warp).
+    unsigned long long lo = ~0ull, hi = 0ull;
+    if (i < n) {
+        const double t[3] = {(x[i] - x0.x) * hinv.x, (x[np + i] - x0.y) * hinv.y,
+                             (x[2 * np + i] - x0.z) * hinv.z};
+        const int ncs[3] = {nc.x, nc.y, nc.z};
+        long long a[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+            const double r = rint(t[d]);
+            if (fabs(t[d] - r) > 1e-6 || r < 0.0 || r >= (double)ncs[d]) ok = false;
+            a[d] = (long long)r;
+        }
+        if (!ok) {
+            atomicAdd(flags, 1u);
+            cell[i] = 0;
+        } else {
+            const long long g = a[0] + (long long)nc.x * (a[1] + (long long)nc.y * a[2]);
+            cell[i] = (int32_t)g;
+            if (atomicAdd(occ + g, 1u) != 0u) atomicAdd(flags + 1, 1u);
+            lo = hi = (unsigned long long)(g - i + (1LL << 62));
+        }
     }
-    if (!ok) {
-        atomicAdd(flags, 1u);
-        cell[i] = 0;
-        return;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long l2 = __shfl_xor_sync(0xffffffffu, lo, o);
+        const unsigned long long h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = l2 < lo ? l2 : lo;
+        hi = h2 > hi ? h2 : hi;
     }
-    const long long g = a[0] + (long long)nc.x * (a[1] + (long long)nc.y * a[2]);
-    cell[i] = (int32_t)g;
-    if (atomicAdd(occ + g, 1u) != 0u) atomicAdd(flags + 1, 1u);
-    const unsigned long long e = (unsigned long long)(g - i + (1LL << 62));
-    atomicMin(ext, e);
-    atomicMax(ext + 1, e);
+    if ((threadIdx.x & 31) == 0 && lo != ~0ull) {
+        atomicMin(ext, lo);
+        atomicMax(ext + 1, hi);
+    }
 }
 
 // Per row: first the delta check of every coded bond (a bond whose code's
