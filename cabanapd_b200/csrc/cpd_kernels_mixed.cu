@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(kBlock)
 // subset of the table); per warp: 2 if every row is the whole table, 3 if
 // every row is the same table subset (the subset is recorded for the warp),
 // 1 if every row is a table subset, else 0.
-// LUT: each bond's entry from the positions (L, as k_code_bonds does) with
-// no code array; else from the codes, which the delta check may rewrite.
+// LUT: each bond's entry from the positions (L, as k_code_bonds does),
+// written to code when it is given; else from the codes, which the delta
+// check may rewrite.
 template <bool LUT>
 __global__ void __launch_bounds__(kBlock)
     k_row_masks(ParticleView p, EllView nl, const unsigned int* delta, uint8_t* code, int ntab,
@@ -334,10 +335,11 @@ __global__ void __launch_bounds__(kBlock)
             // The delta of the records' layout: lattice cells or rows.
             const long long dij = gcell ? (long long)gcell[j] - (long long)gcell[i]
                                         : (long long)(j - i);
-            if (c != generic && (long long)delta[c] - (1LL << 31) != dij) {
-                c = generic;
-                if (!LUT) code[o] = (uint8_t)c;
-            }
+            if (c != generic && (long long)delta[c] - (1LL << 31) != dij) c = generic;
+            // The bond's code: rewritten when its delta fails, written in full
+            // when the codes come from the positions (the mixed path).
+            if (!LUT && c == generic) code[o] = (uint8_t)kMixedGeneric;
+            if (LUT && code) code[o] = (uint8_t)(c < kMixedGeneric ? c : kMixedGeneric);
             if (!subset) continue;
             if (c >= ntab || c <= prev) {
                 subset = false;
@@ -1893,10 +1895,21 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
             // FP64: when every particle sits on its own lattice cell, each
             // entry's delta comes from the geometry and rows are coded from
             // the positions (no per-bond codes); else the byte codes below.
+            // The mixed path takes the geometric deltas of a box in row
+            // order too (its FP32 records go by row), coding each bond in the
+            // mask pass itself.
             int layout = 0;
             std::vector<unsigned int> delta(kDeltaSlots, 0xffffffffu);
-            if (lattice && !tab.empty() && !fp32)
+            if (lattice && !tab.empty())
                 CPD_TRY(lattice_cell_layout(p, h, tab, rows, m, delta, launches, layout, st));
+            if (fp32 && layout == 2) {
+                CPD_TRY(dev_free(m.gcell, st));
+                m.gcell = nullptr;
+                m.grid_cells = 0;
+                m.bytes -= sizeof(int32_t) * (size_t)p.npad;
+                layout = 0;
+                std::fill(delta.begin(), delta.end(), 0xffffffffu);
+            }
             const bool by_codes = layout == 0;
             if (by_codes && (int)tab.size() >= kMixedGeneric) lattice = false;
             if (lattice && !tab.empty()) {
@@ -1986,8 +1999,8 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                         m.warp_pmask, m.gcell, L);
                 else
                     k_row_masks<true><<<blocks_for(rows), kBlock, 0, st>>>(
-                        p, pd.view(), d_delta, m.code, m.ntab, m.pmask, m.warp_kind,
-                        m.warp_pmask, m.gcell, L);
+                        p, pd.view(), d_delta, fp32 ? m.code : nullptr, m.ntab, m.pmask,
+                        m.warp_kind, m.warp_pmask, m.gcell, L);
                 launches++;
                 CPD_TRY(dev_free(d_lut, st));
                 CPD_TRY(dev_free(d_delta, st));
