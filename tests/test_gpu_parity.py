@@ -187,7 +187,7 @@ def test_hertz_regression_on_gpu(cuda, oracle, golden):
     assert s.contact_rebuilds() == o.contact_rebuilds()
 
 
-# DEM packings: the config 3 layout (non-overlapping, free flight over the
+# DEM packings: the 4 M-sphere packing's layout (non-overlapping, free flight over the
 # test's steps) and a compressed one (spacing 2.1 mm < 2 R_max: overlapping
 # pairs from the start, so the Hertz force law is exercised).
 DEM_CASES = {"free": dict(spacing=2.5e-3, dt=2e-6), "compressed": dict(spacing=2.1e-3, dt=1e-7)}
@@ -285,8 +285,8 @@ def test_errors_are_reported(cuda):
 # Throughput-form FP64 path (precision = CPD_FP64). On lattices the PMB bond
 # stage is the stencil kernel: stretch formed without the cancellation of
 # (r - xi)/xi from the exact lattice offsets, pair force from a polynomial
-# accurate to ~2e-16; elsewhere rsqrt-based bond lengths with FMA. Bars (the
-# north star's): per step, from the same state, forces and displacements
+# accurate to ~2e-16; elsewhere rsqrt-based bond lengths with FMA. Bars of
+# the throughput FP64 path: per step, from the same state, forces and displacements
 # within 1e-12 (norm-wise); broken-bond sets identical; totals within 1e-10
 # over a run. The reference's own rounding of s = (r - xi)/xi is ~1e-16
 # absolute per bond, and over a run that is what separates two correct FP64
@@ -352,7 +352,7 @@ def test_fast_elastic_wave(cuda, oracle):
 
 @pytest.mark.parametrize("problem", ["wave", "plate"])
 def test_fast_per_step_from_the_oracle_state(cuda, oracle, problem):
-    """The north star's per-step bar: from the oracle's state at several
+    """The throughput FP64 path's per-step bar: from the oracle's state at several
     points of a run, one GPU step gives u, v and f within 1e-12 (norm-wise)
     of the oracle's step, and the GPU's force of that state is within 1e-12
     of the oracle's."""
@@ -411,7 +411,7 @@ def test_fast_lps_random_notches(cuda, oracle):
 
 # ---------------------------------------------------------------------------
 # Mixed-precision path (precision = CPD_MIXED, PMB): FP32 bond arithmetic with
-# Kahan-compensated sums, FP64 integration. Bars (north star): displacement
+# Kahan-compensated sums, FP64 integration. Bars of the mixed path: displacement
 # <= 1e-6 relative to the FP64 oracle (norm-wise), broken-bond sets identical
 # (FP64 re-test within 1e-4 s0); velocities and forces <= 1e-5.
 MIXED = 2

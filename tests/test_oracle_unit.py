@@ -108,7 +108,7 @@ def test_model_constants(oracle):
 
 def test_critical_timestep_matches(oracle):
     """The package's Input.hpp restatement and the oracle's agree exactly,
-    and config 0's value is 1.7311e-2."""
+    and the 41^3 PMB elastic wave's value is 1.7311e-2."""
     dx = 1.0 / 41.0
     h = 3.0 * dx + 0.01 * dx
     a = critical_timestep(dx, dx, dx, 3, h, 1.0, 1.0)
