@@ -47,6 +47,20 @@ def test_neighbor_count(oracle, golden, m, num, den):
         assert expected == 122
 
 
+def test_four_spacing_horizon_holds_256_neighbours(oracle):
+    """A cubic lattice at a horizon of exactly four spacings (the reference's
+    example decks): interior rows hold the 256 lattice offsets within the
+    cutoff (horizon + 1e-14, the axis points at 4 spacings included), the
+    table size the wide FP64 stencil walk takes."""
+    prob = P.plate_impact(num_cells=(24, 12, 12), steps=1, v0=0.0,
+                          size=(0.2, 0.1, 0.1), horizon_factor=4.0)
+    s = oracle.OracleSystem(prob["params"])
+    P.setup(s, prob, init=False)
+    assert s.neighbor_stats()[0] == 256
+    assert P.plate_impact(num_cells=(24, 12, 12), steps=1, size=(0.2, 0.1, 0.1))[
+        "params"]["horizon"] == 3.01 * 0.2 / 24
+
+
 def test_neighbor_sets_bruteforce(oracle):
     """Every listed pair is within the cutoff and every pair within the cutoff
     is listed (all-pairs check on a jittered cloud)."""
