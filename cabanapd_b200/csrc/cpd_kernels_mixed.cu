@@ -1930,53 +1930,55 @@ int prepare_mixed(const ParticleView& p, const NeighborList& pd, double cutoff, 
                 L.lut = d_lut;
                 tr.mark("spacing+table", st);
                 if (by_codes) {
-                k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code, d_delta);
-                launches++;
-                tr.mark("code", st);
-                CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta, sizeof(unsigned int) * kMixedGeneric,
-                                        cudaMemcpyDeviceToHost, st));
-                {
-                    // Each code's index delta is the one most of 256 rows spread
-                    // over the body hold (the minimum over all bonds where no
-                    // sample holds the code). In a body with voids or holes the
-                    // rows whose neighbours lie across one see shifted deltas;
-                    // the minimum would take a shifted one and leave every other
-                    // row irregular.
-                    const int S = (int)std::min<int64_t>(256, rows);
-                    const int mn = std::max(pd.max_n, 1);
-                    if (S > 0) {
-                        int2* d_samp = nullptr;
-                        CPD_TRY(dev_alloc(&d_samp, sizeof(int2) * (size_t)S * mn, st));
-                        k_sample_rows<<<S, kBlock, 0, st>>>(pd.view(), np, m.code, p.frozen,
-                                                            rows, S, d_samp);
-                        launches++;
-                        std::vector<int2> samp((size_t)S * mn);
-                        CPD_TRY(cudaMemcpyAsync(samp.data(), d_samp, sizeof(int2) * samp.size(),
-                                                cudaMemcpyDeviceToHost, st));
-                        CPD_TRY(cudaStreamSynchronize(st));
-                        CPD_TRY(dev_free(d_samp, st));
-                        std::vector<std::vector<int>> seen(tab.size());
-                        for (const int2& v : samp)
-                            if (v.x < (int)tab.size()) seen[v.x].push_back(v.y);
-                        for (size_t t = 0; t < tab.size(); ++t) {
-                            std::vector<int>& d = seen[t];
-                            if (d.empty()) continue;
-                            std::sort(d.begin(), d.end());
-                            int best = d[0], run = 0, best_run = 0;
-                            for (size_t q = 0; q < d.size(); ++q) {
-                                run = (q > 0 && d[q] == d[q - 1]) ? run + 1 : 1;
-                                if (run > best_run) {
-                                    best_run = run;
-                                    best = d[q];
+                    k_code_bonds<<<blocks_for(rows), kBlock, 0, st>>>(p, pd.view(), L, m.code,
+                                                                      d_delta);
+                    launches++;
+                    tr.mark("code", st);
+                    CPD_TRY(cudaMemcpyAsync(delta.data(), d_delta,
+                                            sizeof(unsigned int) * kMixedGeneric,
+                                            cudaMemcpyDeviceToHost, st));
+                    {
+                        // Each code's index delta is the one most of 256 rows spread
+                        // over the body hold (the minimum over all bonds where no
+                        // sample holds the code). In a body with voids or holes the
+                        // rows whose neighbours lie across one see shifted deltas;
+                        // the minimum would take a shifted one and leave every other
+                        // row irregular.
+                        const int S = (int)std::min<int64_t>(256, rows);
+                        const int mn = std::max(pd.max_n, 1);
+                        if (S > 0) {
+                            int2* d_samp = nullptr;
+                            CPD_TRY(dev_alloc(&d_samp, sizeof(int2) * (size_t)S * mn, st));
+                            k_sample_rows<<<S, kBlock, 0, st>>>(pd.view(), np, m.code, p.frozen,
+                                                                rows, S, d_samp);
+                            launches++;
+                            std::vector<int2> samp((size_t)S * mn);
+                            CPD_TRY(cudaMemcpyAsync(samp.data(), d_samp, sizeof(int2) * samp.size(),
+                                                    cudaMemcpyDeviceToHost, st));
+                            CPD_TRY(cudaStreamSynchronize(st));
+                            CPD_TRY(dev_free(d_samp, st));
+                            std::vector<std::vector<int>> seen(tab.size());
+                            for (const int2& v : samp)
+                                if (v.x < (int)tab.size()) seen[v.x].push_back(v.y);
+                            for (size_t t = 0; t < tab.size(); ++t) {
+                                std::vector<int>& d = seen[t];
+                                if (d.empty()) continue;
+                                std::sort(d.begin(), d.end());
+                                int best = d[0], run = 0, best_run = 0;
+                                for (size_t q = 0; q < d.size(); ++q) {
+                                    run = (q > 0 && d[q] == d[q - 1]) ? run + 1 : 1;
+                                    if (run > best_run) {
+                                        best_run = run;
+                                        best = d[q];
+                                    }
                                 }
+                                delta[t] = (unsigned int)((long long)best + (1LL << 31));
                             }
-                            delta[t] = (unsigned int)((long long)best + (1LL << 31));
+                            CPD_TRY(cudaMemcpyAsync(d_delta, delta.data(),
+                                                    sizeof(unsigned int) * kMixedGeneric,
+                                                    cudaMemcpyHostToDevice, st));
                         }
-                        CPD_TRY(cudaMemcpyAsync(d_delta, delta.data(),
-                                                sizeof(unsigned int) * kMixedGeneric,
-                                                cudaMemcpyHostToDevice, st));
                     }
-                }
                 }
                 CPD_TRY(cudaStreamSynchronize(st));
                 for (size_t t = 0; t < tab.size(); ++t)
