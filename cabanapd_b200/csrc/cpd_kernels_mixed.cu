@@ -1666,16 +1666,29 @@ cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
 {
     layout = 0;
     if (p.n <= 0 || rows <= 0) return cudaSuccess;
-    unsigned long long* d_b = nullptr;
-    cudaError_t e = dev_alloc(&d_b, sizeof(unsigned long long) * 8, st);
-    if (e != cudaSuccess) return e;
+    // Device buffers of this test, freed on every return but the cells kept.
+    struct Buffers {
+        cudaStream_t st;
+        unsigned long long* bounds = nullptr;
+        int32_t* cell = nullptr;
+        uint32_t* occ = nullptr;
+        unsigned int* flags = nullptr;
+        ~Buffers()
+        {
+            if (bounds) dev_free(bounds, st);
+            if (cell) dev_free(cell, st);
+            if (occ) dev_free(occ, st);
+            if (flags) dev_free(flags, st);
+        }
+    } buf{st};
+    CPD_RET(dev_alloc(&buf.bounds, sizeof(unsigned long long) * 8, st));
     const unsigned long long init[8] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, ~0ull, 0ull};
-    CPD_RET(cudaMemcpyAsync(d_b, init, sizeof init, cudaMemcpyHostToDevice, st));
+    CPD_RET(cudaMemcpyAsync(buf.bounds, init, sizeof init, cudaMemcpyHostToDevice, st));
     const int nb = (int)std::min<int64_t>(blocks_for(p.n), 148 * 8);
-    k_bounds<<<nb, kBlock, 0, st>>>(p.x, p.n, p.npad, d_b);
+    k_bounds<<<nb, kBlock, 0, st>>>(p.x, p.n, p.npad, buf.bounds);
     launches++;
     unsigned long long hb[8];
-    CPD_RET(cudaMemcpyAsync(hb, d_b, sizeof hb, cudaMemcpyDeviceToHost, st));
+    CPD_RET(cudaMemcpyAsync(hb, buf.bounds, sizeof hb, cudaMemcpyDeviceToHost, st));
     CPD_RET(cudaStreamSynchronize(st));
     auto from_bits = [](unsigned long long k) {
         const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
@@ -1691,43 +1704,32 @@ cudaError_t lattice_cell_layout(const ParticleView& p, const double* h,
     }
     const int64_t cells = nc[0] * nc[1] * nc[2];
     // A sparse outline would need too many empty records.
-    if (cells > 4 * p.n + 4096 || cells >= ((int64_t)1 << 31)) {
-        dev_free(d_b, st);
-        return cudaSuccess;
-    }
-    int32_t* cell = nullptr;
-    uint32_t* occ = nullptr;
-    unsigned int* flags = nullptr;
-    CPD_RET(dev_alloc(&cell, sizeof(int32_t) * (size_t)p.npad, st));
-    CPD_RET(dev_alloc(&occ, sizeof(uint32_t) * (size_t)cells, st));
-    CPD_RET(dev_alloc(&flags, sizeof(unsigned int) * 2, st));
-    CPD_RET(cudaMemsetAsync(occ, 0, sizeof(uint32_t) * (size_t)cells, st));
-    CPD_RET(cudaMemsetAsync(flags, 0, sizeof(unsigned int) * 2, st));
+    if (cells > 4 * p.n + 4096 || cells >= ((int64_t)1 << 31)) return cudaSuccess;
+    CPD_RET(dev_alloc(&buf.cell, sizeof(int32_t) * (size_t)p.npad, st));
+    CPD_RET(dev_alloc(&buf.occ, sizeof(uint32_t) * (size_t)cells, st));
+    CPD_RET(dev_alloc(&buf.flags, sizeof(unsigned int) * 2, st));
+    CPD_RET(cudaMemsetAsync(buf.occ, 0, sizeof(uint32_t) * (size_t)cells, st));
+    CPD_RET(cudaMemsetAsync(buf.flags, 0, sizeof(unsigned int) * 2, st));
     k_lattice_cells<<<blocks_for(p.n), kBlock, 0, st>>>(
         p.x, p.n, p.npad, make_double3(lo[0], lo[1], lo[2]),
         make_double3(1.0 / h[0], 1.0 / h[1], 1.0 / h[2]),
-        make_int3((int)nc[0], (int)nc[1], (int)nc[2]), cell, occ, flags, d_b + 6);
+        make_int3((int)nc[0], (int)nc[1], (int)nc[2]), buf.cell, buf.occ, buf.flags,
+        buf.bounds + 6);
     launches++;
     unsigned int hf[2];
-    CPD_RET(cudaMemcpyAsync(hf, flags, sizeof hf, cudaMemcpyDeviceToHost, st));
-    CPD_RET(cudaMemcpyAsync(hb + 6, d_b + 6, sizeof(unsigned long long) * 2,
+    CPD_RET(cudaMemcpyAsync(hf, buf.flags, sizeof hf, cudaMemcpyDeviceToHost, st));
+    CPD_RET(cudaMemcpyAsync(hb + 6, buf.bounds + 6, sizeof(unsigned long long) * 2,
                             cudaMemcpyDeviceToHost, st));
     CPD_RET(cudaStreamSynchronize(st));
-    dev_free(occ, st);
-    dev_free(flags, st);
-    dev_free(d_b, st);
-    if (hf[0] != 0u || hf[1] != 0u) {
-        // Off the lattice, or two particles in a cell.
-        dev_free(cell, st);
-        return cudaSuccess;
-    }
+    // Off the lattice, or two particles in a cell.
+    if (hf[0] != 0u || hf[1] != 0u) return cudaSuccess;
     if (hb[6] == hb[7]) {
         // One box in row order: records by row, whose index deltas are the
         // cell deltas.
-        dev_free(cell, st);
         layout = 1;
     } else {
-        m.gcell = cell;
+        m.gcell = buf.cell;
+        buf.cell = nullptr;
         m.grid_cells = cells;
         m.bytes += sizeof(int32_t) * (size_t)p.npad;
         layout = 2;
